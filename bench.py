@@ -1,0 +1,398 @@
+#!/usr/bin/env python
+"""Throughput of the FALM LES step on B200: Mcell/s (and steps/s).
+
+Default workload: the 512x256x256 channel with one actuator-line rotor
+(33.5 M interior cells, h = 1/20, TSR 7, seeded 5% inflow, Poisson tol 1e-6)
+in mixed precision (FP32 storage, FP64 reductions), plus the FP64 step on the
+same case for the mixed/FP64 ratio.  One JSON line on rank 0.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own CUDA step (built from its sources
+into oracle/_ref) on the same grid in FP64 with uniform inflow (the reference
+has no seeded inflow); if that build is absent it times the CPU oracle.
+Multi-GPU (torchrun): every rank runs its own replica of the case (weak
+scaling); the time is the maximum over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "step/s & Mcell/s on 1 B200: mixed vs FP64 at div<=1e-6; adjoint/forward ratio"
+UNIT = "Mcell/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--case", default="channel_large")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- distributed plumbing
+def dist_setup(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region"""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": len(self.rows)}
+        if not self.rows:
+            return out
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in self.rows if num(r[1])]
+        mx = [num(r[2]) for r in self.rows if num(r[2])]
+        out["sm_mhz"] = statistics.median(sm) if sm else None
+        out["sm_max_mhz"] = max(mx) if mx else None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, name in enumerate(names):
+                if r[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        out["reasons"] = sorted(reasons)
+        pw = [num(r[3]) for r in self.rows if num(r[3])]
+        out["power_w_max"] = max(pw) if pw else None
+        return out
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- algorithmic bytes
+def step_bytes(S, n, it, m=2):
+    """bytes per step: S*N*[44 + it*(28 + 6m)] (4 B/value mixed, 8 B FP64); the ALM
+    support term 3*S*N_box is negligible against N and left out"""
+    return S * n * (44 + it * (28 + 6 * m))
+
+
+# values moved per interior cell by one launch of each kernel class (reads + writes,
+# each operand once): used for the per-kernel achieved bandwidth
+KERNEL_VALUES = {
+    "pseudo_u": 10,     # u(3) uu(3) nut(1) in, ua(3) out (ALM force evaluated in-kernel)
+    "utouu_rhs": 7,     # ua(3) in, uu(3) rhs(1) out
+    "res": 4,           # x b in, r rr out
+    "bicg_p": 5,        # r p q in, p pp out
+    "sor": 3,           # x b in, x out (half sweep)
+    "mv_dot1": 3,       # pp rr in, q out
+    "bicg_s": 4,        # r q in, s ss out
+    "mv_dot2": 3,       # ss s in, t out
+    "bicg_xr": 8,       # x pp ss s t rr in, x r out
+    "project": 13,      # ua(3) uu(3) p in, u(3) uu(3) out
+    "sgs_div": 7,       # u(3) uu(3) in, nut out
+}
+
+
+def traffic_for(kernel):
+    """dram bytes per launch from the committed ncu summary, if one exists"""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(kernel)
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args, rank, world, local):
+    import torch
+    from falm_b200 import cases
+    from falm_b200.driver import Simulation
+    case = getattr(cases, args.case)().with_inflow()
+    n = case.grid.n_interior
+    out = {}
+
+    def timed(sim, K, e2e=False):
+        ctx = sim.ctx
+        planes = None
+        if e2e:
+            planes = [torch.from_numpy(sim.inlet_plane(sim.it + 1 + q)).pin_memory() for q in range(K)]
+        torch.cuda.synchronize()
+        barrier(world)
+        l0 = ctx.launches()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stats = []
+        wall0 = time.perf_counter()
+        ev0.record()
+        for q in range(K):
+            if e2e:
+                ctx.set_inlet_plane(planes[q])
+            stats.append(sim.step())
+        ev1.record()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - wall0
+        ms = ev0.elapsed_time(ev1)
+        barrier(world)
+        return ms, stats, ctx.launches() - l0, wall
+
+    sim = Simulation(case, args.precision)
+    for _ in range(args.warmup):
+        sim.step()
+    sim.ctx.profile(True)
+    sim.ctx.profile_read(reset=True)
+    clocks = ClockSampler(local).start()
+    ms, stats, launches, wall = timed(sim, args.steps)
+    clk = clocks.stop()
+    prof = sim.ctx.profile_read(reset=True)
+    sim.ctx.profile(False)
+    ms_max = max_over_ranks(ms, world)
+    S = 4 if args.precision == "mixed" else 8
+    its = [s["it"] for s in stats]
+    mean_it = sum(its) / len(its)
+    value = world * n * args.steps / (ms_max / 1e3) / 1e6
+    peak, peak_kind = peaks()
+    # dominant kernel class by device time
+    cls = max((k for k in prof if k in KERNEL_VALUES), key=lambda k: prof[k][0])
+    tms, tn = prof[cls]
+    avg_ms = tms / max(tn, 1)
+    alg_bytes = KERNEL_VALUES[cls] * S * n
+    achieved = alg_bytes / (avg_ms / 1e3) / 1e9
+    step_b = step_bytes(S, n, mean_it)
+    out.update({
+        "value": value, "ms_per_step": ms_max / args.steps, "steps_per_s": 1e3 * args.steps / ms_max,
+        "launches": launches, "its": its, "divnorm_max": max(s["divnorm"] for s in stats),
+        "err_max": max(s["err"] for s in stats), "clocks": clk,
+        "power": [s["torque"][0] * case.alm.tip_rate[0] for s in stats] if case.alm is not None else None,
+        "roofline": {"bound": "hbm", "kernel": cls, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic_for(cls), "peak_kind": peak_kind,
+                     "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms},
+        "step_roofline": {"bytes_per_step": step_b, "achieved": step_b / (ms_max / args.steps / 1e3) / 1e9,
+                          "frac": step_b / (ms_max / args.steps / 1e3) / 1e9 / peak, "it": mean_it, "m": case.pc_maxit},
+        "profile": {k: {"ms": v[0], "launches": v[1]} for k, v in prof.items() if v[1]},
+        "wall_s": wall,
+    })
+    if not args.no_e2e:
+        ms_e, stats_e, _, wall_e = timed(sim, args.steps, e2e=True)
+        ms_e = max_over_ranks(ms_e, world)
+        ny, nz = case.grid.interior[1], case.grid.interior[2]
+        out["e2e"] = {"value": world * n * args.steps / (ms_e / 1e3) / 1e6, "unit": UNIT,
+                      "h2d_bytes_per_step": 3 * ny * nz * 8,
+                      "d2h_bytes_per_step": 8 * 8 + 2 * 8 * 8,
+                      "ms_per_step": ms_e / args.steps,
+                      "note": "per step: inlet plane H2D from pinned memory, falm_step through the C ABI, "
+                              "step statistics (it, err, div norm, torque, thrust) read back to the host"}
+    sim.close()
+    del sim
+    torch.cuda.empty_cache()
+    if not args.no_fp64 and args.precision == "mixed":
+        sim64 = Simulation(case, "fp64")
+        for _ in range(args.warmup):
+            sim64.step()
+        ms64, st64, _, _ = timed(sim64, args.steps)
+        ms64 = max_over_ranks(ms64, world)
+        out["fp64"] = {"value": world * n * args.steps / (ms64 / 1e3) / 1e6, "ms_per_step": ms64 / args.steps,
+                       "steps_per_s": 1e3 * args.steps / ms64, "its": [s["it"] for s in st64],
+                       "divnorm_max": max(s["divnorm"] for s in st64)}
+        out["mixed_over_fp64"] = out["fp64"]["ms_per_step"] / out["ms_per_step"]
+        sim64.close()
+    return case, out
+
+
+def cpu_baseline(args):
+    """the CPU oracle (OpenMP, all host threads) on a bounded sample of the workload"""
+    from oracle.oracle import CaseStruct, Oracle, build
+    from falm_b200 import cases
+    build()
+    O = Oracle()
+    big = getattr(cases, args.case)()
+    nx, ny, nz = big.grid.interior
+    sx, sy, sz = max(nx // 4, 32), max(ny // 2, 32), max(nz // 2, 32)
+    h = float(big.grid.hx[big.grid.gc])
+    sample = cases.channel(sx, sy, sz, cells_per_radius=round(1 / h), intensity=0.0, tol=big.tol,
+                           hub=(3.2, 0.5 * sy * h, 0.5 * sz * h), name="cpu_sample")
+    cs = CaseStruct(sample)
+    m = O.setup(cs)
+    st = cases.initial_state(sample)
+    O.init_state(cs, m, st)
+    O.step(cs, st, m, sample.dt)
+    t0 = time.perf_counter()
+    steps = 2
+    for q in range(steps):
+        O.step(cs, st, m, (q + 2) * sample.dt)
+    el = time.perf_counter() - t0
+    return {"value": sample.grid.n_interior * steps / el / 1e6, "unit": UNIT, "cores": O.threads(), "kind": "port",
+            "sample": f"{steps} FP64 steps of a {sx}x{sy}x{sz} slice of the case (same h, rotor, tolerance; "
+                      f"uniform inflow) after one warm-up step, CPU oracle on {O.threads()} threads"}
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args, rank, world, local):
+    from falm_b200 import cases
+    ref_so = os.path.join(ROOT, "oracle", "_ref", "libfalmref.so")
+    case = getattr(cases, args.case)()
+    n = case.grid.n_interior
+    if not os.path.exists(ref_so):
+        cb = cpu_baseline(args)
+        return case, {"value": cb["value"], "kind": "port", "cpu_baseline": cb, "device": "cpu"}
+    import tempfile
+    import torch
+    from oracle.oracle import CaseStruct, RefStep
+    cs = CaseStruct(case, use_inflow=False)
+    ref = RefStep(cs, tempfile.mkdtemp(prefix="falmref_"))
+    st = cases.initial_state(case)
+    ref.set("U", st["u"])
+    ref.op("UTOUU")
+    ref.op("SGS")
+    it = 0
+    for _ in range(args.warmup):
+        it += 1
+        ref.step(it * case.dt)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local).start()
+    t0 = time.perf_counter()
+    stats = []
+    for _ in range(args.steps):
+        it += 1
+        stats.append(ref.step(it * case.dt))
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    clk = clocks.stop()
+    ref.close()
+    return case, {"value": n * args.steps / el / 1e6, "ms_per_step": 1e3 * el / args.steps, "device": "gpu",
+                  "its": [s["it"] for s in stats], "clocks": clk, "kind": "reference"}
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_setup(args)
+    from falm_b200 import cases as _c
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        case, r = run_reference(args, rank, 1, local)
+        line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": r.get("ms_per_step"),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "device": r["device"],
+                "config": {"workload": f"{case.name} {case.grid.interior[0]}x{case.grid.interior[1]}x{case.grid.interior[2]}, "
+                                       "reference CUDA step (oracle/_ref), FP64, uniform inflow", "tol": case.tol},
+                "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "its": r.get("its"), "clocks": r.get("clocks")}
+        if "cpu_baseline" in r:
+            line["cpu_baseline"] = r["cpu_baseline"]
+        else:
+            line["cpu_baseline"] = {"value": r["value"], "unit": UNIT, "cores": 0, "kind": "reference",
+                                    "sample": "the reference's own CUDA step (it has no CPU path), full case"}
+        print(json.dumps(line), flush=True)
+        return
+    case, r = run_ours(args, rank, world, local)
+    if rank != 0:
+        return
+    cb = None
+    if world == 1 and not args.no_cpu:
+        try:
+            cb = cpu_baseline(args)
+        except Exception as e:   # the baseline is reported, never required
+            cb = {"value": None, "unit": UNIT, "cores": 0, "kind": "port", "sample": f"failed: {e}"}
+    g = case.grid.interior
+    line = {
+        "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "steps_per_s": r["steps_per_s"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 storage / f64 reductions" if args.precision == "mixed" else "f64",
+        "data": "synthetic (seeded Philox inflow, seed 20261203)",
+        "config": {"workload": f"{case.name} {g[0]}x{g[1]}x{g[2]} channel + 3-blade ALM rotor, {args.precision}",
+                   "cells": case.grid.n_interior, "tol": case.tol, "pc": f"{case.pc} x{case.pc_maxit}",
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "l2": "inputs larger than L2 (one FP32 field is 140 MB)"},
+        "clocks": r["clocks"], "gpu_launches": r["launches"], "roofline": r["roofline"],
+        "step_roofline": r["step_roofline"], "its": r["its"], "divnorm_max": r["divnorm_max"],
+        "err_max": r["err_max"], "profile": r["profile"],
+    }
+    if "e2e" in r:
+        line["e2e"] = r["e2e"]
+    if "fp64" in r:
+        line["fp64"] = r["fp64"]
+        line["mixed_over_fp64"] = r["mixed_over_fp64"]
+    if cb:
+        line["cpu_baseline"] = cb
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

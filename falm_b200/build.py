@@ -1,0 +1,38 @@
+"""Build the in-tree CUDA library falm_b200/libfalm_b200.so for sm_100a.
+
+Run as ``python -m falm_b200.build``; __graft_entry__.build() calls build().
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+SOURCES = [os.path.join(HERE, "csrc", "falm_b200.cu")]
+HEADERS = [os.path.join(HERE, "csrc", f) for f in ("falm_internal.cuh", "common.cuh", "cfd.cuh", "poisson.cuh", "alm_bc.cuh")]
+OUT = os.path.join(HERE, "libfalm_b200.so")
+NVCC_FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
+              "-Xcompiler", "-fPIC", "-shared"]
+
+
+def _stale():
+    if not os.path.exists(OUT):
+        return True
+    t = os.path.getmtime(OUT)
+    deps = SOURCES + HEADERS + [os.path.join(ROOT, "include", "falm_b200.h")]
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force=False, verbose=True):
+    if not force and not _stale():
+        return OUT
+    nvcc = os.environ.get("NVCC", "nvcc")
+    cmd = [nvcc] + NVCC_FLAGS + ["-I", os.path.join(ROOT, "include"), "-o", OUT] + SOURCES
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    return OUT
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv)

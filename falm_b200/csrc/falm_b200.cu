@@ -1,0 +1,946 @@
+// falm_b200: host side of the C ABI (include/falm_b200.h).
+//
+// One context per GPU and grid.  The context owns the 1D metric tables, the
+// Poisson operator tables, the solver work vectors (FalmEq::alloc,
+// src/FalmEq.h:27-40), the device-side reduction workspace and the ALM
+// tables; the caller owns the fields.  Every call is asynchronous on the given
+// stream except those that return scalars on the host.
+#include <vector>
+#include <string>
+#include <cstring>
+#include <cstdio>
+#include <cmath>
+#include <algorithm>
+#include "falm_internal.cuh"
+#include "common.cuh"
+#include "cfd.cuh"
+#include "poisson.cuh"
+#include "alm_bc.cuh"
+
+using namespace fb;
+
+namespace {
+
+inline cudaStream_t S(void *s) { return (cudaStream_t)s; }
+
+int fail(falm_ctx *c, int code, const char *msg) {
+    if (c && c->last_error) *c->last_error = msg;
+    return code;
+}
+
+#define CK(call)                                                                           \
+    do {                                                                                   \
+        cudaError_t _e = (call);                                                           \
+        if (_e != cudaSuccess) {                                                           \
+            if (ctx && ctx->last_error) *ctx->last_error = std::string(#call ": ") + cudaGetErrorString(_e); \
+            return (int)FALM_ERR_CUDA;                                                     \
+        }                                                                                  \
+    } while (0)
+
+#define LAUNCHED()                                                                         \
+    do {                                                                                   \
+        ctx->launches++;                                                                   \
+        cudaError_t _e = cudaGetLastError();                                               \
+        if (_e != cudaSuccess) {                                                           \
+            *ctx->last_error = std::string("launch: ") + cudaGetErrorString(_e);           \
+            return (int)FALM_ERR_CUDA;                                                     \
+        }                                                                                  \
+    } while (0)
+
+cudaEvent_t ev_get(falm_ctx *ctx) {
+    if (!ctx->ev_pool->empty()) {
+        cudaEvent_t e = ctx->ev_pool->back();
+        ctx->ev_pool->pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// launch one kernel of class `cls`; with profiling on, bracket it with an event pair
+template <typename F>
+int launch_k(falm_ctx *ctx, int cls, cudaStream_t st, F &&f) {
+    cudaEvent_t a = nullptr;
+    if (ctx->profiling) {
+        a = ev_get(ctx);
+        cudaEventRecord(a, st);
+    }
+    f();
+    ctx->launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        *ctx->last_error = std::string("launch: ") + cudaGetErrorString(e);
+        return FALM_ERR_CUDA;
+    }
+    if (ctx->profiling) {
+        cudaEvent_t b = ev_get(ctx);
+        cudaEventRecord(b, st);
+        ctx->ev_pending->push_back(falm_ctx::EvRec{cls, a, b});
+    }
+    return FALM_OK;
+}
+
+#define LAUNCH(CLS, ST, ...)                                                                 \
+    do {                                                                                     \
+        int _lrc = launch_k(ctx, (CLS), (ST), [&] { __VA_ARGS__; });                         \
+        if (_lrc) return _lrc;                                                               \
+    } while (0)
+
+int row_grid(const falm_ctx *ctx, const Region3 &R) {
+    long long rows = R.nrows();
+    long long need = (rows + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    long long cap = ctx->red.maxBlocks;
+    return (int)std::max(1LL, std::min(need, cap));
+}
+
+template <typename T> MetricView<T> mview(const falm_ctx *ctx);
+template <> MetricView<double> mview<double>(const falm_ctx *ctx) { return MetricView<double>{ctx->m64}; }
+template <> MetricView<float> mview<float>(const falm_ctx *ctx) { return MetricView<float>{ctx->m32}; }
+
+template <typename T> Op7<T> op7(const falm_ctx *ctx);
+template <> Op7<double> op7<double>(const falm_ctx *ctx) { return Op7<double>{ctx->pt64, (const double *)ctx->A_explicit, ctx->geo.n}; }
+template <> Op7<float> op7<float>(const falm_ctx *ctx) { return Op7<float>{ctx->pt32, (const float *)ctx->A_explicit, ctx->geo.n}; }
+
+int ensure_work(falm_ctx *ctx) {
+    if (ctx->work_mem) return FALM_OK;
+    const size_t n = (size_t)ctx->geo.n, e = ctx->esize;
+    const int nvec = 12;   // rr p q s pp ss t r rhs div xp + ua(3)
+    size_t outlet = 9ull * ctx->geo.sy * ctx->geo.sz;
+    size_t bytes = ((size_t)(nvec + 2) * n + outlet) * e + 256 * 16;
+    void *mem = nullptr;
+    if (cudaMalloc(&mem, bytes) != cudaSuccess) { cudaGetLastError(); return fail(ctx, FALM_ERR_ALLOC, "work vectors: cudaMalloc failed"); }
+    if (cudaMemset(mem, 0, bytes) != cudaSuccess) return fail(ctx, FALM_ERR_CUDA, "work vectors: cudaMemset failed");
+    char *p = (char *)mem;
+    auto take = [&](size_t count) { void *r = p; p += ((count * e + 255) / 256) * 256; return r; };
+    ctx->w_rr = take(n); ctx->w_p = take(n); ctx->w_q = take(n); ctx->w_s = take(n);
+    ctx->w_pp = take(n); ctx->w_ss = take(n); ctx->w_t = take(n); ctx->w_r = take(n);
+    ctx->w_rhs = take(n); ctx->w_div = take(n); ctx->w_xp = take(n);
+    ctx->w_ua = take(3 * n);
+    ctx->w_outlet = take(outlet);
+    ctx->work_mem = mem;
+    return FALM_OK;
+}
+
+// Build the separable Poisson tables.  For a Cartesian control volume
+//   0.5*(g_d(c) + g_d(c+e_d))/ja(c)  with g_d = ja*kx_d^2
+// depends on the index along d only; the table entry is evaluated with the
+// reference's arithmetic (src/falm.h:394-400, app/nedo/main.cpp:43-83) at the
+// cell (i, gc, gc) (resp. (gc, j, gc), (gc, gc, k)).  A dropped (Neumann)
+// coefficient is stored as 0.
+int build_poisson(falm_ctx *ctx, int kind) {
+    const Geom &g = ctx->geo;
+    const std::vector<double> *h[3] = {ctx->hx, ctx->hy, ctx->hz};
+    const int s[3] = {g.sx, g.sy, g.sz};
+    std::vector<double> up[3], um[3];
+    double maxdiag = 0.0;
+    auto gmet = [&](int d, int i, int j, int k) {
+        double vol = (*h[0])[i] * (*h[1])[j] * (*h[2])[k];
+        int id = d == 0 ? i : (d == 1 ? j : k);
+        double kd = 1.0 / (*h[d])[id];
+        return vol * kd * kd;
+    };
+    for (int d = 0; d < 3; d++) {
+        up[d].assign(s[d], 0.0);
+        um[d].assign(s[d], 0.0);
+        for (int q = g.gc; q < s[d] - g.gc; q++) {
+            int c[3] = {g.gc, g.gc, g.gc};
+            c[d] = q;
+            int cp[3] = {c[0], c[1], c[2]}, cm[3] = {c[0], c[1], c[2]};
+            cp[d] += 1; cm[d] -= 1;
+            double jac = (*h[0])[c[0]] * (*h[1])[c[1]] * (*h[2])[c[2]];
+            double gc0 = gmet(d, c[0], c[1], c[2]);
+            double coef_p = 0.5 * (gc0 + gmet(d, cp[0], cp[1], cp[2])) / jac;
+            double coef_m = 0.5 * (gc0 + gmet(d, cm[0], cm[1], cm[2])) / jac;
+            // app/nedo/main.cpp:55 keeps the x+ coefficient (p = 0 guide cell); every other
+            // physical face is Neumann (:60-83, app/lid3d/main.cpp:52-80)
+            int plus_limit = (d == 0 && kind == FALM_BC_CHANNEL) ? s[d] - g.gc : s[d] - g.gc - 1;
+            if (q < plus_limit) up[d][q] = coef_p;
+            if (q > g.gc) um[d][q] = coef_m;
+        }
+    }
+    // maxdiag over the interior: |ac| is separable as well, but take the
+    // exact maximum of the reference's accumulation order
+    for (int k = g.gc; k < g.sz - g.gc; k++)
+        for (int j = g.gc; j < g.sy - g.gc; j++)
+            for (int i = g.gc; i < g.sx - g.gc; i++) {
+                double ac = ((((-up[0][i]) - um[0][i]) - up[1][j]) - um[1][j] - up[2][k]) - um[2][k];
+                maxdiag = std::max(maxdiag, std::fabs(ac));
+            }
+    double scale = 1.0 / maxdiag;
+    // layout: for each d: cm, cp, um, up (s[d] each), then dx0 (sx)
+    size_t tot = 0;
+    for (int d = 0; d < 3; d++) tot += 4 * (size_t)s[d];
+    tot += g.sx;
+    std::vector<double> h64(tot);
+    std::vector<float> h32(tot);
+    size_t off = 0;
+    size_t o_cm[3], o_cp[3], o_um[3], o_up[3], o_dx0;
+    for (int d = 0; d < 3; d++) {
+        o_cm[d] = off; for (int q = 0; q < s[d]; q++) h64[off + q] = um[d][q] * scale; off += s[d];
+        o_cp[d] = off; for (int q = 0; q < s[d]; q++) h64[off + q] = up[d][q] * scale; off += s[d];
+        o_um[d] = off; for (int q = 0; q < s[d]; q++) h64[off + q] = um[d][q]; off += s[d];
+        o_up[d] = off; for (int q = 0; q < s[d]; q++) h64[off + q] = up[d][q]; off += s[d];
+    }
+    o_dx0 = off;
+    for (int q = 0; q < g.sx; q++) h64[off + q] = (-up[0][q]) - um[0][q];
+    off += g.sx;
+    for (size_t q = 0; q < tot; q++) h32[q] = (float)h64[q];
+    if (ctx->op_mem) { cudaFree(ctx->op_mem); ctx->op_mem = nullptr; }
+    void *mem = nullptr;
+    if (cudaMalloc(&mem, tot * (sizeof(double) + sizeof(float))) != cudaSuccess) { cudaGetLastError(); return fail(ctx, FALM_ERR_ALLOC, "poisson tables"); }
+    double *d64 = (double *)mem;
+    float *d32 = (float *)(d64 + tot);
+    if (cudaMemcpy(d64, h64.data(), tot * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(d32, h32.data(), tot * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(ctx, FALM_ERR_CUDA, "poisson tables copy");
+    ctx->op_mem = mem;
+    for (int d = 0; d < 3; d++) {
+        ctx->pt64.cm[d] = d64 + o_cm[d]; ctx->pt64.cp[d] = d64 + o_cp[d]; ctx->pt64.um[d] = d64 + o_um[d]; ctx->pt64.up[d] = d64 + o_up[d];
+        ctx->pt32.cm[d] = d32 + o_cm[d]; ctx->pt32.cp[d] = d32 + o_cp[d]; ctx->pt32.um[d] = d32 + o_um[d]; ctx->pt32.up[d] = d32 + o_up[d];
+    }
+    ctx->pt64.dx0 = d64 + o_dx0; ctx->pt32.dx0 = d32 + o_dx0;
+    ctx->pt64.scale = scale; ctx->pt32.scale = (float)scale;
+    ctx->maxdiag = maxdiag;
+    ctx->op_ready = 1;
+    ctx->bc_kind_op = kind;
+    return FALM_OK;
+}
+
+// ---------------------------------------------------------------- solver driver
+template <typename T>
+int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out, double *err_out, int *outer_out) {
+    int rc = ensure_work(ctx);
+    if (rc) return rc;
+    if (!ctx->op_ready && !ctx->A_explicit) return fail(ctx, FALM_ERR_STATE, "solve: no operator (call falm_eq_poisson_operator or falm_eq_set_matrix)");
+    if (ctx->ls_type != FALM_LS_PBICGSTAB) return fail(ctx, FALM_ERR_ARG, "solve: only PBiCGStab is implemented");
+    const Geom &g = ctx->geo;
+    const Region3 R = interior(g);
+    const int grid = row_grid(ctx, R);
+    const Op7<T> op = op7<T>(ctx);
+    T *rr = (T *)ctx->w_rr, *p = (T *)ctx->w_p, *q = (T *)ctx->w_q, *s = (T *)ctx->w_s, *pp = (T *)ctx->w_pp;
+    T *ss = (T *)ctx->w_ss, *t = (T *)ctx->w_t, *xp = (T *)ctx->w_xp;
+    SolverScalars init;
+    memset(&init, 0, sizeof(init));
+    init.gsize = (double)g.nx * g.ny * g.nz;
+    init.tol = ctx->tol;
+    init.maxit = ctx->maxit;
+    CK(cudaMemcpyAsync(ctx->scal, &init, sizeof(init), cudaMemcpyHostToDevice, st));
+    const T pcw = (T)ctx->pc_relax;
+    const int pct = ctx->pc_type, m = ctx->pc_maxit;
+    SolverScalars *sc = ctx->scal;
+    int total_it = 0, outer = 0;
+    const bool mixed = ctx->precision == FALM_MIXED;
+    const int max_outer = mixed ? ctx->max_outer : 1;
+    // launch the remaining sweeps of one preconditioner application z ~ A^-1 v
+    auto precondition_rest = [&](T *z, const T *v) -> int {
+        if (pct == FALM_LS_SOR) {
+            LAUNCH(FALM_K_SOR, st, k_sor<T><<<grid, kRowThreads, 0, st>>>(g, R, op, z, v, pcw, 1, sc));
+            for (int it = 1; it < m; it++) {
+                LAUNCH(FALM_K_SOR, st, k_sor<T><<<grid, kRowThreads, 0, st>>>(g, R, op, z, v, pcw, 0, sc));
+                LAUNCH(FALM_K_SOR, st, k_sor<T><<<grid, kRowThreads, 0, st>>>(g, R, op, z, v, pcw, 1, sc));
+            }
+        } else if (pct == FALM_LS_JACOBI) {
+            // sweeps 2..m ping-pong between xp and z; the first sweep wrote to
+            // the buffer that makes the last one land in z
+            T *bufs[2] = {z, xp};
+            for (int it = 2; it <= m; it++) {
+                T *dst = bufs[(m - it) & 1], *src = bufs[(m - it + 1) & 1];
+                LAUNCH(FALM_K_SOR, st, k_jacobi<T><<<grid, kRowThreads, 0, st>>>(g, R, op, dst, src, v, sc));
+            }
+        }
+        return FALM_OK;
+    };
+    auto first_target = [&](T *z) -> T * { return (pct == FALM_LS_JACOBI && ((m - 1) & 1)) ? xp : z; };
+    for (outer = 0; outer < max_outer; outer++) {
+        // outer > 0: true residual in FP64; stop when it meets the tolerance
+        LAUNCH(FALM_K_RES, st, k_res<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, r, rr, ctx->red, sc, outer > 0 ? 1 : 0));
+        if (outer > 0) {
+            CK(cudaMemcpyAsync(ctx->scal_host, sc, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (ctx->scal_host->done) break;
+            // restart the iteration count of this pass
+            int zero = 0;
+            CK(cudaMemcpyAsync(&sc->it, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
+            CK(cudaStreamSynchronize(st));
+        }
+        for (;;) {
+            LAUNCH(FALM_K_BICG_P, st, k_bicg_p<T><<<grid, kRowThreads, 0, st>>>(g, R, op, p, q, r, first_target(pp), pct, pcw, sc));
+            if ((rc = precondition_rest(pp, p))) return rc;
+            LAUNCH(FALM_K_MV_DOT1, st, k_mv_dot1<T><<<grid, kRowThreads, 0, st>>>(g, R, op, pp, q, rr, ctx->red, sc));
+            LAUNCH(FALM_K_BICG_S, st, k_bicg_s<T><<<grid, kRowThreads, 0, st>>>(g, R, op, s, q, r, first_target(ss), pct, pcw, sc));
+            if ((rc = precondition_rest(ss, s))) return rc;
+            LAUNCH(FALM_K_MV_DOT2, st, k_mv_dot2<T><<<grid, kRowThreads, 0, st>>>(g, R, op, ss, t, s, ctx->red, sc));
+            LAUNCH(FALM_K_BICG_XR, st, k_bicg_xr<T><<<grid, kRowThreads, 0, st>>>(g, R, x, pp, ss, r, s, t, rr, ctx->red, sc));
+            CK(cudaMemcpyAsync(ctx->scal_host, sc, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (ctx->scal_host->done) break;
+        }
+        total_it += ctx->scal_host->it;
+        if (ctx->scal_host->status == FALM_ERR_NAN) break;
+    }
+    if (mixed && outer >= max_outer) {
+        // report the true residual of the final iterate
+        LAUNCH(FALM_K_RES, st, k_res<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, r, nullptr, ctx->red, nullptr, 0));
+    }
+    if (it_out) *it_out = total_it;
+    if (err_out) *err_out = ctx->scal_host->err;
+    if (outer_out) *outer_out = std::min(outer + 1, max_outer);
+    return ctx->scal_host->status == FALM_ERR_NAN ? fail(ctx, FALM_ERR_NAN, "solve: non-finite scalar") : FALM_OK;
+}
+
+template <typename T>
+int dot_t(falm_ctx *ctx, const T *a, const T *b, int ncol, double *out, cudaStream_t st) {
+    const Region3 R = interior(ctx->geo);
+    LAUNCH(FALM_K_OTHER, st, k_dot<T><<<row_grid(ctx, R), kRowThreads, 0, st>>>(ctx->geo, R, a, b, ncol, ctx->red, &ctx->scal->red[0]));
+    CK(cudaMemcpyAsync(ctx->scal_host, ctx->scal, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    *out = ctx->scal_host->red[0];
+    return FALM_OK;
+}
+
+AlmFuse alm_fuse(const falm_ctx *ctx) {
+    AlmFuse af;
+    memset(&af, 0, sizeof(af));
+    if (!ctx->alm_on || ctx->alm.apcount > kMaxFusedAp) return af;
+    af.apcount = ctx->alm.apcount;
+    af.xyz = ctx->alm.ap_xyz;
+    af.force = ctx->alm.ap_force;
+    af.scal = ctx->alm.scal;
+    af.eps = ctx->alm.euler_eps;
+    double sq = std::sqrt(M_PI) * af.eps;
+    af.eta = 1. / (sq * sq * sq);
+    af.rcut2 = ctx->alm.rcut2;
+    return af;
+}
+
+template <typename T>
+int pseudo_u_t(falm_ctx *ctx, const T *un, const T *u, const T *uu, T *ua, const T *nut, const T *ff, double dt, bool fuse, cudaStream_t st) {
+    const Region3 R = interior(ctx->geo);
+    AlmFuse af;
+    memset(&af, 0, sizeof(af));
+    if (!ff && fuse) af = alm_fuse(ctx);
+    LAUNCH(FALM_K_PSEUDO_U, st, k_pseudo_u<T><<<row_grid(ctx, R), kRowThreads, 0, st>>>(ctx->geo, R, mview<T>(ctx), un, u, uu, ua, nut, ff, af,
+                                                            (T)(1.0 / ctx->Re), (T)dt, ctx->adv));
+    return FALM_OK;
+}
+
+template <typename T>
+int alm_run_t(falm_ctx *ctx, const T *u, T *ff, double t, cudaStream_t st) {
+    LAUNCH(FALM_K_ALM, st, k_alm_force<T><<<1, 256, 0, st>>>(ctx->geo, ctx->alm, ctx->m64.x[0], ctx->m64.x[1], ctx->m64.x[2], u, t));
+    if (ff) {
+        const Region3 R = interior(ctx->geo);
+        LAUNCH(FALM_K_ALM, st, k_alm_project<T><<<row_grid(ctx, R), kRowThreads, 0, st>>>(ctx->geo, R, mview<T>(ctx), ctx->alm, ff));
+    }
+    return FALM_OK;
+}
+
+template <typename T>
+int ubc_t(falm_ctx *ctx, T *u, UPrev<T> up, double dt, double t, cudaStream_t st) {
+    Inflow inf{ctx->inflow_box, ctx->inflow_nb, ctx->inflow_dx, ctx->inlet_plane_valid ? ctx->inlet_plane : nullptr};
+    ctx->inlet_plane_valid = 0;
+    dim3 grid(64, 3);
+    LAUNCH(FALM_K_UBC, st, k_ubc<T><<<grid, 256, 0, st>>>(ctx->geo, ctx->bc_kind, u, up, ctx->m64.x[0], dt, t, ctx->u_inlet, inf));
+    return FALM_OK;
+}
+
+template <typename T>
+int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_t st, falm_step_stats *out) {
+    int rc = ensure_work(ctx);
+    if (rc) return rc;
+    if (!ctx->op_ready) {
+        if ((rc = build_poisson(ctx, ctx->bc_kind))) return rc;
+    }
+    const Geom &g = ctx->geo;
+    T *u = (T *)f->u, *uu = (T *)f->uu, *p = (T *)f->p, *nut = (T *)f->nut, *ff = (T *)f->ff;
+    T *ua = (T *)ctx->w_ua, *rhs = (T *)ctx->w_rhs, *r = (T *)ctx->w_r;
+    const bool chan = ctx->bc_kind == FALM_BC_CHANNEL;
+    // 1. ALM (src/alm/alm.h:66-77) at the previous velocity
+    if (ctx->alm_on) {
+        if ((rc = alm_run_t<T>(ctx, u, ff, t, st))) return rc;
+    }
+    // 2. pseudo-velocity into ua (ALM force projected in-kernel when ff == NULL)
+    if ((rc = pseudo_u_t<T>(ctx, u, u, uu, ua, nut, ff, dt, ctx->alm_on != 0, st))) return rc;
+    // 3. face velocity + [uubc] + RHS in one pass
+    {
+        const Region3 R = facemap(g);
+        T scale = (T)(1.0 / (dt * ctx->maxdiag));
+        if (chan) LAUNCH(FALM_K_UTOUU_RHS, st, k_utouu<T, true, false><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), ua, u, uu, rhs, scale));
+        else LAUNCH(FALM_K_UTOUU_RHS, st, k_utouu<T, true, true><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), ua, u, uu, rhs, scale));
+    }
+    // 4. Poisson
+    int it = 0, outer = 1;
+    double err = 0;
+    rc = solve_t<T>(ctx, p, rhs, r, st, &it, &err, &outer);
+    int solve_status = ctx->scal_host->status;
+    if (rc) return rc;
+    // 5. pbc
+    LAUNCH(FALM_K_PBC, st, k_pbc<T><<<dim3(64, 3), 256, 0, st>>>(g, ctx->bc_kind, p));
+    // 6. keep the previous velocity at the outlet planes, then project
+    if (chan) { LAUNCH(FALM_K_OTHER, st, k_save_outlet<T><<<64, 256, 0, st>>>(g, u, (T *)ctx->w_outlet)); }
+    {
+        const Region3 R = facemap(g);
+        LAUNCH(FALM_K_PROJECT, st, k_project<T><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), u, ua, uu, uu, p, (T)dt));
+    }
+    // 7. ubc
+    if ((rc = ubc_t<T>(ctx, u, UPrev<T>{(const T *)ctx->w_outlet, 1}, dt, t, st))) return rc;
+    // 8. SGS + divergence norm
+    {
+        const Region3 R = interior(g);
+        LAUNCH(FALM_K_SGS_DIV, st, k_sgs_div<T, true><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), ctx->m64, u, nut, (T)ctx->Cs, ctx->sgs, uu,
+                                                                      nullptr, ctx->red, &ctx->scal->red[3]));
+    }
+    CK(cudaMemcpyAsync(ctx->scal_host, ctx->scal, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
+    if (ctx->alm_on) CK(cudaMemcpyAsync(ctx->alm_scal_host, ctx->alm.scal, sizeof(AlmScalars), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (out) {
+        memset(out, 0, sizeof(*out));
+        out->it = it;
+        out->err = err;
+        out->outer = outer;
+        out->status = solve_status;
+        out->divnorm = std::sqrt(ctx->scal_host->red[3]) / ((double)g.nx * g.ny * g.nz);
+        if (ctx->alm_on)
+            for (int q = 0; q < ctx->alm.n_turbine && q < kMaxTurbines; q++) {
+                out->torque[q] = ctx->alm_scal_host->torque[q];
+                out->thrust[q] = ctx->alm_scal_host->thrust[q];
+            }
+    }
+    return FALM_OK;
+}
+
+// run f with a value of the context's storage type (double or float)
+template <typename F>
+int dispatch(const falm_ctx *ctx, F &&f) {
+    if (ctx->precision == FALM_FP64) return f(double(0));
+    return f(float(0));
+}
+
+}  // namespace
+
+extern "C" {
+
+int falm_abi_version(void) { return FALM_B200_ABI_VERSION; }
+
+const char *falm_last_error(const falm_ctx *ctx) { return ctx && ctx->last_error ? ctx->last_error->c_str() : "null context"; }
+
+long long falm_kernel_launches(const falm_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+int falm_create(const falm_grid *grid, int precision, falm_ctx **out) {
+    if (!grid || !out || !grid->x || !grid->y || !grid->z || !grid->hx || !grid->hy || !grid->hz) return FALM_ERR_ARG;
+    if (grid->gc < 2 || grid->sx < 2 * grid->gc + 2 || grid->sy < 2 * grid->gc + 2 || grid->sz < 2 * grid->gc + 2) return FALM_ERR_ARG;
+    if (precision != FALM_FP64 && precision != FALM_MIXED) return FALM_ERR_ARG;
+    *out = nullptr;
+    falm_ctx *ctx = new falm_ctx();
+    memset((void *)ctx, 0, sizeof(*ctx));
+    ctx->last_error = new std::string();
+    ctx->precision = precision;
+    ctx->esize = precision == FALM_FP64 ? sizeof(double) : sizeof(float);
+    Geom &g = ctx->geo;
+    g.sx = grid->sx; g.sy = grid->sy; g.sz = grid->sz; g.gc = grid->gc;
+    g.n = (long long)g.sx * g.sy * g.sz;
+    g.nx = g.sx - 2 * g.gc; g.ny = g.sy - 2 * g.gc; g.nz = g.sz - 2 * g.gc;
+    ctx->hx = new std::vector<double>(grid->hx, grid->hx + g.sx);
+    ctx->hy = new std::vector<double>(grid->hy, grid->hy + g.sy);
+    ctx->hz = new std::vector<double>(grid->hz, grid->hz + g.sz);
+    ctx->xc = new std::vector<double>(grid->x, grid->x + g.sx);
+    ctx->yc = new std::vector<double>(grid->y, grid->y + g.sy);
+    ctx->zc = new std::vector<double>(grid->z, grid->z + g.sz);
+    ctx->alm_host = new std::vector<double>();
+    ctx->ev_pending = new std::vector<falm_ctx::EvRec>();
+    ctx->ev_pool = new std::vector<cudaEvent_t>();
+    ctx->Re = 1e4; ctx->Cs = 0.1; ctx->adv = FALM_ADV_UPWIND3; ctx->sgs = FALM_SGS_SMAGORINSKY;
+    ctx->ls_type = FALM_LS_PBICGSTAB; ctx->maxit = 1000; ctx->tol = 1e-8; ctx->relax = 1.0;
+    ctx->pc_type = FALM_LS_SOR; ctx->pc_maxit = 2; ctx->pc_relax = 1.2; ctx->max_outer = 5;
+    ctx->bc_kind = FALM_BC_CHANNEL; ctx->u_inlet = 1.0;
+    if (cudaGetDevice(&ctx->device) != cudaSuccess) { cudaGetLastError(); falm_destroy(ctx); return FALM_ERR_CUDA; }
+    cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, ctx->device);
+    if (ctx->sm_count <= 0) ctx->sm_count = 148;
+    // metric tables: x, h, k for 3 axes in FP64 then FP32
+    size_t tot = 3 * ((size_t)g.sx + g.sy + g.sz);
+    std::vector<double> m(tot);
+    std::vector<float> mf(tot);
+    size_t off = 0, o_x[3], o_h[3], o_k[3];
+    const std::vector<double> *xs[3] = {ctx->xc, ctx->yc, ctx->zc}, *hs[3] = {ctx->hx, ctx->hy, ctx->hz};
+    const int s[3] = {g.sx, g.sy, g.sz};
+    for (int d = 0; d < 3; d++) {
+        o_x[d] = off; for (int q = 0; q < s[d]; q++) m[off + q] = (*xs[d])[q]; off += s[d];
+        o_h[d] = off; for (int q = 0; q < s[d]; q++) m[off + q] = (*hs[d])[q]; off += s[d];
+        o_k[d] = off; for (int q = 0; q < s[d]; q++) m[off + q] = 1.0 / (*hs[d])[q]; off += s[d];
+    }
+    for (size_t q = 0; q < tot; q++) mf[q] = (float)m[q];
+    if (cudaMalloc(&ctx->metric_mem, tot * (sizeof(double) + sizeof(float))) != cudaSuccess) { cudaGetLastError(); falm_destroy(ctx); return FALM_ERR_ALLOC; }
+    double *d64 = (double *)ctx->metric_mem;
+    float *d32 = (float *)(d64 + tot);
+    cudaMemcpy(d64, m.data(), tot * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(d32, mf.data(), tot * sizeof(float), cudaMemcpyHostToDevice);
+    for (int d = 0; d < 3; d++) {
+        ctx->m64.x[d] = d64 + o_x[d]; ctx->m64.h[d] = d64 + o_h[d]; ctx->m64.k[d] = d64 + o_k[d];
+        ctx->m32.x[d] = d32 + o_x[d]; ctx->m32.h[d] = d32 + o_h[d]; ctx->m32.k[d] = d32 + o_k[d];
+    }
+    // reduction workspace sized to the persistent grid
+    ctx->red.maxBlocks = ctx->sm_count * 8;
+    if (cudaMalloc(&ctx->red.partials, sizeof(double) * 4 * ctx->red.maxBlocks) != cudaSuccess ||
+        cudaMalloc(&ctx->red.counter, sizeof(unsigned int) * 4) != cudaSuccess ||
+        cudaMalloc(&ctx->scal, sizeof(SolverScalars)) != cudaSuccess ||
+        cudaMallocHost(&ctx->scal_host, sizeof(SolverScalars)) != cudaSuccess ||
+        cudaMallocHost(&ctx->alm_scal_host, sizeof(AlmScalars)) != cudaSuccess) {
+        cudaGetLastError();
+        falm_destroy(ctx);
+        return FALM_ERR_ALLOC;
+    }
+    cudaMemset(ctx->red.counter, 0, sizeof(unsigned int) * 4);
+    cudaMemset(ctx->scal, 0, sizeof(SolverScalars));
+    memset(ctx->scal_host, 0, sizeof(SolverScalars));
+    if (cudaDeviceSynchronize() != cudaSuccess) { cudaGetLastError(); falm_destroy(ctx); return FALM_ERR_CUDA; }
+    *out = ctx;
+    return FALM_OK;
+}
+
+int falm_destroy(falm_ctx *ctx) {
+    if (!ctx) return FALM_ERR_ARG;
+    cudaFree(ctx->metric_mem);
+    cudaFree(ctx->op_mem);
+    cudaFree(ctx->work_mem);
+    cudaFree(ctx->red.partials);
+    cudaFree(ctx->red.counter);
+    cudaFree(ctx->scal);
+    cudaFree(ctx->inflow_box);
+    cudaFree(ctx->alm_mem);
+    if (ctx->scal_host) cudaFreeHost(ctx->scal_host);
+    if (ctx->alm_scal_host) cudaFreeHost(ctx->alm_scal_host);
+    delete ctx->hx; delete ctx->hy; delete ctx->hz; delete ctx->xc; delete ctx->yc; delete ctx->zc;
+    delete ctx->alm_host;
+    if (ctx->ev_pending) {
+        for (auto &r : *ctx->ev_pending) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+        delete ctx->ev_pending;
+    }
+    if (ctx->ev_pool) {
+        for (auto e : *ctx->ev_pool) cudaEventDestroy(e);
+        delete ctx->ev_pool;
+    }
+    cudaFree(ctx->inlet_plane);
+    delete ctx->last_error;
+    delete ctx;
+    return FALM_OK;
+}
+
+// ---------------------------------------------------------------- FalmCFD
+int falm_cfd_init(falm_ctx *ctx, double Re, int adv, int sgs, double Cs) {
+    if (!ctx || !(Re > 0) || adv < 0 || adv > 4 || sgs < 0 || sgs > 2) return FALM_ERR_ARG;
+    ctx->Re = Re; ctx->adv = adv; ctx->sgs = sgs; ctx->Cs = Cs;
+    return FALM_OK;
+}
+
+int falm_cfd_pseudo_u(falm_ctx *ctx, const void *un, const void *u, const void *uu, void *ua, const void *nut,
+                      const void *ff, double dt, double t, void *stream) {
+    (void)t;
+    if (!ctx || !un || !u || !uu || !ua || !nut) return FALM_ERR_ARG;
+    if (ua == u || ua == un) return fail(ctx, FALM_ERR_ARG, "pseudo_u: ua aliases u (a data race in the reference's aliased call)");
+    if (!ff && !ctx->alm_on) return fail(ctx, FALM_ERR_NOALM, "pseudo_u: ff is NULL and no ALM is configured");
+    return dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        return pseudo_u_t<T>(ctx, (const T *)un, (const T *)u, (const T *)uu, (T *)ua, (const T *)nut, (const T *)ff, dt, true, S(stream));
+    });
+}
+
+int falm_cfd_utouu(falm_ctx *ctx, const void *u, void *uu, void *stream) {
+    if (!ctx || !u || !uu) return FALM_ERR_ARG;
+    return dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        const Region3 R = facemap(ctx->geo);
+        LAUNCH(FALM_K_UTOUU_RHS, S(stream), k_utouu<T, false, false><<<row_grid(ctx, R), kRowThreads, 0, S(stream)>>>(ctx->geo, R, mview<T>(ctx), (const T *)u,
+                                                                                   (const T *)u, (T *)uu, (T *)nullptr, T(0)));
+        return (int)FALM_OK;
+    });
+}
+
+int falm_cfd_poisson_rhs(falm_ctx *ctx, const void *uu, void *rhs, double dt, double maxdiag, void *stream) {
+    if (!ctx || !uu || !rhs || !(dt > 0) || !(maxdiag > 0)) return FALM_ERR_ARG;
+    return dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        const Region3 R = interior(ctx->geo);
+        LAUNCH(FALM_K_OTHER, S(stream), k_divergence<T><<<row_grid(ctx, R), kRowThreads, 0, S(stream)>>>(ctx->geo, R, mview<T>(ctx), (const T *)uu, (T *)rhs,
+                                                                          (T)(1.0 / (dt * maxdiag)), 1));
+        return (int)FALM_OK;
+    });
+}
+
+int falm_cfd_divergence(falm_ctx *ctx, const void *uu, void *div, void *stream) {
+    if (!ctx || !uu || !div) return FALM_ERR_ARG;
+    return dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        const Region3 R = interior(ctx->geo);
+        LAUNCH(FALM_K_OTHER, S(stream), k_divergence<T><<<row_grid(ctx, R), kRowThreads, 0, S(stream)>>>(ctx->geo, R, mview<T>(ctx), (const T *)uu, (T *)div, T(1), 0));
+        return (int)FALM_OK;
+    });
+}
+
+int falm_cfd_project_p(falm_ctx *ctx, void *u, const void *ua, void *uu, const void *uua, const void *p, double dt, void *stream) {
+    if (!ctx || !u || !ua || !uu || !uua || !p) return FALM_ERR_ARG;
+    return dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        const Region3 R = facemap(ctx->geo);
+        LAUNCH(FALM_K_PROJECT, S(stream), k_project<T><<<row_grid(ctx, R), kRowThreads, 0, S(stream)>>>(ctx->geo, R, mview<T>(ctx), (T *)u, (const T *)ua, (T *)uu,
+                                                                       (const T *)uua, (const T *)p, (T)dt));
+        return (int)FALM_OK;
+    });
+}
+
+int falm_cfd_sgs(falm_ctx *ctx, const void *u, void *nut, void *stream) {
+    if (!ctx || !u || !nut) return FALM_ERR_ARG;
+    return dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        const Region3 R = interior(ctx->geo);
+        LAUNCH(FALM_K_SGS_DIV, S(stream), k_sgs_div<T, false><<<row_grid(ctx, R), kRowThreads, 0, S(stream)>>>(ctx->geo, R, mview<T>(ctx), ctx->m64, (const T *)u, (T *)nut,
+                                                                              (T)ctx->Cs, ctx->sgs, (const T *)nullptr, (T *)nullptr, ctx->red, nullptr));
+        return (int)FALM_OK;
+    });
+}
+
+// ---------------------------------------------------------------- FalmEq
+int falm_eq_init(falm_ctx *ctx, int type, int maxit, double tol, double relax, int pc_type, int pc_maxit, double pc_relax) {
+    if (!ctx || maxit < 1 || pc_maxit < 1 || !(tol >= 0)) return FALM_ERR_ARG;
+    if (type != FALM_LS_PBICGSTAB) return fail(ctx, FALM_ERR_ARG, "eq_init: only PBiCGStab (4) is implemented");
+    if (pc_type != FALM_LS_SOR && pc_type != FALM_LS_JACOBI) return fail(ctx, FALM_ERR_ARG, "eq_init: preconditioner must be SOR (2) or Jacobi (1)");
+    ctx->ls_type = type; ctx->maxit = maxit; ctx->tol = tol; ctx->relax = relax;
+    ctx->pc_type = pc_type; ctx->pc_maxit = pc_maxit; ctx->pc_relax = pc_relax;
+    return FALM_OK;
+}
+
+int falm_eq_poisson_operator(falm_ctx *ctx, int bc_kind, double *maxdiag_out) {
+    if (!ctx || (bc_kind != FALM_BC_CHANNEL && bc_kind != FALM_BC_CAVITY)) return FALM_ERR_ARG;
+    int rc = build_poisson(ctx, bc_kind);
+    if (rc) return rc;
+    if (maxdiag_out) *maxdiag_out = ctx->maxdiag;
+    return FALM_OK;
+}
+
+int falm_eq_set_matrix(falm_ctx *ctx, const void *A) {
+    if (!ctx) return FALM_ERR_ARG;
+    ctx->A_explicit = A;
+    return FALM_OK;
+}
+
+int falm_eq_solve(falm_ctx *ctx, void *x, const void *b, void *r, void *stream, int *it_out, double *err_out) {
+    if (!ctx || !x || !b || !r) return FALM_ERR_ARG;
+    int rc = dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        return solve_t<T>(ctx, (T *)x, (const T *)b, (T *)r, S(stream), it_out, err_out, nullptr);
+    });
+    if (rc) return rc;
+    int st = ctx->scal_host->status;
+    return st == FALM_ERR_MAXIT || st == FALM_ERR_BREAKDOWN ? st : FALM_OK;
+}
+
+int falm_eq_res(falm_ctx *ctx, const void *x, const void *b, void *r, void *stream) {
+    if (!ctx || !x || !b || !r) return FALM_ERR_ARG;
+    if (!ctx->op_ready && !ctx->A_explicit) return fail(ctx, FALM_ERR_STATE, "res: no operator");
+    return dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        const Region3 R = interior(ctx->geo);
+        LAUNCH(FALM_K_RES, S(stream), k_res<T><<<row_grid(ctx, R), kRowThreads, 0, S(stream)>>>(ctx->geo, R, op7<T>(ctx), (const T *)x, (const T *)b, (T *)r,
+                                                                   (T *)nullptr, ctx->red, nullptr, 0));
+        return (int)FALM_OK;
+    });
+}
+
+int falm_eq_sor_sweep(falm_ctx *ctx, void *x, const void *b, double omega, int color, void *stream) {
+    if (!ctx || !x || !b || (color != 0 && color != 1)) return FALM_ERR_ARG;
+    if (!ctx->op_ready && !ctx->A_explicit) return fail(ctx, FALM_ERR_STATE, "sor: no operator");
+    return dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        const Region3 R = interior(ctx->geo);
+        LAUNCH(FALM_K_SOR, S(stream), k_sor<T><<<row_grid(ctx, R), kRowThreads, 0, S(stream)>>>(ctx->geo, R, op7<T>(ctx), (T *)x, (const T *)b, (T)omega, color,
+                                                                   (const SolverScalars *)nullptr));
+        return (int)FALM_OK;
+    });
+}
+
+// ---------------------------------------------------------------- FalmMV
+int falm_mv_mv(falm_ctx *ctx, const void *x, void *ax, void *stream) {
+    if (!ctx || !x || !ax) return FALM_ERR_ARG;
+    if (!ctx->op_ready && !ctx->A_explicit) return fail(ctx, FALM_ERR_STATE, "mv: no operator");
+    return dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        const Region3 R = interior(ctx->geo);
+        LAUNCH(FALM_K_OTHER, S(stream), k_mv<T><<<row_grid(ctx, R), kRowThreads, 0, S(stream)>>>(ctx->geo, R, op7<T>(ctx), (const T *)x, (T *)ax));
+        return (int)FALM_OK;
+    });
+}
+
+int falm_mv_dot(falm_ctx *ctx, const void *a, const void *b, double *out, void *stream) {
+    if (!ctx || !a || !b || !out) return FALM_ERR_ARG;
+    return dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        return dot_t<T>(ctx, (const T *)a, (const T *)b, 1, out, S(stream));
+    });
+}
+
+int falm_mv_normsq(falm_ctx *ctx, const void *a, int ncol, double *out, void *stream) {
+    if (!ctx || !a || !out || ncol < 1) return FALM_ERR_ARG;
+    return dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        return dot_t<T>(ctx, (const T *)a, (const T *)nullptr, ncol, out, S(stream));
+    });
+}
+
+int falm_mv_maxdiag(falm_ctx *ctx, double *out) {
+    if (!ctx || !out) return FALM_ERR_ARG;
+    if (!ctx->A_explicit) {
+        if (!ctx->op_ready) return fail(ctx, FALM_ERR_STATE, "maxdiag: no operator");
+        *out = ctx->maxdiag;
+        return FALM_OK;
+    }
+    unsigned long long *d = nullptr, h = 0;
+    CK(cudaMalloc(&d, sizeof(unsigned long long)));
+    CK(cudaMemset(d, 0, sizeof(unsigned long long)));
+    int rc = dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        const Region3 R = interior(ctx->geo);
+        LAUNCH(FALM_K_OTHER, (cudaStream_t)0, k_absmax<T><<<row_grid(ctx, R), kRowThreads>>>(ctx->geo, R, (const T *)ctx->A_explicit, d));
+        return (int)FALM_OK;
+    });
+    if (rc) { cudaFree(d); return rc; }
+    CK(cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost));
+    cudaFree(d);
+    double v;
+    memcpy(&v, &h, sizeof(v));
+    *out = v;
+    return FALM_OK;
+}
+
+int falm_mv_scale(falm_ctx *ctx, void *a, long long n, double scale, void *stream) {
+    if (!ctx || !a || n < 0) return FALM_ERR_ARG;
+    return dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        LAUNCH(FALM_K_OTHER, (cudaStream_t)0, k_scale<T><<<ctx->sm_count * 4, 256, 0, S(stream)>>>((T *)a, n, (T)scale));
+        return (int)FALM_OK;
+    });
+}
+
+int falm_mv_axby(falm_ctx *ctx, double a, const void *x, double b, const void *y, void *result, long long n, void *stream) {
+    if (!ctx || !x || !y || !result || n < 0) return FALM_ERR_ARG;
+    return dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        LAUNCH(FALM_K_OTHER, (cudaStream_t)0, k_axby<T><<<ctx->sm_count * 4, 256, 0, S(stream)>>>((T)a, (const T *)x, (T)b, (const T *)y, (T *)result, n));
+        return (int)FALM_OK;
+    });
+}
+
+// ---------------------------------------------------------------- boundary conditions
+int falm_bc_init(falm_ctx *ctx, int kind, double u_inlet) {
+    if (!ctx || (kind != FALM_BC_CHANNEL && kind != FALM_BC_CAVITY)) return FALM_ERR_ARG;
+    ctx->bc_kind = kind;
+    ctx->u_inlet = u_inlet;
+    return FALM_OK;
+}
+
+int falm_bc_set_inflow(falm_ctx *ctx, const double *box, int nb, double dx) {
+    if (!ctx) return FALM_ERR_ARG;
+    if (ctx->inflow_box) { cudaFree(ctx->inflow_box); ctx->inflow_box = nullptr; }
+    if (!box) return FALM_OK;
+    if (nb < 2 || !(dx > 0)) return FALM_ERR_ARG;
+    size_t n = 3ull * nb * ctx->geo.ny * ctx->geo.nz;
+    CK(cudaMalloc(&ctx->inflow_box, n * sizeof(double)));
+    CK(cudaMemcpy(ctx->inflow_box, box, n * sizeof(double), cudaMemcpyHostToDevice));
+    ctx->inflow_nb = nb;
+    ctx->inflow_dx = dx;
+    return FALM_OK;
+}
+
+int falm_bc_ubc(falm_ctx *ctx, void *u, const void *uprev, double dt, double t, void *stream) {
+    if (!ctx || !u || !uprev) return FALM_ERR_ARG;
+    return dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        return ubc_t<T>(ctx, (T *)u, UPrev<T>{(const T *)uprev, 0}, dt, t, S(stream));
+    });
+}
+
+int falm_bc_pbc(falm_ctx *ctx, void *p, void *stream) {
+    if (!ctx || !p) return FALM_ERR_ARG;
+    return dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        LAUNCH(FALM_K_PBC, S(stream), k_pbc<T><<<dim3(64, 3), 256, 0, S(stream)>>>(ctx->geo, ctx->bc_kind, (T *)p));
+        return (int)FALM_OK;
+    });
+}
+
+int falm_bc_uubc(falm_ctx *ctx, void *uu, void *stream) {
+    if (!ctx || !uu) return FALM_ERR_ARG;
+    if (ctx->bc_kind != FALM_BC_CAVITY) return FALM_OK;
+    return dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        LAUNCH(FALM_K_OTHER, S(stream), k_uubc<T><<<dim3(64, 3), 256, 0, S(stream)>>>(ctx->geo, (T *)uu));
+        return (int)FALM_OK;
+    });
+}
+
+// ---------------------------------------------------------------- ALM
+int falm_alm_build_aps(int n_station, const double *st_r, const double *st_chord, const double *st_twist,
+                       const double *st_cl, const double *st_cd, int n_attack, int apcount, int n_ap_per_blade,
+                       double radius, double hub_radius, double *ap_r, double *ap_chord, double *ap_twist, double *ap_cl,
+                       double *ap_cd) {
+    if (n_station < 1 || !st_r || !st_chord || !st_twist || !st_cl || !st_cd || n_attack < 1 || apcount < 1 ||
+        n_ap_per_blade < 1 || !ap_r || !ap_chord || !ap_twist || !ap_cl || !ap_cd)
+        return FALM_ERR_ARG;
+    // src/alm/bladeHandler.h:46-104: r = (k+1/2) dr + r_hub, linear interpolation in r/R between
+    // stations (clamped at both ends) of chord, twist and every polar value
+    const double dr = (radius - hub_radius) / n_ap_per_blade;
+    for (int ap = 0; ap < apcount; ap++) {
+        double apr = (ap % n_ap_per_blade + 0.5) * dr + hub_radius;
+        int lo = 0;
+        double w = 0.0;
+        int mode = 2;
+        if (apr < st_r[0]) mode = 0;
+        else if (apr >= st_r[n_station - 1]) mode = 1;
+        else {
+            int i = 0;
+            for (; i < n_station - 1; i++)
+                if (st_r[i] <= apr && st_r[i + 1] > apr) { w = (apr - st_r[i]) / (st_r[i + 1] - st_r[i]); break; }
+            lo = i;
+        }
+        auto interp = [&](const double *v, int stride, int col) {
+            if (mode == 0) return v[col];
+            if (mode == 1) return v[(long long)(n_station - 1) * stride + col];
+            return (1. - w) * v[(long long)lo * stride + col] + w * v[(long long)(lo + 1) * stride + col];
+        };
+        ap_r[ap] = apr;
+        ap_chord[ap] = interp(st_chord, 1, 0);
+        ap_twist[ap] = interp(st_twist, 1, 0);
+        for (int a = 0; a < n_attack; a++) {
+            ap_cl[ap + (long long)a * apcount] = interp(st_cl, n_attack, a);
+            ap_cd[ap + (long long)a * apcount] = interp(st_cd, n_attack, a);
+        }
+    }
+    return FALM_OK;
+}
+
+int falm_alm_init(falm_ctx *ctx, const falm_alm_desc *d) {
+    if (!ctx || !d || d->n_turbine < 1 || d->n_turbine > kMaxTurbines || d->n_blade < 1 || d->n_ap_per_blade < 1 ||
+        d->n_attack < 2 || !(d->euler_eps > 0) || !d->base || !d->hub || !d->tip_rate || !d->motion || !d->angle_type ||
+        !d->ap_r || !d->ap_chord || !d->ap_twist || !d->attack || !d->cl || !d->cd)
+        return FALM_ERR_ARG;
+    const int nt = d->n_turbine, apc = d->n_turbine * d->n_blade * d->n_ap_per_blade, na = d->n_attack;
+    // one allocation: doubles then ints
+    size_t nd = 3 * nt + 3 * nt + nt + 3 * nt + 3 * apc + na + 2 * (size_t)apc * na + 3 * apc + 3 * apc + apc + apc;
+    size_t bytes = nd * sizeof(double) + sizeof(AlmScalars) + nt * sizeof(int) + 512;
+    if (ctx->alm_mem) { cudaFree(ctx->alm_mem); ctx->alm_mem = nullptr; }
+    CK(cudaMalloc(&ctx->alm_mem, bytes));
+    CK(cudaMemset(ctx->alm_mem, 0, bytes));
+    double *p = (double *)ctx->alm_mem;
+    auto put = [&](const double *src, size_t n) -> double * {
+        double *dst = p;
+        p += n;
+        if (src) cudaMemcpy(dst, src, n * sizeof(double), cudaMemcpyHostToDevice);
+        return dst;
+    };
+    AlmDev &a = ctx->alm;
+    a.n_turbine = nt; a.n_blade = d->n_blade; a.n_ap_per_blade = d->n_ap_per_blade; a.n_attack = na; a.apcount = apc;
+    a.radius = d->radius; a.hub_radius = d->hub_radius; a.euler_eps = d->euler_eps; a.pitch = d->pitch;
+    a.rcut2 = 36.0 * d->euler_eps * d->euler_eps;
+    a.base = put(d->base, 3 * nt); a.hub = put(d->hub, 3 * nt); a.tip_rate = put(d->tip_rate, nt); a.motion = put(d->motion, 3 * nt);
+    a.ap_r = put(d->ap_r, apc); a.ap_chord = put(d->ap_chord, apc); a.ap_twist = put(d->ap_twist, apc);
+    a.attack = put(d->attack, na); a.cl = put(d->cl, (size_t)apc * na); a.cd = put(d->cd, (size_t)apc * na);
+    a.ap_xyz = put(nullptr, 3 * apc); a.ap_force = put(nullptr, 3 * apc); a.ap_torque = put(nullptr, apc); a.ap_thrust = put(nullptr, apc);
+    char *q = (char *)p;
+    q = (char *)(((uintptr_t)q + 255) & ~(uintptr_t)255);
+    a.scal = (AlmScalars *)q;
+    q += sizeof(AlmScalars);
+    int *ip = (int *)q;
+    CK(cudaMemcpy(ip, d->angle_type, nt * sizeof(int), cudaMemcpyHostToDevice));
+    a.angle_type = ip;
+    ctx->alm_on = 1;
+    return FALM_OK;
+}
+
+int falm_alm_set_pitch(falm_ctx *ctx, double pitch_deg) {
+    if (!ctx) return FALM_ERR_ARG;
+    if (!ctx->alm_on) return FALM_ERR_NOALM;
+    ctx->alm.pitch = pitch_deg;
+    return FALM_OK;
+}
+
+int falm_alm_run(falm_ctx *ctx, const void *u, void *ff, double t, void *stream, double *torque, double *thrust) {
+    if (!ctx || !u) return FALM_ERR_ARG;
+    if (!ctx->alm_on) return FALM_ERR_NOALM;
+    int rc = dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        return alm_run_t<T>(ctx, (const T *)u, (T *)ff, t, S(stream));
+    });
+    if (rc) return rc;
+    if (torque || thrust) {
+        CK(cudaMemcpyAsync(ctx->alm_scal_host, ctx->alm.scal, sizeof(AlmScalars), cudaMemcpyDeviceToHost, S(stream)));
+        CK(cudaStreamSynchronize(S(stream)));
+        for (int q = 0; q < ctx->alm.n_turbine; q++) {
+            if (torque) torque[q] = ctx->alm_scal_host->torque[q];
+            if (thrust) thrust[q] = ctx->alm_scal_host->thrust[q];
+        }
+    }
+    return FALM_OK;
+}
+
+int falm_alm_get_aps(falm_ctx *ctx, double *xyz, double *force, double *torque, double *thrust) {
+    if (!ctx) return FALM_ERR_ARG;
+    if (!ctx->alm_on) return FALM_ERR_NOALM;
+    CK(cudaDeviceSynchronize());
+    const size_t n = ctx->alm.apcount;
+    if (xyz) CK(cudaMemcpy(xyz, ctx->alm.ap_xyz, 3 * n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (force) CK(cudaMemcpy(force, ctx->alm.ap_force, 3 * n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (torque) CK(cudaMemcpy(torque, ctx->alm.ap_torque, n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (thrust) CK(cudaMemcpy(thrust, ctx->alm.ap_thrust, n * sizeof(double), cudaMemcpyDeviceToHost));
+    return FALM_OK;
+}
+
+// ---------------------------------------------------------------- step
+int falm_step(falm_ctx *ctx, const falm_fields *f, double dt, double t, void *stream, falm_step_stats *st) {
+    if (!ctx || !f || !f->u || !f->uu || !f->p || !f->nut || !(dt > 0)) return FALM_ERR_ARG;
+    return dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        return step_t<T>(ctx, f, dt, t, S(stream), st);
+    });
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int falm_bc_set_inlet_plane(falm_ctx *ctx, const double *plane, void *stream) {
+    if (!ctx || !plane) return FALM_ERR_ARG;
+    const size_t n = 3ull * ctx->geo.ny * ctx->geo.nz;
+    if (!ctx->inlet_plane) CK(cudaMalloc(&ctx->inlet_plane, n * sizeof(double)));
+    CK(cudaMemcpyAsync(ctx->inlet_plane, plane, n * sizeof(double), cudaMemcpyHostToDevice, S(stream)));
+    ctx->inlet_plane_valid = 1;
+    return FALM_OK;
+}
+
+int falm_profile_enable(falm_ctx *ctx, int enable) {
+    if (!ctx) return FALM_ERR_ARG;
+    ctx->profiling = enable ? 1 : 0;
+    return FALM_OK;
+}
+
+int falm_profile_read(falm_ctx *ctx, double *ms, long long *launches, int nclass, int reset) {
+    if (!ctx || nclass < 0) return FALM_ERR_ARG;
+    CK(cudaDeviceSynchronize());
+    for (auto &r : *ctx->ev_pending) {
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, r.a, r.b) == cudaSuccess) {
+            ctx->prof_ms[r.cls] += t;
+            ctx->prof_n[r.cls] += 1;
+        }
+        cudaGetLastError();
+        ctx->ev_pool->push_back(r.a);
+        ctx->ev_pool->push_back(r.b);
+    }
+    ctx->ev_pending->clear();
+    for (int c = 0; c < nclass && c < FALM_K_COUNT; c++) {
+        if (ms) ms[c] = ctx->prof_ms[c];
+        if (launches) launches[c] = ctx->prof_n[c];
+    }
+    if (reset)
+        for (int c = 0; c < FALM_K_COUNT; c++) { ctx->prof_ms[c] = 0; ctx->prof_n[c] = 0; }
+    return FALM_OK;
+}
+
+}  // extern "C"

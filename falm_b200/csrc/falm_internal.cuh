@@ -1,0 +1,143 @@
+// Internal declarations of the falm_b200 library (sm_100a).
+//
+// Data layout in HBM: the reference's column-major SoA over the ghost-padded
+// box (value(idx, col) = ptr[idx + col*N], idx = i + j*sx + k*sx*sy).  Metrics
+// are never stored as 3D planes: every kernel rebuilds ja = hx*hy*hz, kx = 1/h
+// and g = ja*kx*kx from 1D tables (a few KB, L1-resident), which removes the
+// seven metric planes the reference streams through every stencil.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+#include "falm_b200.h"
+
+namespace fb {
+
+constexpr int kMaxTurbines = 8;
+constexpr int kRowThreads = 256;          // threads per block of the row kernels
+constexpr int kWarpsPerBlock = kRowThreads / 32;
+
+// 1D metric tables of one precision (device pointers into one allocation)
+template <typename T>
+struct Metric {
+    const T *x[3];    // cell centres
+    const T *h[3];    // widths
+    const T *k[3];    // 1/h  (kx, src/falm.h:395)
+};
+
+// Poisson operator as separable 1D tables (see poisson.cu for the derivation)
+template <typename T>
+struct PoissonTables {
+    const T *cm[3];   // scaled coefficient towards the minus neighbour  (w, s, b)
+    const T *cp[3];   // scaled coefficient towards the plus neighbour   (e, n, t)
+    const T *um[3];   // unscaled minus coefficients (for the diagonal)
+    const T *up[3];   // unscaled plus coefficients
+    const T *dx0;     // (-e) - w, unscaled, per i: first two terms of the diagonal
+    T scale;          // 1/maxdiag
+};
+
+struct Geom {
+    int sx, sy, sz, gc;
+    long long n;      // sx*sy*sz
+    int nx, ny, nz;   // interior sizes
+    __host__ __device__ inline long long id(int i, int j, int k) const {
+        return (long long)i + (long long)j * sx + (long long)k * sx * sy;
+    }
+};
+
+// device-side solver scalars (one per context)
+struct SolverScalars {
+    double rho, rrho, alpha, beta, omega;
+    double err, gsize, tol;
+    double red[4];      // scratch reduction results
+    int it, maxit, done, status;
+    int first;          // 1 before the first BiCGStab iteration of a solve
+    int pad[3];
+};
+
+struct AlmScalars {
+    double torque[kMaxTurbines], thrust[kMaxTurbines];
+    double bbox[6];     // xmin,xmax,ymin,ymax,zmin,zmax of the AP cloud (+cutoff)
+};
+
+// reduction workspace: per-block partials + arrival counter + results
+struct RedWork {
+    double *partials;     // capacity maxBlocks * 4
+    unsigned int *counter;
+    int maxBlocks;
+};
+
+struct AlmDev {
+    int n_turbine, n_blade, n_ap_per_blade, n_attack, apcount;
+    double radius, hub_radius, euler_eps, pitch, rcut2;
+    const double *base, *hub, *tip_rate, *motion;
+    const int *angle_type;
+    const double *ap_r, *ap_chord, *ap_twist, *attack, *cl, *cd;
+    double *ap_xyz, *ap_force, *ap_torque, *ap_thrust;
+    AlmScalars *scal;
+};
+
+}  // namespace fb
+
+// host-side context
+struct falm_ctx {
+    int precision;
+    fb::Geom geo;
+    int device;
+    // metrics
+    void *metric_mem;                       // one allocation holding both precisions
+    fb::Metric<double> m64;
+    fb::Metric<float> m32;
+    std::vector<double> *hx, *hy, *hz, *xc, *yc, *zc;  // host copies
+    // CFD parameters
+    double Re, Cs;
+    int adv, sgs;
+    // solver parameters
+    int ls_type, maxit, pc_type, pc_maxit;
+    double tol, relax, pc_relax;
+    int max_outer;
+    // Poisson operator
+    int op_ready;
+    int bc_kind_op;
+    double maxdiag;
+    void *op_mem;
+    fb::PoissonTables<double> pt64;
+    fb::PoissonTables<float> pt32;
+    const void *A_explicit;                 // caller-owned 7-column matrix or NULL
+    // BC
+    int bc_kind;
+    double u_inlet;
+    double *inflow_box;                     // device FP64
+    int inflow_nb;
+    double inflow_dx;
+    // work vectors (element size = precision), allocated lazily
+    size_t esize;
+    void *work_mem;
+    void *w_rr, *w_p, *w_q, *w_s, *w_pp, *w_ss, *w_t, *w_r, *w_rhs, *w_ua, *w_div, *w_xp;
+    void *w_outlet;                         // 3 planes x 3 comps of the previous velocity at the outlet
+    // reductions
+    fb::RedWork red;
+    fb::SolverScalars *scal;                // device
+    fb::SolverScalars *scal_host;           // pinned
+    // ALM
+    int alm_on;
+    void *alm_mem;
+    fb::AlmDev alm;
+    std::vector<double> *alm_host;          // host copy of tables
+    fb::AlmScalars *alm_scal_host;          // pinned
+    // bookkeeping
+    long long launches;
+    // per-class event timing (falm_profile_enable)
+    int profiling;
+    struct EvRec { int cls; cudaEvent_t a, b; };
+    std::vector<EvRec> *ev_pending;
+    std::vector<cudaEvent_t> *ev_pool;
+    double prof_ms[FALM_K_COUNT];
+    long long prof_n[FALM_K_COUNT];
+    // streamed inlet plane
+    double *inlet_plane;                    // device 3 x nz x ny
+    int inlet_plane_valid;
+    int sm_count;
+    std::string *last_error;
+};

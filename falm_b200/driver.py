@@ -1,0 +1,65 @@
+"""Step driver: the init and time loop of app/nedo/main.cpp:102-236 (and
+app/lid3d/main.cpp for the cavity) over the falm_b200 C ABI."""
+import numpy as np
+
+from . import cases as C
+from .api import Context
+
+
+class Simulation:
+    def __init__(self, case, precision="fp64", fuse_alm=True, device=None):
+        self.case = case
+        ctx = Context(case.grid, precision, device)
+        ctx.cfd_init(case.Re, case.adv, case.sgs, case.Cs)
+        ctx.eq_init(case.maxit, case.tol, case.pc, case.pc_maxit, case.pc_relax)
+        ctx.bc_init(case.bc, case.u_inlet)
+        self.maxdiag = ctx.poisson_operator(case.bc)
+        if case.inflow is not None:
+            ctx.set_inflow(case.inflow, float(case.grid.hx[case.grid.gc]))
+        if case.alm is not None:
+            ctx.alm_init(case.alm)
+        self.ctx = ctx
+        torch = ctx.torch
+        st = C.initial_state(case)
+        self.u = torch.as_tensor(st["u"], dtype=ctx.dtype, device=ctx.device).contiguous()
+        self.uu, self.p, self.nut = ctx.field(3), ctx.field(1), ctx.field(1)
+        self.ff = None if (fuse_alm and case.alm is not None) else ctx.field(3)
+        ctx.utouu(self.u, self.uu)         # app/nedo/main.cpp:132-133
+        ctx.sgs(self.u, self.nut)
+        self.it = 0
+
+    def t(self):
+        return self.it * self.case.dt
+
+    def step(self):
+        """one main_loop iteration; returns the step statistics"""
+        self.it += 1
+        return self.ctx.step(self.u, self.uu, self.p, self.nut, self.ff, self.case.dt, self.t())
+
+    def inlet_plane(self, it):
+        """inlet velocity of step `it` sampled from the case's inflow box (as the
+        library samples it): 3 x nz x ny, float64"""
+        case = self.case
+        box = case.inflow
+        nx, ny, nz = case.grid.interior
+        if box is None:
+            plane = np.zeros((3, nz, ny))
+            plane[0] = case.u_inlet
+            return plane
+        dx = float(case.grid.hx[case.grid.gc])
+        xs = case.u_inlet * (it * case.dt) / dx
+        fl = np.floor(xs)
+        fr = xs - fl
+        s0 = int(fl) % box.shape[1]
+        s1 = (s0 + 1) % box.shape[1]
+        plane = (1.0 - fr) * box[:, s0] + fr * box[:, s1]
+        plane[0] += case.u_inlet
+        return plane
+
+    def state(self):
+        import torch
+        torch.cuda.synchronize()
+        return {k: getattr(self, k).double().cpu().numpy() for k in ("u", "uu", "p", "nut")}
+
+    def close(self):
+        self.ctx.close()

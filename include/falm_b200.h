@@ -1,0 +1,220 @@
+/*
+ * falm_b200 -- C ABI of the B200 (sm_100a) implementation of FALM's LES step.
+ *
+ * Drop-in boundary for the reference's solver classes: FalmCFD, FalmEq,
+ * FalmMV, Alm::AlmHandler and the application boundary routines.  Every
+ * entry point cites the reference interface it replaces (paths relative to
+ * the reference project ki2098/falm).
+ *
+ * Conventions
+ *  - Fields are caller-owned DEVICE arrays in the reference's layout
+ *    (src/matrix.h:20, src/util.h:74-76): column-major SoA over the box with
+ *    guide cells, value(idx, col) = ptr[idx + col*N], idx = i + j*sx + k*sx*sy,
+ *    N = sx*sy*sz.  Vector fields (u, uu, ff) have 3 columns.
+ *  - Element type of every field pointer (void*) is the context precision:
+ *    double for FALM_FP64, float for FALM_MIXED.  Inner products, norms,
+ *    residual checks and returned scalars are double in both modes.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *    Entry points that return a scalar on the host synchronise that stream;
+ *    the others are asynchronous.
+ *  - Every entry point returns a falm_status; nothing aborts the process.
+ *  - Metrics (ja, kx, g of src/falm.h:383-404) are not passed per call: they
+ *    are evaluated from the 1D control-volume tables given at falm_create,
+ *    which is what the reference builds its 3D metric planes from.
+ */
+#ifndef FALM_B200_H
+#define FALM_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FALM_B200_ABI_VERSION 1
+
+typedef enum {
+    FALM_OK = 0,
+    FALM_ERR_ARG = 1,        /* bad argument (null pointer, size, enum)                    */
+    FALM_ERR_CUDA = 2,       /* CUDA runtime error (see falm_last_error)                   */
+    FALM_ERR_NAN = 3,        /* non-finite value detected in a reduction                   */
+    FALM_ERR_BREAKDOWN = 4,  /* BiCGStab |rho| < FLT_MIN (src/FalmEq.cpp:348)              */
+    FALM_ERR_MAXIT = 5,      /* linear solver stopped at maxit without reaching tol        */
+    FALM_ERR_TIMEOUT = 6,    /* a bounded device-side wait gave up                         */
+    FALM_ERR_ALLOC = 7,      /* device allocation failed                                   */
+    FALM_ERR_STATE = 8,      /* call order (e.g. solve before the operator was built)      */
+    FALM_ERR_NOALM = 9       /* ALM entry point called without falm_alm_init               */
+} falm_status;
+
+typedef enum { FALM_FP64 = 0, FALM_MIXED = 1 } falm_precision;
+
+/* src/FalmCFDDevCall.h (AdvectionSchemeType, SGSType) */
+enum { FALM_ADV_UPWIND1 = 0, FALM_ADV_UPWIND3 = 1, FALM_ADV_QUICK = 2, FALM_ADV_UTOPIA = 3, FALM_ADV_KK = 4 };
+enum { FALM_SGS_EMPTY = 0, FALM_SGS_SMAGORINSKY = 1, FALM_SGS_CSM = 2 };
+/* src/FalmEqDevCall.h:143-149 (SolverType) */
+enum { FALM_LS_EMPTY = 0, FALM_LS_JACOBI = 1, FALM_LS_SOR = 2, FALM_LS_PBICGSTAB = 4 };
+/* boundary-condition sets of the application drivers */
+enum { FALM_BC_CHANNEL = 0,  /* app/nedo, app/windtunnel: inlet, convective outlet, slip y+-, wall z-, slip z+ */
+       FALM_BC_CAVITY  = 1 };/* app/lid3d: walls, lid y+ moving with (1,0,0), zero normal face flux     */
+
+typedef struct falm_ctx falm_ctx;
+
+/* Control-volume description (src/FalmIO.h:99-116, src/FalmMeshBase.h):
+ * shape with guide cells and 1D centre/width tables, HOST pointers (copied). */
+typedef struct {
+    int sx, sy, sz;            /* pdm.shape incl. guide cells            */
+    int gc;                    /* guide cells (src/typedef.h:41), 2      */
+    const double *x, *y, *z;   /* cell centres, lengths sx, sy, sz       */
+    const double *hx, *hy, *hz;/* cell widths,  lengths sx, sy, sz       */
+} falm_grid;
+
+/* Turbines and actuator points (src/alm/turbineHandler.h:13-104,
+ * src/alm/apHandler.h:12-143).  HOST pointers, copied by falm_alm_init. */
+typedef struct {
+    int n_turbine, n_blade, n_ap_per_blade, n_attack;
+    double radius, hub_radius, euler_eps;
+    const double *base;        /* 3*n_turbine                                        */
+    const double *hub;         /* 3*n_turbine, rotor centre in the turbine frame     */
+    const double *tip_rate;    /* n_turbine                                          */
+    const double *motion;      /* 3*n_turbine: amplitude [rad], angular freq, phase  */
+    const int    *angle_type;  /* n_turbine: 0 none, 1 roll, 2 pitch, 3 yaw          */
+    const double *ap_r, *ap_chord, *ap_twist;  /* apcount                           */
+    const double *attack;      /* n_attack [deg]                                     */
+    const double *cl, *cd;     /* apcount*n_attack, (ap, atk) at ap + atk*apcount    */
+    double pitch;              /* collective pitch offset [deg] added to every twist */
+} falm_alm_desc;
+
+/* Fields of one step, caller-owned device arrays (FalmBasicVar, src/falm.h:16-43). */
+typedef struct {
+    void *u;      /* 3N velocity                                            */
+    void *uu;     /* 3N contravariant face velocity                         */
+    void *p;      /* N  pressure                                            */
+    void *nut;    /* N  eddy viscosity                                      */
+    void *ff;     /* 3N ALM body force, or NULL: the force is then evaluated
+                     inside the pseudo-velocity kernel and never stored     */
+} falm_fields;
+
+typedef struct {
+    int    it;          /* Poisson iterations this step (BiCGStab, summed over refinement passes) */
+    double err;         /* final ||r||_2 / N_interior (src/FalmEq.cpp:403)                          */
+    double divnorm;     /* sqrt(sum div^2) / N_interior (app/nedo/main.cpp:194-197,230)             */
+    int    outer;       /* refinement passes (1 in FP64 mode)                                      */
+    int    status;      /* falm_status of the linear solve                                          */
+    double torque[8];   /* per turbine (src/alm/almDevCall.cu:362-370)                              */
+    double thrust[8];
+} falm_step_stats;
+
+/* ---------------- context ---------------------------------------------------------------- */
+/* FalmCore::computation_init (src/falm.h:342-431) minus IO; one GPU, no MPI. */
+int falm_create(const falm_grid *grid, int precision, falm_ctx **out);
+int falm_destroy(falm_ctx *ctx);
+const char *falm_last_error(const falm_ctx *ctx);
+int falm_abi_version(void);
+/* number of this library's kernels launched since creation (for launch accounting) */
+long long falm_kernel_launches(const falm_ctx *ctx);
+
+/* ---------------- FalmCFD (src/FalmCFD.h:15-109, src/FalmCFDDevCall.h) --------------------- */
+int falm_cfd_init(falm_ctx *ctx, double Re, int adv_scheme, int sgs_model, double Cs);
+/* FalmCFD::FSPseudoU (src/FalmCFD.cpp:5-67): ua = un + dt(-adv(u,uu) + vis(u,nut) + ff) on the
+   interior.  ua must not alias u (the reference's aliased call is a data race). ff may be NULL
+   when falm_alm_init was called: the ALM force is then projected inside the kernel. */
+int falm_cfd_pseudo_u(falm_ctx *ctx, const void *un, const void *u, const void *uu, void *ua,
+                      const void *nut, const void *ff, double dt, double t, void *stream);
+/* FalmCFD::UtoUU (src/FalmCFD.cpp:69-129) */
+int falm_cfd_utouu(falm_ctx *ctx, const void *u, void *uu, void *stream);
+/* FalmCFD::MACCalcPoissonRHS (src/FalmCFD.h:96-109) */
+int falm_cfd_poisson_rhs(falm_ctx *ctx, const void *uu, void *rhs, double dt, double maxdiag, void *stream);
+/* FalmCFD::ProjectP (src/FalmCFD.cpp:131-185); u may alias ua and uu may alias uua */
+int falm_cfd_project_p(falm_ctx *ctx, void *u, const void *ua, void *uu, const void *uua,
+                       const void *p, double dt, void *stream);
+/* FalmCFD::SGS (src/FalmCFD.cpp:187-238) */
+int falm_cfd_sgs(falm_ctx *ctx, const void *u, void *nut, void *stream);
+/* FalmCFD::Divergence (src/FalmCFD.h:84-94) */
+int falm_cfd_divergence(falm_ctx *ctx, const void *uu, void *div, void *stream);
+
+/* ---------------- FalmEq (src/FalmEq.h:14-76) -------------------------------------------- */
+/* FalmEq::init (src/FalmEq.h:23-25) */
+int falm_eq_init(falm_ctx *ctx, int type, int maxit, double tol, double relax,
+                 int pc_type, int pc_maxit, double pc_relax);
+/* Poisson operator of the application drivers (app/nedo/main.cpp:25-100,
+   app/lid3d/main.cpp:22-92) + FalmMV::MaxDiag + ScaleMatrix; kept as 1D
+   coefficient tables.  Returns maxdiag. */
+int falm_eq_poisson_operator(falm_ctx *ctx, int bc_kind, double *maxdiag_out);
+/* Use an explicit caller-owned 7-column matrix (columns c,w,e,s,n,b,t,
+   src/dev/FalmEqDevCall.cu:69-75) instead; NULL returns to the Poisson tables. */
+int falm_eq_set_matrix(falm_ctx *ctx, const void *A);
+/* FalmEq::Solve (src/FalmEq.h:56-64) -> PBiCGStab (src/FalmEq.cpp:305-410).  In FALM_MIXED the
+   iteration runs in FP32 storage with FP64 inner products and is wrapped in an FP64
+   true-residual refinement loop.  it/err as FalmEq::it/err (src/FalmEqDevCall.h:27-30). */
+int falm_eq_solve(falm_ctx *ctx, void *x, const void *b, void *r, void *stream, int *it_out, double *err_out);
+/* FalmEq::Res (src/FalmEq.cpp:45-78) */
+int falm_eq_res(falm_ctx *ctx, const void *x, const void *b, void *r, void *stream);
+/* FalmEqDevCall::SORSweep (src/dev/FalmEqDevCall.cu:175-221), one colour */
+int falm_eq_sor_sweep(falm_ctx *ctx, void *x, const void *b, double omega, int color, void *stream);
+
+/* ---------------- FalmMV (src/MV.h:11-136) ------------------------------------------------ */
+int falm_mv_mv(falm_ctx *ctx, const void *x, void *ax, void *stream);
+int falm_mv_dot(falm_ctx *ctx, const void *a, const void *b, double *out, void *stream);
+int falm_mv_normsq(falm_ctx *ctx, const void *a, int ncol, double *out, void *stream);
+int falm_mv_maxdiag(falm_ctx *ctx, double *out);
+int falm_mv_scale(falm_ctx *ctx, void *a, long long n, double scale, void *stream);
+int falm_mv_axby(falm_ctx *ctx, double a, const void *x, double b, const void *y, void *result,
+                 long long n, void *stream);
+
+/* ---------------- boundary conditions (application drivers) -------------------------------- */
+/* kind and inlet velocity (app/windtunnel/bcdevcall.cu:8-22 takes u_inlet) */
+int falm_bc_init(falm_ctx *ctx, int kind, double u_inlet);
+/* Seeded inflow: periodic perturbation box, HOST FP64 array 3 x nb x (sy-2gc) x (sz-2gc)
+   (component-major, then x-plane, then j, then k), sampled at x = u_inlet*t, plane spacing dx.
+   NULL removes it.  No reference counterpart (the reference has uniform inflow only). */
+int falm_bc_set_inflow(falm_ctx *ctx, const double *box, int nb, double dx);
+/* ubc (app/nedo/bc.h, app/lid3d/bc.h): velocity ghost cells.  uprev feeds the convective outlet. */
+int falm_bc_ubc(falm_ctx *ctx, void *u, const void *uprev, double dt, double t, void *stream);
+/* pbc: pressure ghost cells */
+int falm_bc_pbc(falm_ctx *ctx, void *p, void *stream);
+/* uubc (app/lid3d/bc.h): zero wall-normal face flux, cavity only (no-op for the channel) */
+int falm_bc_uubc(falm_ctx *ctx, void *uu, void *stream);
+
+/* ---------------- ALM (src/alm/alm.h:12-140) ----------------------------------------------- */
+/* AlmHandler::init (src/alm/alm.h:20-57) after the AP tables were built */
+int falm_alm_init(falm_ctx *ctx, const falm_alm_desc *desc);
+/* BladeHandler::buildAP (src/alm/bladeHandler.h:16-104), host only: station polars row-major
+   [station][attack]; outputs in the APFrame layout. */
+int falm_alm_build_aps(int n_station, const double *st_r, const double *st_chord, const double *st_twist,
+                       const double *st_cl, const double *st_cd, int n_attack, int apcount,
+                       int n_ap_per_blade, double radius, double hub_radius,
+                       double *ap_r, double *ap_chord, double *ap_twist, double *ap_cl, double *ap_cd);
+/* change the collective pitch offset [deg] */
+int falm_alm_set_pitch(falm_ctx *ctx, double pitch_deg);
+/* AlmHandler::Alm (src/alm/alm.h:66-77): AP forces at time t from u, projected into ff
+   (3N, interior written).  torque/thrust per turbine returned if non-NULL (syncs). */
+int falm_alm_run(falm_ctx *ctx, const void *u, void *ff, double t, void *stream,
+                 double *torque, double *thrust);
+/* AP state after the last ALM evaluation (host FP64 arrays, any may be NULL) */
+int falm_alm_get_aps(falm_ctx *ctx, double *xyz, double *force, double *torque, double *thrust);
+
+/* ---------------- one fused time step ------------------------------------------------------ */
+/* app/nedo/main.cpp:150-204 (channel) / app/lid3d/main.cpp:121-168 (cavity):
+   ALM -> pseudo-velocity -> UtoUU [-> uubc] -> RHS -> Poisson -> pbc -> projection -> ubc ->
+   SGS -> divergence norm, with the race-free pseudo-velocity convention.  t = it*dt. */
+int falm_step(falm_ctx *ctx, const falm_fields *f, double dt, double t, void *stream, falm_step_stats *st);
+
+/* Streamed inflow: the inlet velocity (u,v,w) of the NEXT ubc call as a HOST FP64 array
+   3 x (sz-2gc) x (sy-2gc) (component, then k, then j fastest), copied asynchronously on
+   `stream` (pass pinned memory).  Takes precedence over the inflow box for that one call.
+   No reference counterpart (the reference has uniform inflow only). */
+int falm_bc_set_inlet_plane(falm_ctx *ctx, const double *plane, void *stream);
+
+/* ---------------- instrumentation ----------------------------------------------------------- */
+/* Kernel classes timed with CUDA events when profiling is on (one event pair per launch). */
+enum { FALM_K_ALM = 0, FALM_K_PSEUDO_U, FALM_K_UTOUU_RHS, FALM_K_RES, FALM_K_BICG_P, FALM_K_SOR, FALM_K_MV_DOT1,
+       FALM_K_BICG_S, FALM_K_MV_DOT2, FALM_K_BICG_XR, FALM_K_PBC, FALM_K_PROJECT, FALM_K_UBC, FALM_K_SGS_DIV,
+       FALM_K_OTHER, FALM_K_COUNT };
+int falm_profile_enable(falm_ctx *ctx, int enable);
+/* milliseconds and launch counts per class since the last reset (synchronises the device) */
+int falm_profile_read(falm_ctx *ctx, double *ms, long long *launches, int nclass, int reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

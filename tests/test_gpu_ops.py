@@ -1,0 +1,285 @@
+"""Per-operator parity of the CUDA path (through the C ABI) with the CPU oracle,
+FP64, on seeded random inputs.  The tolerance is relative L2 <= 1e-12: both sides
+evaluate the same expressions and differ by FMA contraction only."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from falm_b200 import cases
+from tests.helpers import dev, faces, host, interior, make_ctx, random_state, rel_l2
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def _setup(oracle, case):
+    from oracle.oracle import CaseStruct
+    cs = CaseStruct(case)
+    m = oracle.setup(cs)
+    return cs, m
+
+
+def _p(a):
+    from oracle.oracle import _p as pp
+    return pp(a)
+
+
+CASES = {
+    "channel": lambda: cases.small_channel(24, 16, 12, intensity=0.05).with_inflow(nb=8),
+    "cavity": lambda: cases.cavity(12),
+    "stretched": lambda: cases.Case("stretched", cases.stretched_grid(20, 14, 12, 0.1), 0, Re=500.0, dt=0.01, tol=1e-10),
+}
+
+
+@pytest.fixture(params=list(CASES))
+def case(request):
+    return CASES[request.param]()
+
+
+@pytest.mark.parametrize("adv", ["Upwind3", "Upwind1", "QUICK", "UTOPIA", "KK"])
+def test_pseudo_u(oracle, lib_built, adv):
+    case = CASES["stretched"]()
+    case.adv = adv
+    cs, m = _setup(oracle, case)
+    st = random_state(case)
+    ua = np.zeros_like(st["u"])
+    oracle.L.oracle_pseudo_u(ctypes.byref(cs.c), _p(st["u"]), _p(st["u"]), _p(st["uu"]), _p(ua), _p(st["nut"]),
+                             _p(m["kx"]), _p(m["g"]), _p(m["ja"]), _p(st["ff"]))
+    ctx = make_ctx(case)
+    u, uu, nut, ff = dev(ctx, st["u"]), dev(ctx, st["uu"]), dev(ctx, st["nut"]), dev(ctx, st["ff"])
+    ua_d = ctx.field(3)
+    ctx.pseudo_u(u, u, uu, ua_d, nut, ff, case.dt)
+    assert rel_l2(interior(host(ua_d), case.grid, 3), interior(ua, case.grid, 3)) < TOL
+
+
+def test_pseudo_u_rejects_alias(lib_built):
+    case = CASES["cavity"]()
+    ctx = make_ctx(case)
+    u = ctx.field(3)
+    with pytest.raises(Exception):
+        ctx.pseudo_u(u, u, ctx.field(3), u, ctx.field(1), ctx.field(3), case.dt)
+
+
+def test_utouu_rhs_project_sgs_div(oracle, lib_built, case):
+    cs, m = _setup(oracle, case)
+    g = case.grid
+    st = random_state(case, seed=11)
+    c = ctypes.byref(cs.c)
+    ctx = make_ctx(case)
+    # UtoUU
+    uu_o = st["uu"].copy()
+    oracle.L.oracle_utouu(c, _p(st["u"]), _p(uu_o), _p(m["kx"]), _p(m["ja"]))
+    u_d, uu_d = dev(ctx, st["u"]), dev(ctx, st["uu"])
+    ctx.utouu(u_d, uu_d)
+    assert rel_l2(faces(host(uu_d), g), faces(uu_o, g)) < TOL
+    # RHS (divergence scaled by 1/(dt maxdiag))
+    rhs_o = np.zeros(g.n)
+    oracle.L.oracle_poisson_rhs(c, _p(uu_o), _p(rhs_o), _p(m["ja"]), m["maxdiag"])
+    rhs_d = ctx.field(1)
+    assert ctx.maxdiag == pytest.approx(m["maxdiag"], rel=1e-14)
+    ctx.poisson_rhs(uu_d, rhs_d, case.dt, ctx.maxdiag)
+    assert rel_l2(interior(host(rhs_d), g), interior(rhs_o, g)) < TOL
+    # projection (in place, the drivers' call)
+    u_o, uu2_o = st["u"].copy(), st["uu"].copy()
+    oracle.L.oracle_project_p(c, _p(u_o), _p(u_o), _p(uu2_o), _p(uu2_o), _p(st["p"]), _p(m["kx"]), _p(m["g"]))
+    u_d, uu_d, p_d = dev(ctx, st["u"]), dev(ctx, st["uu"]), dev(ctx, st["p"])
+    ctx.project_p(u_d, u_d, uu_d, uu_d, p_d, case.dt)
+    assert rel_l2(interior(host(u_d), g, 3), interior(u_o, g, 3)) < TOL
+    assert rel_l2(faces(host(uu_d), g), faces(uu2_o, g)) < TOL
+    # SGS
+    for sgs in ("Smagorinsky", "CSM"):
+        case.sgs = sgs
+        cs2, _ = _setup(oracle, case)
+        nut_o = np.zeros(g.n)
+        oracle.L.oracle_sgs(ctypes.byref(cs2.c), _p(st["u"]), _p(nut_o), _p(m["kx"]), _p(m["ja"]))
+        ctx.cfd_init(case.Re, case.adv, sgs, case.Cs)
+        nut_d = ctx.field(1)
+        ctx.sgs(dev(ctx, st["u"]), nut_d)
+        got = interior(host(nut_d), g)
+        want = interior(nut_o, g)
+        if sgs == "CSM":   # sqrt of a negative cube is NaN in both
+            assert np.array_equal(np.isnan(got), np.isnan(want))
+            got, want = np.nan_to_num(got), np.nan_to_num(want)
+        assert rel_l2(got, want) < TOL
+    # divergence
+    div_o = np.zeros(g.n)
+    oracle.L.oracle_divergence(c, _p(st["uu"]), _p(div_o), _p(m["ja"]))
+    div_d = ctx.field(1)
+    ctx.divergence(dev(ctx, st["uu"]), div_d)
+    assert rel_l2(interior(host(div_d), g), interior(div_o, g)) < TOL
+
+
+def test_operator_mv_dot_res_sor(oracle, lib_built, case):
+    cs, m = _setup(oracle, case)
+    g = case.grid
+    c = ctypes.byref(cs.c)
+    rng = np.random.default_rng(5)
+    x, b = rng.standard_normal(g.n), rng.standard_normal(g.n)
+    ctx = make_ctx(case)
+    xd, bd = dev(ctx, x), dev(ctx, b)
+    ax_o, ax_d = np.zeros(g.n), ctx.field(1)
+    oracle.L.oracle_mv(c, _p(m["A"]), _p(x), _p(ax_o))
+    ctx.mv(xd, ax_d)
+    assert rel_l2(interior(host(ax_d), g), interior(ax_o, g)) < TOL
+    r_o, r_d = np.zeros(g.n), ctx.field(1)
+    oracle.L.oracle_res(c, _p(m["A"]), _p(x), _p(b), _p(r_o))
+    ctx.res(xd, bd, r_d)
+    assert rel_l2(interior(host(r_d), g), interior(r_o, g)) < TOL
+    assert ctx.dot(xd, bd) == pytest.approx(oracle.L.oracle_dot(c, _p(x), _p(b)), rel=1e-13)
+    assert ctx.normsq(xd) == pytest.approx(oracle.L.oracle_normsq(c, _p(x), 1), rel=1e-13)
+    for color in (0, 1):
+        xo = x.copy()
+        oracle.L.oracle_sor_sweep(c, _p(m["A"]), _p(xo), _p(b), 1.2, color)
+        xs = dev(ctx, x)
+        ctx.sor_sweep(xs, bd, 1.2, color)
+        assert rel_l2(interior(host(xs), g), interior(xo, g)) < TOL
+    # the same operator given as an explicit 7-column matrix
+    ctx.set_matrix(dev(ctx, m["A"]))
+    ax2 = ctx.field(1)
+    ctx.mv(xd, ax2)
+    assert rel_l2(interior(host(ax2), g), interior(ax_o, g)) < TOL
+    assert ctx.maxdiag_of() == pytest.approx(1.0, rel=1e-14)
+
+
+@pytest.mark.parametrize("pc", ["SOR", "Jacobi"])
+def test_pbicgstab_fixed_iterations(oracle, lib_built, pc):
+    """FalmEq::PBiCGStab in fixed-iteration mode (tol 0, maxit k): same iterate."""
+    case = CASES["channel"]()
+    case.pc, case.tol, case.maxit = pc, 0.0, 7
+    cs, m = _setup(oracle, case)
+    g = case.grid
+    rng = np.random.default_rng(9)
+    b = np.zeros(g.n)
+    interior(b, g)[...] = rng.standard_normal(interior(b, g).shape)
+    x0 = 0.1 * rng.standard_normal(g.n)
+    xo, ro = x0.copy(), np.zeros(g.n)
+    it_o, err_o = oracle.pbicgstab(cs, m["A"], xo, b, ro)
+    ctx = make_ctx(case)
+    xd, bd, rd = dev(ctx, x0), dev(ctx, b), ctx.field(1)
+    it, err, rc = ctx.solve(xd, bd, rd)
+    assert it == it_o == 7
+    assert err == pytest.approx(err_o, rel=1e-9)
+    assert rel_l2(interior(host(xd), g), interior(xo, g)) < 1e-11
+
+
+def test_pbicgstab_converged(oracle, lib_built):
+    case = CASES["cavity"]()
+    case.tol = 1e-10
+    cs, m = _setup(oracle, case)
+    g = case.grid
+    rng = np.random.default_rng(2)
+    b = np.zeros(g.n)
+    bi = rng.standard_normal(interior(b, g).shape)
+    interior(b, g)[...] = bi - bi.mean()     # compatible with the all-Neumann operator
+    xo, ro = np.zeros(g.n), np.zeros(g.n)
+    it_o, err_o = oracle.pbicgstab(cs, m["A"], xo, b, ro)
+    ctx = make_ctx(case)
+    xd, rd = ctx.field(1), ctx.field(1)
+    it, err, rc = ctx.solve(xd, dev(ctx, b), rd)
+    assert abs(it - it_o) <= 1
+    assert err <= case.tol
+    assert rel_l2(interior(host(xd), g), interior(xo, g)) < 1e-7
+
+
+def test_heat1d_explicit_matrix(lib_built):
+    """test/heat1d2.cpp:217 on the GPU through falm_eq_set_matrix"""
+    from tests.test_oracle_kat import _box_case, heat1d_system
+    shape, A, b, exact = heat1d_system()
+    case = _box_case(shape, 2, h=0.01)
+    case.maxit, case.tol, case.pc, case.pc_maxit, case.pc_relax = 1000, 1e-9, "SOR", 5, 1.5
+    from falm_b200.api import Context
+    ctx = Context(case.grid, "fp64")
+    ctx.eq_init(case.maxit, case.tol, "SOR", 5, 1.5)
+    ctx.set_matrix(dev(ctx, A))
+    xd, rd = ctx.field(1), ctx.field(1)
+    it, err, rc = ctx.solve(xd, dev(ctx, b), rd)
+    assert err <= 1e-9
+    assert rel_l2(host(xd), exact) < 1e-7
+
+
+def test_dot_kat_and_maxdiag(lib_built):
+    """test/dot.py:15-30 on the GPU: exact integer interior sums; MaxDiag of the fields"""
+    from tests.test_oracle_kat import _box_case
+    case = _box_case((12, 12, 12), 1)
+    case.grid.gc = 1
+    k, j, i = np.meshgrid(np.arange(12), np.arange(12), np.arange(12), indexing="ij")
+    a = (300 - (i - 7) ** 2 - (j - 2) ** 2 - (k - 5) ** 2).astype(np.float64).ravel()
+    b = (150 - i ** 2 - (j - 1) ** 2 - (k - 1) ** 2).astype(np.float64).ravel()
+    inside = ((i > 0) & (i < 11) & (j > 0) & (j < 11) & (k > 0) & (k < 11)).ravel()
+    from falm_b200.api import Context
+    # gc = 1 is below the library's minimum of 2: embed the 12^3 box in a 14^3 one
+    big = _box_case((14, 14, 14), 2)
+    ctx = Context(big.grid, "fp64")
+    A = np.zeros((14, 14, 14)); A[1:13, 1:13, 1:13] = a.reshape(12, 12, 12)
+    B = np.zeros((14, 14, 14)); B[1:13, 1:13, 1:13] = b.reshape(12, 12, 12)
+    assert ctx.dot(dev(ctx, A.ravel()), dev(ctx, B.ravel())) == float(np.sum((a * b)[inside]))
+    assert ctx.normsq(dev(ctx, A.ravel())) == float(np.sum((a * a)[inside]))
+    M = np.zeros(7 * 14 ** 3); M[:14 ** 3] = A.ravel()
+    ctx.set_matrix(dev(ctx, M))
+    assert ctx.maxdiag_of() == float(np.abs(a[inside]).max())
+
+
+def test_boundary_conditions(oracle, lib_built, case):
+    cs, m = _setup(oracle, case)
+    g = case.grid
+    c = ctypes.byref(cs.c)
+    st = random_state(case, seed=4)
+    uprev = st["u"] + 0.01
+    t = 0.37
+    ctx = make_ctx(case)
+    u_o = st["u"].copy()
+    oracle.L.oracle_ubc(c, _p(u_o), _p(uprev), t)
+    u_d = dev(ctx, st["u"])
+    ctx.ubc(u_d, dev(ctx, uprev), case.dt, t)
+    # every guide cell the reference writes (faces, not edges/corners) must match exactly
+    np.testing.assert_allclose(host(u_d), u_o, rtol=1e-13, atol=1e-15)
+    p_o = st["p"].copy()
+    oracle.L.oracle_pbc(c, _p(p_o))
+    p_d = dev(ctx, st["p"])
+    ctx.pbc(p_d)
+    np.testing.assert_array_equal(host(p_d), p_o)
+    uu_o = st["uu"].copy()
+    oracle.L.oracle_uubc(c, _p(uu_o))
+    uu_d = dev(ctx, st["uu"])
+    ctx.uubc(uu_d)
+    np.testing.assert_array_equal(host(uu_d), uu_o)
+
+
+def test_alm_forces_and_projection(oracle, lib_built):
+    case = cases.small_channel(40, 28, 28, intensity=0.05)
+    cs, m = _setup(oracle, case)
+    g = case.grid
+    st = random_state(case, seed=21, amp=0.05)
+    for t in (0.0, 0.123, 1.7):
+        ff_o = np.zeros(3 * g.n)
+        out = oracle.alm(cs, st["u"], ff_o, t)
+        ctx = make_ctx(case)
+        ff_d = ctx.field(3)
+        tq, th = ctx.alm_run(dev(ctx, st["u"]), ff_d, t)
+        xyz, f, tqa, tha = ctx.alm_aps(case.alm.apcount)
+        np.testing.assert_allclose(xyz, out["xyz"], rtol=1e-14, atol=1e-14)
+        np.testing.assert_allclose(f, out["force"], rtol=1e-11, atol=1e-14)
+        np.testing.assert_allclose(tq, out["torque"], rtol=1e-12)
+        np.testing.assert_allclose(th, out["thrust"], rtol=1e-12)
+        # projection truncated at 6 eps: relative L2 far below the FP64 budget
+        assert rel_l2(interior(host(ff_d), g, 3), interior(ff_o, g, 3)) < 1e-13
+
+
+def test_alm_pitch_motion(oracle, lib_built):
+    """platform pitch motion (src/alm/almDevCall.cu:43-61, src/falmath.h:412-460)"""
+    case = cases.small_channel(40, 28, 28, intensity=0.0)
+    a = case.alm
+    a.motion = np.array([[np.radians(3.0), 2 * np.pi / 10.0, 0.3]])
+    a.angle_type = np.array([2], dtype=np.int32)
+    a.hub = np.array([[0.0, 0.0, 0.5]])
+    a.base = a.base - np.array([[0.0, 0.0, 0.5]])
+    a.pitch = 2.0
+    cs, m = _setup(oracle, case)
+    st = random_state(case, seed=22, amp=0.05)
+    ff_o = np.zeros(3 * case.grid.n)
+    out = oracle.alm(cs, st["u"], ff_o, 2.5)
+    ctx = make_ctx(case)
+    tq, th = ctx.alm_run(dev(ctx, st["u"]), None, 2.5)
+    np.testing.assert_allclose(tq, out["torque"], rtol=1e-12)
+    np.testing.assert_allclose(th, out["thrust"], rtol=1e-12)

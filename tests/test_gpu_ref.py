@@ -1,0 +1,145 @@
+"""Parity with the reference's OWN CUDA implementation (oracle/_ref/libfalmref.so,
+compiled from the reference's sources by oracle/Makefile) on identical inputs:
+
+  * pins the CPU oracle operator by operator and over whole steps, and
+  * checks the B200 FP64 path against the reference's step: relative L2 <= 1e-10
+    after 10 steps (the difference comes from reduction order and contraction).
+
+Skipped when the prebuilt reference library is absent."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from falm_b200 import cases
+from tests.helpers import faces, interior, random_state, rel_l2
+from tests.test_gpu_step import compare, run_gpu, run_oracle
+
+pytestmark = pytest.mark.gpu
+
+REF_SO = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "libfalmref.so")
+needs_ref = pytest.mark.skipif(not os.path.exists(REF_SO), reason="oracle/_ref not built (needs the reference sources)")
+
+
+def ref_for(case, **kw):
+    from oracle.oracle import CaseStruct, RefStep
+    cs = CaseStruct(case, use_inflow=False, **kw)
+    return RefStep(cs, tempfile.mkdtemp(prefix="falmref_")), cs
+
+
+def ref_run(case, steps, **kw):
+    ref, cs = ref_for(case, **kw)
+    st = cases.initial_state(case)
+    ref.set("U", st["u"])
+    ref.op("UTOUU")
+    ref.op("SGS")
+    stats = [ref.step((it + 1) * case.dt) for it in range(steps)]
+    out = {k: ref.get(n) for k, n in (("u", "U"), ("uu", "UU"), ("p", "P"), ("nut", "NUT"))}
+    ref.close()
+    return out, stats
+
+
+def uniform_inflow_cases():
+    ch = cases.small_channel(32, 20, 20, intensity=0.0)     # the reference has uniform inflow only
+    cav = cases.cavity(16)
+    cav.tol = 1e-10
+    return {"channel": ch, "cavity": cav}
+
+
+@needs_ref
+def test_oracle_ops_match_reference(oracle):
+    import ctypes
+    from oracle.oracle import CaseStruct, _p
+    case = cases.small_channel(24, 16, 16, intensity=0.0)
+    ref, cs = ref_for(case)
+    m = oracle.setup(cs)
+    g = case.grid
+    assert ref.maxdiag() == pytest.approx(m["maxdiag"], rel=1e-15)
+    np.testing.assert_allclose(interior(ref.get("A"), g, 7), interior(m["A"], g, 7), rtol=1e-15, atol=1e-16)
+    st = random_state(case, seed=3)
+    c = ctypes.byref(cs.c)
+    # pseudo-velocity
+    for k in ("U", "UU", "NUT", "FF"):
+        ref.set(k, st[k.lower()])
+    ref.op("PSEUDO_U")
+    ua = np.zeros(3 * g.n)
+    oracle.L.oracle_pseudo_u(c, _p(st["u"]), _p(st["u"]), _p(st["uu"]), _p(ua), _p(st["nut"]), _p(m["kx"]), _p(m["g"]),
+                             _p(m["ja"]), _p(st["ff"]))
+    assert rel_l2(interior(ref.get("U"), g, 3), interior(ua, g, 3)) < 1e-13
+    # UtoUU
+    ref.set("U", st["u"])
+    ref.op("UTOUU")
+    uu = st["uu"].copy()
+    oracle.L.oracle_utouu(c, _p(st["u"]), _p(uu), _p(m["kx"]), _p(m["ja"]))
+    assert rel_l2(faces(ref.get("UU"), g), faces(uu, g)) < 1e-14
+    # RHS
+    ref.op("RHS")
+    rhs = np.zeros(g.n)
+    oracle.L.oracle_poisson_rhs(c, _p(uu), _p(rhs), _p(m["ja"]), m["maxdiag"])
+    assert rel_l2(interior(ref.get("RHS"), g), interior(rhs, g)) < 1e-13
+    # projection, pbc, ubc, SGS
+    for k in ("U", "UU", "P"):
+        ref.set(k, st[k.lower()])
+    ref.op("PBC")
+    p = st["p"].copy()
+    oracle.L.oracle_pbc(c, _p(p))
+    np.testing.assert_array_equal(ref.get("P"), p)
+    ref.op("PROJECT")
+    u, uu = st["u"].copy(), st["uu"].copy()
+    oracle.L.oracle_project_p(c, _p(u), _p(u), _p(uu), _p(uu), _p(p), _p(m["kx"]), _p(m["g"]))
+    assert rel_l2(interior(ref.get("U"), g, 3), interior(u, g, 3)) < 1e-14
+    assert rel_l2(faces(ref.get("UU"), g), faces(uu, g)) < 1e-14
+    uprev = st["u"] + 0.01
+    ref.set("UPREV", uprev)
+    ref.set("U", st["u"])
+    ref.op("UBC", t=0.3)
+    u = st["u"].copy()
+    oracle.L.oracle_ubc(c, _p(u), _p(uprev), 0.3)
+    np.testing.assert_allclose(ref.get("U"), u, rtol=1e-14, atol=1e-16)
+    ref.op("SGS")
+    nut = np.zeros(g.n)
+    oracle.L.oracle_sgs(c, _p(u), _p(nut), _p(m["kx"]), _p(m["ja"]))
+    assert rel_l2(interior(ref.get("NUT"), g), interior(nut, g)) < 1e-13
+    # ALM (dense Gaussian sum in both)
+    ref.set("U", st["u"])
+    s = ref.op("ALM", t=0.41)
+    ff = np.zeros(3 * g.n)
+    out = oracle.alm(cs, st["u"], ff, 0.41)
+    assert s.torque[0] == pytest.approx(out["torque"][0], rel=1e-12)
+    assert s.thrust[0] == pytest.approx(out["thrust"][0], rel=1e-12)
+    assert rel_l2(interior(ref.get("FF"), g, 3), interior(ff, g, 3)) < 1e-12
+    ref.close()
+
+
+@needs_ref
+@pytest.mark.parametrize("name", ["channel", "cavity"])
+def test_oracle_step_matches_reference(oracle, name):
+    case = uniform_inflow_cases()[name]
+    ref, rs = ref_run(case, 10, maxit=6, tol=0.0)
+    got, gs = run_oracle(oracle, case, 10, maxit=6, tol=0.0)
+    err = compare(case, got, ref)
+    for k, v in err.items():
+        assert v < 1e-10, (k, v, err)
+
+
+@needs_ref
+@pytest.mark.parametrize("name", ["channel", "cavity"])
+def test_b200_step_matches_reference(lib_built, name):
+    """north-star parity: FP64 B200 step vs the reference's own step, 10 steps"""
+    case = uniform_inflow_cases()[name]
+    ref, rs = ref_run(case, 10)
+    got, gs, _ = run_gpu(case, 10)
+    for a, b in zip(gs, rs):
+        assert abs(a["it"] - b["it"]) <= 1
+        for x, y in zip(a["torque"] + a["thrust"], b["torque"] + b["thrust"]):
+            assert x == pytest.approx(y, rel=1e-10)
+    err = compare(case, got, ref)
+    for k, v in err.items():
+        assert v < 1e-10, (k, v, err)
+    # fixed-iteration mode removes the stopping-rule sensitivity entirely
+    ref, rs = ref_run(case, 10, maxit=6, tol=0.0)
+    got, gs, _ = run_gpu(case, 10, maxit=6, tol=0.0)
+    err = compare(case, got, ref)
+    for k, v in err.items():
+        assert v < 1e-10, (k, v, err)
