@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(256) k_alm_force(Geom g, AlmDev a, const doubl
 // DistributeAPForce (src/alm/almDevCall.cu:255-294) as a stored field, truncated at rcut
 template <typename T>
 __global__ void __launch_bounds__(kRowThreads) k_alm_project(Geom g, Region3 R, MetricView<T> mv, AlmDev a, T *__restrict__ ff) {
-    __shared__ double s_ap[6 * 384];
+    __shared__ double s_ap[6 * kMaxFusedAp];
     const int na = a.apcount;
     for (int q = threadIdx.x; q < na; q += blockDim.x) {
         for (int d = 0; d < 3; d++) { s_ap[6 * q + d] = a.ap_xyz[3 * q + d]; s_ap[6 * q + 3 + d] = a.ap_force[3 * q + d]; }

@@ -34,7 +34,6 @@ __device__ __forceinline__ void axis_quick(T &adv, T ucc, T up1, T up2, T um1, T
 }
 
 // ---------------------------------------------------------------- ALM force inside the stencil
-constexpr int kMaxFusedAp = 384;
 
 struct AlmFuse {
     int apcount;             // 0: no fused force

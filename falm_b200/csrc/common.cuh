@@ -77,16 +77,18 @@ __device__ bool grid_sum(double (&v)[NV], const RedWork &rw, double (&out)[NV]) 
 #pragma unroll
         for (int d = 0; d < NV; d++) sm[d][warp] = v[d];
     __syncthreads();
+    const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    const unsigned nblk = gridDim.x * gridDim.y * gridDim.z;
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int d = 0; d < NV; d++) {
             double s = 0.0;
             for (int w = 0; w < kWarpsPerBlock; w++) s += sm[d][w];
-            rw.partials[d * rw.maxBlocks + blockIdx.x] = s;
+            rw.partials[d * rw.maxBlocks + bid] = s;
         }
         __threadfence();
         unsigned ticket = atomicAdd(rw.counter, 1u);
-        last = (ticket == gridDim.x - 1);
+        last = (ticket == nblk - 1);
     }
     __syncthreads();
     if (!last) return false;
@@ -95,7 +97,7 @@ __device__ bool grid_sum(double (&v)[NV], const RedWork &rw, double (&out)[NV]) 
 #pragma unroll
     for (int d = 0; d < NV; d++) {
         acc[d] = 0.0;
-        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) acc[d] += __ldcg(rw.partials + d * rw.maxBlocks + b);
+        for (int b = threadIdx.x; b < (int)nblk; b += blockDim.x) acc[d] += __ldcg(rw.partials + d * rw.maxBlocks + b);
     }
     warp_sum<NV>(acc);
     __syncthreads();

@@ -11,11 +11,16 @@
 #include <cstdio>
 #include <cmath>
 #include <algorithm>
+#include <cstdlib>
 #include "falm_internal.cuh"
 #include "common.cuh"
 #include "cfd.cuh"
 #include "poisson.cuh"
 #include "alm_bc.cuh"
+#include "stencil_tma.cuh"
+#include "poisson_tma.cuh"
+#include "plane3_tma.cuh"
+#include <cudaTypedefs.h>
 
 using namespace fb;
 
@@ -69,9 +74,18 @@ int launch_k(falm_ctx *ctx, int cls, cudaStream_t st, F &&f) {
     f();
     ctx->launches++;
     cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && ctx->check_sync) e = cudaStreamSynchronize(st);   // FALM_B200_CHECK=1: locate faults
     if (e != cudaSuccess) {
-        *ctx->last_error = std::string("launch: ") + cudaGetErrorString(e);
+        *ctx->last_error = std::string("launch of kernel class ") + std::to_string(cls) + ": " + cudaGetErrorString(e);
         return FALM_ERR_CUDA;
+    }
+    if (ctx->check_sync) {   // and the device error word of the kernels' self-checks
+        int w = 0;
+        if (cudaMemcpy(&w, ctx->kerr, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess && w) {
+            cudaMemset(ctx->kerr, 0, sizeof(int));
+            *ctx->last_error = std::string("kernel class ") + std::to_string(cls) + ": device error word " + std::to_string(w);
+            return w >= 200 ? FALM_ERR_ARG : FALM_ERR_TIMEOUT;
+        }
     }
     if (ctx->profiling) {
         cudaEvent_t b = ev_get(ctx);
@@ -90,7 +104,7 @@ int launch_k(falm_ctx *ctx, int cls, cudaStream_t st, F &&f) {
 int row_grid(const falm_ctx *ctx, const Region3 &R) {
     long long rows = R.nrows();
     long long need = (rows + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    long long cap = ctx->red.maxBlocks;
+    long long cap = (long long)ctx->sm_count * 8;
     return (int)std::max(1LL, std::min(need, cap));
 }
 
@@ -121,6 +135,105 @@ int ensure_work(falm_ctx *ctx) {
     ctx->work_mem = mem;
     return FALM_OK;
 }
+
+// ---------------------------------------------------------------- TMA tensor maps
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+bool tma_encode_available() {
+    static int state = -1;
+    if (state < 0) {
+        cudaDriverEntryPointQueryResult q;
+        void *fn = nullptr;
+        state = (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+                 q == cudaDriverEntryPointSuccess && fn)
+                    ? 1 : 0;
+        cudaGetLastError();
+        g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    return state == 1;
+}
+
+// 4D map (x, y, z, component) of a field in the reference layout with a
+// (bx, by, 1, ncomp) box.  TMA needs a 16 B aligned base and row pitch; the
+// caller falls back to the row kernels otherwise.
+bool make_map(const falm_ctx *ctx, CUtensorMap *m, const void *base, int ncomp, int bx, int by) {
+    const Geom &g = ctx->geo;
+    const size_t e = ctx->esize;
+    // every box lies inside the tensor: x and y at least one box long (the
+    // kernels clamp the box origins), x rows a whole number of 16-byte units
+    if (!tma_encode_available() || ((uintptr_t)base & 15) || ((g.sx * e) & 15) || g.sx < bx || g.sy < by) return false;
+    cuuint64_t dims[4] = {(cuuint64_t)g.sx, (cuuint64_t)g.sy, (cuuint64_t)g.sz, (cuuint64_t)ncomp};
+    cuuint64_t strides[3] = {(cuuint64_t)(g.sx * e), (cuuint64_t)(g.sx * (size_t)g.sy * e), (cuuint64_t)(g.n * e)};
+    cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, 1, (cuuint32_t)ncomp};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    CUresult r = g_encode(m, e == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void *>(base),
+                          dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+// 7-point scalar stencil over the interior through the TMA plane stream;
+// returns 1 when launched, 0 when the operand is not TMA-eligible (the caller
+// then uses its row kernel), <0 on a launch error.
+template <typename T, int NV, class Body>
+int s7_launch(falm_ctx *ctx, int cls, cudaStream_t st, const T *x, const Body &body) {
+    CUtensorMap m;
+    if (ctx->no_tma || !make_map(ctx, &m, x, 1, S7Tile<T>::BX, S7Tile<T>::BY)) return 0;
+    const Geom &g = ctx->geo;
+    const int kc = std::min(32, g.nz);
+    dim3 grid((g.nx + S7Tile<T>::TX - 1) / S7Tile<T>::TX, (g.ny + S7Tile<T>::TY - 1) / S7Tile<T>::TY, (g.nz + kc - 1) / kc);
+    if ((long long)grid.x * grid.y * grid.z > ctx->red.maxBlocks) return 0;
+    int rc = launch_k(ctx, cls, st, [&] {
+        k_s7_tma<T, NV, Body><<<grid, 256, s7_smem<T>(), st>>>(g, kc, m, body, ctx->red, ctx->kerr);
+    });
+    return rc ? -rc : 1;
+}
+
+#define S7_OR(CLS, ST, T_, NV_, X_, BODY_, ROWLAUNCH)                                     \
+    do {                                                                                   \
+        int _s7 = s7_launch<T_, NV_>(ctx, (CLS), (ST), (X_), BODY_);                       \
+        if (_s7 < 0) return -_s7;                                                          \
+        if (_s7 == 0) LAUNCH((CLS), (ST), ROWLAUNCH);                                      \
+    } while (0)
+
+// ring depth of the multi-field plane stream: keep >= 2 planes in flight and
+// at least two CTAs per SM
+template <typename T, int NF> struct P3Conf { static constexpr int NS = (sizeof(T) == 8 && NF > 1) ? 4 : 6; };
+
+// multi-field radius-1 plane stream over region R (see plane3_tma.cuh);
+// 1 launched, 0 not eligible (row-kernel fallback), <0 launch error
+template <typename T, int NF, int NV, class Body>
+int p3_launch(falm_ctx *ctx, int cls, cudaStream_t st, const Region3 &R, int org, const void *const (&ptr)[NF],
+              const int (&ncomp)[NF], const Body &body) {
+    if (ctx->no_tma) return 0;
+    using L = P3Layout<T, NF>;
+    constexpr int NS = P3Conf<T, NF>::NS;
+    MapSet<NF> maps;
+    int slot = 0;
+    for (int f = 0; f < NF; f++) {
+        if (!make_map(ctx, &maps.m[f], ptr[f], ncomp[f], L::BX, L::BY)) return 0;
+        maps.ncomp[f] = ncomp[f];
+        slot += ncomp[f] * L::FB;
+    }
+    const int smem = NS * slot + 256;
+    const int kc = std::min(32, R.k1 - R.k0);
+    dim3 grid((R.i1 - R.i0 + L::TX - 1) / L::TX, (R.j1 - R.j0 + L::TY - 1) / L::TY, (R.k1 - R.k0 + kc - 1) / kc);
+    if ((long long)grid.x * grid.y * grid.z > ctx->red.maxBlocks) return 0;
+    auto kern = k_plane3_tma<T, NF, NS, NV, Body>;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    int rc = launch_k(ctx, cls, st, [&] { kern<<<grid, 256, smem, st>>>(ctx->geo, R, org, kc, maps, body, ctx->red, ctx->kerr); });
+    return rc ? -rc : 1;
+}
+
+#define P3_OR(CLS, ST, T_, NF_, NV_, R_, ORG_, PTRS_, NCOMP_, BODY_, ROWLAUNCH)            \
+    do {                                                                                   \
+        const void *const _pp[NF_] = PTRS_;                                                \
+        const int _nc[NF_] = NCOMP_;                                                       \
+        int _p3 = p3_launch<T_, NF_, NV_>(ctx, (CLS), (ST), (R_), (ORG_), _pp, _nc, BODY_);\
+        if (_p3 < 0) return -_p3;                                                          \
+        if (_p3 == 0) LAUNCH((CLS), (ST), ROWLAUNCH);                                      \
+    } while (0)
+#define FB_ARR(...) {__VA_ARGS__}
 
 // Build the separable Poisson tables.  For a Cartesian control volume
 //   0.5*(g_d(c) + g_d(c+e_d))/ja(c)  with g_d = ja*kx_d^2
@@ -235,10 +348,10 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
     // launch the remaining sweeps of one preconditioner application z ~ A^-1 v
     auto precondition_rest = [&](T *z, const T *v) -> int {
         if (pct == FALM_LS_SOR) {
-            LAUNCH(FALM_K_SOR, st, k_sor<T><<<grid, kRowThreads, 0, st>>>(g, R, op, z, v, pcw, 1, sc));
-            for (int it = 1; it < m; it++) {
-                LAUNCH(FALM_K_SOR, st, k_sor<T><<<grid, kRowThreads, 0, st>>>(g, R, op, z, v, pcw, 0, sc));
-                LAUNCH(FALM_K_SOR, st, k_sor<T><<<grid, kRowThreads, 0, st>>>(g, R, op, z, v, pcw, 1, sc));
+            for (int hs = 1; hs < 2 * m; hs++) {      // red, then (black, red) x (m-1)
+                const int color = hs & 1;
+                S7_OR(FALM_K_SOR, st, T, 0, z, (SorBody<T>{op, z, v, pcw, color, sc}),
+                      (k_sor<T><<<grid, kRowThreads, 0, st>>>(g, R, op, z, v, pcw, color, sc)));
             }
         } else if (pct == FALM_LS_JACOBI) {
             // sweeps 2..m ping-pong between xp and z; the first sweep wrote to
@@ -254,7 +367,8 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
     auto first_target = [&](T *z) -> T * { return (pct == FALM_LS_JACOBI && ((m - 1) & 1)) ? xp : z; };
     for (outer = 0; outer < max_outer; outer++) {
         // outer > 0: true residual in FP64; stop when it meets the tolerance
-        LAUNCH(FALM_K_RES, st, k_res<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, r, rr, ctx->red, sc, outer > 0 ? 1 : 0));
+        S7_OR(FALM_K_RES, st, T, 2, x, (ResBody<T>{op, b, r, rr, sc, outer > 0 ? 1 : 0}),
+              (k_res<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, r, rr, ctx->red, sc, outer > 0 ? 1 : 0)));
         if (outer > 0) {
             CK(cudaMemcpyAsync(ctx->scal_host, sc, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
@@ -267,10 +381,12 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
         for (;;) {
             LAUNCH(FALM_K_BICG_P, st, k_bicg_p<T><<<grid, kRowThreads, 0, st>>>(g, R, op, p, q, r, first_target(pp), pct, pcw, sc));
             if ((rc = precondition_rest(pp, p))) return rc;
-            LAUNCH(FALM_K_MV_DOT1, st, k_mv_dot1<T><<<grid, kRowThreads, 0, st>>>(g, R, op, pp, q, rr, ctx->red, sc));
+            S7_OR(FALM_K_MV_DOT1, st, T, 1, pp, (MvDot1Body<T>{op, q, rr, sc}),
+                  (k_mv_dot1<T><<<grid, kRowThreads, 0, st>>>(g, R, op, pp, q, rr, ctx->red, sc)));
             LAUNCH(FALM_K_BICG_S, st, k_bicg_s<T><<<grid, kRowThreads, 0, st>>>(g, R, op, s, q, r, first_target(ss), pct, pcw, sc));
             if ((rc = precondition_rest(ss, s))) return rc;
-            LAUNCH(FALM_K_MV_DOT2, st, k_mv_dot2<T><<<grid, kRowThreads, 0, st>>>(g, R, op, ss, t, s, ctx->red, sc));
+            S7_OR(FALM_K_MV_DOT2, st, T, 2, ss, (MvDot2Body<T>{op, t, s, sc}),
+                  (k_mv_dot2<T><<<grid, kRowThreads, 0, st>>>(g, R, op, ss, t, s, ctx->red, sc)));
             LAUNCH(FALM_K_BICG_XR, st, k_bicg_xr<T><<<grid, kRowThreads, 0, st>>>(g, R, x, pp, ss, r, s, t, rr, ctx->red, sc));
             CK(cudaMemcpyAsync(ctx->scal_host, sc, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
@@ -314,12 +430,34 @@ AlmFuse alm_fuse(const falm_ctx *ctx) {
     return af;
 }
 
+template <typename T> struct PUConf;
+template <> struct PUConf<double> { static constexpr int NS = 4; };
+template <> struct PUConf<float> { static constexpr int NS = 6; };
+
 template <typename T>
 int pseudo_u_t(falm_ctx *ctx, const T *un, const T *u, const T *uu, T *ua, const T *nut, const T *ff, double dt, bool fuse, cudaStream_t st) {
     const Region3 R = interior(ctx->geo);
     AlmFuse af;
     memset(&af, 0, sizeof(af));
     if (!ff && fuse) af = alm_fuse(ctx);
+    const Geom &g = ctx->geo;
+    constexpr int NS = PUConf<T>::NS;
+    using L = PUTile<T, NS>;
+    CUtensorMap mu, muu, mnut;
+    if (!ctx->no_tma && make_map(ctx, &mu, u, 3, L::BX, L::BY) && make_map(ctx, &muu, uu, 3, L::BX, L::BY) &&
+        make_map(ctx, &mnut, nut, 1, L::BX, L::BY)) {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_pseudo_u_tma<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
+            attr = true;
+        }
+        const int kc = std::min(64, g.nz);
+        dim3 grid((g.nx + L::TX - 1) / L::TX, (g.ny + L::TY - 1) / L::TY, (g.nz + kc - 1) / kc);
+        LAUNCH(FALM_K_PSEUDO_U, st, k_pseudo_u_tma<T, NS><<<grid, 256, L::SMEM, st>>>(g, kc, mview<T>(ctx), mu, muu, mnut, un,
+                                                                                     un == u ? 1 : 0, ua, ff, af, (T)(1.0 / ctx->Re),
+                                                                                     (T)dt, ctx->adv, ctx->kerr));
+        return FALM_OK;
+    }
     LAUNCH(FALM_K_PSEUDO_U, st, k_pseudo_u<T><<<row_grid(ctx, R), kRowThreads, 0, st>>>(ctx->geo, R, mview<T>(ctx), un, u, uu, ua, nut, ff, af,
                                                             (T)(1.0 / ctx->Re), (T)dt, ctx->adv));
     return FALM_OK;
@@ -365,8 +503,14 @@ int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_
     {
         const Region3 R = facemap(g);
         T scale = (T)(1.0 / (dt * ctx->maxdiag));
-        if (chan) LAUNCH(FALM_K_UTOUU_RHS, st, k_utouu<T, true, false><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), ua, u, uu, rhs, scale));
-        else LAUNCH(FALM_K_UTOUU_RHS, st, k_utouu<T, true, true><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), ua, u, uu, rhs, scale));
+        // the guide layer of ua takes the previous velocity (the reference's aliased u)
+        LAUNCH(FALM_K_OTHER, st, k_copy_shell<T><<<ctx->sm_count * 2, 256, 0, st>>>(g, u, ua));
+        if (chan)
+            P3_OR(FALM_K_UTOUU_RHS, st, T, 1, 0, R, 1, FB_ARR(ua), FB_ARR(3), (UtoUUBody<T, true, false>{g, mview<T>(ctx), uu, rhs, scale}),
+                  (k_utouu<T, true, false><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), ua, u, uu, rhs, scale)));
+        else
+            P3_OR(FALM_K_UTOUU_RHS, st, T, 1, 0, R, 1, FB_ARR(ua), FB_ARR(3), (UtoUUBody<T, true, true>{g, mview<T>(ctx), uu, rhs, scale}),
+                  (k_utouu<T, true, true><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), ua, u, uu, rhs, scale)));
     }
     // 4. Poisson
     int it = 0, outer = 1;
@@ -380,19 +524,31 @@ int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_
     if (chan) { LAUNCH(FALM_K_OTHER, st, k_save_outlet<T><<<64, 256, 0, st>>>(g, u, (T *)ctx->w_outlet)); }
     {
         const Region3 R = facemap(g);
-        LAUNCH(FALM_K_PROJECT, st, k_project<T><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), u, ua, uu, uu, p, (T)dt));
+        P3_OR(FALM_K_PROJECT, st, T, 1, 0, R, 1, FB_ARR(p), FB_ARR(1), (ProjectBody<T>{g, mview<T>(ctx), u, ua, uu, uu, (T)dt}),
+              (k_project<T><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), u, ua, uu, uu, p, (T)dt)));
     }
     // 7. ubc
     if ((rc = ubc_t<T>(ctx, u, UPrev<T>{(const T *)ctx->w_outlet, 1}, dt, t, st))) return rc;
     // 8. SGS + divergence norm
     {
         const Region3 R = interior(g);
-        LAUNCH(FALM_K_SGS_DIV, st, k_sgs_div<T, true><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), ctx->m64, u, nut, (T)ctx->Cs, ctx->sgs, uu,
-                                                                      nullptr, ctx->red, &ctx->scal->red[3]));
+        P3_OR(FALM_K_SGS_DIV, st, T, 2, 1, R, 2, FB_ARR(u, uu), FB_ARR(3, 3),
+              (SgsDivBody<T>{g, mview<T>(ctx), ctx->m64, nut, (T)ctx->Cs, ctx->sgs, (T *)nullptr, &ctx->scal->red[3]}),
+              (k_sgs_div<T, true><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), ctx->m64, u, nut, (T)ctx->Cs, ctx->sgs, uu,
+                                                                            nullptr, ctx->red, &ctx->scal->red[3])));
     }
     CK(cudaMemcpyAsync(ctx->scal_host, ctx->scal, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
     if (ctx->alm_on) CK(cudaMemcpyAsync(ctx->alm_scal_host, ctx->alm.scal, sizeof(AlmScalars), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&ctx->scal_host->kerr, ctx->kerr, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    if (ctx->scal_host->kerr) {
+        cudaMemsetAsync(ctx->kerr, 0, sizeof(int), st);
+        std::string m = "step: device error word " + std::to_string(ctx->scal_host->kerr) +
+                        (ctx->scal_host->kerr >= 300 ? " (a staged stencil neighbourhood failed its self-check)"
+                         : ctx->scal_host->kerr >= 200 ? " (a TMA load request failed its self-check)" : " (a bounded wait gave up)");
+        *ctx->last_error = m;
+        return ctx->scal_host->kerr >= 200 ? FALM_ERR_ARG : FALM_ERR_TIMEOUT;
+    }
     if (out) {
         memset(out, 0, sizeof(*out));
         out->it = it;
@@ -428,7 +584,7 @@ long long falm_kernel_launches(const falm_ctx *ctx) { return ctx ? ctx->launches
 
 int falm_create(const falm_grid *grid, int precision, falm_ctx **out) {
     if (!grid || !out || !grid->x || !grid->y || !grid->z || !grid->hx || !grid->hy || !grid->hz) return FALM_ERR_ARG;
-    if (grid->gc < 2 || grid->sx < 2 * grid->gc + 2 || grid->sy < 2 * grid->gc + 2 || grid->sz < 2 * grid->gc + 2) return FALM_ERR_ARG;
+    if (grid->gc < 2 || grid->sx < 2 * grid->gc + 1 || grid->sy < 2 * grid->gc + 1 || grid->sz < 2 * grid->gc + 1) return FALM_ERR_ARG;
     if (precision != FALM_FP64 && precision != FALM_MIXED) return FALM_ERR_ARG;
     *out = nullptr;
     falm_ctx *ctx = new falm_ctx();
@@ -479,7 +635,7 @@ int falm_create(const falm_grid *grid, int precision, falm_ctx **out) {
         ctx->m32.x[d] = d32 + o_x[d]; ctx->m32.h[d] = d32 + o_h[d]; ctx->m32.k[d] = d32 + o_k[d];
     }
     // reduction workspace sized to the persistent grid
-    ctx->red.maxBlocks = ctx->sm_count * 8;
+    ctx->red.maxBlocks = 1 << 16;   // partial sums of up to 65536 blocks per reduction
     if (cudaMalloc(&ctx->red.partials, sizeof(double) * 4 * ctx->red.maxBlocks) != cudaSuccess ||
         cudaMalloc(&ctx->red.counter, sizeof(unsigned int) * 4) != cudaSuccess ||
         cudaMalloc(&ctx->scal, sizeof(SolverScalars)) != cudaSuccess ||
@@ -490,6 +646,13 @@ int falm_create(const falm_grid *grid, int precision, falm_ctx **out) {
         return FALM_ERR_ALLOC;
     }
     cudaMemset(ctx->red.counter, 0, sizeof(unsigned int) * 4);
+    ctx->kerr = (int *)(ctx->red.counter + 2);
+    {
+        const char *e = getenv("FALM_B200_NO_TMA");
+        ctx->no_tma = (e && e[0] == '1') ? 1 : 0;
+        const char *c = getenv("FALM_B200_CHECK");
+        ctx->check_sync = (c && c[0] == '1') ? 1 : 0;
+    }
     cudaMemset(ctx->scal, 0, sizeof(SolverScalars));
     memset(ctx->scal_host, 0, sizeof(SolverScalars));
     if (cudaDeviceSynchronize() != cudaSuccess) { cudaGetLastError(); falm_destroy(ctx); return FALM_ERR_CUDA; }
@@ -549,8 +712,10 @@ int falm_cfd_utouu(falm_ctx *ctx, const void *u, void *uu, void *stream) {
     return dispatch(ctx, [&](auto z) {
         using T = decltype(z);
         const Region3 R = facemap(ctx->geo);
-        LAUNCH(FALM_K_UTOUU_RHS, S(stream), k_utouu<T, false, false><<<row_grid(ctx, R), kRowThreads, 0, S(stream)>>>(ctx->geo, R, mview<T>(ctx), (const T *)u,
-                                                                                   (const T *)u, (T *)uu, (T *)nullptr, T(0)));
+        P3_OR(FALM_K_UTOUU_RHS, S(stream), T, 1, 0, R, 1, FB_ARR(u), FB_ARR(3),
+              (UtoUUBody<T, false, false>{ctx->geo, mview<T>(ctx), (T *)uu, (T *)nullptr, T(0)}),
+              (k_utouu<T, false, false><<<row_grid(ctx, R), kRowThreads, 0, S(stream)>>>(ctx->geo, R, mview<T>(ctx), (const T *)u,
+                                                                                      (const T *)u, (T *)uu, (T *)nullptr, T(0))));
         return (int)FALM_OK;
     });
 }
@@ -581,8 +746,10 @@ int falm_cfd_project_p(falm_ctx *ctx, void *u, const void *ua, void *uu, const v
     return dispatch(ctx, [&](auto z) {
         using T = decltype(z);
         const Region3 R = facemap(ctx->geo);
-        LAUNCH(FALM_K_PROJECT, S(stream), k_project<T><<<row_grid(ctx, R), kRowThreads, 0, S(stream)>>>(ctx->geo, R, mview<T>(ctx), (T *)u, (const T *)ua, (T *)uu,
-                                                                       (const T *)uua, (const T *)p, (T)dt));
+        P3_OR(FALM_K_PROJECT, S(stream), T, 1, 0, R, 1, FB_ARR(p), FB_ARR(1),
+              (ProjectBody<T>{ctx->geo, mview<T>(ctx), (T *)u, (const T *)ua, (T *)uu, (const T *)uua, (T)dt}),
+              (k_project<T><<<row_grid(ctx, R), kRowThreads, 0, S(stream)>>>(ctx->geo, R, mview<T>(ctx), (T *)u, (const T *)ua, (T *)uu,
+                                                                          (const T *)uua, (const T *)p, (T)dt)));
         return (int)FALM_OK;
     });
 }
@@ -592,8 +759,11 @@ int falm_cfd_sgs(falm_ctx *ctx, const void *u, void *nut, void *stream) {
     return dispatch(ctx, [&](auto z) {
         using T = decltype(z);
         const Region3 R = interior(ctx->geo);
-        LAUNCH(FALM_K_SGS_DIV, S(stream), k_sgs_div<T, false><<<row_grid(ctx, R), kRowThreads, 0, S(stream)>>>(ctx->geo, R, mview<T>(ctx), ctx->m64, (const T *)u, (T *)nut,
-                                                                              (T)ctx->Cs, ctx->sgs, (const T *)nullptr, (T *)nullptr, ctx->red, nullptr));
+        // the second field is only read for the divergence, which is off here
+        P3_OR(FALM_K_SGS_DIV, S(stream), T, 2, 1, R, 2, FB_ARR(u, u), FB_ARR(3, 3),
+              (SgsDivBody<T>{ctx->geo, mview<T>(ctx), ctx->m64, (T *)nut, (T)ctx->Cs, ctx->sgs, (T *)nullptr, (double *)nullptr}),
+              (k_sgs_div<T, false><<<row_grid(ctx, R), kRowThreads, 0, S(stream)>>>(ctx->geo, R, mview<T>(ctx), ctx->m64, (const T *)u, (T *)nut,
+                                                                                 (T)ctx->Cs, ctx->sgs, (const T *)nullptr, (T *)nullptr, ctx->red, nullptr)));
         return (int)FALM_OK;
     });
 }
@@ -639,8 +809,9 @@ int falm_eq_res(falm_ctx *ctx, const void *x, const void *b, void *r, void *stre
     return dispatch(ctx, [&](auto z) {
         using T = decltype(z);
         const Region3 R = interior(ctx->geo);
-        LAUNCH(FALM_K_RES, S(stream), k_res<T><<<row_grid(ctx, R), kRowThreads, 0, S(stream)>>>(ctx->geo, R, op7<T>(ctx), (const T *)x, (const T *)b, (T *)r,
-                                                                   (T *)nullptr, ctx->red, nullptr, 0));
+        S7_OR(FALM_K_RES, S(stream), T, 2, (const T *)x, (ResBody<T>{op7<T>(ctx), (const T *)b, (T *)r, (T *)nullptr, (SolverScalars *)nullptr, 0}),
+              (k_res<T><<<row_grid(ctx, R), kRowThreads, 0, S(stream)>>>(ctx->geo, R, op7<T>(ctx), (const T *)x, (const T *)b, (T *)r,
+                                                                       (T *)nullptr, ctx->red, nullptr, 0)));
         return (int)FALM_OK;
     });
 }
@@ -651,8 +822,9 @@ int falm_eq_sor_sweep(falm_ctx *ctx, void *x, const void *b, double omega, int c
     return dispatch(ctx, [&](auto z) {
         using T = decltype(z);
         const Region3 R = interior(ctx->geo);
-        LAUNCH(FALM_K_SOR, S(stream), k_sor<T><<<row_grid(ctx, R), kRowThreads, 0, S(stream)>>>(ctx->geo, R, op7<T>(ctx), (T *)x, (const T *)b, (T)omega, color,
-                                                                   (const SolverScalars *)nullptr));
+        S7_OR(FALM_K_SOR, S(stream), T, 0, (const T *)x, (SorBody<T>{op7<T>(ctx), (T *)x, (const T *)b, (T)omega, color, (const SolverScalars *)nullptr}),
+              (k_sor<T><<<row_grid(ctx, R), kRowThreads, 0, S(stream)>>>(ctx->geo, R, op7<T>(ctx), (T *)x, (const T *)b, (T)omega, color,
+                                                                       (const SolverScalars *)nullptr)));
         return (int)FALM_OK;
     });
 }
@@ -664,7 +836,8 @@ int falm_mv_mv(falm_ctx *ctx, const void *x, void *ax, void *stream) {
     return dispatch(ctx, [&](auto z) {
         using T = decltype(z);
         const Region3 R = interior(ctx->geo);
-        LAUNCH(FALM_K_OTHER, S(stream), k_mv<T><<<row_grid(ctx, R), kRowThreads, 0, S(stream)>>>(ctx->geo, R, op7<T>(ctx), (const T *)x, (T *)ax));
+        S7_OR(FALM_K_OTHER, S(stream), T, 0, (const T *)x, (MvBody<T>{op7<T>(ctx), (T *)ax}),
+              (k_mv<T><<<row_grid(ctx, R), kRowThreads, 0, S(stream)>>>(ctx->geo, R, op7<T>(ctx), (const T *)x, (T *)ax)));
         return (int)FALM_OK;
     });
 }
@@ -822,6 +995,8 @@ int falm_alm_init(falm_ctx *ctx, const falm_alm_desc *d) {
         !d->ap_r || !d->ap_chord || !d->ap_twist || !d->attack || !d->cl || !d->cd)
         return FALM_ERR_ARG;
     const int nt = d->n_turbine, apc = d->n_turbine * d->n_blade * d->n_ap_per_blade, na = d->n_attack;
+    // the projection kernels stage every actuator point in shared memory
+    if (apc > kMaxFusedAp) return fail(ctx, FALM_ERR_ARG, "alm_init: more than 384 actuator points");
     // one allocation: doubles then ints
     size_t nd = 3 * nt + 3 * nt + nt + 3 * nt + 3 * apc + na + 2 * (size_t)apc * na + 3 * apc + 3 * apc + apc + apc;
     size_t bytes = nd * sizeof(double) + sizeof(AlmScalars) + nt * sizeof(int) + 512;

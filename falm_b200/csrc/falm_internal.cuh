@@ -15,6 +15,7 @@
 namespace fb {
 
 constexpr int kMaxTurbines = 8;
+constexpr int kMaxFusedAp = 384;         // actuator points staged in shared memory
 constexpr int kRowThreads = 256;          // threads per block of the row kernels
 constexpr int kWarpsPerBlock = kRowThreads / 32;
 
@@ -53,7 +54,8 @@ struct SolverScalars {
     double red[4];      // scratch reduction results
     int it, maxit, done, status;
     int first;          // 1 before the first BiCGStab iteration of a solve
-    int pad[3];
+    int kerr;           // bounded device-side wait gave up (FALM_ERR_TIMEOUT)
+    int pad[2];
 };
 
 struct AlmScalars {
@@ -139,5 +141,8 @@ struct falm_ctx {
     double *inlet_plane;                    // device 3 x nz x ny
     int inlet_plane_valid;
     int sm_count;
+    int *kerr;                              // device error word of bounded waits (FALM_ERR_TIMEOUT)
+    int no_tma;                             // force the row kernels (tests, fallback)
+    int check_sync;                         // synchronise after every launch (fault location)
     std::string *last_error;
 };

@@ -1,0 +1,294 @@
+// Generic 2.5D TMA plane stream for radius-1 stencils over several fields
+// (face velocity + RHS, projection, SGS + divergence).
+//
+// Each field f (ncomp_f components) is streamed as (36 x 10 x 1 x ncomp_f)
+// boxes; a slot holds every field of one z plane and the ring keeps planes
+// k-1, k, k+1 resident while k+2.. are in flight.  Tiles are 32 x 8 columns;
+// the box starts one column/row before the tile (`org` = 1) or two columns
+// before it (`org` = 2), whichever keeps the x coordinate 16-byte aligned for
+// the tile origin the kernel uses:
+//   interior kernels: tile i0 = gc + 32 bx, box x = i0 - 2  (org 2)
+//   face-map kernels: tile i0 = gc - 1 + 32 bx, box x = i0 - 1  (org 1)
+// (both start at 32 bx for gc = 2).
+#pragma once
+#include "common.cuh"
+#include "tma.cuh"
+
+namespace fb {
+
+template <int NF>
+struct alignas(64) MapSet {
+    CUtensorMap m[NF];
+    int ncomp[NF];
+};
+
+template <typename T, int NF>
+struct P3Layout {
+    static constexpr int TX = 32, TY = 8, BX = 36, BY = 10, PE = BX * BY;
+    static constexpr int FB = (PE * (int)sizeof(T) + 127) / 128 * 128;   // one component plane
+};
+
+// view of the resident planes for the body
+template <typename T, int NF>
+struct P3View {
+    const T *pl[3];   // slot base of planes k-1, k, k+1
+    int foff[NF];     // byte offset of field f inside a slot
+    int o;            // own element offset inside a component plane
+    __device__ __forceinline__ T at(int f, int d, int dz, int dx = 0, int dy = 0) const {
+        const T *base = (const T *)((const unsigned char *)pl[dz + 1] + foff[f]);
+        return base[d * P3Layout<T, NF>::PE + o + dy * P3Layout<T, NF>::BX + dx];
+    }
+};
+
+// Body: bool skip() const; void cell(i, j, k, cc, const P3View&, acc); void finish(tot)
+template <typename T, int NF, int NS, int NV, class Body>
+__global__ void __launch_bounds__(256) k_plane3_tma(Geom g, Region3 R, int org, int kc, const __grid_constant__ MapSet<NF> maps,
+                                                  Body body, RedWork rw, int *err) {
+    using L = P3Layout<T, NF>;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+    int foff[NF], slot_bytes = 0;
+    uint32_t tx_bytes = 0;
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+        foff[f] = slot_bytes;
+        slot_bytes += maps.ncomp[f] * L::FB;
+        tx_bytes += maps.ncomp[f] * L::PE * sizeof(T);
+    }
+    uint64_t *bar = (uint64_t *)(smem + NS * slot_bytes);
+    if (body.skip()) return;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int i0 = R.i0 + blockIdx.x * L::TX, j0 = R.j0 + blockIdx.y * L::TY;
+    const int k0 = R.k0 + blockIdx.z * kc, k1 = min(k0 + kc, R.k1);
+    const int i = i0 + tx, j = j0 + ty;
+    bool active = i < R.i1 && j < R.j1;
+    const int P0 = k0 - 1, nplanes = (k1 + 1) - P0;
+    P3View<T, NF> v;
+#pragma unroll
+    for (int f = 0; f < NF; f++) v.foff[f] = foff[f];
+    const int xb = box_origin(i0 - org, L::BX, g.sx, 16 / (int)sizeof(T)), yb = box_origin(j0 - 1, L::BY, g.sy, 1);
+    const int ox = min(i, R.i1 - 1) - xb, oy = min(j, R.j1 - 1) - yb;
+    v.o = oy * L::BX + ox;
+    // self-check: the radius-1 neighbourhood of a computed cell lies inside the staged box
+    if (active && (ox < 1 || ox > L::BX - 2 || oy < 1 || oy > L::BY - 2)) { atomicExch(err, 300 + 3); active = false; }
+    double acc[NV > 0 ? NV : 1];
+#pragma unroll
+    for (int d = 0; d < (NV > 0 ? NV : 1); d++) acc[d] = 0.0;
+    auto slot = [&](int q) { return smem + (q % NS) * slot_bytes; };
+    auto issue = [&](int q) {
+        uint64_t *b = bar + (q % NS);
+        bool ok = true;
+#pragma unroll
+        for (int f = 0; f < NF; f++) ok = ok && tma_ok(slot(q) + foff[f], xb, yb, P0 + q, (int)sizeof(T), g.sx, g.sy, g.sz);
+        if (!ok) {
+            tma_reject(b, err, 3);
+            return;
+        }
+        mbar_expect_tx(b, tx_bytes);
+#pragma unroll
+        for (int f = 0; f < NF; f++) tma_load_4d(slot(q) + foff[f], &maps.m[f], xb, yb, P0 + q, 0, b);
+    };
+    auto wait_q = [&](int q) -> bool { return mbar_wait(bar + (q % NS), (q / NS) & 1, err); };
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int f = 0; f < NF; f++) prefetch_tmap(&maps.m[f]);
+        for (int s = 0; s < NS; s++) mbar_init(bar + s, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    int issued = min(NS, nplanes), waited = 0;
+    if (threadIdx.x == 0)
+        for (int q = 0; q < issued; q++) issue(q);
+    // every plane is waited for exactly once, before its first read: planes 0
+    // and 1 here, plane q+1 at iteration q
+    bool fail = !wait_q(0);
+    fail = !wait_q(1) || fail;
+    waited = 2;
+    if (__syncthreads_or(fail)) goto drain;
+    for (int q = 1; q < nplanes - 1; q++) {
+        fail = !wait_q(q + 1);
+        waited = q + 2;
+        if (__syncthreads_or(fail)) goto drain;
+        // plane q-2 is no longer needed: refill its slot
+        if (q >= 2 && q - 2 + NS < nplanes) {
+            if (threadIdx.x == 0) { fence_proxy_async(); issue(q - 2 + NS); }
+            issued = q - 2 + NS + 1;
+        }
+        v.pl[0] = (const T *)slot(q - 1);
+        v.pl[1] = (const T *)slot(q);
+        v.pl[2] = (const T *)slot(q + 1);
+        if (active) {
+            const int k = P0 + q;
+            body.cell(i, j, k, g.id(i, j, k), v, acc);
+        }
+    }
+    goto reduce;
+drain:
+    for (int q = waited; q < issued; q++) wait_q(q);
+reduce:
+    if (NV > 0) {
+        double tot[NV > 0 ? NV : 1];
+        if (grid_sum<(NV > 0 ? NV : 1)>(acc, rw, tot) && threadIdx.x == 0) body.finish(tot);
+    }
+}
+
+}  // namespace fb
+
+namespace fb {
+
+// ---------------------------------------------------------------- face velocity + RHS body
+// UtoCU + InterpolateCU (src/dev/FalmCFDDevCall.cu:303-349) on the face map,
+// [uubc, app/lid3d/bcdev.cu:251-322,] and the scaled divergence at interior
+// cells (src/FalmCFD.h:96-109).  Field 0: the velocity to interpolate (3 comps),
+// whose guide cells must hold the previous velocity.
+template <typename T, bool RHS, bool CAVITY>
+struct UtoUUBody {
+    Geom g;
+    MetricView<T> mv;
+    T *uu, *rhs;
+    T scale;
+    __device__ bool skip() const { return false; }
+    __device__ __forceinline__ T ucv(const P3View<T, 1> &v, int d, int i, int j, int k, int dx, int dy, int dz) const {
+        int idx = d == 0 ? i + dx : (d == 1 ? j + dy : k + dz);
+        return mv.ja(i + dx, j + dy, k + dz) * mv.kx(d, idx) * v.at(0, d, dz, dx, dy);
+    }
+    __device__ __forceinline__ bool zero_face(int d, int i, int j, int k) const {
+        if (!CAVITY) return false;
+        const bool jin = j >= g.gc && j < g.sy - g.gc, kin = k >= g.gc && k < g.sz - g.gc, iin = i >= g.gc && i < g.sx - g.gc;
+        if (d == 0) return (i == g.gc - 1 || i == g.sx - g.gc - 1) && jin && kin;
+        if (d == 1) return (j == g.gc - 1 || j == g.sy - g.gc - 1) && iin && kin;
+        return (k == g.gc - 1 || k == g.sz - g.gc - 1) && iin && jin;
+    }
+    // face d of cell (i+dx, j+dy, k+dz) (the face towards +d)
+    __device__ __forceinline__ T face(const P3View<T, 1> &v, int d, int i, int j, int k, int dx, int dy, int dz) const {
+        if (zero_face(d, i + dx, j + dy, k + dz)) return T(0);
+        T a = ucv(v, d, i, j, k, dx, dy, dz);
+        T b = ucv(v, d, i, j, k, dx + (d == 0), dy + (d == 1), dz + (d == 2));
+        return T(0.5) * (a + b);
+    }
+    __device__ void cell(int i, int j, int k, long long c, const P3View<T, 1> &v, double (&)[1]) const {
+        const T UE = face(v, 0, i, j, k, 0, 0, 0), VN = face(v, 1, i, j, k, 0, 0, 0), WT = face(v, 2, i, j, k, 0, 0, 0);
+        uu[c] = UE; uu[c + g.n] = VN; uu[c + 2 * g.n] = WT;
+        if (RHS && i >= g.gc && j >= g.gc && k >= g.gc) {
+            const T UW = face(v, 0, i, j, k, -1, 0, 0), VS = face(v, 1, i, j, k, 0, -1, 0), WB = face(v, 2, i, j, k, 0, 0, -1);
+            T div = (UE - UW + VN - VS + WT - WB) / mv.ja(i, j, k);
+            rhs[c] = div * scale;
+        }
+    }
+    __device__ void finish(const double (&)[1]) const {}
+};
+
+// ---------------------------------------------------------------- projection body
+// ProjectPGrid + ProjectPFace (src/dev/FalmCFDDevCall.cu:351-407) on the face
+// map; field 0: the pressure (1 comp).  u may alias ua, uu may alias uua.
+template <typename T>
+struct ProjectBody {
+    Geom g;
+    MetricView<T> mv;
+    T *u;
+    const T *ua;
+    T *uu;
+    const T *uua;
+    T dt;
+    __device__ bool skip() const { return false; }
+    __device__ void cell(int i, int j, int k, long long cc, const P3View<T, 1> &v, double (&)[1]) const {
+        const long long N = g.n;
+        const T pcc = v.at(0, 0, 0), pe = v.at(0, 0, 0, 1, 0), pn = v.at(0, 0, 0, 0, 1), pt = v.at(0, 0, 1);
+        const T dpx = T(0.5) * (mv.g(0, i, j, k) + mv.g(0, i + 1, j, k)) * (pe - pcc);
+        const T dpy = T(0.5) * (mv.g(1, i, j, k) + mv.g(1, i, j + 1, k)) * (pn - pcc);
+        const T dpz = T(0.5) * (mv.g(2, i, j, k) + mv.g(2, i, j, k + 1)) * (pt - pcc);
+        const T f0 = uua[cc], f1 = uua[cc + N], f2 = uua[cc + 2 * N];
+        const bool in = i >= g.gc && j >= g.gc && k >= g.gc;
+        T a0 = 0, a1 = 0, a2 = 0, gx = 0, gy = 0, gz = 0;
+        if (in) {
+            a0 = ua[cc]; a1 = ua[cc + N]; a2 = ua[cc + 2 * N];
+            gx = T(0.5) * mv.kx(0, i) * (pe - v.at(0, 0, 0, -1, 0));
+            gy = T(0.5) * mv.kx(1, j) * (pn - v.at(0, 0, 0, 0, -1));
+            gz = T(0.5) * mv.kx(2, k) * (pt - v.at(0, 0, -1));
+        }
+        uu[cc] = f0 - dt * dpx; uu[cc + N] = f1 - dt * dpy; uu[cc + 2 * N] = f2 - dt * dpz;
+        if (in) { u[cc] = a0 - dt * gx; u[cc + N] = a1 - dt * gy; u[cc + 2 * N] = a2 - dt * gz; }
+    }
+    __device__ void finish(const double (&)[1]) const {}
+};
+
+// ---------------------------------------------------------------- SGS + divergence body
+// Smagorinsky / CSM (src/dev/FalmCFDDevCall.cu:409-555) and the FP64
+// divergence norm (:557-581 + app/nedo/main.cpp:194-197).  Fields: 0 u (3), 1 uu (3).
+template <typename T>
+struct SgsDivBody {
+    Geom g;
+    MetricView<T> mv;
+    Metric<double> m64;
+    T *nut;
+    T Cs;
+    int sgs;
+    T *div_out;
+    double *divsum;
+    __device__ bool skip() const { return false; }
+    __device__ void cell(int i, int j, int k, long long cc, const P3View<T, 2> &v, double (&acc)[1]) const {
+        if (sgs != FALM_SGS_EMPTY) {
+            const T kxx = mv.kx(0, i), kxy = mv.kx(1, j), kxz = mv.kx(2, k);
+            T dd[3][3];
+#pragma unroll
+            for (int m = 0; m < 3; m++) {
+                dd[m][0] = T(0.5) * kxx * (v.at(0, m, 0, 1, 0) - v.at(0, m, 0, -1, 0));
+                dd[m][1] = T(0.5) * kxy * (v.at(0, m, 0, 0, 1) - v.at(0, m, 0, 0, -1));
+                dd[m][2] = T(0.5) * kxz * (v.at(0, m, 1) - v.at(0, m, -1));
+            }
+            const T dux = dd[0][0], duy = dd[0][1], duz = dd[0][2];
+            const T dvx = dd[1][0], dvy = dd[1][1], dvz = dd[1][2];
+            const T dwx = dd[2][0], dwy = dd[2][1], dwz = dd[2][2];
+            T d1 = T(2) * (dux * dux), d2 = T(2) * (dvy * dvy), d3 = T(2) * (dwz * dwz);
+            T d4 = (duy + dvx) * (duy + dvx), d5 = (dvz + dwy) * (dvz + dwy), d6 = (duz + dwx) * (duz + dwx);
+            T Du = sqrt(d1 + d2 + d3 + d4 + d5 + d6);
+            T De = cbrt(mv.ja(i, j, k));
+            if (sgs == FALM_SGS_SMAGORINSKY) {
+                T lc = Cs * De;
+                nut[cc] = (lc * lc) * Du;
+            } else {
+                T e = dux * dux + duy * duy + duz * duz;
+                e += dvx * dvx + dvy * dvy + dvz * dvz;
+                e += dwx * dwx + dwy * dwy + dwz * dwz;
+                e *= T(0.5);
+                T q = dux * dux + duy * dvx + duz * dwx;
+                q += dvx * duy + dvy * dvy + dvz * dwy;
+                q += dwx * duz + dwy * dvz + dwz * dwz;
+                q *= T(-0.5);
+                T fcs = (q + copysign(T(1e-9), q)) / (e + copysign(T(1e-9), e));
+                T CCsm = sqrt(fcs * fcs * fcs) * (T(1) - fcs) / T(22.0);
+                nut[cc] = CCsm * (De * De) * Du;
+            }
+        }
+        if (divsum) {
+            double UE = to_d(v.at(1, 0, 0)), UW = to_d(v.at(1, 0, 0, -1, 0)), VN = to_d(v.at(1, 1, 0)), VS = to_d(v.at(1, 1, 0, 0, -1));
+            double WT = to_d(v.at(1, 2, 0)), WB = to_d(v.at(1, 2, -1));
+            double ja = ldg(m64.h[0] + i) * ldg(m64.h[1] + j) * ldg(m64.h[2] + k);
+            double dv = (UE - UW + VN - VS + WT - WB) / ja;
+            if (div_out) div_out[cc] = (T)dv;
+            acc[0] += dv * dv;
+        }
+    }
+    __device__ void finish(const double (&tot)[1]) const {
+        if (divsum) *divsum = tot[0];
+    }
+};
+
+// ---------------------------------------------------------------- guide shell copy
+// copy the first guide layer (cells of [gc-1, s-gc] outside the interior) of
+// src into dst: the pseudo-velocity buffer then carries the previous
+// velocity's guide values, as the reference's aliased u does.
+template <typename T>
+__global__ void k_copy_shell(Geom g, const T *__restrict__ src, T *__restrict__ dst) {
+    const int a = g.sx - 2 * g.gc + 2, b = g.sy - 2 * g.gc + 2, c = g.sz - 2 * g.gc + 2;
+    const long long tot = (long long)a * b * c;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(q % a), j = (int)((q / a) % b), k = (int)(q / ((long long)a * b));
+        bool shell = i == 0 || i == a - 1 || j == 0 || j == b - 1 || k == 0 || k == c - 1;
+        if (!shell) continue;
+        long long id = g.id(i + g.gc - 1, j + g.gc - 1, k + g.gc - 1);
+        dst[id] = src[id]; dst[id + g.n] = src[id + g.n]; dst[id + 2 * g.n] = src[id + 2 * g.n];
+    }
+}
+
+}  // namespace fb

@@ -125,21 +125,39 @@ def test_oracle_step_matches_reference(oracle, name):
 
 @needs_ref
 @pytest.mark.parametrize("name", ["channel", "cavity"])
-def test_b200_step_matches_reference(lib_built, name):
-    """north-star parity: FP64 B200 step vs the reference's own step, 10 steps"""
+def test_b200_step_matches_reference_fixed_iterations(lib_built, name):
+    """north-star parity: FP64 B200 step vs the reference's own step, 10 steps,
+    relative L2 <= 1e-10 on every field.  Fixed-iteration mode (tol 0, maxit 6)
+    removes the stopping rule, so the only differences are rounding order."""
     case = uniform_inflow_cases()[name]
-    ref, rs = ref_run(case, 10)
-    got, gs, _ = run_gpu(case, 10)
+    ref, rs = ref_run(case, 10, maxit=6, tol=0.0)
+    got, gs, _ = run_gpu(case, 10, maxit=6, tol=0.0)
     for a, b in zip(gs, rs):
-        assert abs(a["it"] - b["it"]) <= 1
+        assert a["it"] == b["it"]
         for x, y in zip(a["torque"] + a["thrust"], b["torque"] + b["thrust"]):
             assert x == pytest.approx(y, rel=1e-10)
     err = compare(case, got, ref)
     for k, v in err.items():
         assert v < 1e-10, (k, v, err)
-    # fixed-iteration mode removes the stopping-rule sensitivity entirely
-    ref, rs = ref_run(case, 10, maxit=6, tol=0.0)
-    got, gs, _ = run_gpu(case, 10, maxit=6, tol=0.0)
-    err = compare(case, got, ref)
-    for k, v in err.items():
-        assert v < 1e-10, (k, v, err)
+
+
+@needs_ref
+@pytest.mark.parametrize("name", ["channel", "cavity"])
+def test_b200_step_matches_reference_converged(lib_built, oracle, name):
+    """Convergence mode (the drivers' tol): iteration counts within +-1.  A
+    BiCGStab iterate stopped at a residual tolerance is determined only to that
+    tolerance and Krylov iterations amplify rounding differences, so the pressure
+    is compared at 1e-6 and the velocities at 1e-9; the oracle shows the same
+    spread against the reference, which is checked here too."""
+    case = uniform_inflow_cases()[name]
+    ref, rs = ref_run(case, 10)
+    got, gs, _ = run_gpu(case, 10)
+    orc, os_ = run_oracle(oracle, case, 10)
+    for a, b in zip(gs, rs):
+        assert abs(a["it"] - b["it"]) <= 1
+        for x, y in zip(a["torque"] + a["thrust"], b["torque"] + b["thrust"]):
+            assert x == pytest.approx(y, rel=1e-8)
+    for other in (got, orc):
+        err = compare(case, other, ref)
+        assert err["u"] < 1e-9 and err["uu"] < 1e-9 and err["nut"] < 1e-9, err
+        assert err["p"] < 1e-6, err
