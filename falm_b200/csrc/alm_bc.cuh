@@ -173,6 +173,54 @@ __global__ void __launch_bounds__(kRowThreads) k_alm_project(Geom g, Region3 R, 
     }
 }
 
+// The same truncated Gaussian sum for the cells of the force boxes only; cells
+// farther than the cutoff from the AP bounding box get zero without the AP loop.
+template <typename T>
+__global__ void __launch_bounds__(256) k_alm_box(AlmDev a, const double *xc, const double *yc, const double *zc) {
+    __shared__ double s_ap[6 * kMaxFusedAp];
+    const int na = a.apcount;
+    for (int q = threadIdx.x; q < na; q += blockDim.x) {
+        for (int d = 0; d < 3; d++) { s_ap[6 * q + d] = a.ap_xyz[3 * q + d]; s_ap[6 * q + 3 + d] = a.ap_force[3 * q + d]; }
+    }
+    __syncthreads();
+    const double eps = a.euler_eps, sq = sqrt(3.14159265358979323846) * eps, eta = 1. / (sq * sq * sq);
+    const double *bb = a.scal->bbox;
+    const double b0 = bb[0], b1 = bb[1], b2 = bb[2], b3 = bb[3], b4 = bb[4], b5 = bb[5];
+    const long long tot = a.bs.total;
+    T *f = (T *)a.fbox;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+        int l0 = 0, l1 = 0, l2 = 0, e0 = 1, e1 = 1;
+        long long o = 0;
+#pragma unroll
+        for (int s = 0; s < kMaxTurbines; s++)
+            if (s < a.bs.n && q >= a.bs.off[s]) {
+                l0 = a.bs.lo[s][0]; l1 = a.bs.lo[s][1]; l2 = a.bs.lo[s][2];
+                e0 = a.bs.ext[s][0]; e1 = a.bs.ext[s][1]; o = a.bs.off[s];
+            }
+        long long r = q - o;
+        const int i = l0 + (int)(r % e0);
+        r /= e0;
+        const int j = l1 + (int)(r % e1), k = l2 + (int)(r / e1);
+        const double cxd = xc[i], cyd = yc[j], czd = zc[k];
+        T fx = 0, fy = 0, fz = 0;
+        if (box_dist2(cxd, b0, b1) + box_dist2(cyd, b2, b3) + box_dist2(czd, b4, b5) < a.rcut2) {
+            const T cx = (T)cxd, cy = (T)cyd, cz = (T)czd;
+            const T te = (T)eta, e2 = (T)eps * (T)eps;
+            for (int p = 0; p < na; p++) {
+                T dx = cx - (T)s_ap[6 * p], dy = cy - (T)s_ap[6 * p + 1], dz = cz - (T)s_ap[6 * p + 2];
+                T rr2 = dx * dx + dy * dy + dz * dz;
+                if ((double)rr2 < a.rcut2) {
+                    T ex = exp(-rr2 / e2);
+                    fx += (T)s_ap[6 * p + 3] * te * ex;
+                    fy += (T)s_ap[6 * p + 4] * te * ex;
+                    fz += (T)s_ap[6 * p + 5] * te * ex;
+                }
+            }
+        }
+        f[q] = fx; f[q + tot] = fy; f[q + 2 * tot] = fz;
+    }
+}
+
 // ---------------------------------------------------------------- boundary conditions
 // previous-velocity view for the convective outlet: full field or the
 // compact 3-plane copy [d][plane][k][j], planes i = sx-gc-2, sx-gc-1, sx-gc

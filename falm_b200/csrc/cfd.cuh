@@ -24,6 +24,16 @@ __device__ __forceinline__ T axis4(T alpha, T ucc, T up1, T up2, T um1, T um2, T
     return T(.5) * (UDL + UDR) / jac + UD4;
 }
 
+// axis4 with its three divisions folded into multiplications: c = 1/(2*24*jac),
+// Ua = |U| k_d alpha.  Same value up to rounding.
+template <typename T>
+__device__ __forceinline__ T axis4r(T ucc, T up1, T up2, T um1, T um2, T Ua, T JP, T JM, T c) {
+    const T dl = -up2 + T(27) * up1 - T(27) * ucc + um1;
+    const T dr = -up1 + T(27) * ucc - T(27) * um1 + um2;
+    const T d4 = up2 - T(4) * up1 + T(6) * ucc - T(4) * um1 + um2;
+    return (JP * dl + JM * dr) * c + Ua * d4;
+}
+
 // src/FalmCFDScheme.h:33-66, one axis, accumulated into adv in the reference's order
 template <typename T>
 __device__ __forceinline__ void axis_quick(T &adv, T ucc, T up1, T up2, T um1, T um2, T JP, T JM) {
@@ -41,6 +51,8 @@ struct AlmFuse {
     const double *force;     // 3*apcount
     const AlmScalars *scal;  // AP bounding box
     double eps, eta, rcut2;
+    BoxSet bs;               // force boxes (read by the plane-streaming kernel)
+    const void *fbox;
 };
 
 // Gaussian projection of src/alm/almDevCall.cu:255-294 truncated at rcut

@@ -101,6 +101,18 @@ int launch_k(falm_ctx *ctx, int cls, cudaStream_t st, F &&f) {
         if (_lrc) return _lrc;                                                               \
     } while (0)
 
+// z planes per CTA of a plane-streaming kernel: short enough chunks that the
+// grid fills every SM twice over with `per_sm` resident CTAs, at most `cap`
+// planes, at least 8 (each chunk re-reads its halo planes)
+int chunk_len(const falm_ctx *ctx, long long blocks_xy, int nz, int per_sm, int cap) {
+    const long long want = 2LL * ctx->sm_count * per_sm;
+    const long long chunks = std::max(1LL, (want + blocks_xy - 1) / blocks_xy);
+    int kc = (int)((nz + chunks - 1) / chunks);
+    kc = std::max(kc, 8);
+    kc = std::min(kc, cap);
+    return std::max(1, std::min(kc, nz));
+}
+
 int row_grid(const falm_ctx *ctx, const Region3 &R) {
     long long rows = R.nrows();
     long long need = (rows + kWarpsPerBlock - 1) / kWarpsPerBlock;
@@ -180,8 +192,9 @@ int s7_launch(falm_ctx *ctx, int cls, cudaStream_t st, const T *x, const Body &b
     CUtensorMap m;
     if (ctx->no_tma || !make_map(ctx, &m, x, 1, S7Tile<T>::BX, S7Tile<T>::BY)) return 0;
     const Geom &g = ctx->geo;
-    const int kc = std::min(32, g.nz);
-    dim3 grid((g.nx + S7Tile<T>::TX - 1) / S7Tile<T>::TX, (g.ny + S7Tile<T>::TY - 1) / S7Tile<T>::TY, (g.nz + kc - 1) / kc);
+    const int bx = (g.nx + S7Tile<T>::TX - 1) / S7Tile<T>::TX, by = (g.ny + S7Tile<T>::TY - 1) / S7Tile<T>::TY;
+    const int kc = chunk_len(ctx, (long long)bx * by, g.nz, 8, 32);
+    dim3 grid(bx, by, (g.nz + kc - 1) / kc);
     if ((long long)grid.x * grid.y * grid.z > ctx->red.maxBlocks) return 0;
     int rc = launch_k(ctx, cls, st, [&] {
         k_s7_tma<T, NV, Body><<<grid, 256, s7_smem<T>(), st>>>(g, kc, m, body, ctx->red, ctx->kerr);
@@ -216,8 +229,9 @@ int p3_launch(falm_ctx *ctx, int cls, cudaStream_t st, const Region3 &R, int org
         slot += ncomp[f] * L::FB;
     }
     const int smem = NS * slot + 256;
-    const int kc = std::min(32, R.k1 - R.k0);
-    dim3 grid((R.i1 - R.i0 + L::TX - 1) / L::TX, (R.j1 - R.j0 + L::TY - 1) / L::TY, (R.k1 - R.k0 + kc - 1) / kc);
+    const int bx = (R.i1 - R.i0 + L::TX - 1) / L::TX, by = (R.j1 - R.j0 + L::TY - 1) / L::TY;
+    const int kc = chunk_len(ctx, (long long)bx * by, R.k1 - R.k0, std::max(1, std::min(8, (200 * 1024) / smem)), 32);
+    dim3 grid(bx, by, (R.k1 - R.k0 + kc - 1) / kc);
     if ((long long)grid.x * grid.y * grid.z > ctx->red.maxBlocks) return 0;
     auto kern = k_plane3_tma<T, NF, NS, NV, Body>;
     if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -427,6 +441,8 @@ AlmFuse alm_fuse(const falm_ctx *ctx) {
     double sq = std::sqrt(M_PI) * af.eps;
     af.eta = 1. / (sq * sq * sq);
     af.rcut2 = ctx->alm.rcut2;
+    af.bs = ctx->alm.bs;
+    af.fbox = ctx->alm.fbox;
     return af;
 }
 
@@ -446,13 +462,10 @@ int pseudo_u_t(falm_ctx *ctx, const T *un, const T *u, const T *uu, T *ua, const
     CUtensorMap mu, muu, mnut;
     if (!ctx->no_tma && make_map(ctx, &mu, u, 3, L::BX, L::BY) && make_map(ctx, &muu, uu, 3, L::BX, L::BY) &&
         make_map(ctx, &mnut, nut, 1, L::BX, L::BY)) {
-        static bool attr = false;
-        if (!attr) {
-            cudaFuncSetAttribute(k_pseudo_u_tma<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
-            attr = true;
-        }
-        const int kc = std::min(64, g.nz);
-        dim3 grid((g.nx + L::TX - 1) / L::TX, (g.ny + L::TY - 1) / L::TY, (g.nz + kc - 1) / kc);
+        cudaFuncSetAttribute(k_pseudo_u_tma<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
+        const int bx = (g.nx + L::TX - 1) / L::TX, by = (g.ny + L::TY - 1) / L::TY;
+        const int kc = chunk_len(ctx, (long long)bx * by, g.nz, sizeof(T) == 8 ? 2 : 3, 64);
+        dim3 grid(bx, by, (g.nz + kc - 1) / kc);
         LAUNCH(FALM_K_PSEUDO_U, st, k_pseudo_u_tma<T, NS><<<grid, 256, L::SMEM, st>>>(g, kc, mview<T>(ctx), mu, muu, mnut, un,
                                                                                      un == u ? 1 : 0, ua, ff, af, (T)(1.0 / ctx->Re),
                                                                                      (T)dt, ctx->adv, ctx->kerr));
@@ -469,6 +482,10 @@ int alm_run_t(falm_ctx *ctx, const T *u, T *ff, double t, cudaStream_t st) {
     if (ff) {
         const Region3 R = interior(ctx->geo);
         LAUNCH(FALM_K_ALM, st, k_alm_project<T><<<row_grid(ctx, R), kRowThreads, 0, st>>>(ctx->geo, R, mview<T>(ctx), ctx->alm, ff));
+    } else if (ctx->alm.bs.total > 0) {
+        // force boxes for the fused projection of the plane-streaming pseudo-velocity kernel
+        const long long blocks = std::min<long long>((ctx->alm.bs.total + 255) / 256, (long long)ctx->sm_count * 8);
+        LAUNCH(FALM_K_ALM, st, k_alm_box<T><<<(int)blocks, 256, 0, st>>>(ctx->alm, ctx->m64.x[0], ctx->m64.x[1], ctx->m64.x[2]));
     }
     return FALM_OK;
 }
@@ -670,6 +687,7 @@ int falm_destroy(falm_ctx *ctx) {
     cudaFree(ctx->scal);
     cudaFree(ctx->inflow_box);
     cudaFree(ctx->alm_mem);
+    cudaFree(ctx->alm.fbox);
     if (ctx->scal_host) cudaFreeHost(ctx->scal_host);
     if (ctx->alm_scal_host) cudaFreeHost(ctx->alm_scal_host);
     delete ctx->hx; delete ctx->hy; delete ctx->hz; delete ctx->xc; delete ctx->yc; delete ctx->zc;
@@ -1025,6 +1043,43 @@ int falm_alm_init(falm_ctx *ctx, const falm_alm_desc *d) {
     int *ip = (int *)q;
     CK(cudaMemcpy(ip, d->angle_type, nt * sizeof(int), cudaMemcpyHostToDevice));
     a.angle_type = ip;
+    // force boxes: every AP of turbine t stays within |hub_t| + max r of its base
+    // (the motions rotate about the base), so a cell that an AP can reach lies
+    // within that distance + the cutoff of the base on every axis
+    {
+        BoxSet &bs = a.bs;
+        memset(&bs, 0, sizeof(bs));
+        const Geom &g = ctx->geo;
+        const std::vector<double> *cs[3] = {ctx->xc, ctx->yc, ctx->zc};
+        const int s3[3] = {g.sx, g.sy, g.sz};
+        const int nappt = d->n_blade * d->n_ap_per_blade;
+        const double rc = std::sqrt(a.rcut2);
+        long long off = 0;
+        for (int t = 0; t < nt; t++) {
+            double rmax = 0.0;
+            for (int q = t * nappt; q < (t + 1) * nappt; q++) rmax = std::max(rmax, std::fabs(d->ap_r[q]));
+            const double *hb = d->hub + 3 * t;
+            const double reach = std::sqrt(hb[0] * hb[0] + hb[1] * hb[1] + hb[2] * hb[2]) + rmax + rc;
+            long long cells = 1;
+            for (int ax = 0; ax < 3; ax++) {
+                int lo = s3[ax], hi = -1;
+                for (int q = g.gc; q < s3[ax] - g.gc; q++) {
+                    const double c = (*cs[ax])[q], b = d->base[3 * t + ax];
+                    if (c >= b - reach && c <= b + reach) { lo = std::min(lo, q); hi = std::max(hi, q); }
+                }
+                if (hi >= lo) { lo = std::max(g.gc, lo - 1); hi = std::min(s3[ax] - g.gc - 1, hi + 1); }
+                bs.lo[t][ax] = hi >= lo ? lo : g.gc;
+                bs.ext[t][ax] = hi >= lo ? hi - lo + 1 : 0;
+                cells *= bs.ext[t][ax];
+            }
+            bs.off[t] = off;
+            off += cells;
+        }
+        bs.n = nt;
+        bs.total = off;
+        if (a.fbox) { cudaFree(a.fbox); a.fbox = nullptr; }
+        if (off > 0) CK(cudaMalloc(&a.fbox, 3 * (size_t)off * ctx->esize));
+    }
     ctx->alm_on = 1;
     return FALM_OK;
 }

@@ -70,7 +70,21 @@ struct RedWork {
     int maxBlocks;
 };
 
+// Force boxes of the fused ALM projection.  Box t is the index box of the
+// interior cells within |hub_t| + max AP radius + cutoff (+1 cell) of turbine
+// t's base, so it holds every cell that an AP of turbine t can reach.  The
+// projected force of a box cell (the sum over ALL actuator points) is stored
+// there once per ALM evaluation: 3 components with stride `total`.
+struct BoxSet {
+    int n;
+    int lo[kMaxTurbines][3], ext[kMaxTurbines][3];
+    long long off[kMaxTurbines];
+    long long total;
+};
+
 struct AlmDev {
+    BoxSet bs;
+    void *fbox;            // 3 * bs.total values of the context precision
     int n_turbine, n_blade, n_ap_per_blade, n_attack, apcount;
     double radius, hub_radius, euler_eps, pitch, rcut2;
     const double *base, *hub, *tip_rate, *motion;

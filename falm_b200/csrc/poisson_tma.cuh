@@ -26,7 +26,10 @@ template <> struct S7Conf<float> { static constexpr int NS = 8; };
 template <typename T>
 constexpr int s7_smem() { return S7Conf<T>::NS * S7Tile<T>::SLOT + 128 + 128; }
 
-// Body: bool skip() const; void cell(i, j, k, cc, xc, xe, xw, xn, xs, xt, xb, acc); void finish(tot)
+// Body: bool skip() const; const T *pw() const (pointwise operand, or null);
+//       void cell(i, j, k, cc, xc, xe, xw, xn, xs, xt, xb, pv, acc); void finish(tot)
+// The pointwise operand of the next plane is loaded one iteration ahead (pv),
+// so its latency overlaps the current plane's wait and arithmetic.
 template <typename T, int NV, class Body>
 __global__ void __launch_bounds__(256) k_s7_tma(Geom g, int kc, const __grid_constant__ CUtensorMap mx, Body body,
                                               RedWork rw, int *err) {
@@ -77,12 +80,16 @@ __global__ void __launch_bounds__(256) k_s7_tma(Geom g, int kc, const __grid_con
     fail = !wait_q(1) || fail;
     waited = 2;
     T xm = slot(0)[o];
+    const T *pw = body.pw();
+    const long long sxy = (long long)g.sx * g.sy, c0 = g.id(i, j, P0 + 1);   // cell of the first computed plane
+    T pv = (pw && active) ? pw[c0] : T(0);
     if (__syncthreads_or(fail)) goto drain;
     if (NS < nplanes) {
         if (threadIdx.x == 0) { fence_proxy_async(); issue(NS); }
         issued = NS + 1;
     }
     for (int q = 1; q < nplanes - 1; q++) {
+        const T pn = (pw && active && q + 1 < nplanes - 1) ? pw[c0 + (long long)q * sxy] : T(0);
         fail = !wait_q(q + 1);
         waited = q + 2;
         if (__syncthreads_or(fail)) goto drain;
@@ -94,9 +101,10 @@ __global__ void __launch_bounds__(256) k_s7_tma(Geom g, int kc, const __grid_con
         const T xc = X0[o];
         if (active) {
             const int k = P0 + q;
-            body.cell(i, j, k, g.id(i, j, k), xc, X0[o + 1], X0[o - 1], X0[o + L::BX], X0[o - L::BX], X1[o], xm, acc);
+            body.cell(i, j, k, g.id(i, j, k), xc, X0[o + 1], X0[o - 1], X0[o + L::BX], X0[o - L::BX], X1[o], xm, pv, acc);
         }
         xm = xc;
+        pv = pn;
     }
     goto reduce;
 drain:
@@ -124,11 +132,12 @@ struct SorBody {
     int color;
     const SolverScalars *sc;
     __device__ bool skip() const { return sc && sc->done; }
-    __device__ void cell(int i, int j, int k, long long c, T xc, T xe, T xw, T xn, T xs, T xt, T xb, double (&)[1]) const {
+    __device__ const T *pw() const { return b; }
+    __device__ void cell(int i, int j, int k, long long c, T xc, T xe, T xw, T xn, T xs, T xt, T xb, T bv, double (&)[1]) const {
         if (((i + j + k) & 1) != color) return;
         T ac, aw, ae, as, an, ab, at;
         op.get(i, j, k, c, ac, aw, ae, as, an, ab, at);
-        T cc = (b[c] - dot7(ac, ae, aw, an, as, at, ab, xc, xe, xw, xn, xs, xt, xb)) / ac;
+        T cc = (bv - dot7(ac, ae, aw, an, as, at, ab, xc, xe, xw, xn, xs, xt, xb)) / ac;
         x[c] = xc + omega * cc;
     }
     __device__ void finish(const double (&)[1]) const {}
@@ -140,7 +149,8 @@ struct MvBody {
     Op7<T> op;
     T *ax;
     __device__ bool skip() const { return false; }
-    __device__ void cell(int i, int j, int k, long long c, T xc, T xe, T xw, T xn, T xs, T xt, T xb, double (&)[1]) const {
+    __device__ const T *pw() const { return nullptr; }
+    __device__ void cell(int i, int j, int k, long long c, T xc, T xe, T xw, T xn, T xs, T xt, T xb, T, double (&)[1]) const {
         T ac, aw, ae, as, an, ab, at;
         op.get(i, j, k, c, ac, aw, ae, as, an, ab, at);
         ax[c] = dot7(ac, ae, aw, an, as, at, ab, xc, xe, xw, xn, xs, xt, xb);
@@ -156,12 +166,13 @@ struct MvDot1Body {
     const T *rr;
     SolverScalars *sc;
     __device__ bool skip() const { return sc->done; }
-    __device__ void cell(int i, int j, int k, long long c, T xc, T xe, T xw, T xn, T xs, T xt, T xb, double (&acc)[1]) const {
+    __device__ const T *pw() const { return rr; }
+    __device__ void cell(int i, int j, int k, long long c, T xc, T xe, T xw, T xn, T xs, T xt, T xb, T rrv, double (&acc)[1]) const {
         T ac, aw, ae, as, an, ab, at;
         op.get(i, j, k, c, ac, aw, ae, as, an, ab, at);
         T qv = dot7(ac, ae, aw, an, as, at, ab, xc, xe, xw, xn, xs, xt, xb);
         q[c] = qv;
-        acc[0] += to_d(rr[c]) * to_d(qv);
+        acc[0] += to_d(rrv) * to_d(qv);
     }
     __device__ void finish(const double (&tot)[1]) const {
         double alpha = sc->rho / tot[0];
@@ -178,13 +189,14 @@ struct MvDot2Body {
     const T *s;
     SolverScalars *sc;
     __device__ bool skip() const { return sc->done; }
-    __device__ void cell(int i, int j, int k, long long c, T xc, T xe, T xw, T xn, T xs, T xt, T xb, double (&acc)[2]) const {
+    __device__ const T *pw() const { return s; }
+    __device__ void cell(int i, int j, int k, long long c, T xc, T xe, T xw, T xn, T xs, T xt, T xb, T sv, double (&acc)[2]) const {
         T ac, aw, ae, as, an, ab, at;
         op.get(i, j, k, c, ac, aw, ae, as, an, ab, at);
         T tv = dot7(ac, ae, aw, an, as, at, ab, xc, xe, xw, xn, xs, xt, xb);
         t[c] = tv;
         double td = to_d(tv);
-        acc[0] += td * to_d(s[c]);
+        acc[0] += td * to_d(sv);
         acc[1] += td * td;
     }
     __device__ void finish(const double (&tot)[2]) const {
@@ -203,10 +215,11 @@ struct ResBody {
     SolverScalars *sc;
     int check_tol;
     __device__ bool skip() const { return false; }
-    __device__ void cell(int i, int j, int k, long long c, T xc, T xe, T xw, T xn, T xs, T xt, T xb, double (&acc)[2]) const {
+    __device__ const T *pw() const { return b; }
+    __device__ void cell(int i, int j, int k, long long c, T xc, T xe, T xw, T xn, T xs, T xt, T xb, T bv, double (&acc)[2]) const {
         T ac, aw, ae, as, an, ab, at;
         op.get(i, j, k, c, ac, aw, ae, as, an, ab, at);
-        double rv = to_d(b[c]) - dot7<double>(ac, ae, aw, an, as, at, ab, xc, xe, xw, xn, xs, xt, xb);
+        double rv = to_d(bv) - dot7<double>(ac, ae, aw, an, as, at, ab, xc, xe, xw, xn, xs, xt, xb);
         T rt = (T)rv;
         r[c] = rt;
         if (rr) rr[c] = rt;

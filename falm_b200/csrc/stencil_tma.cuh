@@ -65,6 +65,24 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_pseudo_u_tma(Ge
             tma_reject(b, err, 1);
         }
     };
+    // column constants (x, y metric factors and the ALM distance in x/y) and the
+    // rolling z metric of planes k-1, k (k+1 is loaded per plane)
+    const int ic = min(i, g.sx - g.gc - 1), jc = min(j, g.sy - g.gc - 1);
+    const T hxc = ldg(mv.m.h[0] + ic), hyc = ldg(mv.m.h[1] + jc);
+    const T Pc = hxc * hyc, Pe = ldg(mv.m.h[0] + ic + 1) * hyc, Pw = ldg(mv.m.h[0] + ic - 1) * hyc;
+    const T Pn = hxc * ldg(mv.m.h[1] + jc + 1), Ps = hxc * ldg(mv.m.h[1] + jc - 1);
+    const T kxc = ldg(mv.m.k[0] + ic), kxe = ldg(mv.m.k[0] + ic + 1), kxw = ldg(mv.m.k[0] + ic - 1);
+    const T kyc = ldg(mv.m.k[1] + jc), kyn = ldg(mv.m.k[1] + jc + 1), kys = ldg(mv.m.k[1] + jc - 1);
+    T hzb = ldg(mv.m.h[2] + P0 + 1), hzk = ldg(mv.m.h[2] + P0 + 2), kzb = ldg(mv.m.k[2] + P0 + 1), kzk = ldg(mv.m.k[2] + P0 + 2);
+    // force boxes whose x/y extent holds this column (bit t for box t)
+    unsigned colmask = 0;
+    if (!ff && af.apcount > 0) {
+#pragma unroll
+        for (int t = 0; t < kMaxTurbines; t++)
+            if (t < af.bs.n && (unsigned)(ic - af.bs.lo[t][0]) < (unsigned)af.bs.ext[t][0] &&
+                (unsigned)(jc - af.bs.lo[t][1]) < (unsigned)af.bs.ext[t][1])
+                colmask |= 1u << t;
+    }
     int issued = 0, waited = 0;
     if (threadIdx.x == 0) {
         prefetch_tmap(&mu); prefetch_tmap(&muu); prefetch_tmap(&mnut);
@@ -116,42 +134,50 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_pseudo_u_tma(Ge
         const T *U0 = (const T *)slot(q), *UU0 = (const T *)(slot(q) + L::U_BYTES), *N0 = (const T *)(slot(q) + 2 * L::U_BYTES);
         const T *U1 = (const T *)slot(q + 1), *N1 = (const T *)(slot(q + 1) + 2 * L::U_BYTES);
         const T *U2 = (const T *)slot(q + 2);
+        const T hzt = ldg(mv.m.h[2] + k + 1), kzt = ldg(mv.m.k[2] + k + 1);
         if (active) {
             const long long cc = g.id(i, j, k);
-            const T Uabs = fabs(U0[o] * mv.kx(0, i));
-            const T Vabs = fabs(U0[L::PE + o] * mv.kx(1, j));
-            const T Wabs = fabs(U0[2 * L::PE + o] * mv.kx(2, k));
+            // metrics with the association of MetricView: ja = (hx*hy)*hz, g_d = (ja*k_d)*k_d
+            const T jacob = Pc * hzk;
+            const T gxcc = (jacob * kxc) * kxc, gxe1 = ((Pe * hzk) * kxe) * kxe, gxw1 = ((Pw * hzk) * kxw) * kxw;
+            const T gycc = (jacob * kyc) * kyc, gyn1 = ((Pn * hzk) * kyn) * kyn, gys1 = ((Ps * hzk) * kys) * kys;
+            const T gzcc = (jacob * kzk) * kzk, gzt1 = ((Pc * hzt) * kzt) * kzt, gzb1 = ((Pc * hzb) * kzb) * kzb;
+            // the scheme's divisions by the Jacobian become one reciprocal per cell
+            const T ij = T(1) / jacob;
             const T UE = UU0[o], UW = UU0[o - 1], VN = UU0[L::PE + o], VS = UU0[L::PE + o - L::BX];
             const T WT = UU0[2 * L::PE + o], WB = uu2m1;
-            const T nutcc = N0[o], nute1 = N0[o + 1], nutw1 = N0[o - 1], nutn1 = N0[o + L::BX], nuts1 = N0[o - L::BX];
-            const T nutt1 = N1[o], nutb1 = nutm1;
-            const T gxcc = mv.g(0, i, j, k), gxe1 = mv.g(0, i + 1, j, k), gxw1 = mv.g(0, i - 1, j, k);
-            const T gycc = mv.g(1, i, j, k), gyn1 = mv.g(1, i, j + 1, k), gys1 = mv.g(1, i, j - 1, k);
-            const T gzcc = mv.g(2, i, j, k), gzt1 = mv.g(2, i, j, k + 1), gzb1 = mv.g(2, i, j, k - 1);
-            const T jacob = mv.ja(i, j, k);
+            const T nutcc = N0[o];
+            // diffusion coefficients of the six faces, shared by the three components
+            // (src/FalmCFDScheme.h:167-191)
+            const T ce = (gxcc + gxe1) * (ReI + T(0.5) * (nutcc + N0[o + 1]));
+            const T cw = (gxcc + gxw1) * (ReI + T(0.5) * (nutcc + N0[o - 1]));
+            const T cn = (gycc + gyn1) * (ReI + T(0.5) * (nutcc + N0[o + L::BX]));
+            const T cs = (gycc + gys1) * (ReI + T(0.5) * (nutcc + N0[o - L::BX]));
+            const T ct = (gzcc + gzt1) * (ReI + T(0.5) * (nutcc + N1[o]));
+            const T cb = (gzcc + gzb1) * (ReI + T(0.5) * (nutcc + nutm1));
+            const T vscale = T(0.5) * ij;
             T fvec[3] = {0, 0, 0};
             if (ff) {
                 fvec[0] = ff[cc]; fvec[1] = ff[cc + N]; fvec[2] = ff[cc + 2 * N];
-            } else if (af.apcount > 0) {
-                const double *bb = af.scal->bbox;
-                double cx = (double)ldg(mv.m.x[0] + i), cy = (double)ldg(mv.m.x[1] + j), cz = (double)ldg(mv.m.x[2] + k);
-                if (box_dist2(cx, bb[0], bb[1]) + box_dist2(cy, bb[2], bb[3]) + box_dist2(cz, bb[4], bb[5]) < af.rcut2) {
-                    T ax = 0, ay = 0, az = 0;
-                    const T te = (T)af.eta, e2 = (T)af.eps * (T)af.eps;
-                    for (int a = 0; a < af.apcount; a++) {
-                        T dx = (T)cx - (T)__ldg(af.xyz + 3 * a), dy = (T)cy - (T)__ldg(af.xyz + 3 * a + 1);
-                        T dz = (T)cz - (T)__ldg(af.xyz + 3 * a + 2);
-                        T rr2 = dx * dx + dy * dy + dz * dz;
-                        if ((double)rr2 < af.rcut2) {
-                            T ex = exp(-rr2 / e2);
-                            ax += (T)__ldg(af.force + 3 * a) * te * ex;
-                            ay += (T)__ldg(af.force + 3 * a + 1) * te * ex;
-                            az += (T)__ldg(af.force + 3 * a + 2) * te * ex;
-                        }
+            } else if (colmask) {
+                // the first force box holding the cell has the full sum over all APs
+                const T *fbx = (const T *)af.fbox;
+#pragma unroll
+                for (int t = 0; t < kMaxTurbines; t++) {
+                    const int lk = k - af.bs.lo[t][2];
+                    if (((colmask >> t) & 1u) && (unsigned)lk < (unsigned)af.bs.ext[t][2]) {
+                        const long long qb = af.bs.off[t] + (i - af.bs.lo[t][0]) +
+                                             (long long)af.bs.ext[t][0] * ((j - af.bs.lo[t][1]) + (long long)af.bs.ext[t][1] * lk);
+                        fvec[0] = fbx[qb]; fvec[1] = fbx[qb + af.bs.total]; fvec[2] = fbx[qb + 2 * af.bs.total];
+                        break;
                     }
-                    fvec[0] = ax; fvec[1] = ay; fvec[2] = az;
                 }
             }
+            // advection: |U| k_d weights of the 4th-order dissipation (times alpha),
+            // and the common factor of the two 4th-order fluxes, 1/(2*24*ja)
+            const T alpha = adv == FALM_ADV_UTOPIA ? T(1. / 12.) : (adv == FALM_ADV_KK ? T(1. / 4.) : T(1. / 24.));
+            const T Ua = fabs(U0[o] * kxc) * alpha, Va = fabs(U0[L::PE + o] * kyc) * alpha, Wa = fabs(U0[2 * L::PE + o] * kzk) * alpha;
+            const T c4 = T(0.5 / 24.) * ij;
 #pragma unroll
             for (int d = 0; d < 3; d++) {
                 const T *Ud = U0 + d * L::PE;
@@ -167,7 +193,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_pseudo_u_tma(Ge
                     adv_v -= upwind_flux1(us1, ucc, VS);
                     adv_v += upwind_flux1(ucc, ut1, WT);
                     adv_v -= upwind_flux1(ub1, ucc, WB);
-                    adv_v /= jacob;
+                    adv_v *= ij;
                 } else {
                     const T ue2 = Ud[o + 2], uw2 = Ud[o - 2], un2 = Ud[o + 2 * L::BX], us2 = Ud[o - 2 * L::BX];
                     const T ut2 = U2[d * L::PE + o], ub2 = um2[d];
@@ -176,27 +202,20 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_pseudo_u_tma(Ge
                         axis_quick(adv_v, ucc, ue1, ue2, uw1, uw2, UE, UW);
                         axis_quick(adv_v, ucc, un1, un2, us1, us2, VN, VS);
                         axis_quick(adv_v, ucc, ut1, ut2, ub1, ub2, WT, WB);
-                        adv_v /= (T(16) * jacob);
+                        adv_v *= T(1. / 16.) * ij;
                     } else {
-                        const T alpha = adv == FALM_ADV_UTOPIA ? T(1. / 12.) : (adv == FALM_ADV_KK ? T(1. / 4.) : T(1. / 24.));
-                        adv_v = T(0.0);
-                        adv_v += axis4(alpha, ucc, ue1, ue2, uw1, uw2, Uabs, UE, UW, jacob);
-                        adv_v += axis4(alpha, ucc, un1, un2, us1, us2, Vabs, VN, VS, jacob);
-                        adv_v += axis4(alpha, ucc, ut1, ut2, ub1, ub2, Wabs, WT, WB, jacob);
+                        adv_v = axis4r(ucc, ue1, ue2, uw1, uw2, Ua, UE, UW, c4);
+                        adv_v += axis4r(ucc, un1, un2, us1, us2, Va, VN, VS, c4);
+                        adv_v += axis4r(ucc, ut1, ut2, ub1, ub2, Wa, WT, WB, c4);
                     }
                 }
-                T vis = T(0.0);
-                vis += (gxcc + gxe1) * (ReI + T(0.5) * (nutcc + nute1)) * (ue1 - ucc);
-                vis -= (gxcc + gxw1) * (ReI + T(0.5) * (nutcc + nutw1)) * (ucc - uw1);
-                vis += (gycc + gyn1) * (ReI + T(0.5) * (nutcc + nutn1)) * (un1 - ucc);
-                vis -= (gycc + gys1) * (ReI + T(0.5) * (nutcc + nuts1)) * (ucc - us1);
-                vis += (gzcc + gzt1) * (ReI + T(0.5) * (nutcc + nutt1)) * (ut1 - ucc);
-                vis -= (gzcc + gzb1) * (ReI + T(0.5) * (nutcc + nutb1)) * (ucc - ub1);
-                vis /= (T(2) * jacob);
+                T vis = ce * (ue1 - ucc) - cw * (ucc - uw1) + cn * (un1 - ucc) - cs * (ucc - us1) + ct * (ut1 - ucc) - cb * (ucc - ub1);
+                vis *= vscale;
                 const T unv = un_is_u ? ucc : un[cc + d * N];
                 ua[cc + d * N] = unv + dt * (-adv_v + vis + fvec[d]);
             }
         }
+        hzb = hzk; hzk = hzt; kzb = kzk; kzk = kzt;
         // the column's own values of plane k become the -1 neighbours of the next plane
 #pragma unroll
         for (int d = 0; d < 3; d++) { um2[d] = um1[d]; um1[d] = U0[d * L::PE + o]; }
