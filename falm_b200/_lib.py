@@ -12,7 +12,7 @@ LIB_PATH = os.path.join(_HERE, "libfalm_b200.so")
 
 FALM_OK = 0
 STATUS = {0: "ok", 1: "bad argument", 2: "cuda error", 3: "non-finite value", 4: "breakdown",
-          5: "maxit", 6: "timeout", 7: "alloc", 8: "state", 9: "no alm"}
+          5: "maxit", 6: "timeout", 7: "alloc", 8: "state", 9: "no alm", 10: "over capacity"}
 FP64, MIXED = 0, 1
 ADV = {"Upwind1": 0, "Upwind3": 1, "QUICK": 2, "UTOPIA": 3, "KK": 4}
 SGS = {"Empty": 0, "Smagorinsky": 1, "CSM": 2}
@@ -73,6 +73,7 @@ SIGNATURES = {
     "falm_eq_sor_sweep": [V, P, P, D, I, P],
     "falm_mv_mv": [V, P, P, P],
     "falm_mv_dot": [V, P, P, c_double_p, P],
+    "falm_mv_dot_static": [I, I, I, I, I, P, P, c_double_p, P],
     "falm_mv_normsq": [V, P, I, c_double_p, P],
     "falm_mv_maxdiag": [V, c_double_p],
     "falm_mv_scale": [V, P, LL, D, P],

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <algorithm>
 #include <cstdlib>
+#include <mutex>
 #include "falm_internal.cuh"
 #include "common.cuh"
 #include "cfd.cuh"
@@ -1174,3 +1175,83 @@ int falm_profile_read(falm_ctx *ctx, double *ms, long long *launches, int nclass
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- allocation-free inner product
+// falm_mv_dot_static: the interior inner product of k_dot for callers that hold
+// device fields but may not allocate.  A coupled solver or an in-situ monitor
+// running beside a simulation that has claimed the device memory is such a
+// caller: creating a context (metric tables, reduction workspace, pinned
+// scalars) could fail there, or fragment the other code's memory pool.
+// Everything the reduction needs lives in one fixed device array, so the call
+// allocates nothing:
+//   [0, 8*kStaticDotBlocks)   per-block partial sums (written before use)
+//   counter at kCounterOff    arrival counter; MUST be zero when a call starts
+//                             (device storage starts zeroed, set-up writes
+//                             zero, the last block of every call resets it)
+//   result at kResultOff      the total, copied back to the host
+// The array is shared by all calls on a device: two calls in flight at once
+// (two streams, two host threads) race.
+namespace {
+constexpr int kStaticDotBlocks = 16384;                                   // 8 rows per block: 131072 rows
+constexpr size_t kCounterOff = (size_t)kStaticDotBlocks * sizeof(double);
+constexpr size_t kResultOff = kCounterOff + 64;
+constexpr size_t kStaticDotBytes = kResultOff + 64;                       // 131200 bytes
+constexpr int kMaxStaticDevices = 64;
+std::mutex g_static_mu;
+unsigned char *g_static_ptr[kMaxStaticDevices];
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_dot_scratch[kStaticDotBytes];
+
+namespace {
+// once per device, with that device current: the array's address and a zeroed counter
+int static_scratch(unsigned char **out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return FALM_ERR_CUDA; }
+    if (dev < 0 || dev >= kMaxStaticDevices) return FALM_ERR_ARG;
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_ptr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_dot_scratch) != cudaSuccess || !p) { cudaGetLastError(); return FALM_ERR_CUDA; }
+        if (cudaMemset((unsigned char *)p + kCounterOff, 0, 64) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+            cudaGetLastError();
+            return FALM_ERR_CUDA;
+        }
+        g_static_ptr[dev] = (unsigned char *)p;
+    }
+    *out = g_static_ptr[dev];
+    return FALM_OK;
+}
+}  // namespace
+
+extern "C" int falm_mv_dot_static(int sx, int sy, int sz, int gc, int precision, const void *a, const void *b, double *out,
+                                  void *stream) {
+    if (!a || !b || !out || gc < 1 || sx < 2 * gc + 1 || sy < 2 * gc + 1 || sz < 2 * gc + 1 ||
+        (precision != FALM_FP64 && precision != FALM_MIXED))
+        return FALM_ERR_ARG;
+    const long long rows = (long long)(sy - 2 * gc) * (sz - 2 * gc);
+    const long long blocks = (rows + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    if (blocks > kStaticDotBlocks) return FALM_ERR_SIZE;   // more interior rows than the fixed partial-sum array holds
+    unsigned char *p = nullptr;
+    int rc = static_scratch(&p);
+    if (rc) return rc;
+    Geom g;
+    g.sx = sx; g.sy = sy; g.sz = sz; g.gc = gc;
+    g.n = (long long)sx * sy * sz;
+    g.nx = sx - 2 * gc; g.ny = sy - 2 * gc; g.nz = sz - 2 * gc;
+    const Region3 R = interior(g);
+    RedWork rw{(double *)p, (unsigned int *)(p + kCounterOff), kStaticDotBlocks};
+    double *res = (double *)(p + kResultOff);
+    cudaStream_t st = S(stream);
+    if (precision == FALM_FP64)
+        k_dot<double><<<(int)blocks, kRowThreads, 0, st>>>(g, R, (const double *)a, (const double *)b, 1, rw, res);
+    else
+        k_dot<float><<<(int)blocks, kRowThreads, 0, st>>>(g, R, (const float *)a, (const float *)b, 1, rw, res);
+    if (cudaGetLastError() != cudaSuccess) return FALM_ERR_CUDA;
+    if (cudaMemcpyAsync(out, res, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        cudaGetLastError();
+        return FALM_ERR_CUDA;
+    }
+    return FALM_OK;
+}

@@ -43,7 +43,8 @@ typedef enum {
     FALM_ERR_TIMEOUT = 6,    /* a bounded device-side wait gave up                         */
     FALM_ERR_ALLOC = 7,      /* device allocation failed                                   */
     FALM_ERR_STATE = 8,      /* call order (e.g. solve before the operator was built)      */
-    FALM_ERR_NOALM = 9       /* ALM entry point called without falm_alm_init               */
+    FALM_ERR_NOALM = 9,      /* ALM entry point called without falm_alm_init               */
+    FALM_ERR_SIZE = 10       /* request larger than a fixed capacity (falm_mv_dot_static)  */
 } falm_status;
 
 typedef enum { FALM_FP64 = 0, FALM_MIXED = 1 } falm_precision;
@@ -204,6 +205,24 @@ int falm_step(falm_ctx *ctx, const falm_fields *f, double dt, double t, void *st
    `stream` (pass pinned memory).  Takes precedence over the inflow box for that one call.
    No reference counterpart (the reference has uniform inflow only). */
 int falm_bc_set_inlet_plane(falm_ctx *ctx, const double *plane, void *stream);
+
+/* ---------------- allocation-free inner product --------------------------------------------- */
+/* No reference counterpart.  The interior inner product of falm_mv_dot for callers that hold
+   device fields but may not allocate (a coupled solver or in-situ monitor beside a simulation
+   that has claimed the device memory, where creating a context could fail): no context, and
+   nothing is allocated -- the partial sums, arrival counter and result live in a fixed 128 KiB
+   device array inside the library.
+   - One 256-thread block per 8 interior rows, (sy-2gc)*(sz-2gc) rows: grids with more than
+     131072 interior rows return FALM_ERR_SIZE without touching the device.
+   - The arrival counter must be zero when a call starts: device storage starts zeroed, the
+     set-up writes zero and every call's last block resets it.
+   - All calls on a device share the array: two calls in flight at once (two streams or two
+     host threads) race and give wrong results.
+   - The first call on a device performs the set-up (symbol address, counter reset, a device
+     synchronisation); make it before any stream capture.
+   precision FALM_FP64 (double fields) or FALM_MIXED (float fields); *out is a host double. */
+int falm_mv_dot_static(int sx, int sy, int sz, int gc, int precision, const void *a, const void *b,
+                       double *out, void *stream);
 
 /* ---------------- instrumentation ----------------------------------------------------------- */
 /* Kernel classes timed with CUDA events when profiling is on (one event pair per launch). */
