@@ -253,6 +253,11 @@ def channel_large():
     return channel(512, 256, 256, tol=1e-6, steps=5000, name="channel_large")
 
 
+def channel_half():
+    """512 x 256 x 128: the x/y shape of channel_large with half the planes (profiling case)"""
+    return channel(512, 256, 128, tol=1e-6, steps=5000, name="channel_half")
+
+
 def adjoint_case():
     return channel(128, 64, 64, cells_per_radius=10, steps=200, name="adjoint")
 

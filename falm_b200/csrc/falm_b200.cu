@@ -21,6 +21,7 @@
 #include "stencil_tma.cuh"
 #include "poisson_tma.cuh"
 #include "plane3_tma.cuh"
+#include "sor_rb_tma.cuh"
 #include <cudaTypedefs.h>
 
 using namespace fb;
@@ -174,7 +175,8 @@ bool make_map(const falm_ctx *ctx, CUtensorMap *m, const void *base, int ncomp, 
     const size_t e = ctx->esize;
     // every box lies inside the tensor: x and y at least one box long (the
     // kernels clamp the box origins), x rows a whole number of 16-byte units
-    if (!tma_encode_available() || ((uintptr_t)base & 15) || ((g.sx * e) & 15) || g.sx < bx || g.sy < by) return false;
+    // (the kernels' box x origins are 16-byte aligned for gc = 2)
+    if (!tma_encode_available() || ((uintptr_t)base & 15) || ((g.sx * e) & 15) || g.sx < bx || g.sy < by || g.gc != 2) return false;
     cuuint64_t dims[4] = {(cuuint64_t)g.sx, (cuuint64_t)g.sy, (cuuint64_t)g.sz, (cuuint64_t)ncomp};
     cuuint64_t strides[3] = {(cuuint64_t)(g.sx * e), (cuuint64_t)(g.sx * (size_t)g.sy * e), (cuuint64_t)(g.n * e)};
     cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, 1, (cuuint32_t)ncomp};
@@ -209,6 +211,33 @@ int s7_launch(falm_ctx *ctx, int cls, cudaStream_t st, const T *x, const Body &b
         if (_s7 < 0) return -_s7;                                                          \
         if (_s7 == 0) LAUNCH((CLS), (ST), ROWLAUNCH);                                      \
     } while (0)
+
+// H consecutive red-black half sweeps (first colour c1) in one pass, x_in -> x_out;
+// 1 launched, 0 not eligible, <0 launch error
+template <typename T, int H>
+int sor_rb_launch_h(falm_ctx *ctx, cudaStream_t st, const T *xin, const T *b, T *xout, T omega, int c1, const SolverScalars *sc) {
+    using L = RBTile<T, H>;
+    if (ctx->no_tma || ctx->A_explicit) return 0;
+    CUtensorMap mx, mb;
+    if (!make_map(ctx, &mx, xin, 1, L::BX, L::BY) || !make_map(ctx, &mb, b, 1, L::BX, L::BY)) return 0;
+    const Geom &g = ctx->geo;
+    const int bx = (g.nx + L::TX - 1) / L::TX, by = (g.ny + L::TY - 1) / L::TY;
+    const int kc = chunk_len(ctx, (long long)bx * by, g.nz, sizeof(T) == 4 ? 3 : 2, 32);
+    dim3 grid(bx, by, (g.nz + kc - 1) / kc);
+    cudaFuncSetAttribute(k_sor_rb_tma<T, H>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
+    const PoissonTables<T> tb = op7<T>(ctx).t;
+    int rc = launch_k(ctx, FALM_K_SOR, st, [&] {
+        k_sor_rb_tma<T, H><<<grid, 256, L::SMEM, st>>>(g, kc, mx, mb, tb, xout, omega, c1, sc, ctx->kerr);
+    });
+    return rc ? -rc : 1;
+}
+
+template <typename T>
+int sor_rb_launch(falm_ctx *ctx, cudaStream_t st, int H, const T *xin, const T *b, T *xout, T omega, int c1, const SolverScalars *sc) {
+    if (H == 1) return sor_rb_launch_h<T, 1>(ctx, st, xin, b, xout, omega, c1, sc);
+    if (H == 2) return sor_rb_launch_h<T, 2>(ctx, st, xin, b, xout, omega, c1, sc);
+    return sor_rb_launch_h<T, 3>(ctx, st, xin, b, xout, omega, c1, sc);
+}
 
 // ring depth of the multi-field plane stream: keep >= 2 planes in flight and
 // at least two CTAs per SM
@@ -360,10 +389,20 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
     int total_it = 0, outer = 0;
     const bool mixed = ctx->precision == FALM_MIXED;
     const int max_outer = mixed ? ctx->max_outer : 1;
-    // launch the remaining sweeps of one preconditioner application z ~ A^-1 v
-    auto precondition_rest = [&](T *z, const T *v) -> int {
+    // launch the remaining sweeps of one preconditioner application z ~ A^-1 v;
+    // the temporally blocked sweeps run out of place and swap z with xp
+    auto precondition_rest = [&](T *&z, const T *v) -> int {
         if (pct == FALM_LS_SOR) {
-            for (int hs = 1; hs < 2 * m; hs++) {      // red, then (black, red) x (m-1)
+            int hs = 1;
+            while (hs < 2 * m) {                       // up to 3 half sweeps per pass over HBM
+                const int H = std::min(3, 2 * m - hs);
+                const int r = sor_rb_launch<T>(ctx, st, H, z, v, xp, pcw, hs & 1, sc);
+                if (r < 0) return -r;
+                if (r == 0) break;
+                std::swap(z, xp);
+                hs += H;
+            }
+            for (; hs < 2 * m; hs++) {                // red, then (black, red) x (m-1)
                 const int color = hs & 1;
                 S7_OR(FALM_K_SOR, st, T, 0, z, (SorBody<T>{op, z, v, pcw, color, sc}),
                       (k_sor<T><<<grid, kRowThreads, 0, st>>>(g, R, op, z, v, pcw, color, sc)));

@@ -26,10 +26,37 @@ namespace fb {
 // coefficient 0.5*(g_c+g_nb)/ja depends on one index only), or an explicit
 // caller-owned 7-column matrix for general systems.
 template <typename T>
+struct Coef7 { T ac, aw, ae, as, an, ab, at; };
+
+template <typename T>
 struct Op7 {
     PoissonTables<T> t;
     const T *A;
     long long n;
+    // x/y part of the table operator of one (i, j) column (hoisted out of a z
+    // march): the four in-plane coefficients and the first three terms of the
+    // diagonal's accumulation, so that at_col() rebuilds get() bit for bit
+    struct Col { T aw, ae, as, an, dxy; };
+    __device__ __forceinline__ Col column(int i, int j) const {
+        Col r;
+        if (A) { r.aw = r.ae = r.as = r.an = r.dxy = T(0); return r; }
+        r.aw = ldg(t.cm[0] + i); r.ae = ldg(t.cp[0] + i);
+        r.as = ldg(t.cm[1] + j); r.an = ldg(t.cp[1] + j);
+        r.dxy = (ldg(t.dx0 + i) - ldg(t.up[1] + j)) - ldg(t.um[1] + j);
+        return r;
+    }
+    __device__ __forceinline__ Coef7<T> at_col(const Col &cl, int k, long long c) const {
+        Coef7<T> r;
+        if (A) {
+            r.ac = A[c]; r.aw = A[c + n]; r.ae = A[c + 2 * n]; r.as = A[c + 3 * n];
+            r.an = A[c + 4 * n]; r.ab = A[c + 5 * n]; r.at = A[c + 6 * n];
+        } else {
+            r.aw = cl.aw; r.ae = cl.ae; r.as = cl.as; r.an = cl.an;
+            r.ab = ldg(t.cm[2] + k); r.at = ldg(t.cp[2] + k);
+            r.ac = ((cl.dxy - ldg(t.up[2] + k)) - ldg(t.um[2] + k)) * t.scale;
+        }
+        return r;
+    }
     __device__ __forceinline__ void get(int i, int j, int k, long long c, T &ac, T &aw, T &ae, T &as, T &an, T &ab,
                                         T &at) const {
         if (A) {

@@ -27,7 +27,10 @@ template <typename T>
 constexpr int s7_smem() { return S7Conf<T>::NS * S7Tile<T>::SLOT + 128 + 128; }
 
 // Body: bool skip() const; const T *pw() const (pointwise operand, or null);
-//       void cell(i, j, k, cc, xc, xe, xw, xn, xs, xt, xb, pv, acc); void finish(tot)
+//       const Op7<T> &op_() const;
+//       void cell(i, j, k, cc, a, xc, xe, xw, xn, xs, xt, xb, pv, acc); void finish(tot)
+// The kernel hoists the x/y part of the operator out of the z march and passes
+// the cell's coefficients a (Coef7).
 // The pointwise operand of the next plane is loaded one iteration ahead (pv),
 // so its latency overlaps the current plane's wait and arithmetic.
 template <typename T, int NV, class Body>
@@ -81,15 +84,18 @@ __global__ void __launch_bounds__(256) k_s7_tma(Geom g, int kc, const __grid_con
     waited = 2;
     T xm = slot(0)[o];
     const T *pw = body.pw();
-    const long long sxy = (long long)g.sx * g.sy, c0 = g.id(i, j, P0 + 1);   // cell of the first computed plane
-    T pv = (pw && active) ? pw[c0] : T(0);
+    const long long sxy = (long long)g.sx * g.sy;
+    long long cc = g.id(i, j, P0 + 1);   // cell of the first computed plane
+    T pv = (pw && active) ? pw[cc] : T(0);
+    const Op7<T> &op = body.op_();
+    const typename Op7<T>::Col col = op.column(min(i, g.sx - g.gc - 1), min(j, g.sy - g.gc - 1));
     if (__syncthreads_or(fail)) goto drain;
     if (NS < nplanes) {
         if (threadIdx.x == 0) { fence_proxy_async(); issue(NS); }
         issued = NS + 1;
     }
     for (int q = 1; q < nplanes - 1; q++) {
-        const T pn = (pw && active && q + 1 < nplanes - 1) ? pw[c0 + (long long)q * sxy] : T(0);
+        const T pn = (pw && active && q + 1 < nplanes - 1) ? pw[cc + sxy] : T(0);
         fail = !wait_q(q + 1);
         waited = q + 2;
         if (__syncthreads_or(fail)) goto drain;
@@ -101,10 +107,12 @@ __global__ void __launch_bounds__(256) k_s7_tma(Geom g, int kc, const __grid_con
         const T xc = X0[o];
         if (active) {
             const int k = P0 + q;
-            body.cell(i, j, k, g.id(i, j, k), xc, X0[o + 1], X0[o - 1], X0[o + L::BX], X0[o - L::BX], X1[o], xm, pv, acc);
+            const Coef7<T> a = op.at_col(col, k, cc);
+            body.cell(i, j, k, cc, a, xc, X0[o + 1], X0[o - 1], X0[o + L::BX], X0[o - L::BX], X1[o], xm, pv, acc);
         }
         xm = xc;
         pv = pn;
+        cc += sxy;
     }
     goto reduce;
 drain:
@@ -133,11 +141,11 @@ struct SorBody {
     const SolverScalars *sc;
     __device__ bool skip() const { return sc && sc->done; }
     __device__ const T *pw() const { return b; }
-    __device__ void cell(int i, int j, int k, long long c, T xc, T xe, T xw, T xn, T xs, T xt, T xb, T bv, double (&)[1]) const {
+    __device__ const Op7<T> &op_() const { return op; }
+    __device__ void cell(int i, int j, int k, long long c, const Coef7<T> &a, T xc, T xe, T xw, T xn, T xs, T xt, T xb, T bv,
+                         double (&)[1]) const {
         if (((i + j + k) & 1) != color) return;
-        T ac, aw, ae, as, an, ab, at;
-        op.get(i, j, k, c, ac, aw, ae, as, an, ab, at);
-        T cc = (bv - dot7(ac, ae, aw, an, as, at, ab, xc, xe, xw, xn, xs, xt, xb)) / ac;
+        T cc = (bv - dot7(a.ac, a.ae, a.aw, a.an, a.as, a.at, a.ab, xc, xe, xw, xn, xs, xt, xb)) / a.ac;
         x[c] = xc + omega * cc;
     }
     __device__ void finish(const double (&)[1]) const {}
@@ -150,10 +158,10 @@ struct MvBody {
     T *ax;
     __device__ bool skip() const { return false; }
     __device__ const T *pw() const { return nullptr; }
-    __device__ void cell(int i, int j, int k, long long c, T xc, T xe, T xw, T xn, T xs, T xt, T xb, T, double (&)[1]) const {
-        T ac, aw, ae, as, an, ab, at;
-        op.get(i, j, k, c, ac, aw, ae, as, an, ab, at);
-        ax[c] = dot7(ac, ae, aw, an, as, at, ab, xc, xe, xw, xn, xs, xt, xb);
+    __device__ const Op7<T> &op_() const { return op; }
+    __device__ void cell(int i, int j, int k, long long c, const Coef7<T> &a, T xc, T xe, T xw, T xn, T xs, T xt, T xb, T,
+                         double (&)[1]) const {
+        ax[c] = dot7(a.ac, a.ae, a.aw, a.an, a.as, a.at, a.ab, xc, xe, xw, xn, xs, xt, xb);
     }
     __device__ void finish(const double (&)[1]) const {}
 };
@@ -167,10 +175,10 @@ struct MvDot1Body {
     SolverScalars *sc;
     __device__ bool skip() const { return sc->done; }
     __device__ const T *pw() const { return rr; }
-    __device__ void cell(int i, int j, int k, long long c, T xc, T xe, T xw, T xn, T xs, T xt, T xb, T rrv, double (&acc)[1]) const {
-        T ac, aw, ae, as, an, ab, at;
-        op.get(i, j, k, c, ac, aw, ae, as, an, ab, at);
-        T qv = dot7(ac, ae, aw, an, as, at, ab, xc, xe, xw, xn, xs, xt, xb);
+    __device__ const Op7<T> &op_() const { return op; }
+    __device__ void cell(int i, int j, int k, long long c, const Coef7<T> &a, T xc, T xe, T xw, T xn, T xs, T xt, T xb, T rrv,
+                         double (&acc)[1]) const {
+        T qv = dot7(a.ac, a.ae, a.aw, a.an, a.as, a.at, a.ab, xc, xe, xw, xn, xs, xt, xb);
         q[c] = qv;
         acc[0] += to_d(rrv) * to_d(qv);
     }
@@ -190,10 +198,10 @@ struct MvDot2Body {
     SolverScalars *sc;
     __device__ bool skip() const { return sc->done; }
     __device__ const T *pw() const { return s; }
-    __device__ void cell(int i, int j, int k, long long c, T xc, T xe, T xw, T xn, T xs, T xt, T xb, T sv, double (&acc)[2]) const {
-        T ac, aw, ae, as, an, ab, at;
-        op.get(i, j, k, c, ac, aw, ae, as, an, ab, at);
-        T tv = dot7(ac, ae, aw, an, as, at, ab, xc, xe, xw, xn, xs, xt, xb);
+    __device__ const Op7<T> &op_() const { return op; }
+    __device__ void cell(int i, int j, int k, long long c, const Coef7<T> &a, T xc, T xe, T xw, T xn, T xs, T xt, T xb, T sv,
+                         double (&acc)[2]) const {
+        T tv = dot7(a.ac, a.ae, a.aw, a.an, a.as, a.at, a.ab, xc, xe, xw, xn, xs, xt, xb);
         t[c] = tv;
         double td = to_d(tv);
         acc[0] += td * to_d(sv);
@@ -216,10 +224,10 @@ struct ResBody {
     int check_tol;
     __device__ bool skip() const { return false; }
     __device__ const T *pw() const { return b; }
-    __device__ void cell(int i, int j, int k, long long c, T xc, T xe, T xw, T xn, T xs, T xt, T xb, T bv, double (&acc)[2]) const {
-        T ac, aw, ae, as, an, ab, at;
-        op.get(i, j, k, c, ac, aw, ae, as, an, ab, at);
-        double rv = to_d(bv) - dot7<double>(ac, ae, aw, an, as, at, ab, xc, xe, xw, xn, xs, xt, xb);
+    __device__ const Op7<T> &op_() const { return op; }
+    __device__ void cell(int i, int j, int k, long long c, const Coef7<T> &a, T xc, T xe, T xw, T xn, T xs, T xt, T xb, T bv,
+                         double (&acc)[2]) const {
+        double rv = to_d(bv) - dot7<double>(a.ac, a.ae, a.aw, a.an, a.as, a.at, a.ab, xc, xe, xw, xn, xs, xt, xb);
         T rt = (T)rv;
         r[c] = rt;
         if (rr) rr[c] = rt;
