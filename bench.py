@@ -158,7 +158,7 @@ KERNEL_VALUES = {
     "utouu_rhs": 7,     # ua(3) in, uu(3) rhs(1) out
     "res": 4,           # x b in, r rr out
     "bicg_p": 5,        # r p q in, p pp out
-    "sor": 3,           # x b in, x out (half sweep)
+    "sor": 3,           # x b in, x out (three red-black half sweeps per launch, one HBM pass)
     "mv_dot1": 3,       # pp rr in, q out
     "bicg_s": 4,        # r q in, s ss out
     "mv_dot2": 3,       # ss s in, t out
@@ -379,7 +379,8 @@ def main():
         "config": {"workload": f"{case.name} {g[0]}x{g[1]}x{g[2]} channel + 3-blade ALM rotor, {args.precision}",
                    "cells": case.grid.n_interior, "tol": case.tol, "pc": f"{case.pc} x{case.pc_maxit}",
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                   "l2": "inputs larger than L2 (one FP32 field is 140 MB)"},
+                   "l2": f"inputs larger than L2 (one {'FP32' if args.precision == 'mixed' else 'FP64'} field is "
+                         f"{case.grid.n * (4 if args.precision == 'mixed' else 8) / 1e6:.0f} MB, L2 126 MB)"},
         "clocks": r["clocks"], "gpu_launches": r["launches"], "roofline": r["roofline"],
         "step_roofline": r["step_roofline"], "its": r["its"], "divnorm_max": r["divnorm_max"],
         "err_max": r["err_max"], "profile": r["profile"],

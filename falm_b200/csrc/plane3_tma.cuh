@@ -88,7 +88,9 @@ __global__ void __launch_bounds__(256) k_plane3_tma(Geom g, Region3 R, int org, 
 #pragma unroll
         for (int f = 0; f < NF; f++) tma_load_4d(slot(q) + foff[f], &maps.m[f], xb, yb, P0 + q, 0, b);
     };
-    auto wait_q = [&](int q) -> bool { return mbar_wait(bar + (q % NS), (q / NS) & 1, err); };
+    // warp 0 polls the barriers; the block barrier that follows makes the
+    // landed planes visible to every thread
+    auto wait_q = [&](int q) -> bool { return threadIdx.x >= 32 || mbar_wait(bar + (q % NS), (q / NS) & 1, err); };
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int f = 0; f < NF; f++) prefetch_tmap(&maps.m[f]);
@@ -280,13 +282,26 @@ struct SgsDivBody {
 // velocity's guide values, as the reference's aliased u does.
 template <typename T>
 __global__ void k_copy_shell(Geom g, const T *__restrict__ src, T *__restrict__ dst) {
+    // the shell of the a x b x c box (interior + one guide layer), enumerated
+    // directly: the k = 0, c-1 planes, then the j = 0, b-1 rows, then the
+    // i = 0, a-1 columns of the remaining (b-2) x (c-2) cells
     const int a = g.sx - 2 * g.gc + 2, b = g.sy - 2 * g.gc + 2, c = g.sz - 2 * g.gc + 2;
-    const long long tot = (long long)a * b * c;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
-        int i = (int)(q % a), j = (int)((q / a) % b), k = (int)(q / ((long long)a * b));
-        bool shell = i == 0 || i == a - 1 || j == 0 || j == b - 1 || k == 0 || k == c - 1;
-        if (!shell) continue;
-        long long id = g.id(i + g.gc - 1, j + g.gc - 1, k + g.gc - 1);
+    const int ab = a * b, ac = a * (c - 2), bc = (b - 2) * (c - 2);
+    const int tot = 2 * (ab + ac + bc);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) {
+        int i, j, k, r = q;
+        if (r < 2 * ab) {
+            k = r < ab ? 0 : c - 1; r = r < ab ? r : r - ab;
+            i = r % a; j = r / a;
+        } else if ((r -= 2 * ab) < 2 * ac) {
+            j = r < ac ? 0 : b - 1; r = r < ac ? r : r - ac;
+            i = r % a; k = 1 + r / a;
+        } else {
+            r -= 2 * ac;
+            i = r < bc ? 0 : a - 1; r = r < bc ? r : r - bc;
+            j = 1 + r % (b - 2); k = 1 + r / (b - 2);
+        }
+        const long long id = g.id(i + g.gc - 1, j + g.gc - 1, k + g.gc - 1);
         dst[id] = src[id]; dst[id + g.n] = src[id + g.n]; dst[id + 2 * g.n] = src[id + 2 * g.n];
     }
 }

@@ -67,7 +67,9 @@ __global__ void __launch_bounds__(256) k_s7_tma(Geom g, int kc, const __grid_con
             tma_reject(b, err, 2);
         }
     };
-    auto wait_q = [&](int q) -> bool { return mbar_wait(bar + (q % NS), (q / NS) & 1, err); };
+    // warp 0 polls the barriers; the block barrier that follows makes the
+    // landed planes visible to every thread
+    auto wait_q = [&](int q) -> bool { return threadIdx.x >= 32 || mbar_wait(bar + (q % NS), (q / NS) & 1, err); };
     if (threadIdx.x == 0) {
         prefetch_tmap(&mx);
         for (int s = 0; s < NS; s++) mbar_init(bar + s, 1);
@@ -82,24 +84,21 @@ __global__ void __launch_bounds__(256) k_s7_tma(Geom g, int kc, const __grid_con
     bool fail = !wait_q(0);
     fail = !wait_q(1) || fail;
     waited = 2;
-    T xm = slot(0)[o];
     const T *pw = body.pw();
     const long long sxy = (long long)g.sx * g.sy;
     long long cc = g.id(i, j, P0 + 1);   // cell of the first computed plane
     T pv = (pw && active) ? pw[cc] : T(0);
     const Op7<T> &op = body.op_();
     const typename Op7<T>::Col col = op.column(min(i, g.sx - g.gc - 1), min(j, g.sy - g.gc - 1));
+    T xm;
     if (__syncthreads_or(fail)) goto drain;
-    if (NS < nplanes) {
-        if (threadIdx.x == 0) { fence_proxy_async(); issue(NS); }
-        issued = NS + 1;
-    }
+    xm = slot(0)[o];
     for (int q = 1; q < nplanes - 1; q++) {
         const T pn = (pw && active && q + 1 < nplanes - 1) ? pw[cc + sxy] : T(0);
         fail = !wait_q(q + 1);
         waited = q + 2;
         if (__syncthreads_or(fail)) goto drain;
-        if (q >= 2 && q - 1 + NS < nplanes) {
+        if (q - 1 + NS < nplanes) {   // plane q-1 is no longer read (its value is in xm): refill its slot
             if (threadIdx.x == 0) { fence_proxy_async(); issue(q - 1 + NS); }
             issued = q - 1 + NS + 1;
         }

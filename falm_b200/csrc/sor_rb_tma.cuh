@@ -79,7 +79,9 @@ __global__ void __launch_bounds__(256) k_sor_rb_tma(Geom g, int kc, const __grid
             tma_reject(b, err, 4);
         }
     };
-    auto wait_q = [&](int q) -> bool { return mbar_wait(bar + ((unsigned)q % NS), ((unsigned)q / NS) & 1, err); };
+    // warp 0 polls the barriers; the block barrier that follows makes the
+    // landed planes visible to every thread
+    auto wait_q = [&](int q) -> bool { return threadIdx.x >= 32 || mbar_wait(bar + ((unsigned)q % NS), ((unsigned)q / NS) & 1, err); };
     if (threadIdx.x == 0) {
         prefetch_tmap(&mx); prefetch_tmap(&mb);
         for (unsigned s = 0; s < NS; s++) mbar_init(bar + s, 1);

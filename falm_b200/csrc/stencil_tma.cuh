@@ -94,11 +94,18 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_pseudo_u_tma(Ge
     if (threadIdx.x == 0)
         for (int q = 0; q < first; q++) issue(q);
     issued = first;
-    auto wait_q = [&](int q) -> bool { return mbar_wait(bar + (q % NS), (q / NS) & 1, err); };
+    // warp 0 polls the barriers; the block barrier that follows makes the
+    // landed planes visible to every thread
+    auto wait_q = [&](int q) -> bool { return threadIdx.x >= 32 || mbar_wait(bar + (q % NS), (q / NS) & 1, err); };
+    // every plane is waited for exactly once, before its first read: planes
+    // 0..3 here (iteration q = 2 reads q, q+1, q+2), plane q+2 at iteration q
     bool fail = !wait_q(0);
     fail = !wait_q(1) || fail;
-    waited = 2;
+    fail = !wait_q(2) || fail;
+    fail = !wait_q(3) || fail;
+    waited = 4;
     T um2[3], um1[3], nutm1, uu2m1;
+    if (__syncthreads_or(fail)) goto drain;
     {
         const T *U0 = (const T *)slot(0), *U1 = (const T *)slot(1);
         const T *UU1 = (const T *)(slot(1) + L::U_BYTES), *N1 = (const T *)(slot(1) + 2 * L::U_BYTES);
@@ -107,28 +114,33 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_pseudo_u_tma(Ge
         nutm1 = N1[o];
         uu2m1 = UU1[2 * L::PE + o];
     }
-    // every plane is waited for exactly once, before its first read: planes
-    // 0..3 here (iteration q = 2 reads q, q+1, q+2), plane q+2 at iteration q
-    fail = !wait_q(2) || fail;
-    fail = !wait_q(3) || fail;
-    waited = 4;
-    if (__syncthreads_or(fail)) goto drain;
-    if (threadIdx.x == 0) {
-        fence_proxy_async();
-        for (int q = NS; q < NS + 2 && q < nplanes; q++) issue(q);
+    // planes 0 and 1 now live in registers: refill their slots with planes NS
+    // and NS+1 (iteration q waits for plane q+2, which must already be in flight)
+    __syncthreads();
+    {
+        const int upto = min(NS + 1, nplanes - 1);
+        if (upto >= issued) {
+            if (threadIdx.x == 0) {
+                fence_proxy_async();
+                for (int pl = issued; pl <= upto; pl++) issue(pl);
+            }
+            issued = upto + 1;
+        }
     }
-    issued = min(NS + 2, nplanes);
     for (int q = 2; q < nplanes - 2; q++) {
         // planes q (= k), q+1, q+2 must be resident; q+2 is the new one
         fail = !wait_q(q + 2);
         waited = q + 3;
         if (__syncthreads_or(fail)) goto drain;
-        if (q >= 3 && q - 1 + NS < nplanes) {        // slot of plane q-1 is free: refill it
-            if (threadIdx.x == 0) {
-                fence_proxy_async();
-                issue(q - 1 + NS);
+        {   // planes up to q-1 are no longer read (held in registers): refill their slots
+            const int upto = min(q - 1 + NS, nplanes - 1);
+            if (upto >= issued) {
+                if (threadIdx.x == 0) {
+                    fence_proxy_async();
+                    for (int pl = issued; pl <= upto; pl++) issue(pl);
+                }
+                issued = upto + 1;
             }
-            issued = q - 1 + NS + 1;
         }
         const int k = P0 + q;
         const T *U0 = (const T *)slot(q), *UU0 = (const T *)(slot(q) + L::U_BYTES), *N0 = (const T *)(slot(q) + 2 * L::U_BYTES);

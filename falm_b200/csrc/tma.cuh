@@ -8,16 +8,18 @@
 // completes on the transferred byte count.  No multicast is used: every CTA
 // loads its own boxes from this GPU's memory.
 //
-// Every wait is bounded: after kWaitLimit polls a wait records an error in
-// the context's device error word and returns false, and the kernel drains
-// its own copies (again bounded) before it returns.
+// Every wait is bounded (about one second of clock64 time): a wait that gives
+// up records an error in the context's device error word and returns false,
+// and the kernel drains its own copies (again bounded) before it returns.
+// Warp 0 of a block polls the barriers; a block barrier then publishes the
+// landed data to the other warps.
 #pragma once
 #include <cuda.h>
 #include <stdint.h>
 
 namespace fb {
 
-constexpr unsigned kWaitLimit = 1u << 22;   // polls of try_wait (each may suspend ~ a microsecond)
+constexpr unsigned kWaitLimit = 1u << 28;   // polls of try_wait (the clock64 bound of ~1 s normally ends a wait first)
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -45,17 +47,16 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
-// bounded wait: polls with a growing back-off and gives up after about one
-// second of clock64 time (or kWaitLimit polls); false (and *err set) then
+// bounded wait: try_wait suspends the thread in hardware until the phase
+// completes or a short time limit passes; poll it, checking clock64 every 64
+// polls, and give up after about one second (or kWaitLimit polls): false (and
+// *err set) then
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
-    unsigned ns = 32;
-    for (unsigned it = 0; it < kWaitLimit; it++) {
+    for (unsigned it = 1; it < kWaitLimit; it++) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (clock64() - t0 > 2000000000LL) break;
-        __nanosleep(ns);
-        if (ns < 1024) ns <<= 1;
+        if ((it & 63u) == 0 && clock64() - t0 > 2000000000LL) break;
     }
     if (err) atomicExch(err, FALM_ERR_TIMEOUT);
     return false;
