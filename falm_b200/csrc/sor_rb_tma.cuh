@@ -2,7 +2,7 @@
 // c1^1, ...) of FalmEqDevCall::SORSweep (src/dev/FalmEqDevCall.cu:175-211) in
 // one pass over HBM, out of place (x_in -> x_out).
 //
-// A CTA owns a 64 x 8 tile of columns and a chunk of z planes.  Half sweep h
+// A CTA owns a 32 x 8 tile of columns and a chunk of z planes.  Half sweep h
 // must be evaluated on the tile plus a ring of H-h cells (in x, y and z) for
 // the last one to be exact on the tile, so every plane of x_in and b is staged
 // as one (tile + halo) TMA box.  The z march is a wavefront: when raw plane q
@@ -11,6 +11,11 @@
 // colour (which reads only the other colour, so in-place is exact), then the
 // tile of plane q-H is final and is written to x_out.  Reads come from x_in
 // only, so neighbouring CTAs never see a partially updated field.
+//
+// Each thread owns one horizontal pair of cells (x0, x0+1) of the widest
+// ring: exactly one cell of the pair has a given colour on a given plane, so
+// the thread updates that one in every half sweep whose ring holds it, with
+// the pair's x/y operator coefficients kept in registers.
 #pragma once
 #include "poisson.cuh"
 #include "tma.cuh"
@@ -24,8 +29,10 @@ __device__ __forceinline__ float sor_div(float a, float b) { return __fdividef(a
 
 template <typename T, int H>
 struct RBTile {
-    static constexpr int TX = 64, TY = 8;
-    // x halo of the box: >= H, and box origin i0 - HX = 64 bx + 2 - HX on a
+    static constexpr int TX = 32, TY = 8;
+    static constexpr int R = H - 1;                                  // widest ring (half sweep 1)
+    static constexpr int PX = (TX + 2 * R) / 2, PY = TY + 2 * R;     // pairs per row, rows
+    // x halo of the box: >= H, and box origin i0 - HX = 32 bx + 2 - HX on a
     // 16-byte boundary for gc = 2
     static constexpr int HX = (H <= 2) ? 2 : (sizeof(T) == 4 ? 6 : 4);
     static constexpr int BX = TX + 2 * HX, BY = TY + 2 * H, PE = BX * BY;
@@ -33,8 +40,8 @@ struct RBTile {
     static constexpr int SLOT = 2 * PB;                                   // x plane, then b plane
     // H+2 resident planes + look-ahead; a power of two keeps the slot index a mask
     static constexpr int NS = 8;
-    static constexpr int TAB = (3 * BX + 4 * BY) * (int)sizeof(T);
-    static constexpr int SMEM = NS * SLOT + 128 + ((TAB + 127) / 128) * 128 + 128;
+    static constexpr int SMEM = NS * SLOT + 128 + 128;
+    static_assert(PX * PY <= 256, "one pair per thread");
 };
 
 template <typename T, int H>
@@ -46,24 +53,40 @@ __global__ void __launch_bounds__(256) k_sor_rb_tma(Geom g, int kc, const __grid
     extern __shared__ unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
     uint64_t *bar = (uint64_t *)(smem + NS * L::SLOT);
-    T *tab = (T *)(smem + NS * L::SLOT + 128);
     if (sc && sc->done) return;
     const int i0 = g.gc + blockIdx.x * L::TX, j0 = g.gc + blockIdx.y * L::TY;
     const int k0 = g.gc + blockIdx.z * kc, k1 = min(k0 + kc, g.sz - g.gc);
     const int P0 = k0 - H, nplanes = (k1 + H) - P0;
     const int xb = max(0, box_origin(i0 - L::HX, L::BX, g.sx, 16 / (int)sizeof(T)));
     const int yb = max(0, box_origin(j0 - H, L::BY, g.sy, 1));
-    // x/y operator tables of the box: aw, ae, dx0 per column; as, an, up1, um1 per row
-    T *t_aw = tab, *t_ae = tab + L::BX, *t_dx = tab + 2 * L::BX;
-    T *t_as = tab + 3 * L::BX, *t_an = t_as + L::BY, *t_up = t_an + L::BY, *t_um = t_up + L::BY;
-    for (int q = threadIdx.x; q < L::BX; q += blockDim.x) {
-        const int x = min(xb + q, g.sx - 1);
-        t_aw[q] = ldg(tb.cm[0] + x); t_ae[q] = ldg(tb.cp[0] + x); t_dx[q] = ldg(tb.dx0 + x);
+    const int ilo = g.gc, ihi = g.sx - g.gc, jlo = g.gc, jhi = g.sy - g.gc, klo = g.gc, khi = g.sz - g.gc;
+    // this thread's pair (x0, x0+1) in row y of the widest ring
+    const int t = threadIdx.x;
+    const bool owner = t < L::PX * L::PY;
+    const int x0 = i0 - L::R + 2 * (t % L::PX), y = j0 - L::R + t / L::PX;
+    // cell e (0: x0, 1: x0+1) takes part in half sweep h when it lies in ring
+    // H-h of the tile and inside the interior: bit h-1 of live[e]
+    unsigned live0 = 0u, live1 = 0u;
+#pragma unroll
+    for (int h = 1; h <= H; h++) {
+        const int ring = H - h;
+        const bool yin = owner && y >= j0 - ring && y < j0 + L::TY + ring && y >= jlo && y < jhi;
+        const bool in0 = yin && x0 >= i0 - ring && x0 < i0 + L::TX + ring && x0 >= ilo && x0 < ihi;
+        const bool in1 = yin && x0 + 1 >= i0 - ring && x0 + 1 < i0 + L::TX + ring && x0 + 1 >= ilo && x0 + 1 < ihi;
+        live0 |= (in0 ? 1u : 0u) << (h - 1);
+        live1 |= (in1 ? 1u : 0u) << (h - 1);
     }
-    for (int q = threadIdx.x; q < L::BY; q += blockDim.x) {
-        const int y = min(yb + q, g.sy - 1);
-        t_as[q] = ldg(tb.cm[1] + y); t_an[q] = ldg(tb.cp[1] + y); t_up[q] = ldg(tb.up[1] + y); t_um[q] = ldg(tb.um[1] + y);
+    // x/y operator coefficients of both cells (same association as Op7::get)
+    T aw0, aw1, ae0, ae1, dxy0, dxy1, as, an;
+    {
+        const int yc = min(max(y, 0), g.sy - 1);
+        const int xc0 = min(max(x0, 0), g.sx - 1), xc1 = min(max(x0 + 1, 0), g.sx - 1);
+        as = ldg(tb.cm[1] + yc); an = ldg(tb.cp[1] + yc);
+        const T up1 = ldg(tb.up[1] + yc), um1 = ldg(tb.um[1] + yc);
+        aw0 = ldg(tb.cm[0] + xc0); ae0 = ldg(tb.cp[0] + xc0); dxy0 = (ldg(tb.dx0 + xc0) - up1) - um1;
+        aw1 = ldg(tb.cm[0] + xc1); ae1 = ldg(tb.cp[0] + xc1); dxy1 = (ldg(tb.dx0 + xc1) - up1) - um1;
     }
+    const int o0 = (y - yb) * L::BX + (x0 - xb);   // used only for live cells, which lie inside the box
     auto slot = [&](int q) { return smem + ((unsigned)q % NS) * L::SLOT; };
     // planes outside the tensor (z < 0 or z >= sz) are never read: complete their barrier without a copy
     auto issue = [&](int q) {
@@ -91,8 +114,12 @@ __global__ void __launch_bounds__(256) k_sor_rb_tma(Geom g, int kc, const __grid
     int issued = min((int)NS, nplanes), waited = 0;
     if (threadIdx.x == 0)
         for (int q = 0; q < issued; q++) issue(q);
-    const int ilo = g.gc, ihi = g.sx - g.gc, jlo = g.gc, jhi = g.sy - g.gc, klo = g.gc, khi = g.sz - g.gc;
+    // write-out: thread t copies cell (i0 + t % 32, j0 + t / 32) of the tile
+    const int wx = i0 + (t & (L::TX - 1)), wy = j0 + t / L::TX;
+    const bool writer = t < L::TX * L::TY && wx < ihi && wy < jhi;
+    const int wo = (wy - yb) * L::BX + (wx - xb);
     const long long sxy = (long long)g.sx * g.sy;
+    T *wp = xout + (long long)wx + (long long)wy * g.sx + (long long)k0 * sxy;   // advanced one plane per write-out
     for (int q = 0; q < nplanes; q++) {
         bool fail = !wait_q(q);
         waited = q + 1;
@@ -103,23 +130,17 @@ __global__ void __launch_bounds__(256) k_sor_rb_tma(Geom g, int kc, const __grid
             const int p = q - h, kp = P0 + p, ring = H - h;
             if (p >= 1 && kp >= max(klo, k0 - ring) && kp < min(khi, k1 + ring)) {
                 const int color = (c1 + h - 1) & 1;
-                T *X0 = (T *)slot(p);
-                const T *Xm = (const T *)slot(p - 1), *Xp = (const T *)slot(p + 1);
-                const T *B0 = (const T *)(slot(p) + L::PB);
-                const T ab = ldg(tb.cm[2] + kp), at = ldg(tb.cp[2] + kp), up2 = ldg(tb.up[2] + kp), um2 = ldg(tb.um[2] + kp);
-                const int xs = i0 - ring, ys = j0 - ring;
-                const int Wr = L::TX + 2 * ring, Hh = L::TY + 2 * ring, M = (Wr + 1) >> 1;
-                for (int s = threadIdx.x; s < Hh * M; s += blockDim.x) {
-                    const int r = s / M, m = s - r * M;
-                    const int y = ys + r;
-                    const int x = xs + 2 * m + ((color ^ (xs + y + kp)) & 1);
-                    if (x >= xs + Wr || x < ilo || x >= ihi || y < jlo || y >= jhi) continue;
-                    const int ox = x - xb, oy = y - yb, o = oy * L::BX + ox;
-                    const T aw = t_aw[ox], ae = t_ae[ox], as = t_as[oy], an = t_an[oy];
-                    const T ac = ((((t_dx[ox] - t_up[oy]) - t_um[oy]) - up2) - um2) * tb.scale;
+                const int e = (color ^ (x0 + y + kp)) & 1;          // the pair's cell of this colour
+                if ((((e ? live1 : live0) >> (h - 1)) & 1u) != 0u) {
+                    T *X0 = (T *)slot(p);
+                    const T *Xm = (const T *)slot(p - 1), *Xp = (const T *)slot(p + 1);
+                    const T *B0 = (const T *)(slot(p) + L::PB);
+                    const T ab = ldg(tb.cm[2] + kp), at = ldg(tb.cp[2] + kp);
+                    const T ac = (((e ? dxy1 : dxy0) - ldg(tb.up[2] + kp)) - ldg(tb.um[2] + kp)) * tb.scale;
+                    const int o = o0 + e;
                     const T xc = X0[o];
-                    const T r7 = ac * xc + ae * X0[o + 1] + aw * X0[o - 1] + an * X0[o + L::BX] + as * X0[o - L::BX] +
-                                 at * Xp[o] + ab * Xm[o];
+                    const T r7 = ac * xc + (e ? ae1 : ae0) * X0[o + 1] + (e ? aw1 : aw0) * X0[o - 1] + an * X0[o + L::BX] +
+                                 as * X0[o - L::BX] + at * Xp[o] + ab * Xm[o];
                     X0[o] = xc + omega * sor_div(B0[o] - r7, ac);
                 }
             }
@@ -127,13 +148,10 @@ __global__ void __launch_bounds__(256) k_sor_rb_tma(Geom g, int kc, const __grid
         }
         // the tile of plane q-H is final
         {
-            const int p = q - H, kp = P0 + p;
-            if (p >= 0 && kp >= k0 && kp < k1) {
-                const T *X0 = (const T *)slot(p);
-                for (int s = threadIdx.x; s < L::TX * L::TY; s += blockDim.x) {
-                    const int x = i0 + (s & (L::TX - 1)), y = j0 + s / L::TX;
-                    if (x < ihi && y < jhi) xout[(long long)x + (long long)y * g.sx + kp * sxy] = X0[(y - yb) * L::BX + (x - xb)];
-                }
+            const int kp = P0 + q - H;
+            if (kp >= k0 && kp < k1) {
+                if (writer) *wp = ((const T *)slot(q - H))[wo];
+                wp += sxy;
             }
         }
         // plane q-H-1 was last read by half sweep H above and by the previous
