@@ -241,7 +241,7 @@ int sor_rb_launch(falm_ctx *ctx, cudaStream_t st, int H, const T *xin, const T *
 
 // ring depth of the multi-field plane stream: keep >= 2 planes in flight and
 // at least two CTAs per SM
-template <typename T, int NF> struct P3Conf { static constexpr int NS = (sizeof(T) == 8 && NF > 1) ? 4 : 6; };
+template <typename T, int NF> struct P3Conf { static constexpr int NS = NF > 1 ? 4 : 6; };
 
 // multi-field radius-1 plane stream over region R (see plane3_tma.cuh);
 // 1 launched, 0 not eligible (row-kernel fallback), <0 launch error

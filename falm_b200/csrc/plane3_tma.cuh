@@ -24,7 +24,8 @@ struct alignas(64) MapSet {
 
 template <typename T, int NF>
 struct P3Layout {
-    static constexpr int TX = 32, TY = 8, BX = 36, BY = 10, PE = BX * BY;
+    static constexpr int RY = 2;   // rows per thread: thread (tx, ty) computes rows ty, ty + 8
+    static constexpr int TX = 32, TY = 8 * RY, BX = 36, BY = TY + 2, PE = BX * BY;
     static constexpr int FB = (PE * (int)sizeof(T) + 127) / 128 * 128;   // one component plane
 };
 
@@ -57,20 +58,28 @@ __global__ void __launch_bounds__(256) k_plane3_tma(Geom g, Region3 R, int org, 
     }
     uint64_t *bar = (uint64_t *)(smem + NS * slot_bytes);
     if (body.skip()) return;
+    constexpr int RY = L::RY;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int i0 = R.i0 + blockIdx.x * L::TX, j0 = R.j0 + blockIdx.y * L::TY;
     const int k0 = R.k0 + blockIdx.z * kc, k1 = min(k0 + kc, R.k1);
-    const int i = i0 + tx, j = j0 + ty;
-    bool active = i < R.i1 && j < R.j1;
+    const int i = i0 + tx;
     const int P0 = k0 - 1, nplanes = (k1 + 1) - P0;
     P3View<T, NF> v;
 #pragma unroll
     for (int f = 0; f < NF; f++) v.foff[f] = foff[f];
     const int xb = box_origin(i0 - org, L::BX, g.sx, 16 / (int)sizeof(T)), yb = box_origin(j0 - 1, L::BY, g.sy, 1);
-    const int ox = min(i, R.i1 - 1) - xb, oy = min(j, R.j1 - 1) - yb;
-    v.o = oy * L::BX + ox;
-    // self-check: the radius-1 neighbourhood of a computed cell lies inside the staged box
-    if (active && (ox < 1 || ox > L::BX - 2 || oy < 1 || oy > L::BY - 2)) { atomicExch(err, 300 + 3); active = false; }
+    const int ox = min(i, R.i1 - 1) - xb;
+    int jr[RY], orr[RY];
+    bool act[RY];
+#pragma unroll
+    for (int r = 0; r < RY; r++) {
+        jr[r] = j0 + ty + 8 * r;
+        act[r] = i < R.i1 && jr[r] < R.j1;
+        const int oy = min(jr[r], R.j1 - 1) - yb;
+        orr[r] = oy * L::BX + ox;
+        // self-check: the radius-1 neighbourhood of a computed cell lies inside the staged box
+        if (act[r] && (ox < 1 || ox > L::BX - 2 || oy < 1 || oy > L::BY - 2)) { atomicExch(err, 300 + 3); act[r] = false; }
+    }
     double acc[NV > 0 ? NV : 1];
 #pragma unroll
     for (int d = 0; d < (NV > 0 ? NV : 1); d++) acc[d] = 0.0;
@@ -119,9 +128,13 @@ __global__ void __launch_bounds__(256) k_plane3_tma(Geom g, Region3 R, int org, 
         v.pl[0] = (const T *)slot(q - 1);
         v.pl[1] = (const T *)slot(q);
         v.pl[2] = (const T *)slot(q + 1);
-        if (active) {
-            const int k = P0 + q;
-            body.cell(i, j, k, g.id(i, j, k), v, acc);
+        const int k = P0 + q;
+#pragma unroll
+        for (int r = 0; r < RY; r++) {
+            if (act[r]) {
+                v.o = orr[r];
+                body.cell(i, jr[r], k, g.id(i, jr[r], k), v, acc);
+            }
         }
     }
     goto reduce;

@@ -15,7 +15,8 @@ namespace fb {
 
 template <typename T>
 struct S7Tile {
-    static constexpr int TX = 32, TY = 8, BX = 36, BY = 10, PE = BX * BY;
+    static constexpr int RY = 2;   // rows per thread: thread (tx, ty) computes rows ty, ty + 8, ...
+    static constexpr int TX = 32, TY = 8 * RY, BX = 36, BY = TY + 2, PE = BX * BY;
     static constexpr int SLOT = (PE * (int)sizeof(T) + 127) / 128 * 128;
 };
 
@@ -42,17 +43,25 @@ __global__ void __launch_bounds__(256) k_s7_tma(Geom g, int kc, const __grid_con
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
     uint64_t *bar = (uint64_t *)(smem + NS * L::SLOT);
     if (body.skip()) return;
+    constexpr int RY = L::RY;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int i0 = g.gc + blockIdx.x * L::TX, j0 = g.gc + blockIdx.y * L::TY;
     const int k0 = g.gc + blockIdx.z * kc, k1 = min(k0 + kc, g.sz - g.gc);
-    const int i = i0 + tx, j = j0 + ty;
-    bool active = i < g.sx - g.gc && j < g.sy - g.gc;
+    const int i = i0 + tx;
     const int P0 = k0 - 1, nplanes = (k1 + 1) - P0;   // planes k0-1 .. k1
     const int xb = box_origin(i0 - 2, L::BX, g.sx, 16 / (int)sizeof(T)), yb = box_origin(j0 - 1, L::BY, g.sy, 1);
-    const int ox = min(i, g.sx - g.gc - 1) - xb, oy = min(j, g.sy - g.gc - 1) - yb;
-    const int o = oy * L::BX + ox;
-    // self-check: the radius-1 neighbourhood of a computed cell lies inside the staged box
-    if (active && (ox < 1 || ox > L::BX - 2 || oy < 1 || oy > L::BY - 2)) { atomicExch(err, 300 + 2); active = false; }
+    const int ox = min(i, g.sx - g.gc - 1) - xb;
+    int jr[RY], orr[RY];
+    bool act[RY];
+#pragma unroll
+    for (int r = 0; r < RY; r++) {
+        jr[r] = j0 + ty + 8 * r;
+        act[r] = i < g.sx - g.gc && jr[r] < g.sy - g.gc;
+        const int oy = min(jr[r], g.sy - g.gc - 1) - yb;
+        orr[r] = oy * L::BX + ox;
+        // self-check: the radius-1 neighbourhood of a computed cell lies inside the staged box
+        if (act[r] && (ox < 1 || ox > L::BX - 2 || oy < 1 || oy > L::BY - 2)) { atomicExch(err, 300 + 2); act[r] = false; }
+    }
     double acc[NV > 0 ? NV : 1];
 #pragma unroll
     for (int d = 0; d < (NV > 0 ? NV : 1); d++) acc[d] = 0.0;
@@ -86,32 +95,44 @@ __global__ void __launch_bounds__(256) k_s7_tma(Geom g, int kc, const __grid_con
     waited = 2;
     const T *pw = body.pw();
     const long long sxy = (long long)g.sx * g.sy;
-    long long cc = g.id(i, j, P0 + 1);   // cell of the first computed plane
-    T pv = (pw && active) ? pw[cc] : T(0);
     const Op7<T> &op = body.op_();
-    const typename Op7<T>::Col col = op.column(min(i, g.sx - g.gc - 1), min(j, g.sy - g.gc - 1));
-    T xm;
+    long long ccr[RY];
+    T pv[RY], xm[RY];
+    typename Op7<T>::Col col[RY];
+#pragma unroll
+    for (int r = 0; r < RY; r++) {
+        ccr[r] = g.id(i, jr[r], P0 + 1);   // cell of the first computed plane
+        pv[r] = (pw && act[r]) ? pw[ccr[r]] : T(0);
+        col[r] = op.column(min(i, g.sx - g.gc - 1), min(jr[r], g.sy - g.gc - 1));
+    }
     if (__syncthreads_or(fail)) goto drain;
-    xm = slot(0)[o];
+#pragma unroll
+    for (int r = 0; r < RY; r++) xm[r] = slot(0)[orr[r]];
     for (int q = 1; q < nplanes - 1; q++) {
-        const T pn = (pw && active && q + 1 < nplanes - 1) ? pw[cc + sxy] : T(0);
+        T pn[RY];
+#pragma unroll
+        for (int r = 0; r < RY; r++) pn[r] = (pw && act[r] && q + 1 < nplanes - 1) ? pw[ccr[r] + sxy] : T(0);
         fail = !wait_q(q + 1);
         waited = q + 2;
         if (__syncthreads_or(fail)) goto drain;
-        if (q - 1 + NS < nplanes) {   // plane q-1 is no longer read (its value is in xm): refill its slot
+        if (q - 1 + NS < nplanes) {   // plane q-1 is no longer read (its values are in xm): refill its slot
             if (threadIdx.x == 0) { fence_proxy_async(); issue(q - 1 + NS); }
             issued = q - 1 + NS + 1;
         }
         const T *X0 = slot(q), *X1 = slot(q + 1);
-        const T xc = X0[o];
-        if (active) {
-            const int k = P0 + q;
-            const Coef7<T> a = op.at_col(col, k, cc);
-            body.cell(i, j, k, cc, a, xc, X0[o + 1], X0[o - 1], X0[o + L::BX], X0[o - L::BX], X1[o], xm, pv, acc);
+        const int k = P0 + q;
+#pragma unroll
+        for (int r = 0; r < RY; r++) {
+            const int o = orr[r];
+            const T xc = X0[o];
+            if (act[r]) {
+                const Coef7<T> a = op.at_col(col[r], k, ccr[r]);
+                body.cell(i, jr[r], k, ccr[r], a, xc, X0[o + 1], X0[o - 1], X0[o + L::BX], X0[o - L::BX], X1[o], xm[r], pv[r], acc);
+            }
+            xm[r] = xc;
+            pv[r] = pn[r];
+            ccr[r] += sxy;
         }
-        xm = xc;
-        pv = pn;
-        cc += sxy;
     }
     goto reduce;
 drain:

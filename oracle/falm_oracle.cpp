@@ -898,3 +898,530 @@ void oracle_step(const or_case *c, double *u, double *uu, double *p, double *nut
 }
 
 } // extern "C"
+
+/* ========================================================================
+ * Discrete adjoint of oracle_step (FP64).  No reference counterpart: this is
+ * the adjoint of this project's own discretisation of the step, used to check
+ * the device adjoint.  The Poisson solve is treated as exact (p = A^-1 rhs),
+ * so its adjoint is one solve with the transposed operator.  Supported:
+ * channel and cavity boundaries, the 4th-order schemes (Upwind3, UTOPIA, KK),
+ * Smagorinsky or no SGS model.
+ * ======================================================================== */
+namespace {
+
+struct ApTape {
+    int inside, I, J, K, seg;
+    double xd, yd, zd, theta, apr, ux, ut, urel2, phi, attack, clv, cdv, chord, fl, fd, fx, ft, sgn;
+    double M[3][3];     /* d uvw_tt / d uvw */
+    double nang[3];
+    int tid, type;
+};
+
+/* recompute the AP state of oracle_alm at time t, keeping what the adjoint needs */
+void alm_tape(const or_case *c, const double *u, double t, std::vector<ApTape> &tp, std::vector<double> &xyz,
+              std::vector<double> &force) {
+    Box b(c);
+    const long N = b.n;
+    const or_alm &a = c->alm;
+    const int apcount = a.n_turbine * a.n_blade * a.n_ap_per_blade;
+    const int nappt = a.n_ap_per_blade * a.n_blade;
+    tp.assign(apcount, ApTape());
+    xyz.assign(3 * apcount, 0.0);
+    force.assign(3 * apcount, 0.0);
+    std::vector<double> angle(3 * a.n_turbine, 0.0), angvel(3 * a.n_turbine, 0.0);
+    for (int tid = 0; tid < a.n_turbine; tid++) {
+        int at = a.angle_type[tid];
+        const double *m = a.motion + 3 * tid;
+        if (at) {
+            angle[3 * tid + at - 1] = m[0] * sin(m[1] * t + m[2]);
+            angvel[3 * tid + at - 1] = m[0] * m[1] * cos(m[1] * t + m[2]);
+        }
+    }
+    const double dr = (a.radius - a.hub_radius) / a.n_ap_per_blade;
+    for (int ap = 0; ap < apcount; ap++) {
+        ApTape &T = tp[ap];
+        int tid = ap / nappt, bid = (ap % nappt) / a.n_ap_per_blade;
+        T.tid = tid; T.type = a.angle_type[tid];
+        double tip = a.tip_rate[tid];
+        double theta = tip * t + (2 * kPi / a.n_blade) * bid;
+        double apr = a.ap_r[ap];
+        T.theta = theta; T.apr = apr;
+        double c1[3] = {a.hub[3 * tid], a.hub[3 * tid + 1] + apr * cos(theta), a.hub[3 * tid + 2] + apr * sin(theta)};
+        double nang[3] = {-angle[3 * tid], -angle[3 * tid + 1], -angle[3 * tid + 2]};
+        for (int d = 0; d < 3; d++) T.nang[d] = nang[d];
+        double c0[3];
+        frame_rotation(c1, nang, a.angle_type[tid], c0);
+        for (int d = 0; d < 3; d++) c0[d] += a.base[3 * tid + d];
+        for (int d = 0; d < 3; d++) xyz[3 * ap + d] = c0[d];
+        int I = find_index(c->x, c0[0], b.sx), J = find_index(c->y, c0[1], b.sy), K = find_index(c->z, c0[2], b.sz);
+        T.I = I; T.J = J; T.K = K;
+        T.inside = (I >= b.gc - 1 && I < b.sx - b.gc - 1 && J >= b.gc - 1 && J < b.sy - b.gc - 1 &&
+                    K >= b.gc - 1 && K < b.sz - b.gc - 1);
+        if (!T.inside) continue;
+        T.xd = fabs(c0[0] - c->x[I]) / fabs(c->x[I + 1] - c->x[I]);
+        T.yd = fabs(c0[1] - c->y[J]) / fabs(c->y[J + 1] - c->y[J]);
+        T.zd = fabs(c0[2] - c->z[K]) / fabs(c->z[K + 1] - c->z[K]);
+        long id[8] = {b.id(I, J, K), b.id(I + 1, J, K), b.id(I, J + 1, K), b.id(I + 1, J + 1, K),
+                      b.id(I, J, K + 1), b.id(I + 1, J, K + 1), b.id(I, J + 1, K + 1), b.id(I + 1, J + 1, K + 1)};
+        double uvw[3];
+        for (int d = 0; d < 3; d++) {
+            const double *ud = u + d * N;
+            uvw[d] = trilinear(T.xd, T.yd, T.zd, ud[id[0]], ud[id[1]], ud[id[2]], ud[id[3]], ud[id[4]], ud[id[5]], ud[id[6]], ud[id[7]]);
+        }
+        double rel[3] = {c0[0] - a.base[3 * tid], c0[1] - a.base[3 * tid + 1], c0[2] - a.base[3 * tid + 2]};
+        double tt[3], t0[3], zero[3] = {0, 0, 0};
+        frame_rotation_dt(rel, uvw, &angle[3 * tid], &angvel[3 * tid], a.angle_type[tid], tt);
+        /* the map uvw -> uvw_tt is affine: its matrix from unit vectors */
+        frame_rotation_dt(rel, zero, &angle[3 * tid], &angvel[3 * tid], a.angle_type[tid], t0);
+        for (int q = 0; q < 3; q++) {
+            double e[3] = {0, 0, 0}, o[3];
+            e[q] = 1.0;
+            frame_rotation_dt(rel, e, &angle[3 * tid], &angvel[3 * tid], a.angle_type[tid], o);
+            for (int d = 0; d < 3; d++) T.M[d][q] = o[d] - t0[d];
+        }
+        T.ux = tt[0];
+        T.ut = tip * apr + tt[1] * sin(theta) - tt[2] * cos(theta);
+        T.urel2 = T.ux * T.ux + T.ut * T.ut;
+        T.phi = atan(T.ux / T.ut);
+        T.chord = a.ap_chord[ap];
+        double twist = a.ap_twist[ap] + a.pitch;
+        T.attack = T.phi * 180. / kPi - twist;
+        T.seg = -1;
+        if (T.attack < a.attack[0]) { T.clv = a.cl[ap]; T.cdv = a.cd[ap]; }
+        else if (T.attack >= a.attack[a.n_attack - 1]) {
+            T.clv = a.cl[ap + (long)(a.n_attack - 1) * apcount]; T.cdv = a.cd[ap + (long)(a.n_attack - 1) * apcount];
+        } else {
+            for (int k = 0; k < a.n_attack - 1; k++)
+                if (a.attack[k] <= T.attack && a.attack[k + 1] > T.attack) {
+                    double pw = (T.attack - a.attack[k]) / (a.attack[k + 1] - a.attack[k]);
+                    T.clv = (1. - pw) * a.cl[ap + (long)k * apcount] + pw * a.cl[ap + (long)(k + 1) * apcount];
+                    T.cdv = (1. - pw) * a.cd[ap + (long)k * apcount] + pw * a.cd[ap + (long)(k + 1) * apcount];
+                    T.seg = k;
+                    break;
+                }
+        }
+        T.fl = .5 * T.clv * T.urel2 * T.chord * dr;
+        T.fd = .5 * T.cdv * T.urel2 * T.chord * dr;
+        T.fx = T.fl * cos(T.phi) + T.fd * sin(T.phi);
+        T.sgn = isign(tip);
+        T.ft = (T.fl * sin(T.phi) - T.fd * sin(T.phi)) * T.sgn;
+        double f_tt[3] = {-T.fx, T.ft * sin(theta), -T.ft * cos(theta)};
+        frame_rotation(f_tt, nang, a.angle_type[tid], &force[3 * ap]);
+    }
+}
+
+/* adjoint of alm_tape + projection + the weighted power wP * sum_t tip_t torque_t:
+   aff is the adjoint of the projected force field (interior); adds to au and the gradients */
+void alm_adjoint(const or_case *c, const std::vector<ApTape> &tp, const std::vector<double> &xyz, const double *aff,
+                 double wP, double *au, double *g_pitch, double *g_chord, double *g_twist) {
+    Box b(c);
+    const long N = b.n;
+    const or_alm &a = c->alm;
+    const int apcount = (int)tp.size();
+    const double dr = (a.radius - a.hub_radius) / a.n_ap_per_blade;
+    const double eps = a.euler_eps;
+    const double eta = 1. / ((eps * sqrt(kPi)) * (eps * sqrt(kPi)) * (eps * sqrt(kPi)));
+    /* adjoint of the projection ff(c) = sum_ap F_ap eta exp(-r^2/eps^2) */
+    std::vector<double> aF(3 * apcount, 0.0);
+    for (int k = b.gc; k < b.sz - b.gc; k++)
+        for (int j = b.gc; j < b.sy - b.gc; j++)
+            for (int i = b.gc; i < b.sx - b.gc; i++) {
+                long cid = b.id(i, j, k);
+                double a0 = aff[cid], a1 = aff[cid + N], a2 = aff[cid + 2 * N];
+                if (a0 == 0 && a1 == 0 && a2 == 0) continue;
+                for (int ap = 0; ap < apcount; ap++) {
+                    double rr2 = SQ(c->x[i] - xyz[3 * ap]) + SQ(c->y[j] - xyz[3 * ap + 1]) + SQ(c->z[k] - xyz[3 * ap + 2]);
+                    double w = eta * exp(-rr2 / SQ(eps));
+                    aF[3 * ap] += a0 * w; aF[3 * ap + 1] += a1 * w; aF[3 * ap + 2] += a2 * w;
+                }
+            }
+    for (int ap = 0; ap < apcount; ap++) {
+        const ApTape &T = tp[ap];
+        if (!T.inside) continue;
+        /* force = R(nang) f_tt: R is orthogonal, its adjoint is the rotation by -nang */
+        double an[3] = {-T.nang[0], -T.nang[1], -T.nang[2]};
+        double aftt[3];
+        /* transpose of frame_rotation by nang = frame_rotation by -nang (single-axis rotations) */
+        frame_rotation(&aF[3 * ap], an, T.type, aftt);
+        double afx = -aftt[0];
+        double aft = aftt[1] * sin(T.theta) - aftt[2] * cos(T.theta);
+        /* objective: wP * tip * |ft| * r */
+        aft += wP * a.tip_rate[T.tid] * (double)isign(T.ft) * T.apr;
+        double aft0 = aft * T.sgn;                       /* ft = ft0 * sgn */
+        double s = sin(T.phi), co = cos(T.phi);
+        double afl = afx * co + aft0 * s;
+        double afd = afx * s - aft0 * s;
+        double aphi = afx * (-T.fl * s + T.fd * co) + aft0 * (T.fl - T.fd) * co;
+        double aclv = afl * .5 * T.urel2 * T.chord * dr, acdv = afd * .5 * T.urel2 * T.chord * dr;
+        double aurel2 = afl * .5 * T.clv * T.chord * dr + afd * .5 * T.cdv * T.chord * dr;
+        double achord = afl * .5 * T.clv * T.urel2 * dr + afd * .5 * T.cdv * T.urel2 * dr;
+        double aattack = 0.0;
+        if (T.seg >= 0) {
+            int k = T.seg;
+            double dA = a.attack[k + 1] - a.attack[k];
+            aattack = aclv * (a.cl[ap + (long)(k + 1) * apcount] - a.cl[ap + (long)k * apcount]) / dA +
+                      acdv * (a.cd[ap + (long)(k + 1) * apcount] - a.cd[ap + (long)k * apcount]) / dA;
+        }
+        aphi += aattack * 180. / kPi;
+        g_twist[ap] += -aattack;
+        *g_pitch += -aattack;
+        g_chord[ap] += achord;
+        /* phi = atan(ux/ut), urel2 = ux^2 + ut^2 */
+        double aux = aphi * T.ut / T.urel2 + 2 * T.ux * aurel2;
+        double aut = -aphi * T.ux / T.urel2 + 2 * T.ut * aurel2;
+        double att[3] = {aux, aut * sin(T.theta), -aut * cos(T.theta)};
+        double auvw[3];
+        for (int q = 0; q < 3; q++) auvw[q] = T.M[0][q] * att[0] + T.M[1][q] * att[1] + T.M[2][q] * att[2];
+        const double xd = T.xd, yd = T.yd, zd = T.zd;
+        const double wts[8] = {(1 - xd) * (1 - yd) * (1 - zd), xd * (1 - yd) * (1 - zd), (1 - xd) * yd * (1 - zd), xd * yd * (1 - zd),
+                               (1 - xd) * (1 - yd) * zd, xd * (1 - yd) * zd, (1 - xd) * yd * zd, xd * yd * zd};
+        const int I = T.I, J = T.J, K = T.K;
+        long id[8] = {b.id(I, J, K), b.id(I + 1, J, K), b.id(I, J + 1, K), b.id(I + 1, J + 1, K),
+                      b.id(I, J, K + 1), b.id(I + 1, J, K + 1), b.id(I, J + 1, K + 1), b.id(I + 1, J + 1, K + 1)};
+        for (int d = 0; d < 3; d++)
+            for (int q = 0; q < 8; q++) au[id[q] + d * N] += auvw[d] * wts[q];
+    }
+}
+
+inline double sgnd(double v) { return (v > 0) - (v < 0); }
+
+}  // namespace
+
+extern "C" {
+
+/* A^T of a 7-column matrix over the interior (entries towards cells outside the interior dropped) */
+void oracle_transpose_matrix(const or_case *c, const double *A, double *AT) {
+    Box b(c);
+    const long N = b.n;
+    memset(AT, 0, sizeof(double) * 7 * N);
+    const int gc = b.gc;
+    auto in = [&](int i, int j, int k) { return i >= gc && i < b.sx - gc && j >= gc && j < b.sy - gc && k >= gc && k < b.sz - gc; };
+    for (int k = gc; k < b.sz - gc; k++)
+        for (int j = gc; j < b.sy - gc; j++)
+            for (int i = gc; i < b.sx - gc; i++) {
+                long cc = b.id(i, j, k);
+                AT[cc] = A[cc];
+                /* columns: c w e s n b t; AT(c, west) = A(west cell, east) */
+                if (in(i - 1, j, k)) AT[cc + N] = A[b.id(i - 1, j, k) + 2 * N];
+                if (in(i + 1, j, k)) AT[cc + 2 * N] = A[b.id(i + 1, j, k) + N];
+                if (in(i, j - 1, k)) AT[cc + 3 * N] = A[b.id(i, j - 1, k) + 4 * N];
+                if (in(i, j + 1, k)) AT[cc + 4 * N] = A[b.id(i, j + 1, k) + 3 * N];
+                if (in(i, j, k - 1)) AT[cc + 5 * N] = A[b.id(i, j, k - 1) + 6 * N];
+                if (in(i, j, k + 1)) AT[cc + 6 * N] = A[b.id(i, j, k + 1) + 5 * N];
+            }
+}
+
+int oracle_step_adjoint(const or_case *c, const double *u0, const double *uu0, const double *nut0, const double *p0,
+                        const double *kx, const double *g, const double *ja, const double *A, const double *AT,
+                        double maxdiag, double t, double wP, double *au, double *auu, double *anut,
+                        double *g_pitch, double *g_chord, double *g_twist) {
+    Box b(c);
+    const long N = b.n;
+    const int gc = b.gc, sx = b.sx, sy = b.sy, sz = b.sz;
+    if (c->adv != OR_ADV_UPWIND3 && c->adv != OR_ADV_UTOPIA && c->adv != OR_ADV_KK) return 1;
+    if (c->sgs != OR_SGS_EMPTY && c->sgs != OR_SGS_SMAGORINSKY) return 1;
+    const double dt = c->dt, ReI = 1.0 / c->Re;
+    const double alpha = c->adv == OR_ADV_UTOPIA ? 1. / 12. : (c->adv == OR_ADV_KK ? 1. / 4. : 1. / 24.);
+    const bool chan = c->bc == OR_BC_CHANNEL;
+    auto interior = [&](int i, int j, int k) { return i >= gc && i < sx - gc && j >= gc && j < sy - gc && k >= gc && k < sz - gc; };
+    auto facemap = [&](int i, int j, int k) { return i >= gc - 1 && i < sx - gc && j >= gc - 1 && j < sy - gc && k >= gc - 1 && k < sz - gc; };
+    /* ---------------- forward recomputation */
+    std::vector<double> ff(3 * N, 0.0), xyz, force;
+    std::vector<ApTape> tp;
+    if (c->alm_on) {
+        alm_tape(c, u0, t, tp, xyz, force);
+        int apcount = (int)tp.size();
+        std::vector<double> x2(3 * apcount), f2(3 * apcount), tq(apcount), th(apcount);
+        double ttq[8], tth[8];
+        oracle_alm(c, u0, ff.data(), t, x2.data(), f2.data(), tq.data(), th.data(), ttq, tth);
+    }
+    std::vector<double> ua(u0, u0 + 3 * N);
+    oracle_pseudo_u(c, u0, u0, uu0, ua.data(), nut0, kx, g, ja, ff.data());
+    std::vector<double> uu1(uu0, uu0 + 3 * N), rhs(N, 0.0), res(N, 0.0), p(p0, p0 + N);
+    oracle_utouu(c, ua.data(), uu1.data(), kx, ja);
+    oracle_uubc(c, uu1.data());
+    oracle_poisson_rhs(c, uu1.data(), rhs.data(), ja, maxdiag);
+    int it; double err;
+    oracle_pbicgstab(c, A, p.data(), rhs.data(), res.data(), &it, &err);
+    oracle_pbc(c, p.data());
+    std::vector<double> un(ua), uun(uu1);
+    oracle_project_p(c, un.data(), un.data(), uun.data(), uun.data(), p.data(), kx, g);
+    oracle_ubc(c, un.data(), u0, t);
+    /* ---------------- reverse */
+    std::vector<double> au0(3 * N, 0.0), auu0(3 * N, 0.0), anut0(N, 0.0);
+    /* nut ghosts (and, without an SGS model, every cell) are not written by the step: identity */
+    for (int k = 0; k < sz; k++)
+        for (int j = 0; j < sy; j++)
+            for (int i = 0; i < sx; i++)
+                if (!interior(i, j, k) || c->sgs == OR_SGS_EMPTY) anut0[b.id(i, j, k)] += anut[b.id(i, j, k)];
+    /* (9) SGS on the new velocity */
+    if (c->sgs == OR_SGS_SMAGORINSKY) {
+        for (int k = gc; k < sz - gc; k++)
+            for (int j = gc; j < sy - gc; j++)
+                for (int i = gc; i < sx - gc; i++) {
+                    long cc = b.id(i, j, k);
+                    double an = anut[cc];
+                    if (an == 0) continue;
+                    long e1 = b.id(i + 1, j, k), w1 = b.id(i - 1, j, k), n1 = b.id(i, j + 1, k), s1 = b.id(i, j - 1, k);
+                    long t1 = b.id(i, j, k + 1), b1 = b.id(i, j, k - 1);
+                    double kk[3] = {kx[cc], kx[cc + N], kx[cc + 2 * N]};
+                    double d[3][3];
+                    for (int m = 0; m < 3; m++) {
+                        const double *um = un.data() + m * N;
+                        d[m][0] = 0.5 * kk[0] * (um[e1] - um[w1]);
+                        d[m][1] = 0.5 * kk[1] * (um[n1] - um[s1]);
+                        d[m][2] = 0.5 * kk[2] * (um[t1] - um[b1]);
+                    }
+                    double dux = d[0][0], duy = d[0][1], duz = d[0][2], dvx = d[1][0], dvy = d[1][1], dvz = d[1][2];
+                    double dwx = d[2][0], dwy = d[2][1], dwz = d[2][2];
+                    double S = 2 * SQ(dux) + 2 * SQ(dvy) + 2 * SQ(dwz) + SQ(duy + dvx) + SQ(dvz + dwy) + SQ(duz + dwx);
+                    double Du = sqrt(S);
+                    if (Du == 0) continue;
+                    double lc = c->Cs * cbrt(ja[cc]);
+                    double aS = an * SQ(lc) * 0.5 / Du;
+                    double ad[3][3];
+                    ad[0][0] = aS * 4 * dux; ad[1][1] = aS * 4 * dvy; ad[2][2] = aS * 4 * dwz;
+                    ad[0][1] = ad[1][0] = aS * 2 * (duy + dvx);
+                    ad[1][2] = ad[2][1] = aS * 2 * (dvz + dwy);
+                    ad[0][2] = ad[2][0] = aS * 2 * (duz + dwx);
+                    for (int m = 0; m < 3; m++) {
+                        double *am = au + m * N;
+                        am[e1] += 0.5 * kk[0] * ad[m][0]; am[w1] -= 0.5 * kk[0] * ad[m][0];
+                        am[n1] += 0.5 * kk[1] * ad[m][1]; am[s1] -= 0.5 * kk[1] * ad[m][1];
+                        am[t1] += 0.5 * kk[2] * ad[m][2]; am[b1] -= 0.5 * kk[2] * ad[m][2];
+                    }
+                }
+    }
+    /* (8) velocity boundary conditions, in reverse order of oracle_ubc */
+    std::vector<char> written(N, 0);
+    if (chan) {
+        for (int j = gc; j < sy - gc; j++)
+            for (int i = gc; i < sx - gc; i++) {
+                long o1 = b.id(i, j, sz - gc), o2 = b.id(i, j, sz - gc + 1), i1 = b.id(i, j, sz - gc - 1);
+                /* slip z+: wb = (u, v, 0) of i1; o1 = wb; o2 = 2 wb - u(i1) */
+                for (int d = 0; d < 2; d++) { au[i1 + d * N] += au[o1 + d * N] + au[o2 + d * N]; }
+                au[i1 + 2 * N] += -au[o2 + 2 * N];
+                for (int d = 0; d < 3; d++) { au[o1 + d * N] = 0; au[o2 + d * N] = 0; }
+                written[o1] = written[o2] = 1;
+                o1 = b.id(i, j, gc - 1); o2 = b.id(i, j, gc - 2); i1 = b.id(i, j, gc);
+                for (int d = 0; d < 3; d++) { au[i1 + d * N] += -au[o2 + d * N]; au[o1 + d * N] = 0; au[o2 + d * N] = 0; }
+                written[o1] = written[o2] = 1;
+            }
+        for (int k = gc; k < sz - gc; k++)
+            for (int i = gc; i < sx - gc; i++) {
+                for (int side = 1; side >= 0; side--) {
+                    long o1, o2, i1;
+                    if (side == 1) { o1 = b.id(i, sy - gc, k); o2 = b.id(i, sy - gc + 1, k); i1 = b.id(i, sy - gc - 1, k); }
+                    else { o1 = b.id(i, gc - 1, k); o2 = b.id(i, gc - 2, k); i1 = b.id(i, gc, k); }
+                    /* slip: (u, 0, w) of i1 */
+                    au[i1] += au[o1] + au[o2];
+                    au[i1 + N] += -au[o2 + N];
+                    au[i1 + 2 * N] += au[o1 + 2 * N] + au[o2 + 2 * N];
+                    for (int d = 0; d < 3; d++) { au[o1 + d * N] = 0; au[o2 + d * N] = 0; }
+                    written[o1] = written[o2] = 1;
+                }
+            }
+        for (int k = gc; k < sz - gc; k++)
+            for (int j = gc; j < sy - gc; j++) {
+                int i = sx - gc;
+                long o1 = b.id(i, j, k), o2 = b.id(i + 1, j, k), i1 = b.id(i - 1, j, k), i2 = b.id(i - 2, j, k);
+                double dxi = 1.0 / (c->x[i] - c->x[i - 1]);
+                for (int d = 0; d < 3; d++) {
+                    double aub = au[o1 + d * N] + 2 * au[o2 + d * N];
+                    au[i1 + d * N] += -au[o2 + d * N];
+                    au0[o1 + d * N] += aub * (1 - dt * 0.5 * dxi * 3);
+                    au0[i1 + d * N] += aub * (dt * 0.5 * dxi * 4);
+                    au0[i2 + d * N] += aub * (-dt * 0.5 * dxi);
+                    au[o1 + d * N] = 0; au[o2 + d * N] = 0;
+                }
+                written[o1] = written[o2] = 1;
+                i = gc - 1;
+                long g1 = b.id(i, j, k), g2 = b.id(i - 1, j, k);
+                for (int d = 0; d < 3; d++) { au[g1 + d * N] = 0; au[g2 + d * N] = 0; }
+                written[g1] = written[g2] = 1;
+            }
+    } else {
+        /* cavity: every face reflects about a wall value (lid constant) */
+        for (int j = gc; j < sy - gc; j++)
+            for (int i = gc; i < sx - gc; i++)
+                for (int d = 0; d < 3; d++) {
+                    double *a = au + d * N;
+                    long g4[4] = {b.id(i, j, gc - 1), b.id(i, j, gc - 2), b.id(i, j, sz - gc), b.id(i, j, sz - gc + 1)};
+                    long s4[4] = {b.id(i, j, gc), b.id(i, j, gc + 1), b.id(i, j, sz - gc - 1), b.id(i, j, sz - gc - 2)};
+                    for (int q = 3; q >= 0; q--) { a[s4[q]] += -a[g4[q]]; a[g4[q]] = 0; written[g4[q]] = 1; }
+                }
+        for (int k = gc; k < sz - gc; k++)
+            for (int i = gc; i < sx - gc; i++)
+                for (int d = 0; d < 3; d++) {
+                    double *a = au + d * N;
+                    long g4[4] = {b.id(i, gc - 1, k), b.id(i, gc - 2, k), b.id(i, sy - gc, k), b.id(i, sy - gc + 1, k)};
+                    long s4[4] = {b.id(i, gc, k), b.id(i, gc + 1, k), b.id(i, sy - gc - 1, k), b.id(i, sy - gc - 2, k)};
+                    for (int q = 3; q >= 0; q--) { a[s4[q]] += -a[g4[q]]; a[g4[q]] = 0; written[g4[q]] = 1; }
+                }
+        for (int k = gc; k < sz - gc; k++)
+            for (int j = gc; j < sy - gc; j++)
+                for (int d = 0; d < 3; d++) {
+                    double *a = au + d * N;
+                    long g4[4] = {b.id(gc - 1, j, k), b.id(gc - 2, j, k), b.id(sx - gc, j, k), b.id(sx - gc + 1, j, k)};
+                    long s4[4] = {b.id(gc, j, k), b.id(gc + 1, j, k), b.id(sx - gc - 1, j, k), b.id(sx - gc - 2, j, k)};
+                    for (int q = 3; q >= 0; q--) { a[s4[q]] += -a[g4[q]]; a[g4[q]] = 0; written[g4[q]] = 1; }
+                }
+    }
+    /* cells the step never writes carry the previous velocity: identity */
+    for (long n = 0; n < N; n++) {
+        int i = (int)(n % sx), j = (int)((n / sx) % sy), k = (int)(n / ((long)sx * sy));
+        if (!interior(i, j, k) && !written[n])
+            for (int d = 0; d < 3; d++) { au0[n + d * N] += au[n + d * N]; au[n + d * N] = 0; }
+    }
+    /* (7) projection: u = ua - dt kx dp/2 (interior), uu = uu1 - dt g dp (face map) */
+    std::vector<double> aua(3 * N, 0.0), auu1(3 * N, 0.0), ap(N, 0.0);
+    for (int k = gc; k < sz - gc; k++)
+        for (int j = gc; j < sy - gc; j++)
+            for (int i = gc; i < sx - gc; i++) {
+                long cc = b.id(i, j, k);
+                long nb[3][2] = {{b.id(i + 1, j, k), b.id(i - 1, j, k)}, {b.id(i, j + 1, k), b.id(i, j - 1, k)}, {b.id(i, j, k + 1), b.id(i, j, k - 1)}};
+                for (int d = 0; d < 3; d++) {
+                    double a = au[cc + d * N];
+                    aua[cc + d * N] += a;
+                    ap[nb[d][0]] += -dt * 0.5 * kx[cc + d * N] * a;
+                    ap[nb[d][1]] += dt * 0.5 * kx[cc + d * N] * a;
+                }
+            }
+    for (long n = 0; n < N; n++) {
+        int i = (int)(n % sx), j = (int)((n / sx) % sy), k = (int)(n / ((long)sx * sy));
+        if (!facemap(i, j, k)) {   /* uu cells outside the face map carry over */
+            for (int d = 0; d < 3; d++) auu0[n + d * N] += auu[n + d * N];
+            continue;
+        }
+        long nb[3] = {b.id(i + 1, j, k), b.id(i, j + 1, k), b.id(i, j, k + 1)};
+        for (int d = 0; d < 3; d++) {
+            double a = auu[n + d * N];
+            auu1[n + d * N] += a;
+            double cf = dt * 0.5 * (g[n + d * N] + g[nb[d] + d * N]);
+            ap[nb[d]] += -cf * a;
+            ap[n] += cf * a;
+        }
+    }
+    /* (5) pressure boundary conditions, in reverse order of oracle_pbc */
+    for (int j = gc; j < sy - gc; j++)
+        for (int i = gc; i < sx - gc; i++) {
+            ap[b.id(i, j, sz - gc - 1)] += ap[b.id(i, j, sz - gc)]; ap[b.id(i, j, sz - gc)] = 0;
+            ap[b.id(i, j, gc)] += ap[b.id(i, j, gc - 1)]; ap[b.id(i, j, gc - 1)] = 0;
+        }
+    for (int k = gc; k < sz - gc; k++)
+        for (int i = gc; i < sx - gc; i++) {
+            ap[b.id(i, sy - gc - 1, k)] += ap[b.id(i, sy - gc, k)]; ap[b.id(i, sy - gc, k)] = 0;
+            ap[b.id(i, gc, k)] += ap[b.id(i, gc - 1, k)]; ap[b.id(i, gc - 1, k)] = 0;
+        }
+    for (int k = gc; k < sz - gc; k++)
+        for (int j = gc; j < sy - gc; j++) {
+            if (chan) ap[b.id(sx - gc, j, k)] = 0;
+            else { ap[b.id(sx - gc - 1, j, k)] += ap[b.id(sx - gc, j, k)]; ap[b.id(sx - gc, j, k)] = 0; }
+            ap[b.id(gc, j, k)] += ap[b.id(gc - 1, j, k)]; ap[b.id(gc - 1, j, k)] = 0;
+        }
+    for (long n = 0; n < N; n++) {   /* remaining ghost entries of p are not read by the projection of interior data */
+        int i = (int)(n % sx), j = (int)((n / sx) % sy), k = (int)(n / ((long)sx * sy));
+        if (!interior(i, j, k)) ap[n] = 0;
+    }
+    /* (4) transposed Poisson solve: arhs = A^-T ap */
+    std::vector<double> arhs(N, 0.0), r2(N, 0.0);
+    oracle_pbicgstab(c, AT, arhs.data(), ap.data(), r2.data(), &it, &err);
+    /* (3) rhs = div(uu1)/ja / (dt maxdiag) on the interior */
+    const double scale = 1.0 / (dt * maxdiag);
+    for (int k = gc; k < sz - gc; k++)
+        for (int j = gc; j < sy - gc; j++)
+            for (int i = gc; i < sx - gc; i++) {
+                long cc = b.id(i, j, k);
+                double a = arhs[cc] * scale / ja[cc];
+                auu1[cc] += a; auu1[b.id(i - 1, j, k)] -= a;
+                auu1[cc + N] += a; auu1[b.id(i, j - 1, k) + N] -= a;
+                auu1[cc + 2 * N] += a; auu1[b.id(i, j, k - 1) + 2 * N] -= a;
+            }
+    if (c->bc == OR_BC_CAVITY) {   /* uubc zeroes the wall-normal faces */
+        for (int k = gc; k < sz - gc; k++)
+            for (int j = gc; j < sy - gc; j++) { auu1[b.id(gc - 1, j, k)] = 0; auu1[b.id(sx - gc - 1, j, k)] = 0; }
+        for (int k = gc; k < sz - gc; k++)
+            for (int i = gc; i < sx - gc; i++) { auu1[b.id(i, gc - 1, k) + N] = 0; auu1[b.id(i, sy - gc - 1, k) + N] = 0; }
+        for (int j = gc; j < sy - gc; j++)
+            for (int i = gc; i < sx - gc; i++) { auu1[b.id(i, j, gc - 1) + 2 * N] = 0; auu1[b.id(i, j, sz - gc - 1) + 2 * N] = 0; }
+    }
+    /* UtoUU: uu1 = 0.5 (uc(c) + uc(c+e_d)) on the face map, uc = ja kx ua on [gc-1, s-gc] */
+    for (int k = gc - 1; k < sz - gc; k++)
+        for (int j = gc - 1; j < sy - gc; j++)
+            for (int i = gc - 1; i < sx - gc; i++) {
+                long cc = b.id(i, j, k);
+                long nb[3] = {b.id(i + 1, j, k), b.id(i, j + 1, k), b.id(i, j, k + 1)};
+                for (int d = 0; d < 3; d++) {
+                    double a = 0.5 * auu1[cc + d * N];
+                    aua[cc + d * N] += a * ja[cc] * kx[cc + d * N];
+                    aua[nb[d] + d * N] += a * ja[nb[d]] * kx[nb[d] + d * N];
+                }
+            }
+    /* (2) pseudo-velocity: ua = u0 + dt(-adv + vis + ff) on the interior; ghosts of ua are u0's */
+    std::vector<double> aff(3 * N, 0.0);
+    for (long n = 0; n < N; n++) {
+        int i = (int)(n % sx), j = (int)((n / sx) % sy), k = (int)(n / ((long)sx * sy));
+        if (!interior(i, j, k))
+            for (int d = 0; d < 3; d++) au0[n + d * N] += aua[n + d * N];
+    }
+    for (int k = gc; k < sz - gc; k++)
+        for (int j = gc; j < sy - gc; j++)
+            for (int i = gc; i < sx - gc; i++) {
+                long cc = b.id(i, j, k);
+                long e1 = b.id(i + 1, j, k), w1 = b.id(i - 1, j, k), n1 = b.id(i, j + 1, k), s1 = b.id(i, j - 1, k);
+                long t1 = b.id(i, j, k + 1), b1 = b.id(i, j, k - 1);
+                long e2 = b.id(i + 2, j, k), w2 = b.id(i - 2, j, k), n2 = b.id(i, j + 2, k), s2 = b.id(i, j - 2, k);
+                long t2 = b.id(i, j, k + 2), b2 = b.id(i, j, k - 2);
+                const long nbp[3][2] = {{e1, e2}, {n1, n2}, {t1, t2}}, nbm[3][2] = {{w1, w2}, {s1, s2}, {b1, b2}};
+                const long facep[3] = {cc, cc + N, cc + 2 * N}, facem[3] = {w1, s1 + N, b1 + 2 * N};
+                const long gm[3] = {w1, s1, b1}, gp[3] = {e1, n1, t1};
+                double jac = ja[cc];
+                double Uc[3], Ua[3];
+                for (int q = 0; q < 3; q++) { Uc[q] = u0[cc + q * N] * kx[cc + q * N]; Ua[q] = fabs(Uc[q]); }
+                double aUa[3] = {0, 0, 0};
+                for (int d = 0; d < 3; d++) {
+                    double a = aua[cc + d * N];
+                    if (a == 0) continue;
+                    const double *ud = u0 + d * N;
+                    double *aud = au0.data() + d * N;
+                    aud[cc] += a;
+                    aff[cc + d * N] += dt * a;
+                    double aadv = -dt * a, avis = dt * a / (2 * jac);
+                    double ucc = ud[cc];
+                    for (int ax = 0; ax < 3; ax++) {
+                        double up1 = ud[nbp[ax][0]], up2 = ud[nbp[ax][1]], um1 = ud[nbm[ax][0]], um2 = ud[nbm[ax][1]];
+                        double JP = uu0[facep[ax]], JM = uu0[facem[ax]];
+                        double L = -up2 + 27 * up1 - 27 * ucc + um1, R = -up1 + 27 * ucc - 27 * um1 + um2;
+                        double D = up2 - 4 * up1 + 6 * ucc - 4 * um1 + um2;
+                        double f = 0.5 / (24. * jac);
+                        auu0[facep[ax]] += aadv * f * L;
+                        auu0[facem[ax]] += aadv * f * R;
+                        aUa[ax] += aadv * D * alpha;
+                        double s = Ua[ax] * alpha;
+                        aud[nbp[ax][1]] += aadv * (-f * JP + s);
+                        aud[nbp[ax][0]] += aadv * (f * (27 * JP - JM) - 4 * s);
+                        aud[cc] += aadv * (f * (-27 * JP + 27 * JM) + 6 * s);
+                        aud[nbm[ax][0]] += aadv * (f * (JP - 27 * JM) - 4 * s);
+                        aud[nbm[ax][1]] += aadv * (f * JM + s);
+                        /* diffusion faces +ax and -ax */
+                        double Gp = g[cc + ax * N] + g[gp[ax] + ax * N], Gm = g[cc + ax * N] + g[gm[ax] + ax * N];
+                        double Np = ReI + 0.5 * (nut0[cc] + nut0[gp[ax]]), Nm = ReI + 0.5 * (nut0[cc] + nut0[gm[ax]]);
+                        double dp = up1 - ucc, dm = ucc - um1;
+                        aud[nbp[ax][0]] += avis * Gp * Np; aud[cc] -= avis * Gp * Np;
+                        aud[cc] -= avis * Gm * Nm; aud[nbm[ax][0]] += avis * Gm * Nm;
+                        anut0[cc] += avis * 0.5 * (Gp * dp - Gm * dm);
+                        anut0[gp[ax]] += avis * 0.5 * Gp * dp;
+                        anut0[gm[ax]] -= avis * 0.5 * Gm * dm;
+                    }
+                }
+                for (int q = 0; q < 3; q++) au0[cc + q * N] += aUa[q] * sgnd(Uc[q]) * kx[cc + q * N];
+            }
+    /* (1) ALM force and the power term of the objective */
+    if (c->alm_on) alm_adjoint(c, tp, xyz, aff.data(), wP, au0.data(), g_pitch, g_chord, g_twist);
+    memcpy(au, au0.data(), sizeof(double) * 3 * N);
+    memcpy(auu, auu0.data(), sizeof(double) * 3 * N);
+    memcpy(anut, anut0.data(), sizeof(double) * N);
+    return 0;
+}
+
+} // extern "C"

@@ -104,6 +104,20 @@ void oracle_step(const or_case *c, double *u, double *uu, double *p, double *nut
                  double t, or_stats *st);
 int oracle_num_threads(void);
 
+/* Discrete adjoint of oracle_step (no reference counterpart; FP64, exact
+ * Poisson solve).  u0, uu0, nut0, p0: state at the start of the step; t: the
+ * step's time; wP: weight of this step's rotor power sum_t tip_t torque_t in
+ * the objective.  au, auu, anut: adjoint of the state after the step on
+ * entry, of the state before it on return.  The gradients of the objective
+ * with respect to the collective pitch [deg] and the per-AP chord and twist
+ * [deg] are added into g_pitch, g_chord, g_twist.  AT: oracle_transpose_matrix(A).
+ * Returns 1 for an unsupported scheme or SGS model. */
+void oracle_transpose_matrix(const or_case *c, const double *A, double *AT);
+int oracle_step_adjoint(const or_case *c, const double *u0, const double *uu0, const double *nut0, const double *p0,
+                        const double *kx, const double *g, const double *ja, const double *A, const double *AT,
+                        double maxdiag, double t, double wP, double *au, double *auu, double *anut,
+                        double *g_pitch, double *g_chord, double *g_twist);
+
 #ifdef __cplusplus
 }
 #endif

@@ -112,6 +112,8 @@ class Oracle:
             "oracle_alm": [C, dp, dp, D, dp, dp, dp, dp, dp, dp],
             "oracle_step": [C, dp, dp, dp, dp, dp, dp, dp, dp, dp, D, D, ctypes.POINTER(OrStats)],
             "oracle_num_threads": [],
+            "oracle_transpose_matrix": [C, dp, dp],
+            "oracle_step_adjoint": [C, dp, dp, dp, dp, dp, dp, dp, dp, dp, D, D, D, dp, dp, dp, dp, dp, dp],
         }
         for k, v in sig.items():
             getattr(L, k).argtypes = v
@@ -121,7 +123,7 @@ class Oracle:
         for k in ("oracle_metrics", "oracle_pseudo_u", "oracle_utouu", "oracle_divergence", "oracle_poisson_rhs",
                   "oracle_project_p", "oracle_sgs", "oracle_mv", "oracle_res", "oracle_sor_sweep",
                   "oracle_pbicgstab", "oracle_ubc", "oracle_pbc", "oracle_uubc", "oracle_build_aps",
-                  "oracle_alm", "oracle_step"):
+                  "oracle_alm", "oracle_step", "oracle_transpose_matrix"):
             getattr(L, k).restype = None
 
     def threads(self):
@@ -153,6 +155,44 @@ class Oracle:
         it, err = ctypes.c_int(), ctypes.c_double()
         self.L.oracle_pbicgstab(ctypes.byref(cs.c), _p(A), _p(x), _p(b), _p(r), ctypes.byref(it), ctypes.byref(err))
         return it.value, err.value
+
+    def power(self, cs, stats):
+        """rotor power of a step: sum over turbines of torque * tip rate (src/alm/alm.h:133)"""
+        tip = cs.alm_arrays["tip_rate"]
+        return float(sum(tq * tr for tq, tr in zip(stats["torque"], tip)))
+
+    def objective(self, cs, m, st0, steps, it0):
+        """J = mean rotor power over `steps` steps from state st0 (step n at time (it0 + n) dt)"""
+        st = {k: v.copy() for k, v in st0.items()}
+        J = 0.0
+        for q in range(steps):
+            J += self.power(cs, self.step(cs, st, m, (it0 + q + 1) * cs.case.dt)) / steps
+        return J
+
+    def adjoint(self, cs, m, st0, steps, it0):
+        """J and its gradient with respect to (collective pitch, per-AP chord, per-AP
+        twist) by the discrete adjoint of the steps (all states kept in memory)"""
+        c = ctypes.byref(cs.c)
+        n = cs.case.grid.n
+        AT = np.zeros(7 * n)
+        self.L.oracle_transpose_matrix(c, _p(m["A"]), _p(AT))
+        st = {k: v.copy() for k, v in st0.items()}
+        states, J = [], 0.0
+        for q in range(steps):
+            states.append({k: st[k].copy() for k in ("u", "uu", "nut", "p")})
+            J += self.power(cs, self.step(cs, st, m, (it0 + q + 1) * cs.case.dt)) / steps
+        a = cs.c.alm
+        apc = a.n_turbine * a.n_blade * a.n_ap_per_blade
+        gp, gch, gtw = np.zeros(1), np.zeros(apc), np.zeros(apc)
+        au, auu, anut = np.zeros(3 * n), np.zeros(3 * n), np.zeros(n)
+        for q in reversed(range(steps)):
+            S = states[q]
+            rc = self.L.oracle_step_adjoint(c, _p(S["u"]), _p(S["uu"]), _p(S["nut"]), _p(S["p"]), _p(m["kx"]), _p(m["g"]),
+                                            _p(m["ja"]), _p(m["A"]), _p(AT), m["maxdiag"], (it0 + q + 1) * cs.case.dt,
+                                            1.0 / steps, _p(au), _p(auu), _p(anut), _p(gp), _p(gch), _p(gtw))
+            if rc:
+                raise ValueError("oracle_step_adjoint: unsupported scheme or SGS model")
+        return J, float(gp[0]), gch, gtw
 
     def alm(self, cs, u, ff, t):
         a = cs.c.alm
