@@ -41,6 +41,7 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward cost ratio")
     return ap.parse_args()
 
 
@@ -300,6 +301,42 @@ def cpu_baseline(args):
                       f"uniform inflow) after one warm-up step, CPU oracle on {O.threads()} threads"}
 
 
+# ---------------------------------------------------------------- adjoint cost
+def adjoint_ratio(steps=200, checkpoint=20):
+    """cost of the mean-power gradient by the discrete adjoint (forward with
+    checkpoints, recomputation, reverse sweep) over the plain forward window, on
+    the 128x64x64 adjoint case (rotor radius 10 cells, 32 APs per blade), FP64"""
+    import torch
+    from falm_b200 import adjoint as A
+    from falm_b200 import cases
+    from falm_b200.driver import Simulation
+    case = cases.adjoint_case().with_inflow()
+    sim = Simulation(case, "fp64")
+    for _ in range(10):
+        sim.step()
+    start = (sim.it, A._clone(sim))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    J = A.objective(sim, steps)
+    torch.cuda.synchronize()
+    t_fwd = time.perf_counter() - t0
+    A._restore(sim, start[1])
+    sim.it = start[0]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    J2, gp, gc, gt = A.mean_power_gradient(sim, steps, checkpoint)
+    torch.cuda.synchronize()
+    t_adj = time.perf_counter() - t0
+    sim.close()
+    g = case.grid.interior
+    return {"workload": f"{case.name} {g[0]}x{g[1]}x{g[2]} + rotor (R = 10 cells, 3x32 APs), FP64, tol {case.tol}",
+            "objective": f"mean rotor power over {steps} steps", "checkpoint_every": checkpoint,
+            "forward_ms": 1e3 * t_fwd, "gradient_ms": 1e3 * t_adj, "ratio": t_adj / t_fwd,
+            "J": J2, "dJ_dpitch": gp, "n_params": 1 + len(gc) + len(gt),
+            "note": "gradient_ms = forward window with checkpoints + segment recomputation + reverse sweep "
+                    "(transposed Poisson solve to 1e-12 relative); wall clock, each step synchronises"}
+
+
 # ---------------------------------------------------------------- reference arm
 def run_reference(args, rank, world, local):
     from falm_b200 import cases
@@ -392,6 +429,11 @@ def main():
         line["mixed_over_fp64"] = r["mixed_over_fp64"]
     if cb:
         line["cpu_baseline"] = cb
+    if world == 1 and not args.no_adjoint:
+        try:
+            line["adjoint"] = adjoint_ratio()
+        except Exception as e:   # reported, never required
+            line["adjoint"] = {"error": str(e)}
     print(json.dumps(line), flush=True)
 
 

@@ -1,0 +1,123 @@
+"""Gradients of the time-averaged rotor power by the discrete adjoint of the step.
+
+The objective over a window of M steps starting from a state S0 is
+
+    J = (1/M) sum_{n=1..M} P_n,   P_n = sum over turbines of torque x tip rate
+
+(the power of src/alm/alm.h:133, evaluated by the ALM at the start of step n).
+`mean_power_gradient` runs the window forward keeping a checkpoint of the
+state every `checkpoint` steps, then sweeps back: each segment is recomputed
+from its checkpoint (its states held on the device) and falm_step_adjoint
+maps the adjoint state back one step at a time, accumulating dJ/d(collective
+pitch, per-AP chord, per-AP twist).  Memory: one checkpoint per segment plus
+the states of one segment.
+
+`MeanPower` wraps the same computation as a torch.autograd.Function; it is
+used only to check the gradients (torch.autograd.gradcheck-style comparisons),
+not as a training path.
+"""
+import numpy as np
+
+FIELDS = ("u", "uu", "p", "nut")
+
+
+def _power(sim, stats):
+    tip = np.asarray(sim.case.alm.tip_rate, dtype=np.float64)
+    return float(sum(tq * tr for tq, tr in zip(stats["torque"], tip)))
+
+
+def _clone(sim):
+    return {k: getattr(sim, k).clone() for k in FIELDS}
+
+
+def _restore(sim, st):
+    for k in FIELDS:
+        getattr(sim, k).copy_(st[k])
+
+
+def objective(sim, steps):
+    """J over the next `steps` steps of sim (advances sim)"""
+    J = 0.0
+    for _ in range(steps):
+        J += _power(sim, sim.step()) / steps
+    return J
+
+
+def mean_power_gradient(sim, steps, checkpoint=20):
+    """J over the next `steps` steps of sim and its gradient (pitch, chord[apcount],
+    twist[apcount]) by the discrete adjoint; sim ends after the window"""
+    ctx = sim.ctx
+    torch = ctx.torch
+    if ctx.precision != "fp64":
+        raise ValueError("the discrete adjoint runs in FP64 contexts")
+    apc = sim.case.alm.apcount
+    ckpts, J = [], 0.0
+    it0 = sim.it
+    for q in range(steps):
+        if q % checkpoint == 0:
+            ckpts.append((sim.it, _clone(sim)))
+        J += _power(sim, sim.step()) / steps
+    end_state, end_it = _clone(sim), sim.it
+    n = sim.case.grid.n
+    dev, dt = ctx.device, sim.case.dt
+    au = torch.zeros(3 * n, dtype=torch.float64, device=dev)
+    auu = torch.zeros(3 * n, dtype=torch.float64, device=dev)
+    anut = torch.zeros(n, dtype=torch.float64, device=dev)
+    grad = torch.zeros(1 + 2 * apc, dtype=torch.float64, device=dev)
+    for s in reversed(range(len(ckpts))):
+        it_s, st_s = ckpts[s]
+        seg = min(checkpoint, it0 + steps - it_s)
+        # recompute the segment, keeping the state at the start of each step
+        _restore(sim, st_s)
+        sim.it = it_s
+        states = []
+        for q in range(seg):
+            states.append(_clone(sim))
+            sim.step()
+        states.append({"u": sim.u.clone()})   # the velocity after the segment's last step
+        for q in reversed(range(seg)):
+            S = states[q]
+            ctx.step_adjoint(S["u"], S["uu"], S["p"], S["nut"], dt, (it_s + q + 1) * dt, 1.0 / steps, au, auu, anut, grad,
+                             u_after=states[q + 1]["u"])
+    _restore(sim, end_state)
+    sim.it = end_it
+    g = grad.cpu().numpy()
+    return J, float(g[0]), g[1:1 + apc].copy(), g[1 + apc:].copy()
+
+
+def _set_params(sim, params):
+    """apply (pitch, chord[apcount], twist[apcount]) to the simulation's ALM"""
+    alm = sim.case.alm
+    apc = alm.apcount
+    p = np.asarray(params, dtype=np.float64)
+    alm.pitch = float(p[0])
+    alm.aps["chord"] = p[1:1 + apc].copy()
+    alm.aps["twist"] = p[1 + apc:1 + 2 * apc].copy()
+    sim.ctx.alm_init(alm)
+
+
+def parameters(sim):
+    alm = sim.case.alm
+    return np.concatenate([[alm.pitch], np.asarray(alm.aps["chord"], dtype=np.float64),
+                           np.asarray(alm.aps["twist"], dtype=np.float64)])
+
+
+def make_mean_power(torch):
+    """the torch.autograd.Function (built lazily so that importing this module needs no torch)"""
+
+    class MeanPower(torch.autograd.Function):
+        @staticmethod
+        def forward(fctx, params, sim, start, steps, checkpoint):
+            _set_params(sim, params.detach().cpu().numpy())
+            _restore(sim, start[1])
+            sim.it = start[0]
+            J, gp, gc, gt = mean_power_gradient(sim, steps, checkpoint)
+            fctx.save_for_backward(torch.as_tensor(np.concatenate([[gp], gc, gt]), dtype=params.dtype))
+            return params.new_tensor(J)
+
+        @staticmethod
+        def backward(fctx, gJ):
+            (g,) = fctx.saved_tensors
+            return gJ * g, None, None, None, None
+
+    return MeanPower

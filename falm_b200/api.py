@@ -218,6 +218,16 @@ class Context:
         return {"it": st.it, "err": st.err, "divnorm": st.divnorm, "outer": st.outer, "status": st.status,
                 "torque": list(st.torque[:n]), "thrust": list(st.thrust[:n])}
 
+    def step_adjoint(self, u, uu, p, nut, dt, t, w_power, au, auu, anut, grad, u_after=None):
+        """falm_step_adjoint: maps the adjoint of the state after the step (au, auu,
+        anut, in place) to the state before it and adds the step's gradient into grad;
+        u_after (the velocity after the step) spares the recomputation of the step"""
+        fl = L.Fields(_ptr(u), _ptr(uu), _ptr(p), _ptr(nut), None)
+        f1 = L.Fields(_ptr(u_after), None, None, None, None) if u_after is not None else None
+        self._check(self.lib.falm_step_adjoint(self.h, ctypes.byref(fl), ctypes.byref(f1) if f1 is not None else None, dt, t,
+                                               w_power, _ptr(au), _ptr(auu), _ptr(anut), _ptr(grad), self.stream()),
+                    "step_adjoint")
+
 
 def build_aps(stations, n_turbine, n_blade, n_ap_per_blade, radius, hub_radius):
     """BladeHandler::buildAP (src/alm/bladeHandler.h:16-104) through the C ABI (host only)."""

@@ -22,6 +22,7 @@
 #include "poisson_tma.cuh"
 #include "plane3_tma.cuh"
 #include "sor_rb_tma.cuh"
+#include "adjoint.cuh"
 #include <cudaTypedefs.h>
 
 using namespace fb;
@@ -722,6 +723,7 @@ int falm_destroy(falm_ctx *ctx) {
     cudaFree(ctx->metric_mem);
     cudaFree(ctx->op_mem);
     cudaFree(ctx->work_mem);
+    cudaFree(ctx->adj_mem);
     cudaFree(ctx->red.partials);
     cudaFree(ctx->red.counter);
     cudaFree(ctx->scal);
@@ -1292,5 +1294,117 @@ extern "C" int falm_mv_dot_static(int sx, int sy, int sz, int gc, int precision,
         cudaGetLastError();
         return FALM_ERR_CUDA;
     }
+    return FALM_OK;
+}
+
+// ---------------------------------------------------------------- discrete adjoint of the step
+namespace {
+
+struct AdjWork {
+    double *uc, *uuc, *pc, *nutc, *au0, *auu0, *anut0, *aua, *auu1, *aff, *ap, *arhs, *r, *AT, *aF;
+};
+
+__global__ void k_adj_zero_interior(Geom g, double *a) {
+    ADJ_FOR_BOX(g.gc, g.sx - g.gc, g.gc, g.sy - g.gc, g.gc, g.sz - g.gc, i, j, k) { a[g.id(i, j, k)] = 0; }
+}
+
+int adj_work(falm_ctx *ctx, AdjWork *w) {
+    const size_t n = (size_t)ctx->geo.n;
+    const size_t apc = ctx->alm_on ? (size_t)ctx->alm.apcount : 0;
+    const size_t counts[15] = {3 * n, 3 * n, n, n, 3 * n, 3 * n, n, 3 * n, 3 * n, 3 * n, n, n, n, 7 * n, 3 * apc + 1};
+    size_t bytes = 0;
+    for (int q = 0; q < 15; q++) bytes += (counts[q] * sizeof(double) + 255) / 256 * 256;
+    if (!ctx->adj_mem) {
+        if (cudaMalloc(&ctx->adj_mem, bytes) != cudaSuccess) { cudaGetLastError(); ctx->adj_mem = nullptr; return fail(ctx, FALM_ERR_ALLOC, "step_adjoint: workspace"); }
+    }
+    char *p = (char *)ctx->adj_mem;
+    double **dst[15] = {&w->uc, &w->uuc, &w->pc, &w->nutc, &w->au0, &w->auu0, &w->anut0, &w->aua, &w->auu1, &w->aff, &w->ap,
+                        &w->arhs, &w->r, &w->AT, &w->aF};
+    for (int q = 0; q < 15; q++) { *dst[q] = (double *)p; p += (counts[q] * sizeof(double) + 255) / 256 * 256; }
+    return FALM_OK;
+}
+
+}  // namespace
+
+extern "C" int falm_step_adjoint(falm_ctx *ctx, const falm_fields *f0, const falm_fields *f1, double dt, double t, double w_power,
+                                 void *au, void *auu, void *anut, double *grad, void *stream) {
+    if (!ctx || !f0 || !f0->u || !f0->uu || !f0->p || !f0->nut || !au || !auu || !anut || !grad || !(dt > 0)) return FALM_ERR_ARG;
+    if (ctx->precision != FALM_FP64) return fail(ctx, FALM_ERR_ARG, "step_adjoint: FP64 contexts only");
+    if (ctx->adv != FALM_ADV_UPWIND3 && ctx->adv != FALM_ADV_UTOPIA && ctx->adv != FALM_ADV_KK)
+        return fail(ctx, FALM_ERR_ARG, "step_adjoint: the 4th-order advection schemes (Upwind3, UTOPIA, KK) only");
+    if (ctx->sgs != FALM_SGS_EMPTY && ctx->sgs != FALM_SGS_SMAGORINSKY) return fail(ctx, FALM_ERR_ARG, "step_adjoint: Smagorinsky or no SGS model only");
+    int rc = ensure_work(ctx);
+    if (rc) return rc;
+    AdjWork w;
+    if ((rc = adj_work(ctx, &w))) return rc;
+    const Geom &g = ctx->geo;
+    const size_t n = (size_t)g.n, nb = n * sizeof(double);
+    cudaStream_t st = S(stream);
+    const double *un;
+    if (f1 && f1->u) {
+        // the state after the step is given: only the ALM state of the step is needed again
+        un = (const double *)f1->u;
+        if (ctx->alm_on && (rc = alm_run_t<double>(ctx, (const double *)f0->u, nullptr, t, st))) return rc;
+    } else {
+        // forward recomputation of the step on copies of the state
+        CK(cudaMemcpyAsync(w.uc, f0->u, 3 * nb, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(w.uuc, f0->uu, 3 * nb, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(w.pc, f0->p, nb, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(w.nutc, f0->nut, nb, cudaMemcpyDeviceToDevice, st));
+        falm_fields fc{w.uc, w.uuc, w.pc, w.nutc, nullptr};
+        falm_step_stats sst;
+        if ((rc = step_t<double>(ctx, &fc, dt, t, st, &sst))) return rc;
+        un = w.uc;
+    }
+    // reverse sweep
+    for (double *z : {w.au0, w.auu0, w.aua, w.auu1, w.aff}) CK(cudaMemsetAsync(z, 0, 3 * nb, st));
+    for (double *z : {w.ap, w.arhs}) CK(cudaMemsetAsync(z, 0, nb, st));
+    CK(cudaMemcpyAsync(w.anut0, anut, nb, cudaMemcpyDeviceToDevice, st));
+    const int grid = ctx->sm_count * 8;
+    const MetricView<double> mv = mview<double>(ctx);
+    double *pu = (double *)au, *puu = (double *)auu, *pnut = (double *)anut;
+    if (ctx->sgs == FALM_SGS_SMAGORINSKY) {
+        LAUNCH(FALM_K_OTHER, st, k_adj_zero_interior<<<grid, 256, 0, st>>>(g, w.anut0));
+        LAUNCH(FALM_K_OTHER, st, k_adj_sgs<<<grid, 256, 0, st>>>(g, mv, un, pnut, pu, ctx->Cs));
+    }
+    LAUNCH(FALM_K_OTHER, st, k_adj_ubc<<<dim3(64, 3), 256, 0, st>>>(g, ctx->bc_kind, pu, w.au0, ctx->m64.x[0], dt));
+    LAUNCH(FALM_K_OTHER, st, k_adj_carry_edges<<<grid, 256, 0, st>>>(g, pu, w.au0, 3));
+    LAUNCH(FALM_K_OTHER, st, k_adj_project<<<grid, 256, 0, st>>>(g, mv, pu, puu, w.aua, w.auu1, w.auu0, w.ap, dt));
+    LAUNCH(FALM_K_OTHER, st, k_adj_pbc<<<dim3(64, 3), 256, 0, st>>>(g, ctx->bc_kind, w.ap));
+    LAUNCH(FALM_K_OTHER, st, k_adj_zero_ghosts<<<grid, 256, 0, st>>>(g, w.ap));
+    // transposed Poisson solve, to 1e-12 of the adjoint right-hand side's norm
+    LAUNCH(FALM_K_OTHER, st, k_adj_transpose_op<<<grid, 256, 0, st>>>(g, op7<double>(ctx), w.AT));
+    double apn = 0.0;
+    if ((rc = dot_t<double>(ctx, w.ap, w.ap, 1, &apn, st))) return rc;
+    if (apn > 0) {
+        const void *a_saved = ctx->A_explicit;
+        const double tol_saved = ctx->tol;
+        ctx->A_explicit = w.AT;
+        ctx->tol = 1e-12 * sqrt(apn) / ((double)g.nx * g.ny * g.nz);
+        int it = 0, outer = 0;
+        double err = 0;
+        rc = solve_t<double>(ctx, w.arhs, w.ap, w.r, st, &it, &err, &outer);
+        ctx->A_explicit = a_saved;
+        ctx->tol = tol_saved;
+        if (rc) return rc;
+    }
+    const double scale = 1.0 / (dt * ctx->maxdiag);
+    LAUNCH(FALM_K_OTHER, st, k_adj_rhs<<<grid, 256, 0, st>>>(g, mv, w.arhs, w.auu1, scale));
+    if (ctx->bc_kind == FALM_BC_CAVITY) LAUNCH(FALM_K_OTHER, st, k_adj_uubc<<<grid, 256, 0, st>>>(g, w.auu1));
+    LAUNCH(FALM_K_OTHER, st, k_adj_utouu<<<grid, 256, 0, st>>>(g, mv, w.auu1, w.aua));
+    LAUNCH(FALM_K_OTHER, st, k_adj_carry_ghosts<<<grid, 256, 0, st>>>(g, w.aua, w.au0));
+    const double alpha = ctx->adv == FALM_ADV_UTOPIA ? 1. / 12. : (ctx->adv == FALM_ADV_KK ? 1. / 4. : 1. / 24.);
+    LAUNCH(FALM_K_OTHER, st, k_adj_pseudo_u<<<grid, 256, 0, st>>>(g, mv, (const double *)f0->u, (const double *)f0->uu,
+                                                                  (const double *)f0->nut, w.aua, w.au0, w.auu0, w.anut0, w.aff,
+                                                                  1.0 / ctx->Re, dt, alpha));
+    if (ctx->alm_on) {
+        const int apc = ctx->alm.apcount;
+        LAUNCH(FALM_K_ALM, st, k_adj_alm_project<<<apc, 256, 0, st>>>(g, ctx->alm, ctx->m64.x[0], ctx->m64.x[1], ctx->m64.x[2], w.aff, w.aF));
+        LAUNCH(FALM_K_ALM, st, k_adj_alm_ap<<<(apc + 127) / 128, 128, 0, st>>>(g, ctx->alm, ctx->m64.x[0], ctx->m64.x[1], ctx->m64.x[2],
+                                                                              (const double *)f0->u, t, w.aF, w_power, w.au0, grad));
+    }
+    CK(cudaMemcpyAsync(pu, w.au0, 3 * nb, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(puu, w.auu0, 3 * nb, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(pnut, w.anut0, nb, cudaMemcpyDeviceToDevice, st));
     return FALM_OK;
 }

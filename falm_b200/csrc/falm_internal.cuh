@@ -130,6 +130,7 @@ struct falm_ctx {
     // work vectors (element size = precision), allocated lazily
     size_t esize;
     void *work_mem;
+    void *adj_mem;                          // discrete-adjoint workspace (allocated on first use)
     void *w_rr, *w_p, *w_q, *w_s, *w_pp, *w_ss, *w_t, *w_r, *w_rhs, *w_ua, *w_div, *w_xp;
     void *w_outlet;                         // 3 planes x 3 comps of the previous velocity at the outlet
     // reductions

@@ -206,6 +206,22 @@ int falm_step(falm_ctx *ctx, const falm_fields *f, double dt, double t, void *st
    No reference counterpart (the reference has uniform inflow only). */
 int falm_bc_set_inlet_plane(falm_ctx *ctx, const double *plane, void *stream);
 
+/* ---------------- discrete adjoint of the step ---------------------------------------------- */
+/* No reference counterpart.  Adjoint of falm_step for FP64 contexts (Upwind3/UTOPIA/KK advection,
+   Smagorinsky or no SGS, channel or cavity), with the Poisson solve treated as exact (its adjoint is
+   one solve with the transposed operator, to 1e-12 of its right-hand side).  f0: the DEVICE state
+   (u, uu, p, nut; ff unused) at the start of the step, left unchanged; t: that step's time (as given
+   to falm_step); w_power: the weight of this step's rotor power (sum over turbines of torque x tip
+   rate) in the objective.  au (3N), auu (3N), anut (N): DEVICE adjoint of the state after the step
+   on entry, of the state before it on return.  grad: DEVICE array of 1 + 2*apcount doubles
+   (collective pitch [deg], per-AP chord, per-AP twist [deg]) to which the step's gradient
+   contributions are added.  f1: the DEVICE state after the step (only its u is read), or NULL:
+   the step is then recomputed internally from f0 (the context's solver tolerance applies).
+   With f1 given only the ALM is re-evaluated, so a driver that keeps the states of a segment
+   pays one forward step less per adjoint step. */
+int falm_step_adjoint(falm_ctx *ctx, const falm_fields *f0, const falm_fields *f1, double dt, double t,
+                      double w_power, void *au, void *auu, void *anut, double *grad, void *stream);
+
 /* ---------------- allocation-free inner product --------------------------------------------- */
 /* No reference counterpart.  The interior inner product of falm_mv_dot for callers that hold
    device fields but may not allocate (a coupled solver or in-situ monitor beside a simulation
