@@ -45,7 +45,10 @@ def objective(sim, steps):
 
 def mean_power_gradient(sim, steps, checkpoint=20):
     """J over the next `steps` steps of sim and its gradient (pitch, chord[apcount],
-    twist[apcount]) by the discrete adjoint; sim ends after the window"""
+    twist[apcount]) by the discrete adjoint; sim ends after the window.  The states
+    of the last segment are kept from the forward pass; the other segments are
+    recomputed from their checkpoints (checkpoint >= steps keeps every state and
+    recomputes nothing)."""
     ctx = sim.ctx
     torch = ctx.torch
     if ctx.precision != "fp64":
@@ -53,10 +56,15 @@ def mean_power_gradient(sim, steps, checkpoint=20):
     apc = sim.case.alm.apcount
     ckpts, J = [], 0.0
     it0 = sim.it
+    last = ((steps - 1) // checkpoint) * checkpoint   # first step of the last segment
+    kept = []
     for q in range(steps):
         if q % checkpoint == 0:
             ckpts.append((sim.it, _clone(sim)))
+        if q >= last:
+            kept.append(_clone(sim))
         J += _power(sim, sim.step()) / steps
+    kept.append({"u": sim.u.clone()})
     end_state, end_it = _clone(sim), sim.it
     n = sim.case.grid.n
     dev, dt = ctx.device, sim.case.dt
@@ -67,14 +75,17 @@ def mean_power_gradient(sim, steps, checkpoint=20):
     for s in reversed(range(len(ckpts))):
         it_s, st_s = ckpts[s]
         seg = min(checkpoint, it0 + steps - it_s)
-        # recompute the segment, keeping the state at the start of each step
-        _restore(sim, st_s)
-        sim.it = it_s
-        states = []
-        for q in range(seg):
-            states.append(_clone(sim))
-            sim.step()
-        states.append({"u": sim.u.clone()})   # the velocity after the segment's last step
+        if s == len(ckpts) - 1:
+            states = kept   # kept from the forward pass
+        else:
+            # recompute the segment, keeping the state at the start of each step
+            _restore(sim, st_s)
+            sim.it = it_s
+            states = []
+            for q in range(seg):
+                states.append(_clone(sim))
+                sim.step()
+            states.append({"u": sim.u.clone()})   # the velocity after the segment's last step
         for q in reversed(range(seg)):
             S = states[q]
             ctx.step_adjoint(S["u"], S["uu"], S["p"], S["nut"], dt, (it_s + q + 1) * dt, 1.0 / steps, au, auu, anut, grad,

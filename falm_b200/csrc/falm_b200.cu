@@ -362,6 +362,12 @@ int build_poisson(falm_ctx *ctx, int kind) {
     ctx->maxdiag = maxdiag;
     ctx->op_ready = 1;
     ctx->bc_kind_op = kind;
+    // the coefficient of cell q towards q+1 equals that of q+1 towards q on every
+    // axis (uniform spacing): the operator is symmetric over the interior
+    ctx->op_symmetric = 1;
+    for (int d = 0; d < 3; d++)
+        for (int q = g.gc; q + 1 < s[d] - g.gc; q++)
+            if (std::fabs(up[d][q] - um[d][q + 1]) > 1e-13 * std::fabs(up[d][q])) ctx->op_symmetric = 0;
     return FALM_OK;
 }
 
@@ -1301,8 +1307,18 @@ extern "C" int falm_mv_dot_static(int sx, int sy, int sz, int gc, int precision,
 namespace {
 
 struct AdjWork {
-    double *uc, *uuc, *pc, *nutc, *au0, *auu0, *anut0, *aua, *auu1, *aff, *ap, *arhs, *r, *AT, *aF;
+    double *uc, *uuc, *pc, *nutc, *au0, *auu0, *anut0, *aua, *auu1, *aff, *ap, *arhs, *r, *AT, *aF, *arhs1;
 };
+
+// initial guess of the transposed solve: linear extrapolation from the two
+// previous (normalised) solutions, y <- 2 y - y_prev, y_prev <- old y
+__global__ void k_adj_extrapolate(double *y, double *yprev, long long n) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const double a = y[q];
+        y[q] = 2 * a - yprev[q];
+        yprev[q] = a;
+    }
+}
 
 __global__ void k_adj_zero_interior(Geom g, double *a) {
     ADJ_FOR_BOX(g.gc, g.sx - g.gc, g.gc, g.sy - g.gc, g.gc, g.sz - g.gc, i, j, k) { a[g.id(i, j, k)] = 0; }
@@ -1311,16 +1327,17 @@ __global__ void k_adj_zero_interior(Geom g, double *a) {
 int adj_work(falm_ctx *ctx, AdjWork *w) {
     const size_t n = (size_t)ctx->geo.n;
     const size_t apc = ctx->alm_on ? (size_t)ctx->alm.apcount : 0;
-    const size_t counts[15] = {3 * n, 3 * n, n, n, 3 * n, 3 * n, n, 3 * n, 3 * n, 3 * n, n, n, n, 7 * n, 3 * apc + 1};
+    const size_t counts[16] = {3 * n, 3 * n, n, n, 3 * n, 3 * n, n, 3 * n, 3 * n, 3 * n, n, n, n, 7 * n, 3 * apc + 1, n};
     size_t bytes = 0;
-    for (int q = 0; q < 15; q++) bytes += (counts[q] * sizeof(double) + 255) / 256 * 256;
+    for (int q = 0; q < 16; q++) bytes += (counts[q] * sizeof(double) + 255) / 256 * 256;
     if (!ctx->adj_mem) {
         if (cudaMalloc(&ctx->adj_mem, bytes) != cudaSuccess) { cudaGetLastError(); ctx->adj_mem = nullptr; return fail(ctx, FALM_ERR_ALLOC, "step_adjoint: workspace"); }
+        if (cudaMemset(ctx->adj_mem, 0, bytes) != cudaSuccess) { cudaGetLastError(); return fail(ctx, FALM_ERR_CUDA, "step_adjoint: workspace"); }
     }
     char *p = (char *)ctx->adj_mem;
-    double **dst[15] = {&w->uc, &w->uuc, &w->pc, &w->nutc, &w->au0, &w->auu0, &w->anut0, &w->aua, &w->auu1, &w->aff, &w->ap,
-                        &w->arhs, &w->r, &w->AT, &w->aF};
-    for (int q = 0; q < 15; q++) { *dst[q] = (double *)p; p += (counts[q] * sizeof(double) + 255) / 256 * 256; }
+    double **dst[16] = {&w->uc, &w->uuc, &w->pc, &w->nutc, &w->au0, &w->auu0, &w->anut0, &w->aua, &w->auu1, &w->aff, &w->ap,
+                        &w->arhs, &w->r, &w->AT, &w->aF, &w->arhs1};
+    for (int q = 0; q < 16; q++) { *dst[q] = (double *)p; p += (counts[q] * sizeof(double) + 255) / 256 * 256; }
     return FALM_OK;
 }
 
@@ -1358,7 +1375,9 @@ extern "C" int falm_step_adjoint(falm_ctx *ctx, const falm_fields *f0, const fal
     }
     // reverse sweep
     for (double *z : {w.au0, w.auu0, w.aua, w.auu1, w.aff}) CK(cudaMemsetAsync(z, 0, 3 * nb, st));
-    for (double *z : {w.ap, w.arhs}) CK(cudaMemsetAsync(z, 0, nb, st));
+    // arhs and arhs1 keep the previous two calls' transposed-Poisson solutions: the
+    // initial guess of this call's solve extrapolates them
+    CK(cudaMemsetAsync(w.ap, 0, nb, st));
     CK(cudaMemcpyAsync(w.anut0, anut, nb, cudaMemcpyDeviceToDevice, st));
     const int grid = ctx->sm_count * 8;
     const MetricView<double> mv = mview<double>(ctx);
@@ -1372,15 +1391,25 @@ extern "C" int falm_step_adjoint(falm_ctx *ctx, const falm_fields *f0, const fal
     LAUNCH(FALM_K_OTHER, st, k_adj_project<<<grid, 256, 0, st>>>(g, mv, pu, puu, w.aua, w.auu1, w.auu0, w.ap, dt));
     LAUNCH(FALM_K_OTHER, st, k_adj_pbc<<<dim3(64, 3), 256, 0, st>>>(g, ctx->bc_kind, w.ap));
     LAUNCH(FALM_K_OTHER, st, k_adj_zero_ghosts<<<grid, 256, 0, st>>>(g, w.ap));
-    // transposed Poisson solve, to 1e-12 of the adjoint right-hand side's norm
-    LAUNCH(FALM_K_OTHER, st, k_adj_transpose_op<<<grid, 256, 0, st>>>(g, op7<double>(ctx), w.AT));
+    // transposed Poisson solve, warm-started; a
+    // symmetric table operator is its own transpose, otherwise the transpose is
+    // built as an explicit 7-column matrix
+    const bool use_tables = !ctx->A_explicit && ctx->op_symmetric;
+    if (!use_tables) LAUNCH(FALM_K_OTHER, st, k_adj_transpose_op<<<grid, 256, 0, st>>>(g, op7<double>(ctx), w.AT));
+    // the right-hand side is normalised to unit norm (the solver's breakdown test
+    // |rho| < FLT_MIN is absolute) and the solution is kept normalised as the next guess
     double apn = 0.0;
     if ((rc = dot_t<double>(ctx, w.ap, w.ap, 1, &apn, st))) return rc;
+    apn = sqrt(apn);
     if (apn > 0) {
+        LAUNCH(FALM_K_OTHER, st, k_scale<double><<<grid, 256, 0, st>>>(w.ap, (long long)n, 1.0 / apn));
         const void *a_saved = ctx->A_explicit;
         const double tol_saved = ctx->tol;
-        ctx->A_explicit = w.AT;
-        ctx->tol = 1e-12 * sqrt(apn) / ((double)g.nx * g.ny * g.nz);
+        if (!use_tables) ctx->A_explicit = w.AT;
+        LAUNCH(FALM_K_OTHER, st, k_adj_extrapolate<<<grid, 256, 0, st>>>(w.arhs, w.arhs1, (long long)n));
+        // relative residual 1e-6 (1e-12 when the context's tolerance is below 1e-12):
+        // well below the gradient accuracy the forward solve's tolerance allows
+        ctx->tol = (tol_saved < 1e-12 ? 1e-12 : 1e-6) / ((double)g.nx * g.ny * g.nz);
         int it = 0, outer = 0;
         double err = 0;
         rc = solve_t<double>(ctx, w.arhs, w.ap, w.r, st, &it, &err, &outer);
@@ -1388,8 +1417,8 @@ extern "C" int falm_step_adjoint(falm_ctx *ctx, const falm_fields *f0, const fal
         ctx->tol = tol_saved;
         if (rc) return rc;
     }
-    const double scale = 1.0 / (dt * ctx->maxdiag);
-    LAUNCH(FALM_K_OTHER, st, k_adj_rhs<<<grid, 256, 0, st>>>(g, mv, w.arhs, w.auu1, scale));
+    const double scale = apn / (dt * ctx->maxdiag);   // arhs holds the solution for the normalised right-hand side
+    if (apn > 0) LAUNCH(FALM_K_OTHER, st, k_adj_rhs<<<grid, 256, 0, st>>>(g, mv, w.arhs, w.auu1, scale));
     if (ctx->bc_kind == FALM_BC_CAVITY) LAUNCH(FALM_K_OTHER, st, k_adj_uubc<<<grid, 256, 0, st>>>(g, w.auu1));
     LAUNCH(FALM_K_OTHER, st, k_adj_utouu<<<grid, 256, 0, st>>>(g, mv, w.auu1, w.aua));
     LAUNCH(FALM_K_OTHER, st, k_adj_carry_ghosts<<<grid, 256, 0, st>>>(g, w.aua, w.au0));

@@ -115,6 +115,7 @@ struct falm_ctx {
     int max_outer;
     // Poisson operator
     int op_ready;
+    int op_symmetric;                       // the table operator equals its transpose over the interior
     int bc_kind_op;
     double maxdiag;
     void *op_mem;

@@ -209,7 +209,8 @@ int falm_bc_set_inlet_plane(falm_ctx *ctx, const double *plane, void *stream);
 /* ---------------- discrete adjoint of the step ---------------------------------------------- */
 /* No reference counterpart.  Adjoint of falm_step for FP64 contexts (Upwind3/UTOPIA/KK advection,
    Smagorinsky or no SGS, channel or cavity), with the Poisson solve treated as exact (its adjoint is
-   one solve with the transposed operator, to 1e-12 of its right-hand side).  f0: the DEVICE state
+   one solve with the transposed operator, started from an extrapolation of the previous calls', to a
+   relative residual of 1e-6, or 1e-12 when the context's tolerance is below 1e-12).  f0: the DEVICE state
    (u, uu, p, nut; ff unused) at the start of the step, left unchanged; t: that step's time (as given
    to falm_step); w_power: the weight of this step's rotor power (sum over turbines of torque x tip
    rate) in the objective.  au (3N), auu (3N), anut (N): DEVICE adjoint of the state after the step
