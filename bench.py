@@ -67,13 +67,20 @@ def barrier(world):
 
 
 def max_over_ranks(x, world):
+    """the maximum of x over the ranks (nccl on the GPUs, gloo on the host)"""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_rate(world, cells, steps, ms_max):
+    """whole-job Mcell/s of `world` independent replicas, timed by the slowest rank"""
+    return world * cells * steps / (ms_max / 1e3) / 1e6
 
 
 # ---------------------------------------------------------------- clocks
@@ -225,7 +232,7 @@ def run_ours(args, rank, world, local):
     S = 4 if args.precision == "mixed" else 8
     its = [s["it"] for s in stats]
     mean_it = sum(its) / len(its)
-    value = world * n * args.steps / (ms_max / 1e3) / 1e6
+    value = replica_rate(world, n, args.steps, ms_max)
     peak, peak_kind = peaks()
     # dominant kernel class by device time
     cls = max((k for k in prof if k in KERNEL_VALUES), key=lambda k: prof[k][0])
@@ -251,7 +258,7 @@ def run_ours(args, rank, world, local):
         ms_e, stats_e, _, wall_e = timed(sim, args.steps, e2e=True)
         ms_e = max_over_ranks(ms_e, world)
         ny, nz = case.grid.interior[1], case.grid.interior[2]
-        out["e2e"] = {"value": world * n * args.steps / (ms_e / 1e3) / 1e6, "unit": UNIT,
+        out["e2e"] = {"value": replica_rate(world, n, args.steps, ms_e), "unit": UNIT,
                       "h2d_bytes_per_step": 3 * ny * nz * 8,
                       "d2h_bytes_per_step": 8 * 8 + 2 * 8 * 8,
                       "ms_per_step": ms_e / args.steps,
@@ -266,7 +273,7 @@ def run_ours(args, rank, world, local):
             sim64.step()
         ms64, st64, _, _ = timed(sim64, args.steps)
         ms64 = max_over_ranks(ms64, world)
-        out["fp64"] = {"value": world * n * args.steps / (ms64 / 1e3) / 1e6, "ms_per_step": ms64 / args.steps,
+        out["fp64"] = {"value": replica_rate(world, n, args.steps, ms64), "ms_per_step": ms64 / args.steps,
                        "steps_per_s": 1e3 * args.steps / ms64, "its": [s["it"] for s in st64],
                        "divnorm_max": max(s["divnorm"] for s in st64)}
         out["mixed_over_fp64"] = out["fp64"]["ms_per_step"] / out["ms_per_step"]
