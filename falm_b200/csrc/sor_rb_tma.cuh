@@ -120,7 +120,24 @@ __global__ void __launch_bounds__(256) k_sor_rb_tma(Geom g, int kc, const __grid
     const int wo = (wy - yb) * L::BX + (wx - xb);
     const long long sxy = (long long)g.sx * g.sy;
     T *wp = xout + (long long)wx + (long long)wy * g.sx + (long long)k0 * sxy;   // advanced one plane per write-out
+    // registers rolled along the march: slot base of planes q, q-1, ..., q-H-1
+    // and the z operator tables (cm, cp, up, um) of planes q-1, ..., q-H
+    unsigned char *sl[H + 2];
+    T zab[H], zat[H], zup[H], zum[H];
+#pragma unroll
+    for (int m = 0; m < H + 2; m++) sl[m] = slot(-1 - m);
+#pragma unroll
+    for (int h = 0; h < H; h++) { zab[h] = zat[h] = zup[h] = zum[h] = T(0); }
     for (int q = 0; q < nplanes; q++) {
+#pragma unroll
+        for (int m = H + 1; m > 0; m--) sl[m] = sl[m - 1];
+        sl[0] = slot(q);
+#pragma unroll
+        for (int h = H - 1; h > 0; h--) { zab[h] = zab[h - 1]; zat[h] = zat[h - 1]; zup[h] = zup[h - 1]; zum[h] = zum[h - 1]; }
+        {
+            const int kz = min(max(P0 + q - 1, 0), g.sz - 1);
+            zab[0] = ldg(tb.cm[2] + kz); zat[0] = ldg(tb.cp[2] + kz); zup[0] = ldg(tb.up[2] + kz); zum[0] = ldg(tb.um[2] + kz);
+        }
         bool fail = !wait_q(q);
         waited = q + 1;
         if (__syncthreads_or(fail)) goto drain;
@@ -132,11 +149,11 @@ __global__ void __launch_bounds__(256) k_sor_rb_tma(Geom g, int kc, const __grid
                 const int color = (c1 + h - 1) & 1;
                 const int e = (color ^ (x0 + y + kp)) & 1;          // the pair's cell of this colour
                 if ((((e ? live1 : live0) >> (h - 1)) & 1u) != 0u) {
-                    T *X0 = (T *)slot(p);
-                    const T *Xm = (const T *)slot(p - 1), *Xp = (const T *)slot(p + 1);
-                    const T *B0 = (const T *)(slot(p) + L::PB);
-                    const T ab = ldg(tb.cm[2] + kp), at = ldg(tb.cp[2] + kp);
-                    const T ac = (((e ? dxy1 : dxy0) - ldg(tb.up[2] + kp)) - ldg(tb.um[2] + kp)) * tb.scale;
+                    T *X0 = (T *)sl[h];
+                    const T *Xm = (const T *)sl[h + 1], *Xp = (const T *)sl[h - 1];
+                    const T *B0 = (const T *)(sl[h] + L::PB);
+                    const T ab = zab[h - 1], at = zat[h - 1];
+                    const T ac = (((e ? dxy1 : dxy0) - zup[h - 1]) - zum[h - 1]) * tb.scale;
                     const int o = o0 + e;
                     const T xc = X0[o];
                     const T r7 = ac * xc + (e ? ae1 : ae0) * X0[o + 1] + (e ? aw1 : aw0) * X0[o - 1] + an * X0[o + L::BX] +
@@ -150,7 +167,7 @@ __global__ void __launch_bounds__(256) k_sor_rb_tma(Geom g, int kc, const __grid
         {
             const int kp = P0 + q - H;
             if (kp >= k0 && kp < k1) {
-                if (writer) *wp = ((const T *)slot(q - H))[wo];
+                if (writer) *wp = ((const T *)sl[H])[wo];
                 wp += sxy;
             }
         }
