@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <mutex>
+#include <unordered_map>
 #include "falm_internal.cuh"
 #include "common.cuh"
 #include "cfd.cuh"
@@ -121,6 +122,30 @@ int row_grid(const falm_ctx *ctx, const Region3 &R) {
     long long need = (rows + kWarpsPerBlock - 1) / kWarpsPerBlock;
     long long cap = (long long)ctx->sm_count * 8;
     return (int)std::max(1LL, std::min(need, cap));
+}
+
+// one wave of a row kernel: as many blocks as are resident at once on all SMs
+// (the kernel's occupancy, looked up once per kernel), at most one warp per row
+template <typename K>
+int row_grid_wave(const falm_ctx *ctx, const Region3 &R, K kernel) {
+    static std::mutex mu;
+    static std::unordered_map<const void *, int> per_sm_of;
+    int per_sm = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = per_sm_of.find((const void *)kernel);
+        if (it != per_sm_of.end()) per_sm = it->second;
+    }
+    if (per_sm <= 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kRowThreads, 0) != cudaSuccess || per_sm <= 0) {
+            cudaGetLastError();
+            return row_grid(ctx, R);
+        }
+        std::lock_guard<std::mutex> lk(mu);
+        per_sm_of[(const void *)kernel] = per_sm;
+    }
+    const long long need = ((long long)R.nrows() + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    return (int)std::max(1LL, std::min(need, (long long)ctx->sm_count * per_sm));
 }
 
 template <typename T> MetricView<T> mview(const falm_ctx *ctx);
@@ -233,8 +258,31 @@ int sor_rb_launch_h(falm_ctx *ctx, cudaStream_t st, const T *xin, const T *b, T 
     return rc ? -rc : 1;
 }
 
+// three FP32 half sweeps on the 28 x 16 tile; 1 launched, 0 not eligible, <0 launch error
+template <typename T>
+int sor_rb2_launch(falm_ctx *ctx, cudaStream_t st, const T *xin, const T *b, T *xout, T omega, int c1, const SolverScalars *sc) {
+    using L = RB2Tile<T>;
+    if (ctx->no_tma || ctx->A_explicit) return 0;
+    CUtensorMap mx, mb;
+    if (!make_map(ctx, &mx, xin, 1, L::BX, L::BY) || !make_map(ctx, &mb, b, 1, L::BXB, L::BYB)) return 0;
+    const Geom &g = ctx->geo;
+    const int bx = (g.nx + L::TX - 1) / L::TX, by = (g.ny + L::TY - 1) / L::TY;
+    const int kc = chunk_len(ctx, (long long)bx * by, g.nz, 4, 32);
+    dim3 grid(bx, by, (g.nz + kc - 1) / kc);
+    cudaFuncSetAttribute(k_sor_rb2_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
+    const PoissonTables<T> tb = op7<T>(ctx).t;
+    int rc = launch_k(ctx, FALM_K_SOR, st, [&] {
+        k_sor_rb2_tma<T><<<grid, L::NT, L::SMEM, st>>>(g, kc, mx, mb, tb, xout, omega, c1, sc, ctx->kerr);
+    });
+    return rc ? -rc : 1;
+}
+
 template <typename T>
 int sor_rb_launch(falm_ctx *ctx, cudaStream_t st, int H, const T *xin, const T *b, T *xout, T omega, int c1, const SolverScalars *sc) {
+    if (H == 3 && sizeof(T) == 4 && !ctx->sor_v1) {
+        const int r = sor_rb2_launch<T>(ctx, st, xin, b, xout, omega, c1, sc);
+        if (r != 0) return r;
+    }
     if (H == 1) return sor_rb_launch_h<T, 1>(ctx, st, xin, b, xout, omega, c1, sc);
     if (H == 2) return sor_rb_launch_h<T, 2>(ctx, st, xin, b, xout, omega, c1, sc);
     return sor_rb_launch_h<T, 3>(ctx, st, xin, b, xout, omega, c1, sc);
@@ -381,6 +429,8 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
     const Geom &g = ctx->geo;
     const Region3 R = interior(g);
     const int grid = row_grid(ctx, R);
+    const int grid_p = row_grid_wave(ctx, R, k_bicg_p<T>), grid_s = row_grid_wave(ctx, R, k_bicg_s<T>);
+    const int grid_xr = row_grid_wave(ctx, R, k_bicg_xr<T>);
     const Op7<T> op = op7<T>(ctx);
     T *rr = (T *)ctx->w_rr, *p = (T *)ctx->w_p, *q = (T *)ctx->w_q, *s = (T *)ctx->w_s, *pp = (T *)ctx->w_pp;
     T *ss = (T *)ctx->w_ss, *t = (T *)ctx->w_t, *xp = (T *)ctx->w_xp;
@@ -440,15 +490,15 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
             CK(cudaStreamSynchronize(st));
         }
         for (;;) {
-            LAUNCH(FALM_K_BICG_P, st, k_bicg_p<T><<<grid, kRowThreads, 0, st>>>(g, R, op, p, q, r, first_target(pp), pct, pcw, sc));
+            LAUNCH(FALM_K_BICG_P, st, k_bicg_p<T><<<grid_p, kRowThreads, 0, st>>>(g, R, op, p, q, r, first_target(pp), pct, pcw, sc));
             if ((rc = precondition_rest(pp, p))) return rc;
             S7_OR(FALM_K_MV_DOT1, st, T, 1, pp, (MvDot1Body<T>{op, q, rr, sc}),
                   (k_mv_dot1<T><<<grid, kRowThreads, 0, st>>>(g, R, op, pp, q, rr, ctx->red, sc)));
-            LAUNCH(FALM_K_BICG_S, st, k_bicg_s<T><<<grid, kRowThreads, 0, st>>>(g, R, op, s, q, r, first_target(ss), pct, pcw, sc));
+            LAUNCH(FALM_K_BICG_S, st, k_bicg_s<T><<<grid_s, kRowThreads, 0, st>>>(g, R, op, s, q, r, first_target(ss), pct, pcw, sc));
             if ((rc = precondition_rest(ss, s))) return rc;
             S7_OR(FALM_K_MV_DOT2, st, T, 2, ss, (MvDot2Body<T>{op, t, s, sc}),
                   (k_mv_dot2<T><<<grid, kRowThreads, 0, st>>>(g, R, op, ss, t, s, ctx->red, sc)));
-            LAUNCH(FALM_K_BICG_XR, st, k_bicg_xr<T><<<grid, kRowThreads, 0, st>>>(g, R, x, pp, ss, r, s, t, rr, ctx->red, sc));
+            LAUNCH(FALM_K_BICG_XR, st, k_bicg_xr<T><<<grid_xr, kRowThreads, 0, st>>>(g, R, x, pp, ss, r, s, t, rr, ctx->red, sc));
             CK(cudaMemcpyAsync(ctx->scal_host, sc, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             if (ctx->scal_host->done) break;
@@ -714,6 +764,8 @@ int falm_create(const falm_grid *grid, int precision, falm_ctx **out) {
     {
         const char *e = getenv("FALM_B200_NO_TMA");
         ctx->no_tma = (e && e[0] == '1') ? 1 : 0;
+        const char *v = getenv("FALM_B200_SOR_V1");
+        ctx->sor_v1 = (v && v[0] == '1') ? 1 : 0;
         const char *c = getenv("FALM_B200_CHECK");
         ctx->check_sync = (c && c[0] == '1') ? 1 : 0;
     }

@@ -41,9 +41,29 @@ struct P3View {
     }
 };
 
-// Body: bool skip() const; void cell(i, j, k, cc, const P3View&, acc); void finish(tot)
+// metric factors of the 3 x 3 columns around (i, j) and of planes k-1..k+1, with
+// MetricView's association (ja = (hx*hy)*hz, g_d = (ja*k_d)*k_d); offsets -1, 0, +1
+template <typename T>
+struct ColMet {
+    T hx[3], kx[3], hy[3], ky[3], hz[3], kz[3];
+    __device__ __forceinline__ T ja(int dx, int dy, int dz) const { return (hx[1 + dx] * hy[1 + dy]) * hz[1 + dz]; }
+    __device__ __forceinline__ T k(int d, int dx, int dy, int dz) const { return d == 0 ? kx[1 + dx] : (d == 1 ? ky[1 + dy] : kz[1 + dz]); }
+    __device__ __forceinline__ T g(int d, int dx, int dy, int dz) const {
+        const T kk = k(d, dx, dy, dz);
+        return (ja(dx, dy, dz) * kk) * kk;
+    }
+};
+
+// pointwise operands of a body that has none
+struct NoPW {};
+
+// Body: bool skip() const; MetricView<T> mv; type PW (the cell's pointwise
+//       operands) and PW pw_load(i, j, k, cc) const;
+//       void cell(i, j, k, cc, const P3View&, const ColMet&, const PW&, acc); void finish(tot)
+// The pointwise operands of a plane are loaded before the wait for the plane
+// ahead, for every row of the thread, so their latency overlaps the wait.
 template <typename T, int NF, int NS, int NV, class Body>
-__global__ void __launch_bounds__(256) k_plane3_tma(Geom g, Region3 R, int org, int kc, const __grid_constant__ MapSet<NF> maps,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_plane3_tma(Geom g, Region3 R, int org, int kc, const __grid_constant__ MapSet<NF> maps,
                                                   Body body, RedWork rw, int *err) {
     using L = P3Layout<T, NF>;
     extern __shared__ unsigned char smem_raw[];
@@ -83,6 +103,22 @@ __global__ void __launch_bounds__(256) k_plane3_tma(Geom g, Region3 R, int org, 
     double acc[NV > 0 ? NV : 1];
 #pragma unroll
     for (int d = 0; d < (NV > 0 ? NV : 1); d++) acc[d] = 0.0;
+    // column metric factors (x shared by the rows, y per row); z per plane below
+    ColMet<T> cm[RY];
+    {
+        const MetricView<T> &mv = body.mv;
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const int ic = min(max(i - 1 + q, 0), g.sx - 1);
+            const T hxv = ldg(mv.m.h[0] + ic), kxv = ldg(mv.m.k[0] + ic);
+#pragma unroll
+            for (int r = 0; r < RY; r++) {
+                const int jc = min(max(jr[r] - 1 + q, 0), g.sy - 1);
+                cm[r].hx[q] = hxv; cm[r].kx[q] = kxv;
+                cm[r].hy[q] = ldg(mv.m.h[1] + jc); cm[r].ky[q] = ldg(mv.m.k[1] + jc);
+            }
+        }
+    }
     auto slot = [&](int q) { return smem + (q % NS) * slot_bytes; };
     auto issue = [&](int q) {
         uint64_t *b = bar + (q % NS);
@@ -117,6 +153,11 @@ __global__ void __launch_bounds__(256) k_plane3_tma(Geom g, Region3 R, int org, 
     waited = 2;
     if (__syncthreads_or(fail)) goto drain;
     for (int q = 1; q < nplanes - 1; q++) {
+        const int k = P0 + q;
+        typename Body::PW pwv[RY];
+#pragma unroll
+        for (int r = 0; r < RY; r++)
+            if (act[r]) pwv[r] = body.pw_load(i, jr[r], k, g.id(i, jr[r], k));
         fail = !wait_q(q + 1);
         waited = q + 2;
         if (__syncthreads_or(fail)) goto drain;
@@ -128,12 +169,19 @@ __global__ void __launch_bounds__(256) k_plane3_tma(Geom g, Region3 R, int org, 
         v.pl[0] = (const T *)slot(q - 1);
         v.pl[1] = (const T *)slot(q);
         v.pl[2] = (const T *)slot(q + 1);
-        const int k = P0 + q;
+        T hzv[3], kzv[3];
+#pragma unroll
+        for (int q2 = 0; q2 < 3; q2++) {
+            const int kc2 = min(max(k - 1 + q2, 0), g.sz - 1);
+            hzv[q2] = ldg(body.mv.m.h[2] + kc2); kzv[q2] = ldg(body.mv.m.k[2] + kc2);
+        }
 #pragma unroll
         for (int r = 0; r < RY; r++) {
             if (act[r]) {
                 v.o = orr[r];
-                body.cell(i, jr[r], k, g.id(i, jr[r], k), v, acc);
+#pragma unroll
+                for (int q2 = 0; q2 < 3; q2++) { cm[r].hz[q2] = hzv[q2]; cm[r].kz[q2] = kzv[q2]; }
+                body.cell(i, jr[r], k, g.id(i, jr[r], k), v, cm[r], pwv[r], acc);
             }
         }
     }
@@ -162,10 +210,11 @@ struct UtoUUBody {
     MetricView<T> mv;
     T *uu, *rhs;
     T scale;
+    using PW = NoPW;
     __device__ bool skip() const { return false; }
-    __device__ __forceinline__ T ucv(const P3View<T, 1> &v, int d, int i, int j, int k, int dx, int dy, int dz) const {
-        int idx = d == 0 ? i + dx : (d == 1 ? j + dy : k + dz);
-        return mv.ja(i + dx, j + dy, k + dz) * mv.kx(d, idx) * v.at(0, d, dz, dx, dy);
+    __device__ PW pw_load(int, int, int, long long) const { return PW{}; }
+    __device__ __forceinline__ T ucv(const P3View<T, 1> &v, const ColMet<T> &cm, int d, int dx, int dy, int dz) const {
+        return cm.ja(dx, dy, dz) * cm.k(d, dx, dy, dz) * v.at(0, d, dz, dx, dy);
     }
     __device__ __forceinline__ bool zero_face(int d, int i, int j, int k) const {
         if (!CAVITY) return false;
@@ -175,18 +224,21 @@ struct UtoUUBody {
         return (k == g.gc - 1 || k == g.sz - g.gc - 1) && iin && jin;
     }
     // face d of cell (i+dx, j+dy, k+dz) (the face towards +d)
-    __device__ __forceinline__ T face(const P3View<T, 1> &v, int d, int i, int j, int k, int dx, int dy, int dz) const {
+    __device__ __forceinline__ T face(const P3View<T, 1> &v, const ColMet<T> &cm, int d, int i, int j, int k, int dx, int dy,
+                                      int dz) const {
         if (zero_face(d, i + dx, j + dy, k + dz)) return T(0);
-        T a = ucv(v, d, i, j, k, dx, dy, dz);
-        T b = ucv(v, d, i, j, k, dx + (d == 0), dy + (d == 1), dz + (d == 2));
+        T a = ucv(v, cm, d, dx, dy, dz);
+        T b = ucv(v, cm, d, dx + (d == 0), dy + (d == 1), dz + (d == 2));
         return T(0.5) * (a + b);
     }
-    __device__ void cell(int i, int j, int k, long long c, const P3View<T, 1> &v, double (&)[1]) const {
-        const T UE = face(v, 0, i, j, k, 0, 0, 0), VN = face(v, 1, i, j, k, 0, 0, 0), WT = face(v, 2, i, j, k, 0, 0, 0);
+    __device__ void cell(int i, int j, int k, long long c, const P3View<T, 1> &v, const ColMet<T> &cm, const PW &,
+                         double (&)[1]) const {
+        const T UE = face(v, cm, 0, i, j, k, 0, 0, 0), VN = face(v, cm, 1, i, j, k, 0, 0, 0), WT = face(v, cm, 2, i, j, k, 0, 0, 0);
         uu[c] = UE; uu[c + g.n] = VN; uu[c + 2 * g.n] = WT;
         if (RHS && i >= g.gc && j >= g.gc && k >= g.gc) {
-            const T UW = face(v, 0, i, j, k, -1, 0, 0), VS = face(v, 1, i, j, k, 0, -1, 0), WB = face(v, 2, i, j, k, 0, 0, -1);
-            T div = (UE - UW + VN - VS + WT - WB) / mv.ja(i, j, k);
+            const T UW = face(v, cm, 0, i, j, k, -1, 0, 0), VS = face(v, cm, 1, i, j, k, 0, -1, 0), WB = face(v, cm, 2, i, j, k, 0, 0, -1);
+            // 1/ja as the product of the inverse widths
+            T div = (UE - UW + VN - VS + WT - WB) * ((cm.kx[1] * cm.ky[1]) * cm.kz[1]);
             rhs[c] = div * scale;
         }
     }
@@ -205,21 +257,32 @@ struct ProjectBody {
     T *uu;
     const T *uua;
     T dt;
+    // face velocity (f) and cell velocity (a, interior cells only) before the correction
+    struct PW { T f0, f1, f2, a0, a1, a2; };
     __device__ bool skip() const { return false; }
-    __device__ void cell(int i, int j, int k, long long cc, const P3View<T, 1> &v, double (&)[1]) const {
+    __device__ PW pw_load(int i, int j, int k, long long cc) const {
+        const long long N = g.n;
+        PW w;
+        w.f0 = uua[cc]; w.f1 = uua[cc + N]; w.f2 = uua[cc + 2 * N];
+        w.a0 = w.a1 = w.a2 = T(0);
+        if (i >= g.gc && j >= g.gc && k >= g.gc) { w.a0 = ua[cc]; w.a1 = ua[cc + N]; w.a2 = ua[cc + 2 * N]; }
+        return w;
+    }
+    __device__ void cell(int i, int j, int k, long long cc, const P3View<T, 1> &v, const ColMet<T> &cm, const PW &w,
+                         double (&)[1]) const {
         const long long N = g.n;
         const T pcc = v.at(0, 0, 0), pe = v.at(0, 0, 0, 1, 0), pn = v.at(0, 0, 0, 0, 1), pt = v.at(0, 0, 1);
-        const T dpx = T(0.5) * (mv.g(0, i, j, k) + mv.g(0, i + 1, j, k)) * (pe - pcc);
-        const T dpy = T(0.5) * (mv.g(1, i, j, k) + mv.g(1, i, j + 1, k)) * (pn - pcc);
-        const T dpz = T(0.5) * (mv.g(2, i, j, k) + mv.g(2, i, j, k + 1)) * (pt - pcc);
-        const T f0 = uua[cc], f1 = uua[cc + N], f2 = uua[cc + 2 * N];
+        const T dpx = T(0.5) * (cm.g(0, 0, 0, 0) + cm.g(0, 1, 0, 0)) * (pe - pcc);
+        const T dpy = T(0.5) * (cm.g(1, 0, 0, 0) + cm.g(1, 0, 1, 0)) * (pn - pcc);
+        const T dpz = T(0.5) * (cm.g(2, 0, 0, 0) + cm.g(2, 0, 0, 1)) * (pt - pcc);
+        const T f0 = w.f0, f1 = w.f1, f2 = w.f2;
         const bool in = i >= g.gc && j >= g.gc && k >= g.gc;
         T a0 = 0, a1 = 0, a2 = 0, gx = 0, gy = 0, gz = 0;
         if (in) {
-            a0 = ua[cc]; a1 = ua[cc + N]; a2 = ua[cc + 2 * N];
-            gx = T(0.5) * mv.kx(0, i) * (pe - v.at(0, 0, 0, -1, 0));
-            gy = T(0.5) * mv.kx(1, j) * (pn - v.at(0, 0, 0, 0, -1));
-            gz = T(0.5) * mv.kx(2, k) * (pt - v.at(0, 0, -1));
+            a0 = w.a0; a1 = w.a1; a2 = w.a2;
+            gx = T(0.5) * cm.kx[1] * (pe - v.at(0, 0, 0, -1, 0));
+            gy = T(0.5) * cm.ky[1] * (pn - v.at(0, 0, 0, 0, -1));
+            gz = T(0.5) * cm.kz[1] * (pt - v.at(0, 0, -1));
         }
         uu[cc] = f0 - dt * dpx; uu[cc + N] = f1 - dt * dpy; uu[cc + 2 * N] = f2 - dt * dpz;
         if (in) { u[cc] = a0 - dt * gx; u[cc + N] = a1 - dt * gy; u[cc + 2 * N] = a2 - dt * gz; }
@@ -240,10 +303,13 @@ struct SgsDivBody {
     int sgs;
     T *div_out;
     double *divsum;
+    using PW = NoPW;
     __device__ bool skip() const { return false; }
-    __device__ void cell(int i, int j, int k, long long cc, const P3View<T, 2> &v, double (&acc)[1]) const {
+    __device__ PW pw_load(int, int, int, long long) const { return PW{}; }
+    __device__ void cell(int i, int j, int k, long long cc, const P3View<T, 2> &v, const ColMet<T> &cm, const PW &,
+                         double (&acc)[1]) const {
         if (sgs != FALM_SGS_EMPTY) {
-            const T kxx = mv.kx(0, i), kxy = mv.kx(1, j), kxz = mv.kx(2, k);
+            const T kxx = cm.kx[1], kxy = cm.ky[1], kxz = cm.kz[1];
             T dd[3][3];
 #pragma unroll
             for (int m = 0; m < 3; m++) {
@@ -257,7 +323,7 @@ struct SgsDivBody {
             T d1 = T(2) * (dux * dux), d2 = T(2) * (dvy * dvy), d3 = T(2) * (dwz * dwz);
             T d4 = (duy + dvx) * (duy + dvx), d5 = (dvz + dwy) * (dvz + dwy), d6 = (duz + dwx) * (duz + dwx);
             T Du = sqrt(d1 + d2 + d3 + d4 + d5 + d6);
-            T De = cbrt(mv.ja(i, j, k));
+            T De = cbrt(cm.ja(0, 0, 0));
             if (sgs == FALM_SGS_SMAGORINSKY) {
                 T lc = Cs * De;
                 nut[cc] = (lc * lc) * Du;
@@ -278,8 +344,10 @@ struct SgsDivBody {
         if (divsum) {
             double UE = to_d(v.at(1, 0, 0)), UW = to_d(v.at(1, 0, 0, -1, 0)), VN = to_d(v.at(1, 1, 0)), VS = to_d(v.at(1, 1, 0, 0, -1));
             double WT = to_d(v.at(1, 2, 0)), WB = to_d(v.at(1, 2, -1));
-            double ja = ldg(m64.h[0] + i) * ldg(m64.h[1] + j) * ldg(m64.h[2] + k);
-            double dv = (UE - UW + VN - VS + WT - WB) / ja;
+            // 1/ja as the product of the three FP64 inverse widths (one rounding
+            // step per factor instead of a division)
+            const double ija = ldg(m64.k[0] + i) * ldg(m64.k[1] + j) * ldg(m64.k[2] + k);
+            double dv = (UE - UW + VN - VS + WT - WB) * ija;
             if (div_out) div_out[cc] = (T)dv;
             acc[0] += dv * dv;
         }

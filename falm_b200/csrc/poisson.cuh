@@ -57,6 +57,16 @@ struct Op7 {
         }
         return r;
     }
+    // z part of the table operator of one plane, shared by every column of a
+    // tile: with a column's Col it gives at_col()'s coefficients
+    struct ZPl { T ab, at, zp, zm; };
+    __device__ __forceinline__ ZPl zplane(int k) const {
+        ZPl z;
+        if (A) { z.ab = z.at = z.zp = z.zm = T(0); return z; }
+        z.ab = ldg(t.cm[2] + k); z.at = ldg(t.cp[2] + k); z.zp = ldg(t.up[2] + k); z.zm = ldg(t.um[2] + k);
+        return z;
+    }
+    __device__ __forceinline__ T ac_col(const Col &cl, const ZPl &z) const { return ((cl.dxy - z.zp) - z.zm) * t.scale; }
     __device__ __forceinline__ void get(int i, int j, int k, long long c, T &ac, T &aw, T &ae, T &as, T &an, T &ab,
                                         T &at) const {
         if (A) {
@@ -74,7 +84,25 @@ struct Op7 {
         if (A) return A[c];
         return ((((ldg(t.dx0 + i) - ldg(t.up[1] + j)) - ldg(t.um[1] + j)) - ldg(t.up[2] + k)) - ldg(t.um[2] + k)) * t.scale;
     }
+    // the four terms of the diagonal's accumulation that are fixed along an x
+    // row (j, k), so that diag_row() rebuilds diag() bit for bit
+    struct RowD { T yp, ym, zp, zm; };
+    __device__ __forceinline__ RowD row(int j, int k) const {
+        RowD r;
+        if (A) { r.yp = r.ym = r.zp = r.zm = T(0); return r; }
+        r.yp = ldg(t.up[1] + j); r.ym = ldg(t.um[1] + j); r.zp = ldg(t.up[2] + k); r.zm = ldg(t.um[2] + k);
+        return r;
+    }
+    __device__ __forceinline__ T diag_row(const RowD &rd, int i, long long c) const {
+        if (A) return A[c];
+        return ((((ldg(t.dx0 + i) - rd.yp) - rd.ym) - rd.zp) - rd.zm) * t.scale;
+    }
 };
+
+// the SOR / Jacobi correction (b - Ax)/ac: IEEE division in FP64; in FP32
+// (mixed precision) the fast division, within 2 ulp
+__device__ __forceinline__ double sor_div(double a, double b) { return a / b; }
+__device__ __forceinline__ float sor_div(float a, float b) { return __fdividef(a, b); }
 
 // ac*xc + ae*xe + aw*xw + an*xn + as*xs + at*xt + ab*xb  (src/dev/MVDevCall.cu:181)
 template <typename T, typename A>
@@ -207,10 +235,16 @@ __global__ void __launch_bounds__(kRowThreads) k_jacobi(Geom g, Region3 R, Op7<T
 //   Jacobi: z = v/ac
 template <typename T>
 __device__ __forceinline__ T pc_first(int pc_type, int i, int j, int k, T v, T ac, T omega) {
-    if (pc_type == FALM_LS_SOR) return (((i + j + k) & 1) == 0) ? omega * (v / ac) : T(0);
-    if (pc_type == FALM_LS_JACOBI) return v / ac;
+    if (pc_type == FALM_LS_SOR) return (((i + j + k) & 1) == 0) ? omega * sor_div(v, ac) : T(0);
+    if (pc_type == FALM_LS_JACOBI) return sor_div(v, ac);
     return T(0);
 }
+
+// The vector steps below walk an x row with the 32 lanes of a warp in chunks
+// of 32*kRowILP cells (cell u of a chunk at i + 32u): the loads of a chunk are
+// issued before any of its arithmetic, so a warp keeps kRowILP requests per
+// operand in flight.
+constexpr int kRowILP = 4;
 
 // ---------------------------------------------------------------- BiCGStab steps
 template <typename T>
@@ -219,11 +253,31 @@ __global__ void __launch_bounds__(kRowThreads) k_bicg_p(Geom g, Region3 R, Op7<T
     if (sc->done) return;
     const int first = sc->first;
     const T beta = (T)sc->beta, omega = (T)sc->omega;
-    FB_FOR_ROWS(R, j, k) FB_FOR_I(R, i) {
-        long long c = g.id(i, j, k);
-        T pv = first ? r[c] : r[c] + beta * (p[c] - omega * q[c]);   // src/dev/FalmEqDevCall.cu:261
-        p[c] = pv;
-        pp[c] = pc_first<T>(pc_type, i, j, k, pv, op.diag(i, j, k, c), pc_omega);
+    FB_FOR_ROWS(R, j, k) {
+        const typename Op7<T>::RowD rd = op.row(j, k);
+        const long long c0 = g.id(0, j, k);
+        for (int ib = R.i0 + (threadIdx.x & 31); ib < R.i1; ib += 32 * kRowILP) {
+            T rv[kRowILP], pv[kRowILP], qv[kRowILP];
+#pragma unroll
+            for (int u = 0; u < kRowILP; u++) {
+                const int i = ib + 32 * u;
+                rv[u] = pv[u] = qv[u] = T(0);
+                if (i < R.i1) {
+                    rv[u] = r[c0 + i];
+                    if (!first) { pv[u] = p[c0 + i]; qv[u] = q[c0 + i]; }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kRowILP; u++) {
+                const int i = ib + 32 * u;
+                if (i < R.i1) {
+                    const long long c = c0 + i;
+                    const T v = first ? rv[u] : rv[u] + beta * (pv[u] - omega * qv[u]);   // src/dev/FalmEqDevCall.cu:261
+                    p[c] = v;
+                    pp[c] = pc_first<T>(pc_type, i, j, k, v, op.diag_row(rd, i, c), pc_omega);
+                }
+            }
+        }
     }
 }
 
@@ -251,11 +305,28 @@ __global__ void __launch_bounds__(kRowThreads) k_bicg_s(Geom g, Region3 R, Op7<T
     const T *__restrict__ q, const T *__restrict__ r, T *__restrict__ ss, int pc_type, T pc_omega, const SolverScalars *sc) {
     if (sc->done) return;
     const T alpha = (T)sc->alpha;
-    FB_FOR_ROWS(R, j, k) FB_FOR_I(R, i) {
-        long long c = g.id(i, j, k);
-        T sv = r[c] - alpha * q[c];                                   // src/dev/FalmEqDevCall.cu:284
-        s[c] = sv;
-        ss[c] = pc_first<T>(pc_type, i, j, k, sv, op.diag(i, j, k, c), pc_omega);
+    FB_FOR_ROWS(R, j, k) {
+        const typename Op7<T>::RowD rd = op.row(j, k);
+        const long long c0 = g.id(0, j, k);
+        for (int ib = R.i0 + (threadIdx.x & 31); ib < R.i1; ib += 32 * kRowILP) {
+            T rv[kRowILP], qv[kRowILP];
+#pragma unroll
+            for (int u = 0; u < kRowILP; u++) {
+                const int i = ib + 32 * u;
+                rv[u] = qv[u] = T(0);
+                if (i < R.i1) { rv[u] = r[c0 + i]; qv[u] = q[c0 + i]; }
+            }
+#pragma unroll
+            for (int u = 0; u < kRowILP; u++) {
+                const int i = ib + 32 * u;
+                if (i < R.i1) {
+                    const long long c = c0 + i;
+                    const T sv = rv[u] - alpha * qv[u];                   // src/dev/FalmEqDevCall.cu:284
+                    s[c] = sv;
+                    ss[c] = pc_first<T>(pc_type, i, j, k, sv, op.diag_row(rd, i, c), pc_omega);
+                }
+            }
+        }
     }
 }
 
@@ -287,14 +358,33 @@ __global__ void __launch_bounds__(kRowThreads) k_bicg_xr(Geom g, Region3 R, T *_
     if (sc->done) return;
     const T alpha = (T)sc->alpha, omega = (T)sc->omega;
     double acc[2] = {0.0, 0.0};
-    FB_FOR_ROWS(R, j, k) FB_FOR_I(R, i) {
-        long long c = g.id(i, j, k);
-        x[c] += alpha * pp[c] + omega * ss[c];                         // src/dev/FalmEqDevCall.cu:307
-        T rv = s[c] - omega * t[c];                                    // :330
-        r[c] = rv;
-        double rd = to_d(rv);
-        acc[0] += rd * rd;
-        acc[1] += rd * to_d(rr[c]);
+    FB_FOR_ROWS(R, j, k) {
+        const long long c0 = g.id(0, j, k);
+        for (int ib = R.i0 + (threadIdx.x & 31); ib < R.i1; ib += 32 * kRowILP) {
+            T xv[kRowILP], ppv[kRowILP], ssv[kRowILP], sv[kRowILP], tv[kRowILP], rrv[kRowILP];
+#pragma unroll
+            for (int u = 0; u < kRowILP; u++) {
+                const int i = ib + 32 * u;
+                xv[u] = ppv[u] = ssv[u] = sv[u] = tv[u] = rrv[u] = T(0);
+                if (i < R.i1) {
+                    const long long c = c0 + i;
+                    xv[u] = x[c]; ppv[u] = pp[c]; ssv[u] = ss[c]; sv[u] = s[c]; tv[u] = t[c]; rrv[u] = rr[c];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kRowILP; u++) {
+                const int i = ib + 32 * u;
+                if (i < R.i1) {
+                    const long long c = c0 + i;
+                    x[c] = xv[u] + (alpha * ppv[u] + omega * ssv[u]);      // src/dev/FalmEqDevCall.cu:307
+                    const T rv = sv[u] - omega * tv[u];                    // :330
+                    r[c] = rv;
+                    const double rd = to_d(rv);
+                    acc[0] += rd * rd;
+                    acc[1] += rd * to_d(rrv[u]);
+                }
+            }
+        }
     }
     double tot[2];
     if (grid_sum<2>(acc, rw, tot) && threadIdx.x == 0) {

@@ -24,20 +24,30 @@ template <typename T> struct S7Conf;
 template <> struct S7Conf<double> { static constexpr int NS = 6; };
 template <> struct S7Conf<float> { static constexpr int NS = 8; };
 
+// resident CTAs per SM asked of the register allocator: 4 for FP32 arithmetic
+// on an FP32 field (at most 64 registers), fewer where the body works in FP64
+template <typename T, class Body>
+constexpr int s7_minb() { return (sizeof(T) == 4 && sizeof(typename Body::V) == 4) ? 4 : (sizeof(T) == 4 ? 3 : 2); }
+
 template <typename T>
 constexpr int s7_smem() { return S7Conf<T>::NS * S7Tile<T>::SLOT + 128 + 128; }
 
-// Body: bool skip() const; const T *pw() const (pointwise operand, or null);
-//       const Op7<T> &op_() const;
+// Body: type V (the stencil's arithmetic type: T, or double for an FP64
+//       residual of an FP32 field); bool skip() const; const T *pw() const
+//       (pointwise operand, or null); const Op7<T> &op_() const;
 //       void cell(i, j, k, cc, a, xc, xe, xw, xn, xs, xt, xb, pv, acc); void finish(tot)
-// The kernel hoists the x/y part of the operator out of the z march and passes
-// the cell's coefficients a (Coef7).
+// The kernel hoists the x/y part of the operator out of the z march, loads the
+// z part once per plane for all rows of a thread, and passes the cell's
+// coefficients a (Coef7<V>) and neighbours in V: the column coefficients are
+// converted once per column, the -1 neighbour is carried from the previous
+// plane already converted.
 // The pointwise operand of the next plane is loaded one iteration ahead (pv),
 // so its latency overlaps the current plane's wait and arithmetic.
 template <typename T, int NV, class Body>
-__global__ void __launch_bounds__(256) k_s7_tma(Geom g, int kc, const __grid_constant__ CUtensorMap mx, Body body,
+__global__ void __launch_bounds__(256, (s7_minb<T, Body>())) k_s7_tma(Geom g, int kc, const __grid_constant__ CUtensorMap mx, Body body,
                                               RedWork rw, int *err) {
     using L = S7Tile<T>;
+    using V = typename Body::V;
     constexpr int NS = S7Conf<T>::NS;
     extern __shared__ unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
@@ -97,17 +107,20 @@ __global__ void __launch_bounds__(256) k_s7_tma(Geom g, int kc, const __grid_con
     const long long sxy = (long long)g.sx * g.sy;
     const Op7<T> &op = body.op_();
     long long ccr[RY];
-    T pv[RY], xm[RY];
+    T pv[RY];
+    V xm[RY];
     typename Op7<T>::Col col[RY];
+    V cwv[RY], cev[RY], csv[RY], cnv[RY];
 #pragma unroll
     for (int r = 0; r < RY; r++) {
         ccr[r] = g.id(i, jr[r], P0 + 1);   // cell of the first computed plane
         pv[r] = (pw && act[r]) ? pw[ccr[r]] : T(0);
         col[r] = op.column(min(i, g.sx - g.gc - 1), min(jr[r], g.sy - g.gc - 1));
+        cwv[r] = (V)col[r].aw; cev[r] = (V)col[r].ae; csv[r] = (V)col[r].as; cnv[r] = (V)col[r].an;
     }
     if (__syncthreads_or(fail)) goto drain;
 #pragma unroll
-    for (int r = 0; r < RY; r++) xm[r] = slot(0)[orr[r]];
+    for (int r = 0; r < RY; r++) xm[r] = (V)slot(0)[orr[r]];
     for (int q = 1; q < nplanes - 1; q++) {
         T pn[RY];
 #pragma unroll
@@ -121,13 +134,22 @@ __global__ void __launch_bounds__(256) k_s7_tma(Geom g, int kc, const __grid_con
         }
         const T *X0 = slot(q), *X1 = slot(q + 1);
         const int k = P0 + q;
+        const typename Op7<T>::ZPl zp = op.zplane(k);
+        const V abv = (V)zp.ab, atv = (V)zp.at;
 #pragma unroll
         for (int r = 0; r < RY; r++) {
             const int o = orr[r];
-            const T xc = X0[o];
+            const V xc = (V)X0[o];
             if (act[r]) {
-                const Coef7<T> a = op.at_col(col[r], k, ccr[r]);
-                body.cell(i, jr[r], k, ccr[r], a, xc, X0[o + 1], X0[o - 1], X0[o + L::BX], X0[o - L::BX], X1[o], xm[r], pv[r], acc);
+                Coef7<V> a;
+                if (op.A) {
+                    const Coef7<T> e = op.at_col(col[r], k, ccr[r]);
+                    a = Coef7<V>{(V)e.ac, (V)e.aw, (V)e.ae, (V)e.as, (V)e.an, (V)e.ab, (V)e.at};
+                } else {
+                    a = Coef7<V>{(V)op.ac_col(col[r], zp), cwv[r], cev[r], csv[r], cnv[r], abv, atv};
+                }
+                body.cell(i, jr[r], k, ccr[r], a, xc, (V)X0[o + 1], (V)X0[o - 1], (V)X0[o + L::BX], (V)X0[o - L::BX], (V)X1[o], xm[r],
+                          pv[r], acc);
             }
             xm[r] = xc;
             pv[r] = pn[r];
@@ -153,6 +175,7 @@ __device__ __forceinline__ T dot7(T ac, T ae, T aw, T an, T as, T at, T ab, T xc
 // red-black SOR half sweep (src/dev/FalmEqDevCall.cu:175-211), in place
 template <typename T>
 struct SorBody {
+    using V = T;
     Op7<T> op;
     T *x;
     const T *b;
@@ -174,6 +197,7 @@ struct SorBody {
 // ax = A x (src/dev/MVDevCall.cu:152-183)
 template <typename T>
 struct MvBody {
+    using V = T;
     Op7<T> op;
     T *ax;
     __device__ bool skip() const { return false; }
@@ -189,6 +213,7 @@ struct MvBody {
 // q = A pp and alpha = rho / (rr . q)
 template <typename T>
 struct MvDot1Body {
+    using V = T;
     Op7<T> op;
     T *q;
     const T *rr;
@@ -212,6 +237,7 @@ struct MvDot1Body {
 // t = A ss and omega = (t.s)/(t.t)
 template <typename T>
 struct MvDot2Body {
+    using V = T;
     Op7<T> op;
     T *t;
     const T *s;
@@ -237,6 +263,7 @@ struct MvDot2Body {
 // r = b - A x (FP64 arithmetic), rr = r, solver start (see k_res)
 template <typename T>
 struct ResBody {
+    using V = double;
     Op7<T> op;
     const T *b;
     T *r, *rr;
@@ -245,8 +272,8 @@ struct ResBody {
     __device__ bool skip() const { return false; }
     __device__ const T *pw() const { return b; }
     __device__ const Op7<T> &op_() const { return op; }
-    __device__ void cell(int i, int j, int k, long long c, const Coef7<T> &a, T xc, T xe, T xw, T xn, T xs, T xt, T xb, T bv,
-                         double (&acc)[2]) const {
+    __device__ void cell(int i, int j, int k, long long c, const Coef7<double> &a, double xc, double xe, double xw, double xn,
+                         double xs, double xt, double xb, T bv, double (&acc)[2]) const {
         double rv = to_d(bv) - dot7<double>(a.ac, a.ae, a.aw, a.an, a.as, a.at, a.ab, xc, xe, xw, xn, xs, xt, xb);
         T rt = (T)rv;
         r[c] = rt;

@@ -17,15 +17,11 @@
 // the thread updates that one in every half sweep whose ring holds it, with
 // the pair's x/y operator coefficients kept in registers.
 #pragma once
+#include <type_traits>
 #include "poisson.cuh"
 #include "tma.cuh"
 
 namespace fb {
-
-// the SOR correction (b - Ax)/ac: IEEE division in FP64; in FP32 (mixed
-// precision) the fast division, within 2 ulp
-__device__ __forceinline__ double sor_div(double a, double b) { return a / b; }
-__device__ __forceinline__ float sor_div(float a, float b) { return __fdividef(a, b); }
 
 template <typename T, int H>
 struct RBTile {
@@ -173,6 +169,215 @@ __global__ void __launch_bounds__(256) k_sor_rb_tma(Geom g, int kc, const __grid
         }
         // plane q-H-1 was last read by half sweep H above and by the previous
         // iteration's write-out, both behind a barrier: refill its slot
+        {
+            const int qn = q - H - 1 + (int)NS;
+            if (q - H - 1 >= 0 && qn < nplanes) {
+                if (threadIdx.x == 0) { fence_proxy_async(); issue(qn); }
+                issued = qn + 1;
+            }
+        }
+    }
+    return;
+drain:
+    for (int q = waited; q < issued; q++) wait_q(q);
+}
+
+}  // namespace fb
+
+namespace fb {
+
+// Three half sweeps per pass on a 28 x 16 tile (FP32 path).
+//
+// Same wavefront as k_sor_rb_tma; the work of a half sweep is laid out for
+// shared-memory banks and issue slots:
+//  * 160 threads; thread t owns pair column m = t % 16 (cells x0 = i0-2+2m and
+//    x0+1) in rows rw and rw+10 of the widest ring (rw = t / 16), so a half
+//    warp covers one row and the two halves of a warp cover adjacent rows.
+//    Same-colour cells of adjacent rows sit on opposite bank parities (the box
+//    pitch is even), so every shared access of a half sweep is one wavefront.
+//  * the two rows of a thread have the same parity, hence the same colour
+//    offset e: one test and one address per half sweep serve both updates,
+//    with the x coefficients shared.
+//  * the right-hand side is staged as its own (32 x 20) box covering just the
+//    cells a half sweep updates.
+template <typename T>
+struct RB2Tile {
+    static constexpr int H = 3, R = H - 1;
+    static constexpr int TX = 28, TY = 16;
+    static constexpr int AL = 16 / (int)sizeof(T);                       // TMA x alignment (elements)
+    static constexpr int HX = H + ((2 - H) % AL + AL) % AL;              // i0 - HX on the alignment for gc = 2
+    static constexpr int BX = (HX + TX + H + AL - 1) / AL * AL, BY = TY + 2 * H, PE = BX * BY;
+    static constexpr int BXB = 32, BYB = TY + 2 * R, PEB = BXB * BYB;    // right-hand side box from i0 - 2
+    static constexpr int PBX = (PE * (int)sizeof(T) + 127) / 128 * 128, PBB = (PEB * (int)sizeof(T) + 127) / 128 * 128;
+    static constexpr int SLOT = PBX + PBB;
+    static constexpr int NS = 8;
+    static constexpr int PX = 16, PY = TY + 2 * R, HALF = PY / 2;        // pairs per row, rows, rows per set
+    static constexpr int NT = PX * HALF;                                  // threads
+    static constexpr int SMEM = NS * SLOT + 128 + 128;
+    static_assert(PY % 4 == 0, "the two rows of a thread have the same parity");
+    static_assert(R <= 2 && TX + R <= 2 * PX - 2, "the pair columns (x from i0 - 2) cover the widest ring");
+};
+
+template <typename T>
+__global__ void __launch_bounds__(RB2Tile<T>::NT) k_sor_rb2_tma(Geom g, int kc, const __grid_constant__ CUtensorMap mx,
+                                                              const __grid_constant__ CUtensorMap mb, PoissonTables<T> tb,
+                                                              T *__restrict__ xout, T omega, int c1, const SolverScalars *sc,
+                                                              int *err) {
+    using L = RB2Tile<T>;
+    constexpr int H = L::H;
+    constexpr unsigned NS = L::NS;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+    uint64_t *bar = (uint64_t *)(smem + NS * L::SLOT);
+    if (sc && sc->done) return;
+    const int i0 = g.gc + blockIdx.x * L::TX, j0 = g.gc + blockIdx.y * L::TY;
+    const int k0 = g.gc + blockIdx.z * kc, k1 = min(k0 + kc, g.sz - g.gc);
+    const int P0 = k0 - H, nplanes = (k1 + H) - P0;
+    const int xb = max(0, box_origin(i0 - L::HX, L::BX, g.sx, L::AL));
+    const int yb = max(0, box_origin(j0 - H, L::BY, g.sy, 1));
+    const int xbb = max(0, box_origin(i0 - 2, L::BXB, g.sx, L::AL));
+    const int ybb = max(0, box_origin(j0 - L::R, L::BYB, g.sy, 1));
+    const int ilo = g.gc, ihi = g.sx - g.gc, jlo = g.gc, jhi = g.sy - g.gc, klo = g.gc, khi = g.sz - g.gc;
+    const int t = threadIdx.x;
+    const int x0 = i0 - 2 + 2 * (t % L::PX);
+    const int yr[2] = {j0 - L::R + t / L::PX, j0 - L::R + t / L::PX + L::HALF};
+    // live bits: bit 3*(2s+e) + h-1 when cell e of set s takes part in half sweep h
+    // (inside ring H-h of the tile and inside the interior), after a check that
+    // its radius-1 neighbourhood lies in the staged boxes
+    unsigned live = 0u;
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            const int x = x0 + e, y = yr[s];
+            unsigned bits = 0u;
+#pragma unroll
+            for (int h = 1; h <= H; h++) {
+                const int ring = H - h;
+                const bool in = y >= j0 - ring && y < j0 + L::TY + ring && y >= jlo && y < jhi && x >= i0 - ring &&
+                                x < i0 + L::TX + ring && x >= ilo && x < ihi;
+                bits |= (in ? 1u : 0u) << (h - 1);
+            }
+            if (bits && (x - 1 < xb || x + 1 >= xb + L::BX || y - 1 < yb || y + 1 >= yb + L::BY || x < xbb ||
+                         x >= xbb + L::BXB || y < ybb || y >= ybb + L::BYB)) {
+                atomicExch(err, 300 + 5);
+                bits = 0u;
+            }
+            live |= bits << (3 * (2 * s + e));
+        }
+    }
+    // x coefficients of the pair's two cells, y coefficients of the two rows
+    T aw[2], ae[2], an[2], as[2], dxy[2][2];
+    {
+        const int xc0 = min(max(x0, 0), g.sx - 1), xc1 = min(max(x0 + 1, 0), g.sx - 1);
+        aw[0] = ldg(tb.cm[0] + xc0); ae[0] = ldg(tb.cp[0] + xc0);
+        aw[1] = ldg(tb.cm[0] + xc1); ae[1] = ldg(tb.cp[0] + xc1);
+        const T d0 = ldg(tb.dx0 + xc0), d1 = ldg(tb.dx0 + xc1);
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+            const int yc = min(max(yr[s], 0), g.sy - 1);
+            as[s] = ldg(tb.cm[1] + yc); an[s] = ldg(tb.cp[1] + yc);
+            const T up1 = ldg(tb.up[1] + yc), um1 = ldg(tb.um[1] + yc);
+            dxy[s][0] = (d0 - up1) - um1;   // same association as Op7::get
+            dxy[s][1] = (d1 - up1) - um1;
+        }
+    }
+    // element offsets of cell x0 in the x box and the right-hand side box (set 0;
+    // set 1 is HALF rows further); used only for live cells
+    const int ox = (yr[0] - yb) * L::BX + (x0 - xb);
+    const int obx = (yr[0] - ybb) * L::BXB + (x0 - xbb);
+    auto slot = [&](int q) { return smem + ((unsigned)q % NS) * L::SLOT; };
+    auto issue = [&](int q) {
+        uint64_t *b = bar + ((unsigned)q % NS);
+        const int z = P0 + q;
+        if (z < 0 || z >= g.sz) { mbar_arrive(b); return; }
+        unsigned char *s = slot(q);
+        if (tma_ok(s, xb, yb, z, (int)sizeof(T), g.sx, g.sy, g.sz) && tma_ok(s + L::PBX, xbb, ybb, z, (int)sizeof(T), g.sx, g.sy, g.sz)) {
+            mbar_expect_tx(b, (L::PE + L::PEB) * sizeof(T));
+            tma_load_4d(s, &mx, xb, yb, z, 0, b);
+            tma_load_4d(s + L::PBX, &mb, xbb, ybb, z, 0, b);
+        } else {
+            tma_reject(b, err, 5);
+        }
+    };
+    auto wait_q = [&](int q) -> bool { return threadIdx.x >= 32 || mbar_wait(bar + ((unsigned)q % NS), ((unsigned)q / NS) & 1, err); };
+    if (threadIdx.x == 0) {
+        prefetch_tmap(&mx); prefetch_tmap(&mb);
+        for (unsigned s = 0; s < NS; s++) mbar_init(bar + s, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    int issued = min((int)NS, nplanes), waited = 0;
+    if (threadIdx.x == 0)
+        for (int q = 0; q < issued; q++) issue(q);
+    const long long sxy = (long long)g.sx * g.sy;
+    unsigned char *sl[H + 2];
+    T zab[H], zat[H], zup[H], zum[H];
+#pragma unroll
+    for (int m = 0; m < H + 2; m++) sl[m] = slot(-1 - m);
+#pragma unroll
+    for (int h = 0; h < H; h++) { zab[h] = zat[h] = zup[h] = zum[h] = T(0); }
+    const T scale = tb.scale;
+    for (int q = 0; q < nplanes; q++) {
+#pragma unroll
+        for (int m = H + 1; m > 0; m--) sl[m] = sl[m - 1];
+        sl[0] = slot(q);
+#pragma unroll
+        for (int h = H - 1; h > 0; h--) { zab[h] = zab[h - 1]; zat[h] = zat[h - 1]; zup[h] = zup[h - 1]; zum[h] = zum[h - 1]; }
+        {
+            const int kz = min(max(P0 + q - 1, 0), g.sz - 1);
+            zab[0] = ldg(tb.cm[2] + kz); zat[0] = ldg(tb.cp[2] + kz); zup[0] = ldg(tb.up[2] + kz); zum[0] = ldg(tb.um[2] + kz);
+        }
+        bool fail = !wait_q(q);
+        waited = q + 1;
+        if (__syncthreads_or(fail)) goto drain;
+#pragma unroll
+        for (int h = 1; h <= H; h++) {
+            const int p = q - h, kp = P0 + p, ring = H - h;
+            if (p >= 1 && kp >= max(klo, k0 - ring) && kp < min(khi, k1 + ring)) {
+                const int color = (c1 + h - 1) & 1;
+                const int e = (color ^ (x0 + yr[0] + kp)) & 1;   // the pairs' cell of this colour (both rows)
+                const unsigned l0 = (live >> (3 * e + h - 1)) & 1u, l1 = (live >> (3 * (2 + e) + h - 1)) & 1u;
+                T *X0 = (T *)sl[h];
+                const T *Xm = (const T *)sl[h + 1], *Xp = (const T *)sl[h - 1];
+                const T *B0 = (const T *)(sl[h] + L::PBX);
+                const T ab = zab[h - 1], at = zat[h - 1], zu = zup[h - 1], zm = zum[h - 1];
+                const T awe = e ? aw[1] : aw[0], aee = e ? ae[1] : ae[0];
+#pragma unroll
+                for (int s = 0; s < 2; s++) {
+                    if (s == 0 ? l0 : l1) {
+                        const int o = ox + s * L::HALF * L::BX + e;
+                        const T ac = (((e ? dxy[s][1] : dxy[s][0]) - zu) - zm) * scale;
+                        const T xc = X0[o];
+                        const T r7 = ac * xc + aee * X0[o + 1] + awe * X0[o - 1] + an[s] * X0[o + L::BX] + as[s] * X0[o - L::BX] +
+                                     at * Xp[o] + ab * Xm[o];
+                        X0[o] = xc + omega * sor_div(B0[obx + s * L::HALF * L::BXB + e] - r7, ac);
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        // the tile of plane q-H is final: pairs of cells out, two per row and thread step
+        {
+            const int kp = P0 + q - H;
+            if (kp >= k0 && kp < k1) {
+                const T *Xf = (const T *)sl[H];
+                T *plane = xout + (long long)kp * sxy;
+                for (int w = t; w < (L::TX / 2) * L::TY; w += L::NT) {
+                    const int wx = i0 + 2 * (w % (L::TX / 2)), wy = j0 + w / (L::TX / 2);
+                    if (wx < ihi && wy < jhi) {
+                        const int so = (wy - yb) * L::BX + (wx - xb);
+                        const long long go = (long long)wy * g.sx + wx;
+                        if (wx + 1 < ihi) {
+                            using V2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+                            *reinterpret_cast<V2 *>(plane + go) = *reinterpret_cast<const V2 *>(Xf + so);
+                        } else {
+                            plane[go] = Xf[so];
+                        }
+                    }
+                }
+            }
+        }
         {
             const int qn = q - H - 1 + (int)NS;
             if (q - H - 1 >= 0 && qn < nplanes) {
