@@ -65,10 +65,10 @@ __device__ __forceinline__ void warp_sum(double (&v)[NV]) {
 // Deterministic grid reduction.  Every block stores one partial per value;
 // the last block to arrive sums the partials in a fixed order and returns
 // true (all its threads), with the totals in out[] (valid in every thread of
-// that block).  Other blocks return false.
-template <int NV>
+// that block).  Other blocks return false.  NW: warps per block.
+template <int NV, int NW = kWarpsPerBlock>
 __device__ bool grid_sum(double (&v)[NV], const RedWork &rw, double (&out)[NV]) {
-    __shared__ double sm[NV][kWarpsPerBlock];
+    __shared__ double sm[NV][NW];
     __shared__ bool last;
     __shared__ double tot[NV];
     warp_sum<NV>(v);
@@ -83,7 +83,7 @@ __device__ bool grid_sum(double (&v)[NV], const RedWork &rw, double (&out)[NV]) 
 #pragma unroll
         for (int d = 0; d < NV; d++) {
             double s = 0.0;
-            for (int w = 0; w < kWarpsPerBlock; w++) s += sm[d][w];
+            for (int w = 0; w < NW; w++) s += sm[d][w];
             rw.partials[d * rw.maxBlocks + bid] = s;
         }
         __threadfence();
@@ -109,7 +109,7 @@ __device__ bool grid_sum(double (&v)[NV], const RedWork &rw, double (&out)[NV]) 
 #pragma unroll
         for (int d = 0; d < NV; d++) {
             double s = 0.0;
-            for (int w = 0; w < kWarpsPerBlock; w++) s += sm[d][w];
+            for (int w = 0; w < NW; w++) s += sm[d][w];
             tot[d] = s;
         }
         *rw.counter = 0u;

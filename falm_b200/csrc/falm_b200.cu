@@ -559,13 +559,20 @@ int pseudo_u_t(falm_ctx *ctx, const T *un, const T *u, const T *uu, T *ua, const
     CUtensorMap mu, muu, mnut;
     if (!ctx->no_tma && make_map(ctx, &mu, u, 3, L::BX, L::BY) && make_map(ctx, &muu, uu, 3, L::BX, L::BY) &&
         make_map(ctx, &mnut, nut, 1, L::BX, L::BY)) {
-        cudaFuncSetAttribute(k_pseudo_u_tma<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
+        auto kern = k_pseudo_u_tma<T, NS, FALM_ADV_KK>;
+        switch (ctx->adv) {
+            case FALM_ADV_UPWIND1: kern = k_pseudo_u_tma<T, NS, FALM_ADV_UPWIND1>; break;
+            case FALM_ADV_UPWIND3: kern = k_pseudo_u_tma<T, NS, FALM_ADV_UPWIND3>; break;
+            case FALM_ADV_QUICK: kern = k_pseudo_u_tma<T, NS, FALM_ADV_QUICK>; break;
+            case FALM_ADV_UTOPIA: kern = k_pseudo_u_tma<T, NS, FALM_ADV_UTOPIA>; break;
+            default: break;
+        }
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
         const int bx = (g.nx + L::TX - 1) / L::TX, by = (g.ny + L::TY - 1) / L::TY;
         const int kc = chunk_len(ctx, (long long)bx * by, g.nz, sizeof(T) == 8 ? 2 : 3, 64);
         dim3 grid(bx, by, (g.nz + kc - 1) / kc);
-        LAUNCH(FALM_K_PSEUDO_U, st, k_pseudo_u_tma<T, NS><<<grid, 256, L::SMEM, st>>>(g, kc, mview<T>(ctx), mu, muu, mnut, un,
-                                                                                     un == u ? 1 : 0, ua, ff, af, (T)(1.0 / ctx->Re),
-                                                                                     (T)dt, ctx->adv, ctx->kerr));
+        LAUNCH(FALM_K_PSEUDO_U, st, kern<<<grid, 256, L::SMEM, st>>>(g, kc, mview<T>(ctx), mu, muu, mnut, un, un == u ? 1 : 0, ua, ff, af,
+                                                                    (T)(1.0 / ctx->Re), (T)dt, ctx->kerr));
         return FALM_OK;
     }
     LAUNCH(FALM_K_PSEUDO_U, st, k_pseudo_u<T><<<row_grid(ctx, R), kRowThreads, 0, st>>>(ctx->geo, R, mview<T>(ctx), un, u, uu, ua, nut, ff, af,

@@ -23,6 +23,22 @@
 
 namespace fb {
 
+// one red-black SOR update of cell c from its six neighbours, with the fused
+// multiply-adds spelled out so that every blocked kernel rounds the same way:
+// x_c + omega (b_c - (ac x_c + ae x_e + aw x_w + an x_n + as x_s + at x_t + ab x_b)) / ac
+template <typename T>
+__device__ __forceinline__ T sor_point(T ac, T ae, T aw, T an, T as, T at, T ab, T xc, T xe, T xw, T xn, T xs, T xt, T xb, T bc,
+                                       T omega) {
+    T r7 = ac * xc;
+    r7 = fma(ae, xe, r7);
+    r7 = fma(aw, xw, r7);
+    r7 = fma(an, xn, r7);
+    r7 = fma(as, xs, r7);
+    r7 = fma(at, xt, r7);
+    r7 = fma(ab, xb, r7);
+    return fma(omega, sor_div(bc - r7, ac), xc);
+}
+
 template <typename T, int H>
 struct RBTile {
     static constexpr int TX = 32, TY = 8;
@@ -151,10 +167,8 @@ __global__ void __launch_bounds__(256) k_sor_rb_tma(Geom g, int kc, const __grid
                     const T ab = zab[h - 1], at = zat[h - 1];
                     const T ac = (((e ? dxy1 : dxy0) - zup[h - 1]) - zum[h - 1]) * tb.scale;
                     const int o = o0 + e;
-                    const T xc = X0[o];
-                    const T r7 = ac * xc + (e ? ae1 : ae0) * X0[o + 1] + (e ? aw1 : aw0) * X0[o - 1] + an * X0[o + L::BX] +
-                                 as * X0[o - L::BX] + at * Xp[o] + ab * Xm[o];
-                    X0[o] = xc + omega * sor_div(B0[o] - r7, ac);
+                    X0[o] = sor_point(ac, e ? ae1 : ae0, e ? aw1 : aw0, an, as, at, ab, X0[o], X0[o + 1], X0[o - 1], X0[o + L::BX],
+                                      X0[o - L::BX], Xp[o], Xm[o], B0[o], omega);
                 }
             }
             __syncthreads();
@@ -311,17 +325,27 @@ __global__ void __launch_bounds__(RB2Tile<T>::NT) k_sor_rb2_tma(Geom g, int kc, 
     if (threadIdx.x == 0)
         for (int q = 0; q < issued; q++) issue(q);
     const long long sxy = (long long)g.sx * g.sy;
-    unsigned char *sl[H + 2];
-    T zab[H], zat[H], zup[H], zum[H];
+    // write-out: this thread's cell pairs w = t and t + NT of the tile (14 pairs
+    // per row): offsets in the x box and in a plane of x_out, -1 when outside
+    constexpr int NW = ((L::TX / 2) * L::TY + L::NT - 1) / L::NT;
+    int wso[NW], wgo[NW];
+    bool wpair[NW];
 #pragma unroll
-    for (int m = 0; m < H + 2; m++) sl[m] = slot(-1 - m);
+    for (int n = 0; n < NW; n++) {
+        const int w = t + n * L::NT;
+        const int wx = i0 + 2 * (w % (L::TX / 2)), wy = j0 + w / (L::TX / 2);
+        const bool ok = w < (L::TX / 2) * L::TY && wx < ihi && wy < jhi;
+        wso[n] = ok ? (wy - yb) * L::BX + (wx - xb) : -1;
+        wgo[n] = wy * g.sx + wx;
+        wpair[n] = wx + 1 < ihi;
+    }
+    T zab[H], zat[H], zup[H], zum[H];
 #pragma unroll
     for (int h = 0; h < H; h++) { zab[h] = zat[h] = zup[h] = zum[h] = T(0); }
     const T scale = tb.scale;
     for (int q = 0; q < nplanes; q++) {
-#pragma unroll
-        for (int m = H + 1; m > 0; m--) sl[m] = sl[m - 1];
-        sl[0] = slot(q);
+        // slot of plane q - m
+        auto sl = [&](int m) { return smem + ((unsigned)(q - m) % NS) * L::SLOT; };
 #pragma unroll
         for (int h = H - 1; h > 0; h--) { zab[h] = zab[h - 1]; zat[h] = zat[h - 1]; zup[h] = zup[h - 1]; zum[h] = zum[h - 1]; }
         {
@@ -338,9 +362,9 @@ __global__ void __launch_bounds__(RB2Tile<T>::NT) k_sor_rb2_tma(Geom g, int kc, 
                 const int color = (c1 + h - 1) & 1;
                 const int e = (color ^ (x0 + yr[0] + kp)) & 1;   // the pairs' cell of this colour (both rows)
                 const unsigned l0 = (live >> (3 * e + h - 1)) & 1u, l1 = (live >> (3 * (2 + e) + h - 1)) & 1u;
-                T *X0 = (T *)sl[h];
-                const T *Xm = (const T *)sl[h + 1], *Xp = (const T *)sl[h - 1];
-                const T *B0 = (const T *)(sl[h] + L::PBX);
+                T *X0 = (T *)sl(h);
+                const T *Xm = (const T *)sl(h + 1), *Xp = (const T *)sl(h - 1);
+                const T *B0 = (const T *)(sl(h) + L::PBX);
                 const T ab = zab[h - 1], at = zat[h - 1], zu = zup[h - 1], zm = zum[h - 1];
                 const T awe = e ? aw[1] : aw[0], aee = e ? ae[1] : ae[0];
 #pragma unroll
@@ -348,31 +372,27 @@ __global__ void __launch_bounds__(RB2Tile<T>::NT) k_sor_rb2_tma(Geom g, int kc, 
                     if (s == 0 ? l0 : l1) {
                         const int o = ox + s * L::HALF * L::BX + e;
                         const T ac = (((e ? dxy[s][1] : dxy[s][0]) - zu) - zm) * scale;
-                        const T xc = X0[o];
-                        const T r7 = ac * xc + aee * X0[o + 1] + awe * X0[o - 1] + an[s] * X0[o + L::BX] + as[s] * X0[o - L::BX] +
-                                     at * Xp[o] + ab * Xm[o];
-                        X0[o] = xc + omega * sor_div(B0[obx + s * L::HALF * L::BXB + e] - r7, ac);
+                        X0[o] = sor_point(ac, aee, awe, an[s], as[s], at, ab, X0[o], X0[o + 1], X0[o - 1], X0[o + L::BX], X0[o - L::BX],
+                                          Xp[o], Xm[o], B0[obx + s * L::HALF * L::BXB + e], omega);
                     }
                 }
             }
             __syncthreads();
         }
-        // the tile of plane q-H is final: pairs of cells out, two per row and thread step
+        // the tile of plane q-H is final: pairs of cells out
         {
             const int kp = P0 + q - H;
             if (kp >= k0 && kp < k1) {
-                const T *Xf = (const T *)sl[H];
+                const T *Xf = (const T *)sl(H);
                 T *plane = xout + (long long)kp * sxy;
-                for (int w = t; w < (L::TX / 2) * L::TY; w += L::NT) {
-                    const int wx = i0 + 2 * (w % (L::TX / 2)), wy = j0 + w / (L::TX / 2);
-                    if (wx < ihi && wy < jhi) {
-                        const int so = (wy - yb) * L::BX + (wx - xb);
-                        const long long go = (long long)wy * g.sx + wx;
-                        if (wx + 1 < ihi) {
+#pragma unroll
+                for (int n = 0; n < NW; n++) {
+                    if (wso[n] >= 0) {
+                        if (wpair[n]) {
                             using V2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
-                            *reinterpret_cast<V2 *>(plane + go) = *reinterpret_cast<const V2 *>(Xf + so);
+                            *reinterpret_cast<V2 *>(plane + wgo[n]) = *reinterpret_cast<const V2 *>(Xf + wso[n]);
                         } else {
-                            plane[go] = Xf[so];
+                            plane[wgo[n]] = Xf[wso[n]];
                         }
                     }
                 }

@@ -28,12 +28,15 @@ struct PUTile {
     static constexpr uint32_t TX_BYTES = 7 * PE * sizeof(T);
 };
 
-// race-free FSPseudoU (src/dev/FalmCFDDevCall.cu:10-301), same expressions as k_pseudo_u
-template <typename T, int NS>
+// race-free FSPseudoU (src/dev/FalmCFDDevCall.cu:10-301), same expressions as
+// k_pseudo_u; one instantiation per advection scheme ADV (FALM_ADV_*), so the
+// three components' arithmetic is straight-line code
+template <typename T, int NS, int ADV>
 __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_pseudo_u_tma(Geom g, int kc, MetricView<T> mv,
     const __grid_constant__ CUtensorMap mu, const __grid_constant__ CUtensorMap muu,
     const __grid_constant__ CUtensorMap mnut, const T *__restrict__ un, int un_is_u, T *__restrict__ ua,
-    const T *__restrict__ ff, AlmFuse af, T ReI, T dt, int adv, int *err) {
+    const T *__restrict__ ff, AlmFuse af, T ReI, T dt, int *err) {
+    constexpr int adv = ADV;
     using L = PUTile<T, NS>;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bar = (uint64_t *)(smem + NS * L::SLOT);
@@ -197,7 +200,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_pseudo_u_tma(Ge
                 const T ue1 = Ud[o + 1], uw1 = Ud[o - 1], un1 = Ud[o + L::BX], us1 = Ud[o - L::BX];
                 const T ut1 = U1[d * L::PE + o], ub1 = um1[d];
                 T adv_v;
-                if (adv == FALM_ADV_UPWIND1) {
+                if constexpr (adv == FALM_ADV_UPWIND1) {
                     adv_v = T(0);
                     adv_v += upwind_flux1(ucc, ue1, UE);
                     adv_v -= upwind_flux1(uw1, ucc, UW);
@@ -209,7 +212,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_pseudo_u_tma(Ge
                 } else {
                     const T ue2 = Ud[o + 2], uw2 = Ud[o - 2], un2 = Ud[o + 2 * L::BX], us2 = Ud[o - 2 * L::BX];
                     const T ut2 = U2[d * L::PE + o], ub2 = um2[d];
-                    if (adv == FALM_ADV_QUICK) {
+                    if constexpr (adv == FALM_ADV_QUICK) {
                         adv_v = T(0.);
                         axis_quick(adv_v, ucc, ue1, ue2, uw1, uw2, UE, UW);
                         axis_quick(adv_v, ucc, un1, un2, us1, us2, VN, VS);

@@ -20,6 +20,8 @@
 namespace fb {
 
 constexpr unsigned kWaitLimit = 1u << 28;   // polls of try_wait (the clock64 bound of ~1 s normally ends a wait first)
+constexpr unsigned kSuspendNs = 200000;     // suspend-time hint of one try_wait (ns): the thread sleeps until the phase
+                                            // completes or this much time has passed
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -39,24 +41,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(parity)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(kSuspendNs)
         : "memory");
     return ok != 0;
 }
 
 // bounded wait: try_wait suspends the thread in hardware until the phase
-// completes or a short time limit passes; poll it, checking clock64 every 64
-// polls, and give up after about one second (or kWaitLimit polls): false (and
-// *err set) then
+// completes or the suspend-time hint passes; poll it, checking clock64 every
+// 4 polls, and give up after about one second (or kWaitLimit polls): false
+// (and *err set) then
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     for (unsigned it = 1; it < kWaitLimit; it++) {
         if (mbar_try_wait(bar, parity)) return true;
-        if ((it & 63u) == 0 && clock64() - t0 > 2000000000LL) break;
+        if ((it & 3u) == 0 && clock64() - t0 > 2000000000LL) break;
     }
     if (err) atomicExch(err, FALM_ERR_TIMEOUT);
     return false;
