@@ -279,9 +279,11 @@ int sor_rb2_launch(falm_ctx *ctx, cudaStream_t st, const T *xin, const T *b, T *
 
 template <typename T>
 int sor_rb_launch(falm_ctx *ctx, cudaStream_t st, int H, const T *xin, const T *b, T *xout, T omega, int c1, const SolverScalars *sc) {
-    if (H == 3 && sizeof(T) == 4 && !ctx->sor_v1) {
-        const int r = sor_rb2_launch<T>(ctx, st, xin, b, xout, omega, c1, sc);
-        if (r != 0) return r;
+    if constexpr (sizeof(T) == 4) {
+        if (H == 3 && !ctx->sor_v1) {
+            const int r = sor_rb2_launch<T>(ctx, st, xin, b, xout, omega, c1, sc);
+            if (r != 0) return r;
+        }
     }
     if (H == 1) return sor_rb_launch_h<T, 1>(ctx, st, xin, b, xout, omega, c1, sc);
     if (H == 2) return sor_rb_launch_h<T, 2>(ctx, st, xin, b, xout, omega, c1, sc);

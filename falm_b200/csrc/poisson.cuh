@@ -100,9 +100,15 @@ struct Op7 {
 };
 
 // the SOR / Jacobi correction (b - Ax)/ac: IEEE division in FP64; in FP32
-// (mixed precision) the fast division, within 2 ulp
+// (mixed precision) the numerator times the hardware reciprocal approximation
+// (PTX rcp.approx, 1 ulp), within 2 ulp of the quotient
+__device__ __forceinline__ float rcp_approx(float b) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(b));
+    return r;
+}
 __device__ __forceinline__ double sor_div(double a, double b) { return a / b; }
-__device__ __forceinline__ float sor_div(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ float sor_div(float a, float b) { return a * rcp_approx(b); }
 
 // ac*xc + ae*xe + aw*xw + an*xn + as*xs + at*xt + ab*xb  (src/dev/MVDevCall.cu:181)
 template <typename T, typename A>

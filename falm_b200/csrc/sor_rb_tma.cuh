@@ -210,10 +210,13 @@ namespace fb {
 //    Same-colour cells of adjacent rows sit on opposite bank parities (the box
 //    pitch is even), so every shared access of a half sweep is one wavefront.
 //  * the two rows of a thread have the same parity, hence the same colour
-//    offset e: one test and one address per half sweep serve both updates,
-//    with the x coefficients shared.
+//    offset e: both updates run as one pair through the packed FP32 units
+//    (fma/add/mul.f32x2), each lane rounding exactly as the scalar
+//    sor_point() does.
 //  * the right-hand side is staged as its own (32 x 20) box covering just the
 //    cells a half sweep updates.
+//  * the plane loop is unrolled over the NS slots, so every slot address is a
+//    constant offset.
 template <typename T>
 struct RB2Tile {
     static constexpr int H = 3, R = H - 1;
@@ -232,14 +235,34 @@ struct RB2Tile {
     static_assert(R <= 2 && TX + R <= 2 * PX - 2, "the pair columns (x from i0 - 2) cover the widest ring");
 };
 
+// a . b + c etc. on both lanes, each lane rounded as the scalar operation
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+// the two same-colour updates of a thread (lane s: row set s), lane by lane
+// the operations of sor_point()
+__device__ __forceinline__ float2 sor_point2(float2 ac, float2 ae, float2 aw, float2 an, float2 as, float2 at, float2 ab, float2 xc,
+                                             float2 xe, float2 xw, float2 xn, float2 xs, float2 xt, float2 xb, float2 bc, float2 omega) {
+    float2 r7 = __fmul2_rn(ac, xc);
+    r7 = __ffma2_rn(ae, xe, r7);
+    r7 = __ffma2_rn(aw, xw, r7);
+    r7 = __ffma2_rn(an, xn, r7);
+    r7 = __ffma2_rn(as, xs, r7);
+    r7 = __ffma2_rn(at, xt, r7);
+    r7 = __ffma2_rn(ab, xb, r7);
+    const float2 d = __ffma2_rn(r7, f2(-1.f, -1.f), bc);                 // bc - r7, one rounding
+    const float2 c = __fmul2_rn(d, f2(rcp_approx(ac.x), rcp_approx(ac.y)));
+    return __ffma2_rn(omega, c, xc);
+}
+
 template <typename T>
-__global__ void __launch_bounds__(RB2Tile<T>::NT) k_sor_rb2_tma(Geom g, int kc, const __grid_constant__ CUtensorMap mx,
+__global__ void __launch_bounds__(RB2Tile<T>::NT, 4) k_sor_rb2_tma(Geom g, int kc, const __grid_constant__ CUtensorMap mx,
                                                               const __grid_constant__ CUtensorMap mb, PoissonTables<T> tb,
                                                               T *__restrict__ xout, T omega, int c1, const SolverScalars *sc,
                                                               int *err) {
+    static_assert(std::is_same<T, float>::value, "packed FP32 arithmetic");
     using L = RB2Tile<T>;
     constexpr int H = L::H;
-    constexpr unsigned NS = L::NS;
+    constexpr int NS = L::NS;
     extern __shared__ unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
     uint64_t *bar = (uint64_t *)(smem + NS * L::SLOT);
@@ -280,32 +303,45 @@ __global__ void __launch_bounds__(RB2Tile<T>::NT) k_sor_rb2_tma(Geom g, int kc, 
             live |= bits << (3 * (2 * s + e));
         }
     }
-    // x coefficients of the pair's two cells, y coefficients of the two rows
-    T aw[2], ae[2], an[2], as[2], dxy[2][2];
+    // coefficients as lane pairs: x ones (cell e, both lanes alike), y ones per
+    // row set, dxy per (set, e); same association as Op7::get
+    float2 aw2[2], ae2[2], an2, as2, dxy2[2];
     {
         const int xc0 = min(max(x0, 0), g.sx - 1), xc1 = min(max(x0 + 1, 0), g.sx - 1);
-        aw[0] = ldg(tb.cm[0] + xc0); ae[0] = ldg(tb.cp[0] + xc0);
-        aw[1] = ldg(tb.cm[0] + xc1); ae[1] = ldg(tb.cp[0] + xc1);
-        const T d0 = ldg(tb.dx0 + xc0), d1 = ldg(tb.dx0 + xc1);
+        const float aw0 = ldg(tb.cm[0] + xc0), ae0 = ldg(tb.cp[0] + xc0), aw1 = ldg(tb.cm[0] + xc1), ae1 = ldg(tb.cp[0] + xc1);
+        aw2[0] = f2(aw0, aw0); aw2[1] = f2(aw1, aw1); ae2[0] = f2(ae0, ae0); ae2[1] = f2(ae1, ae1);
+        const float d0 = ldg(tb.dx0 + xc0), d1 = ldg(tb.dx0 + xc1);
+        float as_[2], an_[2], dd[2][2];
 #pragma unroll
         for (int s = 0; s < 2; s++) {
             const int yc = min(max(yr[s], 0), g.sy - 1);
-            as[s] = ldg(tb.cm[1] + yc); an[s] = ldg(tb.cp[1] + yc);
-            const T up1 = ldg(tb.up[1] + yc), um1 = ldg(tb.um[1] + yc);
-            dxy[s][0] = (d0 - up1) - um1;   // same association as Op7::get
-            dxy[s][1] = (d1 - up1) - um1;
+            as_[s] = ldg(tb.cm[1] + yc); an_[s] = ldg(tb.cp[1] + yc);
+            const float up1 = ldg(tb.up[1] + yc), um1 = ldg(tb.um[1] + yc);
+            dd[s][0] = (d0 - up1) - um1;
+            dd[s][1] = (d1 - up1) - um1;
+        }
+        as2 = f2(as_[0], as_[1]); an2 = f2(an_[0], an_[1]);
+        dxy2[0] = f2(dd[0][0], dd[1][0]); dxy2[1] = f2(dd[0][1], dd[1][1]);
+    }
+    // element offsets of cell x0 of each row set in the x box and the
+    // right-hand side box, clamped into the boxes (exact for live cells; a
+    // lane whose cell is not live computes on some staged cell and stores nothing)
+    int ox[2], ob[2];
+    {
+        const int xcl = min(max(x0, xb + 1), xb + L::BX - 3), xbl = min(max(x0, xbb), xbb + L::BXB - 2);
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+            const int ycl = min(max(yr[s], yb + 1), yb + L::BY - 2), ybl = min(max(yr[s], ybb), ybb + L::BYB - 1);
+            ox[s] = (ycl - yb) * L::BX + (xcl - xb);
+            ob[s] = (ybl - ybb) * L::BXB + (xbl - xbb);
         }
     }
-    // element offsets of cell x0 in the x box and the right-hand side box (set 0;
-    // set 1 is HALF rows further); used only for live cells
-    const int ox = (yr[0] - yb) * L::BX + (x0 - xb);
-    const int obx = (yr[0] - ybb) * L::BXB + (x0 - xbb);
-    auto slot = [&](int q) { return smem + ((unsigned)q % NS) * L::SLOT; };
+    const int par0 = (x0 + yr[0]) & 1;
     auto issue = [&](int q) {
-        uint64_t *b = bar + ((unsigned)q % NS);
+        uint64_t *b = bar + (q % NS);
         const int z = P0 + q;
         if (z < 0 || z >= g.sz) { mbar_arrive(b); return; }
-        unsigned char *s = slot(q);
+        unsigned char *s = smem + (q % NS) * L::SLOT;
         if (tma_ok(s, xb, yb, z, (int)sizeof(T), g.sx, g.sy, g.sz) && tma_ok(s + L::PBX, xbb, ybb, z, (int)sizeof(T), g.sx, g.sy, g.sz)) {
             mbar_expect_tx(b, (L::PE + L::PEB) * sizeof(T));
             tma_load_4d(s, &mx, xb, yb, z, 0, b);
@@ -314,14 +350,14 @@ __global__ void __launch_bounds__(RB2Tile<T>::NT) k_sor_rb2_tma(Geom g, int kc, 
             tma_reject(b, err, 5);
         }
     };
-    auto wait_q = [&](int q) -> bool { return threadIdx.x >= 32 || mbar_wait(bar + ((unsigned)q % NS), ((unsigned)q / NS) & 1, err); };
+    auto wait_q = [&](int q) -> bool { return threadIdx.x >= 32 || mbar_wait(bar + (q % NS), (q / NS) & 1, err); };
     if (threadIdx.x == 0) {
         prefetch_tmap(&mx); prefetch_tmap(&mb);
-        for (unsigned s = 0; s < NS; s++) mbar_init(bar + s, 1);
+        for (int s = 0; s < NS; s++) mbar_init(bar + s, 1);
         mbar_fence_init();
     }
     __syncthreads();
-    int issued = min((int)NS, nplanes), waited = 0;
+    int issued = min(NS, nplanes), waited = 0;
     if (threadIdx.x == 0)
         for (int q = 0; q < issued; q++) issue(q);
     const long long sxy = (long long)g.sx * g.sy;
@@ -339,70 +375,73 @@ __global__ void __launch_bounds__(RB2Tile<T>::NT) k_sor_rb2_tma(Geom g, int kc, 
         wgo[n] = wy * g.sx + wx;
         wpair[n] = wx + 1 < ihi;
     }
-    T zab[H], zat[H], zup[H], zum[H];
+    // z coefficients of planes q-1 .. q-H as lane pairs (ab, at; -up, -um)
+    float2 zab[H], zat[H], zpn[H], zmn[H];
 #pragma unroll
-    for (int h = 0; h < H; h++) { zab[h] = zat[h] = zup[h] = zum[h] = T(0); }
-    const T scale = tb.scale;
-    for (int q = 0; q < nplanes; q++) {
-        // slot of plane q - m
-        auto sl = [&](int m) { return smem + ((unsigned)(q - m) % NS) * L::SLOT; };
+    for (int h = 0; h < H; h++) zab[h] = zat[h] = zpn[h] = zmn[h] = f2(0.f, 0.f);
+    const float2 sc2 = f2(tb.scale, tb.scale), om2 = f2(omega, omega);
+    for (int q0 = 0; q0 < nplanes; q0 += NS) {
 #pragma unroll
-        for (int h = H - 1; h > 0; h--) { zab[h] = zab[h - 1]; zat[h] = zat[h - 1]; zup[h] = zup[h - 1]; zum[h] = zum[h - 1]; }
-        {
-            const int kz = min(max(P0 + q - 1, 0), g.sz - 1);
-            zab[0] = ldg(tb.cm[2] + kz); zat[0] = ldg(tb.cp[2] + kz); zup[0] = ldg(tb.up[2] + kz); zum[0] = ldg(tb.um[2] + kz);
-        }
-        bool fail = !wait_q(q);
-        waited = q + 1;
-        if (__syncthreads_or(fail)) goto drain;
+        for (int u = 0; u < NS; u++) {
+            const int q = q0 + u;
+            if (q >= nplanes) break;
+            // slot of plane q - m (a constant once unrolled)
+            auto sl = [&](int m) { return smem + ((u - m + 2 * NS) % NS) * L::SLOT; };
 #pragma unroll
-        for (int h = 1; h <= H; h++) {
-            const int p = q - h, kp = P0 + p, ring = H - h;
-            if (p >= 1 && kp >= max(klo, k0 - ring) && kp < min(khi, k1 + ring)) {
-                const int color = (c1 + h - 1) & 1;
-                const int e = (color ^ (x0 + yr[0] + kp)) & 1;   // the pairs' cell of this colour (both rows)
-                const unsigned l0 = (live >> (3 * e + h - 1)) & 1u, l1 = (live >> (3 * (2 + e) + h - 1)) & 1u;
-                T *X0 = (T *)sl(h);
-                const T *Xm = (const T *)sl(h + 1), *Xp = (const T *)sl(h - 1);
-                const T *B0 = (const T *)(sl(h) + L::PBX);
-                const T ab = zab[h - 1], at = zat[h - 1], zu = zup[h - 1], zm = zum[h - 1];
-                const T awe = e ? aw[1] : aw[0], aee = e ? ae[1] : ae[0];
+            for (int h = H - 1; h > 0; h--) { zab[h] = zab[h - 1]; zat[h] = zat[h - 1]; zpn[h] = zpn[h - 1]; zmn[h] = zmn[h - 1]; }
+            {
+                const int kz = min(max(P0 + q - 1, 0), g.sz - 1);
+                const float vab = ldg(tb.cm[2] + kz), vat = ldg(tb.cp[2] + kz), vup = ldg(tb.up[2] + kz), vum = ldg(tb.um[2] + kz);
+                zab[0] = f2(vab, vab); zat[0] = f2(vat, vat); zpn[0] = f2(-vup, -vup); zmn[0] = f2(-vum, -vum);
+            }
+            bool fail = !wait_q(q);
+            waited = q + 1;
+            if (__syncthreads_or(fail)) goto drain;
 #pragma unroll
-                for (int s = 0; s < 2; s++) {
-                    if (s == 0 ? l0 : l1) {
-                        const int o = ox + s * L::HALF * L::BX + e;
-                        const T ac = (((e ? dxy[s][1] : dxy[s][0]) - zu) - zm) * scale;
-                        X0[o] = sor_point(ac, aee, awe, an[s], as[s], at, ab, X0[o], X0[o + 1], X0[o - 1], X0[o + L::BX], X0[o - L::BX],
-                                          Xp[o], Xm[o], B0[obx + s * L::HALF * L::BXB + e], omega);
+            for (int h = 1; h <= H; h++) {
+                const int p = q - h, kp = P0 + p, ring = H - h;
+                if (p >= 1 && kp >= max(klo, k0 - ring) && kp < min(khi, k1 + ring)) {
+                    const int color = (c1 + h - 1) & 1;
+                    const int e = (color ^ par0 ^ kp) & 1;   // the pairs' cell of this colour (both row sets)
+                    const unsigned l0 = (live >> (3 * e + h - 1)) & 1u, l1 = (live >> (3 * (2 + e) + h - 1)) & 1u;
+                    if (l0 | l1) {
+                        float *X0 = (float *)sl(h);
+                        const float *Xm = (const float *)sl(h + 1), *Xp = (const float *)sl(h - 1);
+                        const float *B0 = (const float *)(sl(h) + L::PBX);
+                        const int o0 = ox[0] + e, o1 = ox[1] + e;
+                        const float2 ac = __fmul2_rn(__fadd2_rn(__fadd2_rn(e ? dxy2[1] : dxy2[0], zpn[h - 1]), zmn[h - 1]), sc2);
+                        const float2 xc = f2(X0[o0], X0[o1]);
+                        const float2 r = sor_point2(ac, e ? ae2[1] : ae2[0], e ? aw2[1] : aw2[0], an2, as2, zat[h - 1], zab[h - 1], xc,
+                                                    f2(X0[o0 + 1], X0[o1 + 1]), f2(X0[o0 - 1], X0[o1 - 1]),
+                                                    f2(X0[o0 + L::BX], X0[o1 + L::BX]), f2(X0[o0 - L::BX], X0[o1 - L::BX]),
+                                                    f2(Xp[o0], Xp[o1]), f2(Xm[o0], Xm[o1]), f2(B0[ob[0] + e], B0[ob[1] + e]), om2);
+                        if (l0) X0[o0] = r.x;
+                        if (l1) X0[o1] = r.y;
                     }
                 }
+                __syncthreads();
             }
-            __syncthreads();
-        }
-        // the tile of plane q-H is final: pairs of cells out
-        {
-            const int kp = P0 + q - H;
-            if (kp >= k0 && kp < k1) {
-                const T *Xf = (const T *)sl(H);
-                T *plane = xout + (long long)kp * sxy;
+            // the tile of plane q-H is final: pairs of cells out
+            {
+                const int kp = P0 + q - H;
+                if (kp >= k0 && kp < k1) {
+                    const float *Xf = (const float *)sl(H);
+                    float *plane = xout + (long long)kp * sxy;
 #pragma unroll
-                for (int n = 0; n < NW; n++) {
-                    if (wso[n] >= 0) {
-                        if (wpair[n]) {
-                            using V2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
-                            *reinterpret_cast<V2 *>(plane + wgo[n]) = *reinterpret_cast<const V2 *>(Xf + wso[n]);
-                        } else {
-                            plane[wgo[n]] = Xf[wso[n]];
+                    for (int n = 0; n < NW; n++) {
+                        if (wso[n] >= 0) {
+                            if (wpair[n]) *reinterpret_cast<float2 *>(plane + wgo[n]) = *reinterpret_cast<const float2 *>(Xf + wso[n]);
+                            else plane[wgo[n]] = Xf[wso[n]];
                         }
                     }
                 }
             }
-        }
-        {
-            const int qn = q - H - 1 + (int)NS;
-            if (q - H - 1 >= 0 && qn < nplanes) {
-                if (threadIdx.x == 0) { fence_proxy_async(); issue(qn); }
-                issued = qn + 1;
+            {
+                const int qn = q - H - 1 + NS;
+                if (q - H - 1 >= 0 && qn < nplanes) {
+                    if (threadIdx.x == 0) { fence_proxy_async(); issue(qn); }
+                    issued = qn + 1;
+                }
             }
         }
     }
