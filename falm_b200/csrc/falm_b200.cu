@@ -479,8 +479,10 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
     };
     auto first_target = [&](T *z) -> T * { return (pct == FALM_LS_JACOBI && ((m - 1) & 1)) ? xp : z; };
     for (outer = 0; outer < max_outer; outer++) {
-        // outer > 0: true residual in FP64; stop when it meets the tolerance
-        S7_OR(FALM_K_RES, st, T, 2, x, (ResBody<T>{op, b, r, rr, sc, outer > 0 ? 1 : 0}),
+        // outer > 0: true residual in FP64; stop when it meets the tolerance.
+        // The first pass stores the residual in rr only (r equals rr until the
+        // pass's first k_bicg_xr, which writes r; the iteration reads rr before)
+        S7_OR(FALM_K_RES, st, T, 2, x, (ResBody<T>{op, b, outer > 0 ? r : nullptr, rr, sc, outer > 0 ? 1 : 0}),
               (k_res<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, r, rr, ctx->red, sc, outer > 0 ? 1 : 0)));
         if (outer > 0) {
             CK(cudaMemcpyAsync(ctx->scal_host, sc, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
@@ -491,12 +493,15 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
             CK(cudaMemcpyAsync(&sc->it, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
             CK(cudaStreamSynchronize(st));
         }
+        bool first_it = true;
         for (;;) {
-            LAUNCH(FALM_K_BICG_P, st, k_bicg_p<T><<<grid_p, kRowThreads, 0, st>>>(g, R, op, p, q, r, first_target(pp), pct, pcw, sc));
+            const T *rin = first_it ? rr : r;
+            first_it = false;
+            LAUNCH(FALM_K_BICG_P, st, k_bicg_p<T><<<grid_p, kRowThreads, 0, st>>>(g, R, op, p, q, rin, first_target(pp), pct, pcw, sc));
             if ((rc = precondition_rest(pp, p))) return rc;
             S7_OR(FALM_K_MV_DOT1, st, T, 1, pp, (MvDot1Body<T>{op, q, rr, sc}),
                   (k_mv_dot1<T><<<grid, kRowThreads, 0, st>>>(g, R, op, pp, q, rr, ctx->red, sc)));
-            LAUNCH(FALM_K_BICG_S, st, k_bicg_s<T><<<grid_s, kRowThreads, 0, st>>>(g, R, op, s, q, r, first_target(ss), pct, pcw, sc));
+            LAUNCH(FALM_K_BICG_S, st, k_bicg_s<T><<<grid_s, kRowThreads, 0, st>>>(g, R, op, s, q, rin, first_target(ss), pct, pcw, sc));
             if ((rc = precondition_rest(ss, s))) return rc;
             S7_OR(FALM_K_MV_DOT2, st, T, 2, ss, (MvDot2Body<T>{op, t, s, sc}),
                   (k_mv_dot2<T><<<grid, kRowThreads, 0, st>>>(g, R, op, ss, t, s, ctx->red, sc)));
@@ -510,6 +515,9 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
     }
     if (mixed && outer >= max_outer) {
         // report the true residual of the final iterate
+        LAUNCH(FALM_K_RES, st, k_res<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, r, nullptr, ctx->red, nullptr, 0));
+    } else if (std::min(outer, max_outer - 1) == 0 && ctx->scal_host->it == 0) {
+        // no iteration followed the first residual, which went to rr only
         LAUNCH(FALM_K_RES, st, k_res<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, r, nullptr, ctx->red, nullptr, 0));
     }
     if (it_out) *it_out = total_it;

@@ -276,7 +276,7 @@ struct ResBody {
                          double xs, double xt, double xb, T bv, double (&acc)[2]) const {
         double rv = to_d(bv) - dot7<double>(a.ac, a.ae, a.aw, a.an, a.as, a.at, a.ab, xc, xe, xw, xn, xs, xt, xb);
         T rt = (T)rv;
-        r[c] = rt;
+        if (r) r[c] = rt;
         if (rr) rr[c] = rt;
         acc[0] += rv * rv;
         acc[1] += to_d(rt) * to_d(rt);
