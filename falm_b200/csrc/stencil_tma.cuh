@@ -77,6 +77,14 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_pseudo_u_tma(Ge
     const T kxc = ldg(mv.m.k[0] + ic), kxe = ldg(mv.m.k[0] + ic + 1), kxw = ldg(mv.m.k[0] + ic - 1);
     const T kyc = ldg(mv.m.k[1] + jc), kyn = ldg(mv.m.k[1] + jc + 1), kys = ldg(mv.m.k[1] + jc - 1);
     T hzb = ldg(mv.m.h[2] + P0 + 1), hzk = ldg(mv.m.h[2] + P0 + 2), kzb = ldg(mv.m.k[2] + P0 + 1), kzk = ldg(mv.m.k[2] + P0 + 2);
+    // The face factors g_d(c) + g_d(c+-e_d) of the diffusion, g_d = ja k_d^2 and
+    // ja = hx hy hz, separate: an x/y face's is hz times a column constant, a z
+    // face's is hx hy times a plane constant (the reference's values up to
+    // rounding); 1/ja is the product of the inverse widths.
+    const T kxc2 = kxc * kxc, kyc2 = kyc * kyc;
+    const T Axe = Pc * kxc2 + Pe * (kxe * kxe), Axw = Pc * kxc2 + Pw * (kxw * kxw);
+    const T Ayn = Pc * kyc2 + Pn * (kyn * kyn), Ays = Pc * kyc2 + Ps * (kys * kys);
+    const T kxy = kxc * kyc;
     // force boxes whose x/y extent holds this column (bit t for box t)
     unsigned colmask = 0;
     if (!ff && af.apcount > 0) {
@@ -152,24 +160,21 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_pseudo_u_tma(Ge
         const T hzt = ldg(mv.m.h[2] + k + 1), kzt = ldg(mv.m.k[2] + k + 1);
         if (active) {
             const long long cc = g.id(i, j, k);
-            // metrics with the association of MetricView: ja = (hx*hy)*hz, g_d = (ja*k_d)*k_d
-            const T jacob = Pc * hzk;
-            const T gxcc = (jacob * kxc) * kxc, gxe1 = ((Pe * hzk) * kxe) * kxe, gxw1 = ((Pw * hzk) * kxw) * kxw;
-            const T gycc = (jacob * kyc) * kyc, gyn1 = ((Pn * hzk) * kyn) * kyn, gys1 = ((Ps * hzk) * kys) * kys;
-            const T gzcc = (jacob * kzk) * kzk, gzt1 = ((Pc * hzt) * kzt) * kzt, gzb1 = ((Pc * hzb) * kzb) * kzb;
-            // the scheme's divisions by the Jacobian become one reciprocal per cell
-            const T ij = T(1) / jacob;
+            const T hzkz2 = hzk * (kzk * kzk);
+            const T Bzt = hzkz2 + hzt * (kzt * kzt), Bzb = hzkz2 + hzb * (kzb * kzb);
+            // the scheme's divisions by the Jacobian become multiplications by 1/ja
+            const T ij = kxy * kzk;
             const T UE = UU0[o], UW = UU0[o - 1], VN = UU0[L::PE + o], VS = UU0[L::PE + o - L::BX];
             const T WT = UU0[2 * L::PE + o], WB = uu2m1;
             const T nutcc = N0[o];
             // diffusion coefficients of the six faces, shared by the three components
             // (src/FalmCFDScheme.h:167-191)
-            const T ce = (gxcc + gxe1) * (ReI + T(0.5) * (nutcc + N0[o + 1]));
-            const T cw = (gxcc + gxw1) * (ReI + T(0.5) * (nutcc + N0[o - 1]));
-            const T cn = (gycc + gyn1) * (ReI + T(0.5) * (nutcc + N0[o + L::BX]));
-            const T cs = (gycc + gys1) * (ReI + T(0.5) * (nutcc + N0[o - L::BX]));
-            const T ct = (gzcc + gzt1) * (ReI + T(0.5) * (nutcc + N1[o]));
-            const T cb = (gzcc + gzb1) * (ReI + T(0.5) * (nutcc + nutm1));
+            const T ce = (hzk * Axe) * (ReI + T(0.5) * (nutcc + N0[o + 1]));
+            const T cw = (hzk * Axw) * (ReI + T(0.5) * (nutcc + N0[o - 1]));
+            const T cn = (hzk * Ayn) * (ReI + T(0.5) * (nutcc + N0[o + L::BX]));
+            const T cs = (hzk * Ays) * (ReI + T(0.5) * (nutcc + N0[o - L::BX]));
+            const T ct = (Pc * Bzt) * (ReI + T(0.5) * (nutcc + N1[o]));
+            const T cb = (Pc * Bzb) * (ReI + T(0.5) * (nutcc + nutm1));
             const T vscale = T(0.5) * ij;
             T fvec[3] = {0, 0, 0};
             if (ff) {
