@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SOURCES = [os.path.join(HERE, "csrc", "falm_b200.cu")]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in ("falm_internal.cuh", "common.cuh", "cfd.cuh", "poisson.cuh", "alm_bc.cuh",
-                                                 "tma.cuh", "stencil_tma.cuh", "poisson_tma.cuh", "plane3_tma.cuh", "sor_rb_tma.cuh", "adjoint.cuh")]
+                                                 "tma.cuh", "stencil_tma.cuh", "poisson_tma.cuh", "plane3_tma.cuh", "sor_rb_tma.cuh", "adjoint.cuh", "pair.cuh")]
 OUT = os.path.join(HERE, "libfalm_b200.so")
 NVCC_FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-shared"]

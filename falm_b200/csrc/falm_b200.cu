@@ -225,6 +225,7 @@ int s7_launch(falm_ctx *ctx, int cls, cudaStream_t st, const T *x, const Body &b
     const int kc = chunk_len(ctx, (long long)bx * by, g.nz, 8, 32);
     dim3 grid(bx, by, (g.nz + kc - 1) / kc);
     if ((long long)grid.x * grid.y * grid.z > ctx->red.maxBlocks) return 0;
+    if (s7_smem<T>() > 48 * 1024) cudaFuncSetAttribute(k_s7_tma<T, NV, Body>, cudaFuncAttributeMaxDynamicSharedMemorySize, s7_smem<T>());
     int rc = launch_k(ctx, cls, st, [&] {
         k_s7_tma<T, NV, Body><<<grid, 256, s7_smem<T>(), st>>>(g, kc, m, body, ctx->red, ctx->kerr);
     });

@@ -2,21 +2,27 @@
 // half sweep, operator application fused with the BiCGStab inner products).
 //
 // The stencil operand streams through a ring of shared-memory slots, one
-// (36 x 10) TMA box per z plane: the 32 x 8 tile, one halo row on each y side
+// (68 x 18) TMA box per z plane: the 64 x 16 tile, one halo row on each y side
 // and two halo columns on each x side (the box starts at i0-2 so that its x
-// coordinate is 16-byte aligned).  The column's value at k-1 is kept in a
-// register, k+1 comes from the next slot.  Pointwise operands (right-hand
-// side, shadow residual, ...) are read with ordinary coalesced loads.
+// coordinate is 16-byte aligned).  Each thread owns two adjacent cells (x, x+1)
+// in each of two rows: the pair's values are one 64-bit (FP32) shared or
+// global access, and FP32 arithmetic runs on the packed pipe.  The column's
+// value at k-1 is kept in registers, k+1 comes from the next slot.  Pointwise
+// operands (right-hand side, shadow residual, ...) are read with ordinary
+// coalesced pair loads.  A field is streamed only when its row pitch is a
+// multiple of 16 bytes, so the interior width is even and every pair is
+// either inside the interior or outside it.
 #pragma once
 #include "poisson.cuh"
+#include "pair.cuh"
 #include "tma.cuh"
 
 namespace fb {
 
 template <typename T>
 struct S7Tile {
-    static constexpr int RY = 2;   // rows per thread: thread (tx, ty) computes rows ty, ty + 8, ...
-    static constexpr int TX = 32, TY = 8 * RY, BX = 36, BY = TY + 2, PE = BX * BY;
+    static constexpr int RY = 2;   // rows per thread: thread (tx, ty) computes rows ty, ty + 8
+    static constexpr int TX = 64, TY = 8 * RY, BX = TX + 4, BY = TY + 2, PE = BX * BY;
     static constexpr int SLOT = (PE * (int)sizeof(T) + 127) / 128 * 128;
 };
 
@@ -24,10 +30,10 @@ template <typename T> struct S7Conf;
 template <> struct S7Conf<double> { static constexpr int NS = 6; };
 template <> struct S7Conf<float> { static constexpr int NS = 8; };
 
-// resident CTAs per SM asked of the register allocator: 4 for FP32 arithmetic
-// on an FP32 field (at most 64 registers), fewer where the body works in FP64
+// resident CTAs per SM asked of the register allocator: 3 for FP32 arithmetic
+// on an FP32 field (at most 85 registers), 2 where the body works in FP64
 template <typename T, class Body>
-constexpr int s7_minb() { return (sizeof(T) == 4 && sizeof(typename Body::V) == 4) ? 4 : (sizeof(T) == 4 ? 3 : 2); }
+constexpr int s7_minb() { return (sizeof(T) == 4 && sizeof(typename Body::V) == 4) ? 3 : 2; }
 
 template <typename T>
 constexpr int s7_smem() { return S7Conf<T>::NS * S7Tile<T>::SLOT + 128 + 128; }
@@ -35,12 +41,12 @@ constexpr int s7_smem() { return S7Conf<T>::NS * S7Tile<T>::SLOT + 128 + 128; }
 // Body: type V (the stencil's arithmetic type: T, or double for an FP64
 //       residual of an FP32 field); bool skip() const; const T *pw() const
 //       (pointwise operand, or null); const Op7<T> &op_() const;
-//       void cell(i, j, k, cc, a, xc, xe, xw, xn, xs, xt, xb, pv, acc); void finish(tot)
+//       void cell2(i, j, k, cc, a, xc, xe, xw, xn, xs, xt, xb, pv, acc): the
+//       cells (i, j, k) and (i+1, j, k), with coefficient and value pairs;
+//       void finish(tot)
 // The kernel hoists the x/y part of the operator out of the z march, loads the
-// z part once per plane for all rows of a thread, and passes the cell's
-// coefficients a (Coef7<V>) and neighbours in V: the column coefficients are
-// converted once per column, the -1 neighbour is carried from the previous
-// plane already converted.
+// z part once per plane for all rows of a thread, converts the column
+// coefficients once, and carries the -1 neighbour pair from the previous plane.
 // The pointwise operand of the next plane is loaded one iteration ahead (pv),
 // so its latency overlaps the current plane's wait and arithmetic.
 template <typename T, int NV, class Body>
@@ -48,6 +54,8 @@ __global__ void __launch_bounds__(256, (s7_minb<T, Body>())) k_s7_tma(Geom g, in
                                               RedWork rw, int *err) {
     using L = S7Tile<T>;
     using V = typename Body::V;
+    using T2 = P2<T>;
+    using V2 = P2<V>;
     constexpr int NS = S7Conf<T>::NS;
     extern __shared__ unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
@@ -57,20 +65,25 @@ __global__ void __launch_bounds__(256, (s7_minb<T, Body>())) k_s7_tma(Geom g, in
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int i0 = g.gc + blockIdx.x * L::TX, j0 = g.gc + blockIdx.y * L::TY;
     const int k0 = g.gc + blockIdx.z * kc, k1 = min(k0 + kc, g.sz - g.gc);
-    const int i = i0 + tx;
+    const int i = i0 + 2 * tx;                              // the pair's first cell
+    const int ihi = g.sx - g.gc, jhi = g.sy - g.gc;
     const int P0 = k0 - 1, nplanes = (k1 + 1) - P0;   // planes k0-1 .. k1
     const int xb = box_origin(i0 - 2, L::BX, g.sx, 16 / (int)sizeof(T)), yb = box_origin(j0 - 1, L::BY, g.sy, 1);
-    const int ox = min(i, g.sx - g.gc - 1) - xb;
+    const int ic = min(i, ihi - 2);                         // clamped pair (inactive threads read a staged pair)
+    const int ox = ic - xb;
     int jr[RY], orr[RY];
     bool act[RY];
 #pragma unroll
     for (int r = 0; r < RY; r++) {
         jr[r] = j0 + ty + 8 * r;
-        act[r] = i < g.sx - g.gc && jr[r] < g.sy - g.gc;
-        const int oy = min(jr[r], g.sy - g.gc - 1) - yb;
+        act[r] = i < ihi && jr[r] < jhi;
+        const int oy = min(jr[r], jhi - 1) - yb;
         orr[r] = oy * L::BX + ox;
-        // self-check: the radius-1 neighbourhood of a computed cell lies inside the staged box
-        if (act[r] && (ox < 1 || ox > L::BX - 2 || oy < 1 || oy > L::BY - 2)) { atomicExch(err, 300 + 2); act[r] = false; }
+        // self-check: the radius-1 neighbourhood of a computed pair lies inside the staged box, pair-aligned
+        if (act[r] && (ox < 1 || ox + 2 > L::BX - 1 || oy < 1 || oy > L::BY - 2 || (orr[r] & 1))) {
+            atomicExch(err, 300 + 2);
+            act[r] = false;
+        }
     }
     double acc[NV > 0 ? NV : 1];
 #pragma unroll
@@ -107,24 +120,35 @@ __global__ void __launch_bounds__(256, (s7_minb<T, Body>())) k_s7_tma(Geom g, in
     const long long sxy = (long long)g.sx * g.sy;
     const Op7<T> &op = body.op_();
     long long ccr[RY];
-    T pv[RY];
-    V xm[RY];
-    typename Op7<T>::Col col[RY];
-    V cwv[RY], cev[RY], csv[RY], cnv[RY];
+    T2 pv[RY];
+    V2 xm[RY];
+    bool pwr[RY];
+    // x coefficients of the pair (both rows), y ones and the diagonal's x/y part per row
+    V2 cw, ce;
+    V2 csv[RY], cnv[RY];
+    T2 dxy[RY];
+    typename Op7<T>::Col col0[RY], col1[RY];
 #pragma unroll
     for (int r = 0; r < RY; r++) {
         ccr[r] = g.id(i, jr[r], P0 + 1);   // cell of the first computed plane
-        pv[r] = (pw && act[r]) ? pw[ccr[r]] : T(0);
-        col[r] = op.column(min(i, g.sx - g.gc - 1), min(jr[r], g.sy - g.gc - 1));
-        cwv[r] = (V)col[r].aw; cev[r] = (V)col[r].ae; csv[r] = (V)col[r].as; cnv[r] = (V)col[r].an;
+        pwr[r] = pw && act[r];
+        pv[r] = pwr[r] ? ld2(pw + ccr[r]) : mk2(T(0), T(0));
+        const int jc = min(jr[r], jhi - 1);
+        col0[r] = op.column(ic, jc);
+        col1[r] = op.column(ic + 1, jc);
+        csv[r] = mk2((V)col0[r].as, (V)col0[r].as);
+        cnv[r] = mk2((V)col0[r].an, (V)col0[r].an);
+        dxy[r] = mk2(col0[r].dxy, col1[r].dxy);
     }
+    cw = mk2((V)col0[0].aw, (V)col1[0].aw);
+    ce = mk2((V)col0[0].ae, (V)col1[0].ae);
     if (__syncthreads_or(fail)) goto drain;
 #pragma unroll
-    for (int r = 0; r < RY; r++) xm[r] = (V)slot(0)[orr[r]];
+    for (int r = 0; r < RY; r++) xm[r] = cvt2<V, T>(ld2(slot(0) + orr[r]));
     for (int q = 1; q < nplanes - 1; q++) {
-        T pn[RY];
+        T2 pn[RY];
 #pragma unroll
-        for (int r = 0; r < RY; r++) pn[r] = (pw && act[r] && q + 1 < nplanes - 1) ? pw[ccr[r] + sxy] : T(0);
+        for (int r = 0; r < RY; r++) pn[r] = (pwr[r] && q + 1 < nplanes - 1) ? ld2(pw + ccr[r] + sxy) : mk2(T(0), T(0));
         fail = !wait_q(q + 1);
         waited = q + 2;
         if (__syncthreads_or(fail)) goto drain;
@@ -135,21 +159,27 @@ __global__ void __launch_bounds__(256, (s7_minb<T, Body>())) k_s7_tma(Geom g, in
         const T *X0 = slot(q), *X1 = slot(q + 1);
         const int k = P0 + q;
         const typename Op7<T>::ZPl zp = op.zplane(k);
-        const V abv = (V)zp.ab, atv = (V)zp.at;
+        const V2 abv = mk2((V)zp.ab, (V)zp.ab), atv = mk2((V)zp.at, (V)zp.at);
+        const T2 zpp = mk2(zp.zp, zp.zp), zmm = mk2(zp.zm, zp.zm), scl = mk2(op.t.scale, op.t.scale);
 #pragma unroll
         for (int r = 0; r < RY; r++) {
             const int o = orr[r];
-            const V xc = (V)X0[o];
+            const T2 c2 = ld2(X0 + o);
+            const V2 xc = cvt2<V, T>(c2);
             if (act[r]) {
-                Coef7<V> a;
+                Coef7<V2> a;
                 if (op.A) {
-                    const Coef7<T> e = op.at_col(col[r], k, ccr[r]);
-                    a = Coef7<V>{(V)e.ac, (V)e.aw, (V)e.ae, (V)e.as, (V)e.an, (V)e.ab, (V)e.at};
+                    const Coef7<T> e0 = op.at_col(col0[r], k, ccr[r]), e1 = op.at_col(col1[r], k, ccr[r] + 1);
+                    a = Coef7<V2>{mk2((V)e0.ac, (V)e1.ac), mk2((V)e0.aw, (V)e1.aw), mk2((V)e0.ae, (V)e1.ae), mk2((V)e0.as, (V)e1.as),
+                                  mk2((V)e0.an, (V)e1.an), mk2((V)e0.ab, (V)e1.ab), mk2((V)e0.at, (V)e1.at)};
                 } else {
-                    a = Coef7<V>{(V)op.ac_col(col[r], zp), cwv[r], cev[r], csv[r], cnv[r], abv, atv};
+                    // ((dxy - up_z) - um_z) * scale, as Op7::at_col
+                    const T2 ac = mul2(sub2(sub2(dxy[r], zpp), zmm), scl);
+                    a = Coef7<V2>{cvt2<V, T>(ac), cw, ce, csv[r], cnv[r], abv, atv};
                 }
-                body.cell(i, jr[r], k, ccr[r], a, xc, (V)X0[o + 1], (V)X0[o - 1], (V)X0[o + L::BX], (V)X0[o - L::BX], (V)X1[o], xm[r],
-                          pv[r], acc);
+                const V xw0 = (V)X0[o - 1], xe1 = (V)X0[o + 2];
+                body.cell2(i, jr[r], k, ccr[r], a, xc, mk2(xc.y, xe1), mk2(xw0, xc.x), cvt2<V, T>(ld2(X0 + o + L::BX)),
+                           cvt2<V, T>(ld2(X0 + o - L::BX)), cvt2<V, T>(ld2(X1 + o)), xm[r], pv[r], acc);
             }
             xm[r] = xc;
             pv[r] = pn[r];
@@ -167,12 +197,8 @@ reduce:
 }
 
 // ---------------------------------------------------------------- bodies
-template <typename T>
-__device__ __forceinline__ T dot7(T ac, T ae, T aw, T an, T as, T at, T ab, T xc, T xe, T xw, T xn, T xs, T xt, T xb) {
-    return ac * xc + ae * xe + aw * xw + an * xn + as * xs + at * xt + ab * xb;
-}
-
-// red-black SOR half sweep (src/dev/FalmEqDevCall.cu:175-211), in place
+// red-black SOR half sweep (src/dev/FalmEqDevCall.cu:175-211), in place: the
+// pair's cell of this colour, with the scalar operations of the row kernel
 template <typename T>
 struct SorBody {
     using V = T;
@@ -185,11 +211,13 @@ struct SorBody {
     __device__ bool skip() const { return sc && sc->done; }
     __device__ const T *pw() const { return b; }
     __device__ const Op7<T> &op_() const { return op; }
-    __device__ void cell(int i, int j, int k, long long c, const Coef7<T> &a, T xc, T xe, T xw, T xn, T xs, T xt, T xb, T bv,
-                         double (&)[1]) const {
-        if (((i + j + k) & 1) != color) return;
-        T cc = (bv - dot7(a.ac, a.ae, a.aw, a.an, a.as, a.at, a.ab, xc, xe, xw, xn, xs, xt, xb)) / a.ac;
-        x[c] = xc + omega * cc;
+    __device__ void cell2(int i, int j, int k, long long c, const Coef7<P2<T>> &a, P2<T> xc, P2<T> xe, P2<T> xw, P2<T> xn, P2<T> xs,
+                          P2<T> xt, P2<T> xb, P2<T> bv, double (&)[1]) const {
+        const int e = (color ^ (i + j + k)) & 1;
+        auto L = [e](P2<T> v) { return e ? v.y : v.x; };
+        const T ac = L(a.ac), xcc = L(xc);
+        const T r7 = ac * xcc + L(a.ae) * L(xe) + L(a.aw) * L(xw) + L(a.an) * L(xn) + L(a.as) * L(xs) + L(a.at) * L(xt) + L(a.ab) * L(xb);
+        x[c + e] = xcc + omega * ((L(bv) - r7) / ac);
     }
     __device__ void finish(const double (&)[1]) const {}
 };
@@ -203,9 +231,9 @@ struct MvBody {
     __device__ bool skip() const { return false; }
     __device__ const T *pw() const { return nullptr; }
     __device__ const Op7<T> &op_() const { return op; }
-    __device__ void cell(int i, int j, int k, long long c, const Coef7<T> &a, T xc, T xe, T xw, T xn, T xs, T xt, T xb, T,
-                         double (&)[1]) const {
-        ax[c] = dot7(a.ac, a.ae, a.aw, a.an, a.as, a.at, a.ab, xc, xe, xw, xn, xs, xt, xb);
+    __device__ void cell2(int i, int j, int k, long long c, const Coef7<P2<T>> &a, P2<T> xc, P2<T> xe, P2<T> xw, P2<T> xn, P2<T> xs,
+                          P2<T> xt, P2<T> xb, P2<T>, double (&)[1]) const {
+        st2(ax + c, dot7p(a.ac, a.ae, a.aw, a.an, a.as, a.at, a.ab, xc, xe, xw, xn, xs, xt, xb));
     }
     __device__ void finish(const double (&)[1]) const {}
 };
@@ -221,11 +249,12 @@ struct MvDot1Body {
     __device__ bool skip() const { return sc->done; }
     __device__ const T *pw() const { return rr; }
     __device__ const Op7<T> &op_() const { return op; }
-    __device__ void cell(int i, int j, int k, long long c, const Coef7<T> &a, T xc, T xe, T xw, T xn, T xs, T xt, T xb, T rrv,
-                         double (&acc)[1]) const {
-        T qv = dot7(a.ac, a.ae, a.aw, a.an, a.as, a.at, a.ab, xc, xe, xw, xn, xs, xt, xb);
-        q[c] = qv;
-        acc[0] += to_d(rrv) * to_d(qv);
+    __device__ void cell2(int i, int j, int k, long long c, const Coef7<P2<T>> &a, P2<T> xc, P2<T> xe, P2<T> xw, P2<T> xn, P2<T> xs,
+                          P2<T> xt, P2<T> xb, P2<T> rrv, double (&acc)[1]) const {
+        const P2<T> qv = dot7p(a.ac, a.ae, a.aw, a.an, a.as, a.at, a.ab, xc, xe, xw, xn, xs, xt, xb);
+        st2(q + c, qv);
+        acc[0] += to_d(rrv.x) * to_d(qv.x);
+        acc[0] += to_d(rrv.y) * to_d(qv.y);
     }
     __device__ void finish(const double (&tot)[1]) const {
         double alpha = sc->rho / tot[0];
@@ -245,13 +274,15 @@ struct MvDot2Body {
     __device__ bool skip() const { return sc->done; }
     __device__ const T *pw() const { return s; }
     __device__ const Op7<T> &op_() const { return op; }
-    __device__ void cell(int i, int j, int k, long long c, const Coef7<T> &a, T xc, T xe, T xw, T xn, T xs, T xt, T xb, T sv,
-                         double (&acc)[2]) const {
-        T tv = dot7(a.ac, a.ae, a.aw, a.an, a.as, a.at, a.ab, xc, xe, xw, xn, xs, xt, xb);
-        t[c] = tv;
-        double td = to_d(tv);
-        acc[0] += td * to_d(sv);
-        acc[1] += td * td;
+    __device__ void cell2(int i, int j, int k, long long c, const Coef7<P2<T>> &a, P2<T> xc, P2<T> xe, P2<T> xw, P2<T> xn, P2<T> xs,
+                          P2<T> xt, P2<T> xb, P2<T> sv, double (&acc)[2]) const {
+        const P2<T> tv = dot7p(a.ac, a.ae, a.aw, a.an, a.as, a.at, a.ab, xc, xe, xw, xn, xs, xt, xb);
+        st2(t + c, tv);
+        const double t0 = to_d(tv.x), t1 = to_d(tv.y);
+        acc[0] += t0 * to_d(sv.x);
+        acc[0] += t1 * to_d(sv.y);
+        acc[1] += t0 * t0;
+        acc[1] += t1 * t1;
     }
     __device__ void finish(const double (&tot)[2]) const {
         double omega = tot[0] / tot[1];
@@ -272,14 +303,17 @@ struct ResBody {
     __device__ bool skip() const { return false; }
     __device__ const T *pw() const { return b; }
     __device__ const Op7<T> &op_() const { return op; }
-    __device__ void cell(int i, int j, int k, long long c, const Coef7<double> &a, double xc, double xe, double xw, double xn,
-                         double xs, double xt, double xb, T bv, double (&acc)[2]) const {
-        double rv = to_d(bv) - dot7<double>(a.ac, a.ae, a.aw, a.an, a.as, a.at, a.ab, xc, xe, xw, xn, xs, xt, xb);
-        T rt = (T)rv;
-        if (r) r[c] = rt;
-        if (rr) rr[c] = rt;
-        acc[0] += rv * rv;
-        acc[1] += to_d(rt) * to_d(rt);
+    __device__ void cell2(int i, int j, int k, long long c, const Coef7<double2> &a, double2 xc, double2 xe, double2 xw, double2 xn,
+                          double2 xs, double2 xt, double2 xb, P2<T> bv, double (&acc)[2]) const {
+        const double2 ax = dot7p(a.ac, a.ae, a.aw, a.an, a.as, a.at, a.ab, xc, xe, xw, xn, xs, xt, xb);
+        const double r0 = to_d(bv.x) - ax.x, r1 = to_d(bv.y) - ax.y;
+        const P2<T> rt = mk2((T)r0, (T)r1);
+        if (r) st2(r + c, rt);
+        if (rr) st2(rr + c, rt);
+        acc[0] += r0 * r0;
+        acc[0] += r1 * r1;
+        acc[1] += to_d(rt.x) * to_d(rt.x);
+        acc[1] += to_d(rt.y) * to_d(rt.y);
     }
     __device__ void finish(const double (&tot)[2]) const {
         if (!sc) return;

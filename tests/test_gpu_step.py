@@ -51,10 +51,12 @@ def small_cases():
     ch = cases.small_channel(32, 20, 20, intensity=0.05).with_inflow(nb=8)
     cav = cases.cavity(16)
     cav.tol = 1e-10
-    return {"channel": ch, "cavity": cav}
+    # wide enough (nx >= 64) for every plane stream, including the 7-point one
+    wide = cases.small_channel(72, 20, 16, intensity=0.05).with_inflow(nb=8)
+    return {"channel": ch, "cavity": cav, "wide": wide}
 
 
-@pytest.mark.parametrize("name", ["channel", "cavity"])
+@pytest.mark.parametrize("name", ["channel", "cavity", "wide"])
 def test_step_fp64_fixed_iterations(oracle, lib_built, name):
     case = small_cases()[name]
     ref, rs = run_oracle(oracle, case, 10, maxit=6, tol=0.0)
@@ -127,11 +129,13 @@ def test_step_launch_count_and_statuses(lib_built):
         assert np.isfinite(s["divnorm"])
 
 
+@pytest.mark.parametrize("shape", [(40, 20, 72), (72, 20, 40)])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_step_tma_matches_row_kernels_multichunk(lib_built, monkeypatch, precision):
-    """Several z chunks per column (nz = 72) and partial x/y tiles: the TMA plane
-    streams and the row kernels give the same steps."""
-    case = cases.small_channel(40, 20, 72, intensity=0.05).with_inflow(nb=8)
+def test_step_tma_matches_row_kernels_multichunk(lib_built, monkeypatch, precision, shape):
+    """Several z chunks per column and partial x/y tiles: the TMA plane streams
+    and the row kernels give the same steps (the 7-point stream's 64-wide tile
+    needs nx >= 64)."""
+    case = cases.small_channel(*shape, intensity=0.05).with_inflow(nb=8)
     outs = []
     for no_tma in ("1", "0"):
         monkeypatch.setenv("FALM_B200_NO_TMA", no_tma)
