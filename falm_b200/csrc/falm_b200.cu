@@ -14,6 +14,8 @@
 #include <cstdlib>
 #include <mutex>
 #include <unordered_map>
+#include <map>
+#include <tuple>
 #include "falm_internal.cuh"
 #include "common.cuh"
 #include "cfd.cuh"
@@ -105,16 +107,45 @@ int launch_k(falm_ctx *ctx, int cls, cudaStream_t st, F &&f) {
         if (_lrc) return _lrc;                                                               \
     } while (0)
 
-// z planes per CTA of a plane-streaming kernel: short enough chunks that the
-// grid fills every SM twice over with `per_sm` resident CTAs, at most `cap`
-// planes, at least 8 (each chunk re-reads its halo planes)
-int chunk_len(const falm_ctx *ctx, long long blocks_xy, int nz, int per_sm, int cap) {
-    const long long want = 2LL * ctx->sm_count * per_sm;
-    const long long chunks = std::max(1LL, (want + blocks_xy - 1) / blocks_xy);
-    int kc = (int)((nz + chunks - 1) / chunks);
-    kc = std::max(kc, 8);
-    kc = std::min(kc, cap);
-    return std::max(1, std::min(kc, nz));
+// resident CTAs per SM of a kernel at a launch shape, looked up once per
+// kernel and shape
+template <typename K>
+int resident_per_sm(K kernel, int threads, int smem) {
+    static std::mutex mu;
+    static std::map<std::tuple<const void *, int, int>, int> known;
+    const auto key = std::make_tuple((const void *)kernel, threads, smem);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = known.find(key);
+        if (it != known.end()) return it->second;
+    }
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess || n <= 0) {
+        cudaGetLastError();
+        n = 1;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    known[key] = n;
+    return n;
+}
+
+// z planes per CTA of a plane-streaming kernel: the chunk length kc in
+// [8, cap] that minimises the modelled time ceil(CTAs / resident slots) *
+// (kc + halo + 2): the CTAs run in waves of SMs x per_sm, and a CTA's time
+// grows with its planes (the halo planes included) plus a start-up of about
+// two planes.  Ties keep the longer chunk.
+int chunk_len(const falm_ctx *ctx, long long blocks_xy, int nz, int per_sm, int cap, int halo) {
+    const long long slots = (long long)ctx->sm_count * std::max(1, per_sm);
+    const int lo = std::min(8, nz), hi = std::max(lo, std::min(cap, nz));
+    int best = hi;
+    long long best_t = -1;
+    for (int kc = hi; kc >= lo; kc--) {
+        const long long ctas = blocks_xy * ((nz + kc - 1) / kc);
+        const long long t = ((ctas + slots - 1) / slots) * (kc + halo + 2);
+        if (best_t < 0 || t < best_t) { best_t = t; best = kc; }
+    }
+    return std::max(1, best);
 }
 
 int row_grid(const falm_ctx *ctx, const Region3 &R) {
@@ -222,7 +253,7 @@ int s7_launch(falm_ctx *ctx, int cls, cudaStream_t st, const T *x, const Body &b
     if (ctx->no_tma || !make_map(ctx, &m, x, 1, S7Tile<T>::BX, S7Tile<T>::BY)) return 0;
     const Geom &g = ctx->geo;
     const int bx = (g.nx + S7Tile<T>::TX - 1) / S7Tile<T>::TX, by = (g.ny + S7Tile<T>::TY - 1) / S7Tile<T>::TY;
-    const int kc = chunk_len(ctx, (long long)bx * by, g.nz, 8, 32);
+    const int kc = chunk_len(ctx, (long long)bx * by, g.nz, resident_per_sm(k_s7_tma<T, NV, Body>, 256, s7_smem<T>()), 64, 2);
     dim3 grid(bx, by, (g.nz + kc - 1) / kc);
     if ((long long)grid.x * grid.y * grid.z > ctx->red.maxBlocks) return 0;
     if (s7_smem<T>() > 48 * 1024) cudaFuncSetAttribute(k_s7_tma<T, NV, Body>, cudaFuncAttributeMaxDynamicSharedMemorySize, s7_smem<T>());
@@ -249,7 +280,7 @@ int sor_rb_launch_h(falm_ctx *ctx, cudaStream_t st, const T *xin, const T *b, T 
     if (!make_map(ctx, &mx, xin, 1, L::BX, L::BY) || !make_map(ctx, &mb, b, 1, L::BX, L::BY)) return 0;
     const Geom &g = ctx->geo;
     const int bx = (g.nx + L::TX - 1) / L::TX, by = (g.ny + L::TY - 1) / L::TY;
-    const int kc = chunk_len(ctx, (long long)bx * by, g.nz, sizeof(T) == 4 ? 3 : 2, 32);
+    const int kc = chunk_len(ctx, (long long)bx * by, g.nz, resident_per_sm(k_sor_rb_tma<T, H>, 256, L::SMEM), 64, 2 * H);
     dim3 grid(bx, by, (g.nz + kc - 1) / kc);
     cudaFuncSetAttribute(k_sor_rb_tma<T, H>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
     const PoissonTables<T> tb = op7<T>(ctx).t;
@@ -268,7 +299,7 @@ int sor_rb2_launch(falm_ctx *ctx, cudaStream_t st, const T *xin, const T *b, T *
     if (!make_map(ctx, &mx, xin, 1, L::BX, L::BY) || !make_map(ctx, &mb, b, 1, L::BXB, L::BYB)) return 0;
     const Geom &g = ctx->geo;
     const int bx = (g.nx + L::TX - 1) / L::TX, by = (g.ny + L::TY - 1) / L::TY;
-    const int kc = chunk_len(ctx, (long long)bx * by, g.nz, 4, 32);
+    const int kc = chunk_len(ctx, (long long)bx * by, g.nz, resident_per_sm(k_sor_rb2_tma<T>, L::NT, L::SMEM), 64, 2 * L::H);
     dim3 grid(bx, by, (g.nz + kc - 1) / kc);
     cudaFuncSetAttribute(k_sor_rb2_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
     const PoissonTables<T> tb = op7<T>(ctx).t;
@@ -312,10 +343,10 @@ int p3_launch(falm_ctx *ctx, int cls, cudaStream_t st, const Region3 &R, int org
     }
     const int smem = NS * slot + 256;
     const int bx = (R.i1 - R.i0 + L::TX - 1) / L::TX, by = (R.j1 - R.j0 + L::TY - 1) / L::TY;
-    const int kc = chunk_len(ctx, (long long)bx * by, R.k1 - R.k0, std::max(1, std::min(8, (200 * 1024) / smem)), 32);
+    auto kern = k_plane3_tma<T, NF, NS, NV, Body>;
+    const int kc = chunk_len(ctx, (long long)bx * by, R.k1 - R.k0, resident_per_sm(kern, 256, smem), 64, 2);
     dim3 grid(bx, by, (R.k1 - R.k0 + kc - 1) / kc);
     if ((long long)grid.x * grid.y * grid.z > ctx->red.maxBlocks) return 0;
-    auto kern = k_plane3_tma<T, NF, NS, NV, Body>;
     if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     int rc = launch_k(ctx, cls, st, [&] { kern<<<grid, 256, smem, st>>>(ctx->geo, R, org, kc, maps, body, ctx->red, ctx->kerr); });
     return rc ? -rc : 1;
@@ -578,9 +609,9 @@ int pseudo_u_t(falm_ctx *ctx, const T *un, const T *u, const T *uu, T *ua, const
             case FALM_ADV_UTOPIA: kern = k_pseudo_u_tma<T, NS, FALM_ADV_UTOPIA>; break;
             default: break;
         }
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
         const int bx = (g.nx + L::TX - 1) / L::TX, by = (g.ny + L::TY - 1) / L::TY;
-        const int kc = chunk_len(ctx, (long long)bx * by, g.nz, sizeof(T) == 8 ? 2 : 3, 64);
+        const int kc = chunk_len(ctx, (long long)bx * by, g.nz, resident_per_sm(kern, 256, L::SMEM), 64, 4);
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
         dim3 grid(bx, by, (g.nz + kc - 1) / kc);
         LAUNCH(FALM_K_PSEUDO_U, st, kern<<<grid, 256, L::SMEM, st>>>(g, kc, mview<T>(ctx), mu, muu, mnut, un, un == u ? 1 : 0, ua, ff, af,
                                                                     (T)(1.0 / ctx->Re), (T)dt, ctx->kerr));
