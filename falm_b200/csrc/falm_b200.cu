@@ -341,6 +341,8 @@ int p3_launch(falm_ctx *ctx, int cls, cudaStream_t st, const Region3 &R, int org
         maps.ncomp[f] = ncomp[f];
         slot += ncomp[f] * L::FB;
     }
+    // the kernel lays the slot out from the body's component counts
+    if (slot != (Body::NC0 + Body::NC1) * L::FB) return -fail(ctx, FALM_ERR_ARG, "plane stream: field components do not match the body");
     const int smem = NS * slot + 256;
     const int bx = (R.i1 - R.i0 + L::TX - 1) / L::TX, by = (R.j1 - R.j0 + L::TY - 1) / L::TY;
     auto kern = k_plane3_tma<T, NF, NS, NV, Body>;

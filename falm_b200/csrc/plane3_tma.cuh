@@ -68,15 +68,11 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_plane3_tma(Geom
     using L = P3Layout<T, NF>;
     extern __shared__ unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
-    int foff[NF], slot_bytes = 0;
-    uint32_t tx_bytes = 0;
-#pragma unroll
-    for (int f = 0; f < NF; f++) {
-        foff[f] = slot_bytes;
-        slot_bytes += maps.ncomp[f] * L::FB;
-        tx_bytes += maps.ncomp[f] * L::PE * sizeof(T);
-    }
-    uint64_t *bar = (uint64_t *)(smem + NS * slot_bytes);
+    // slot layout from the body's component counts (compile-time offsets)
+    constexpr int FOFF1 = Body::NC0 * L::FB, SLOTB = (Body::NC0 + Body::NC1) * L::FB;
+    constexpr uint32_t TXB = (Body::NC0 + Body::NC1) * L::PE * sizeof(T);
+    static_assert(NF == 1 ? Body::NC1 == 0 : Body::NC1 > 0, "component counts match the fields");
+    uint64_t *bar = (uint64_t *)(smem + NS * SLOTB);
     if (body.skip()) return;
     constexpr int RY = L::RY;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
@@ -85,8 +81,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_plane3_tma(Geom
     const int i = i0 + tx;
     const int P0 = k0 - 1, nplanes = (k1 + 1) - P0;
     P3View<T, NF> v;
-#pragma unroll
-    for (int f = 0; f < NF; f++) v.foff[f] = foff[f];
+    v.foff[0] = 0;
+    if (NF > 1) v.foff[NF - 1] = FOFF1;
     const int xb = box_origin(i0 - org, L::BX, g.sx, 16 / (int)sizeof(T)), yb = box_origin(j0 - 1, L::BY, g.sy, 1);
     const int ox = min(i, R.i1 - 1) - xb;
     int jr[RY], orr[RY];
@@ -103,10 +99,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_plane3_tma(Geom
     double acc[NV > 0 ? NV : 1];
 #pragma unroll
     for (int d = 0; d < (NV > 0 ? NV : 1); d++) acc[d] = 0.0;
-    // column metric factors (x shared by the rows, y per row); z per plane below
+    // column metric factors (x shared by the rows, y per row); z rolled per plane below
     ColMet<T> cm[RY];
+    const MetricView<T> &mv = body.mv;
     {
-        const MetricView<T> &mv = body.mv;
 #pragma unroll
         for (int q = 0; q < 3; q++) {
             const int ic = min(max(i - 1 + q, 0), g.sx - 1);
@@ -119,23 +115,24 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_plane3_tma(Geom
             }
         }
     }
-    auto slot = [&](int q) { return smem + (q % NS) * slot_bytes; };
-    auto issue = [&](int q) {
-        uint64_t *b = bar + (q % NS);
+    // plane q into slot s = q % NS (the caller passes s, a constant in the march)
+    auto issue = [&](int q, int s) {
+        uint64_t *b = bar + s;
+        unsigned char *dst = smem + s * SLOTB;
         bool ok = true;
 #pragma unroll
-        for (int f = 0; f < NF; f++) ok = ok && tma_ok(slot(q) + foff[f], xb, yb, P0 + q, (int)sizeof(T), g.sx, g.sy, g.sz);
+        for (int f = 0; f < NF; f++) ok = ok && tma_ok(dst + (f ? FOFF1 : 0), xb, yb, P0 + q, (int)sizeof(T), g.sx, g.sy, g.sz);
         if (!ok) {
             tma_reject(b, err, 3);
             return;
         }
-        mbar_expect_tx(b, tx_bytes);
+        mbar_expect_tx(b, TXB);
 #pragma unroll
-        for (int f = 0; f < NF; f++) tma_load_4d(slot(q) + foff[f], &maps.m[f], xb, yb, P0 + q, 0, b);
+        for (int f = 0; f < NF; f++) tma_load_4d(dst + (f ? FOFF1 : 0), &maps.m[f], xb, yb, P0 + q, 0, b);
     };
     // warp 0 polls the barriers; the block barrier that follows makes the
     // landed planes visible to every thread
-    auto wait_q = [&](int q) -> bool { return threadIdx.x >= 32 || mbar_wait(bar + (q % NS), (q / NS) & 1, err); };
+    auto wait_s = [&](int s, int parity) -> bool { return threadIdx.x >= 32 || mbar_wait(bar + s, parity, err); };
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int f = 0; f < NF; f++) prefetch_tmap(&maps.m[f]);
@@ -145,49 +142,64 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_plane3_tma(Geom
     __syncthreads();
     int issued = min(NS, nplanes), waited = 0;
     if (threadIdx.x == 0)
-        for (int q = 0; q < issued; q++) issue(q);
+        for (int q = 0; q < issued; q++) issue(q, q % NS);
     // every plane is waited for exactly once, before its first read: planes 0
     // and 1 here, plane q+1 at iteration q
-    bool fail = !wait_q(0);
-    fail = !wait_q(1) || fail;
+    bool fail = !wait_s(0, 0);
+    fail = !wait_s(1 % NS, 1 / NS) || fail;
     waited = 2;
     if (__syncthreads_or(fail)) goto drain;
-    for (int q = 1; q < nplanes - 1; q++) {
-        const int k = P0 + q;
-        typename Body::PW pwv[RY];
+    {
+        const long long sxy = (long long)g.sx * g.sy;
+        long long ccr[RY];
 #pragma unroll
-        for (int r = 0; r < RY; r++)
-            if (act[r]) pwv[r] = body.pw_load(i, jr[r], k, g.id(i, jr[r], k));
-        fail = !wait_q(q + 1);
-        waited = q + 2;
-        if (__syncthreads_or(fail)) goto drain;
-        // plane q-2 is no longer needed: refill its slot
-        if (q >= 2 && q - 2 + NS < nplanes) {
-            if (threadIdx.x == 0) { fence_proxy_async(); issue(q - 2 + NS); }
-            issued = q - 2 + NS + 1;
-        }
-        v.pl[0] = (const T *)slot(q - 1);
-        v.pl[1] = (const T *)slot(q);
-        v.pl[2] = (const T *)slot(q + 1);
-        T hzv[3], kzv[3];
+        for (int r = 0; r < RY; r++) ccr[r] = g.id(i, jr[r], P0 + 1);
+        // z metric factors of planes k-1, k, k+1 (rolled)
+        T hz0 = ldg(mv.m.h[2] + max(P0, 0)), kz0 = ldg(mv.m.k[2] + max(P0, 0));
+        T hz1 = ldg(mv.m.h[2] + P0 + 1), kz1 = ldg(mv.m.k[2] + P0 + 1);
+        // the march, unrolled over the slots: plane q = q0 + u is in slot u
+        int ph = 0;   // (q0 / NS) & 1
+        for (int q0 = 0; q0 < nplanes - 1; q0 += NS, ph ^= 1) {
 #pragma unroll
-        for (int q2 = 0; q2 < 3; q2++) {
-            const int kc2 = min(max(k - 1 + q2, 0), g.sz - 1);
-            hzv[q2] = ldg(body.mv.m.h[2] + kc2); kzv[q2] = ldg(body.mv.m.k[2] + kc2);
-        }
+            for (int u = 0; u < NS; u++) {
+                const int q = q0 + u;
+                if (q < 1) continue;
+                if (q >= nplanes - 1) break;
+                const int k = P0 + q;
+                typename Body::PW pwv[RY];
 #pragma unroll
-        for (int r = 0; r < RY; r++) {
-            if (act[r]) {
-                v.o = orr[r];
+                for (int r = 0; r < RY; r++)
+                    if (act[r]) pwv[r] = body.pw_load(i, jr[r], k, ccr[r]);
+                const int kn = min(k + 1, g.sz - 1);
+                const T hz2 = ldg(mv.m.h[2] + kn), kz2 = ldg(mv.m.k[2] + kn);
+                fail = !wait_s((u + 1) % NS, (u + 1 < NS) ? ph : ph ^ 1);
+                waited = q + 2;
+                if (__syncthreads_or(fail)) goto drain;
+                // plane q-2 is no longer needed: refill its slot
+                if (q >= 2 && q - 2 + NS < nplanes) {
+                    if (threadIdx.x == 0) { fence_proxy_async(); issue(q - 2 + NS, (u + NS - 2) % NS); }
+                    issued = q - 2 + NS + 1;
+                }
+                v.pl[0] = (const T *)(smem + ((u + NS - 1) % NS) * SLOTB);
+                v.pl[1] = (const T *)(smem + u * SLOTB);
+                v.pl[2] = (const T *)(smem + ((u + 1) % NS) * SLOTB);
 #pragma unroll
-                for (int q2 = 0; q2 < 3; q2++) { cm[r].hz[q2] = hzv[q2]; cm[r].kz[q2] = kzv[q2]; }
-                body.cell(i, jr[r], k, g.id(i, jr[r], k), v, cm[r], pwv[r], acc);
+                for (int r = 0; r < RY; r++) {
+                    if (act[r]) {
+                        v.o = orr[r];
+                        cm[r].hz[0] = hz0; cm[r].hz[1] = hz1; cm[r].hz[2] = hz2;
+                        cm[r].kz[0] = kz0; cm[r].kz[1] = kz1; cm[r].kz[2] = kz2;
+                        body.cell(i, jr[r], k, ccr[r], v, cm[r], pwv[r], acc);
+                    }
+                    ccr[r] += sxy;
+                }
+                hz0 = hz1; hz1 = hz2; kz0 = kz1; kz1 = kz2;
             }
         }
     }
     goto reduce;
 drain:
-    for (int q = waited; q < issued; q++) wait_q(q);
+    for (int q = waited; q < issued; q++) wait_s(q % NS, (q / NS) & 1);
 reduce:
     if (NV > 0) {
         double tot[NV > 0 ? NV : 1];
@@ -210,6 +222,7 @@ struct UtoUUBody {
     MetricView<T> mv;
     T *uu, *rhs;
     T scale;
+    static constexpr int NC0 = 3, NC1 = 0;   // field: the velocity to interpolate
     using PW = NoPW;
     __device__ bool skip() const { return false; }
     __device__ PW pw_load(int, int, int, long long) const { return PW{}; }
@@ -257,6 +270,7 @@ struct ProjectBody {
     T *uu;
     const T *uua;
     T dt;
+    static constexpr int NC0 = 1, NC1 = 0;   // field: the pressure
     // face velocity (f) and cell velocity (a, interior cells only) before the correction
     struct PW { T f0, f1, f2, a0, a1, a2; };
     __device__ bool skip() const { return false; }
@@ -303,6 +317,7 @@ struct SgsDivBody {
     int sgs;
     T *div_out;
     double *divsum;
+    static constexpr int NC0 = 3, NC1 = 3;   // fields: the cell velocity, the face velocity
     using PW = NoPW;
     __device__ bool skip() const { return false; }
     __device__ PW pw_load(int, int, int, long long) const { return PW{}; }

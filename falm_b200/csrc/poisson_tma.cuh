@@ -88,10 +88,11 @@ __global__ void __launch_bounds__(256, (s7_minb<T, Body>())) k_s7_tma(Geom g, in
     double acc[NV > 0 ? NV : 1];
 #pragma unroll
     for (int d = 0; d < (NV > 0 ? NV : 1); d++) acc[d] = 0.0;
-    auto slot = [&](int q) { return (const T *)(smem + (q % NS) * L::SLOT); };
-    auto issue = [&](int q) {
-        uint64_t *b = bar + (q % NS);
-        unsigned char *dst = smem + (q % NS) * L::SLOT;
+    auto slot = [&](int s) { return (const T *)(smem + s * L::SLOT); };
+    // plane q into slot s = q % NS (the caller passes s, a constant in the march)
+    auto issue = [&](int q, int s) {
+        uint64_t *b = bar + s;
+        unsigned char *dst = smem + s * L::SLOT;
         if (tma_ok(dst, xb, yb, P0 + q, (int)sizeof(T), g.sx, g.sy, g.sz)) {
             mbar_expect_tx(b, L::PE * sizeof(T));
             tma_load_4d(dst, &mx, xb, yb, P0 + q, 0, b);
@@ -101,7 +102,7 @@ __global__ void __launch_bounds__(256, (s7_minb<T, Body>())) k_s7_tma(Geom g, in
     };
     // warp 0 polls the barriers; the block barrier that follows makes the
     // landed planes visible to every thread
-    auto wait_q = [&](int q) -> bool { return threadIdx.x >= 32 || mbar_wait(bar + (q % NS), (q / NS) & 1, err); };
+    auto wait_s = [&](int s, int parity) -> bool { return threadIdx.x >= 32 || mbar_wait(bar + s, parity, err); };
     if (threadIdx.x == 0) {
         prefetch_tmap(&mx);
         for (int s = 0; s < NS; s++) mbar_init(bar + s, 1);
@@ -110,11 +111,11 @@ __global__ void __launch_bounds__(256, (s7_minb<T, Body>())) k_s7_tma(Geom g, in
     __syncthreads();
     int issued = min(NS, nplanes), waited = 0;
     if (threadIdx.x == 0)
-        for (int q = 0; q < issued; q++) issue(q);
+        for (int q = 0; q < issued; q++) issue(q, q % NS);
     // every plane is waited for exactly once, before its first read: planes 0
     // and 1 here, plane q+1 at iteration q
-    bool fail = !wait_q(0);
-    fail = !wait_q(1) || fail;
+    bool fail = !wait_s(0, 0);
+    fail = !wait_s(1, 0) || fail;
     waited = 2;
     const T *pw = body.pw();
     const long long sxy = (long long)g.sx * g.sy;
@@ -145,18 +146,24 @@ __global__ void __launch_bounds__(256, (s7_minb<T, Body>())) k_s7_tma(Geom g, in
     if (__syncthreads_or(fail)) goto drain;
 #pragma unroll
     for (int r = 0; r < RY; r++) xm[r] = cvt2<V, T>(ld2(slot(0) + orr[r]));
-    for (int q = 1; q < nplanes - 1; q++) {
+    // the march, unrolled over the slots: plane q = q0 + u is in slot u
+    for (int q0 = 0, ph = 0; q0 < nplanes - 1; q0 += NS, ph ^= 1) {
+#pragma unroll
+      for (int u = 0; u < NS; u++) {
+        const int q = q0 + u;
+        if (q < 1) continue;
+        if (q >= nplanes - 1) break;
         T2 pn[RY];
 #pragma unroll
         for (int r = 0; r < RY; r++) pn[r] = (pwr[r] && q + 1 < nplanes - 1) ? ld2(pw + ccr[r] + sxy) : mk2(T(0), T(0));
-        fail = !wait_q(q + 1);
+        fail = !wait_s((u + 1) % NS, (u + 1 < NS) ? ph : ph ^ 1);
         waited = q + 2;
         if (__syncthreads_or(fail)) goto drain;
         if (q - 1 + NS < nplanes) {   // plane q-1 is no longer read (its values are in xm): refill its slot
-            if (threadIdx.x == 0) { fence_proxy_async(); issue(q - 1 + NS); }
+            if (threadIdx.x == 0) { fence_proxy_async(); issue(q - 1 + NS, (u + NS - 1) % NS); }
             issued = q - 1 + NS + 1;
         }
-        const T *X0 = slot(q), *X1 = slot(q + 1);
+        const T *X0 = slot(u), *X1 = slot((u + 1) % NS);
         const int k = P0 + q;
         const typename Op7<T>::ZPl zp = op.zplane(k);
         const V2 abv = mk2((V)zp.ab, (V)zp.ab), atv = mk2((V)zp.at, (V)zp.at);
@@ -185,10 +192,11 @@ __global__ void __launch_bounds__(256, (s7_minb<T, Body>())) k_s7_tma(Geom g, in
             pv[r] = pn[r];
             ccr[r] += sxy;
         }
+      }
     }
     goto reduce;
 drain:
-    for (int q = waited; q < issued; q++) wait_q(q);
+    for (int q = waited; q < issued; q++) wait_s(q % NS, (q / NS) & 1);
 reduce:
     if (NV > 0) {
         double tot[NV > 0 ? NV : 1];
