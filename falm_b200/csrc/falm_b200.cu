@@ -299,7 +299,9 @@ int sor_rb2_launch(falm_ctx *ctx, cudaStream_t st, const T *xin, const T *b, T *
     if (!make_map(ctx, &mx, xin, 1, L::BX, L::BY) || !make_map(ctx, &mb, b, 1, L::BXB, L::BYB)) return 0;
     const Geom &g = ctx->geo;
     const int bx = (g.nx + L::TX - 1) / L::TX, by = (g.ny + L::TY - 1) / L::TY;
-    const int kc = chunk_len(ctx, (long long)bx * by, g.nz, resident_per_sm(k_sor_rb2_tma<T>, L::NT, L::SMEM), 64, 2 * L::H);
+    // a CTA runs kc + 3H iterations and stages at most ZMAX planes of z coefficients
+    const int kc = chunk_len(ctx, (long long)bx * by, g.nz, resident_per_sm(k_sor_rb2_tma<T>, L::NT, L::SMEM),
+                             std::min(64, L::ZMAX - 2 * L::H), 3 * L::H);
     dim3 grid(bx, by, (g.nz + kc - 1) / kc);
     cudaFuncSetAttribute(k_sor_rb2_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
     const PoissonTables<T> tb = op7<T>(ctx).t;

@@ -200,23 +200,31 @@ drain:
 
 namespace fb {
 
-// Three half sweeps per pass on a 28 x 16 tile (FP32 path).
+// Three half sweeps per pass on a 28 x 16 tile (FP32 path), skewed wavefront.
 //
-// Same wavefront as k_sor_rb_tma; the work of a half sweep is laid out for
-// shared-memory banks and issue slots:
+// Half sweep h of plane p runs at iteration q = p + 2h - 1 (planes q-1, q-3 and
+// q-5 at iteration q).  Half sweep h reads the other colour of planes p-1, p,
+// p+1, which half sweep h-1 finished at iterations q-3, q-2 and q-1 and which
+// half sweep h+1 changes only from iteration q+1 on; so the three half sweeps
+// of an iteration touch disjoint data and run without barriers between them,
+// and one block barrier per iteration (after the new plane has landed) keeps
+// every warp within one iteration of the others.  Plane p is final after
+// iteration p+5 and written out at iteration p+6; the ring holds planes q-6..q
+// plus NS-7 planes in flight.
+//
+// Work layout:
 //  * 160 threads; thread t owns pair column m = t % 16 (cells x0 = i0-2+2m and
 //    x0+1) in rows rw and rw+10 of the widest ring (rw = t / 16), so a half
 //    warp covers one row and the two halves of a warp cover adjacent rows.
 //    Same-colour cells of adjacent rows sit on opposite bank parities (the box
 //    pitch is even), so every shared access of a half sweep is one wavefront.
 //  * the two rows of a thread have the same parity, hence the same colour
-//    offset e: both updates run as one pair through the packed FP32 units
+//    offset e: both updates run as one pair through the packed FP32 pipe
 //    (fma/add/mul.f32x2), each lane rounding exactly as the scalar
 //    sor_point() does.
 //  * the right-hand side is staged as its own (32 x 20) box covering just the
-//    cells a half sweep updates.
-//  * the plane loop is unrolled over the NS slots, so every slot address is a
-//    constant offset.
+//    cells a half sweep updates; the chunk's z coefficients are staged once.
+//  * the march is unrolled over the NS slots, so slot addresses are constants.
 template <typename T>
 struct RB2Tile {
     static constexpr int H = 3, R = H - 1;
@@ -227,10 +235,11 @@ struct RB2Tile {
     static constexpr int BXB = 32, BYB = TY + 2 * R, PEB = BXB * BYB;    // right-hand side box from i0 - 2
     static constexpr int PBX = (PE * (int)sizeof(T) + 127) / 128 * 128, PBB = (PEB * (int)sizeof(T) + 127) / 128 * 128;
     static constexpr int SLOT = PBX + PBB;
-    static constexpr int NS = 8;
+    static constexpr int NS = 10;                                         // 7 resident planes + 3 in flight
+    static constexpr int ZMAX = 72;                                       // z coefficient planes staged (kc <= ZMAX - 2H)
     static constexpr int PX = 16, PY = TY + 2 * R, HALF = PY / 2;        // pairs per row, rows, rows per set
     static constexpr int NT = PX * HALF;                                  // threads
-    static constexpr int SMEM = NS * SLOT + 128 + 128;
+    static constexpr int SMEM = NS * SLOT + ZMAX * 4 * (int)sizeof(T) + 128 + 128;
     static_assert(PY % 4 == 0, "the two rows of a thread have the same parity");
     static_assert(R <= 2 && TX + R <= 2 * PX - 2, "the pair columns (x from i0 - 2) cover the widest ring");
 };
@@ -255,21 +264,23 @@ __device__ __forceinline__ float2 sor_point2(float2 ac, float2 ae, float2 aw, fl
 }
 
 template <typename T>
-__global__ void __launch_bounds__(RB2Tile<T>::NT, 4) k_sor_rb2_tma(Geom g, int kc, const __grid_constant__ CUtensorMap mx,
-                                                              const __grid_constant__ CUtensorMap mb, PoissonTables<T> tb,
-                                                              T *__restrict__ xout, T omega, int c1, const SolverScalars *sc,
-                                                              int *err) {
+__global__ void __launch_bounds__(RB2Tile<T>::NT, 3) k_sor_rb2_tma(Geom g, int kc, const __grid_constant__ CUtensorMap mx,
+                                                                 const __grid_constant__ CUtensorMap mb, PoissonTables<T> tb,
+                                                                 T *__restrict__ xout, T omega, int c1, const SolverScalars *sc,
+                                                                 int *err) {
     static_assert(std::is_same<T, float>::value, "packed FP32 arithmetic");
     using L = RB2Tile<T>;
     constexpr int H = L::H;
     constexpr int NS = L::NS;
     extern __shared__ unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
-    uint64_t *bar = (uint64_t *)(smem + NS * L::SLOT);
+    float4 *ztab = (float4 *)(smem + NS * L::SLOT);                      // per staged plane: ab, at, -up, -um
+    uint64_t *bar = (uint64_t *)(smem + NS * L::SLOT + L::ZMAX * 4 * sizeof(T));
     if (sc && sc->done) return;
     const int i0 = g.gc + blockIdx.x * L::TX, j0 = g.gc + blockIdx.y * L::TY;
     const int k0 = g.gc + blockIdx.z * kc, k1 = min(k0 + kc, g.sz - g.gc);
     const int P0 = k0 - H, nplanes = (k1 + H) - P0;
+    if (nplanes > L::ZMAX) { if (threadIdx.x == 0) atomicExch(err, 300 + 6); return; }
     const int xb = max(0, box_origin(i0 - L::HX, L::BX, g.sx, L::AL));
     const int yb = max(0, box_origin(j0 - H, L::BY, g.sy, 1));
     const int xbb = max(0, box_origin(i0 - 2, L::BXB, g.sx, L::AL));
@@ -337,29 +348,35 @@ __global__ void __launch_bounds__(RB2Tile<T>::NT, 4) k_sor_rb2_tma(Geom g, int k
         }
     }
     const int par0 = (x0 + yr[0]) & 1;
-    auto issue = [&](int q) {
-        uint64_t *b = bar + (q % NS);
+    // plane q into slot s = q % NS (the caller passes s)
+    auto issue = [&](int q, int s) {
+        uint64_t *b = bar + s;
         const int z = P0 + q;
         if (z < 0 || z >= g.sz) { mbar_arrive(b); return; }
-        unsigned char *s = smem + (q % NS) * L::SLOT;
-        if (tma_ok(s, xb, yb, z, (int)sizeof(T), g.sx, g.sy, g.sz) && tma_ok(s + L::PBX, xbb, ybb, z, (int)sizeof(T), g.sx, g.sy, g.sz)) {
+        unsigned char *d = smem + s * L::SLOT;
+        if (tma_ok(d, xb, yb, z, (int)sizeof(T), g.sx, g.sy, g.sz) && tma_ok(d + L::PBX, xbb, ybb, z, (int)sizeof(T), g.sx, g.sy, g.sz)) {
             mbar_expect_tx(b, (L::PE + L::PEB) * sizeof(T));
-            tma_load_4d(s, &mx, xb, yb, z, 0, b);
-            tma_load_4d(s + L::PBX, &mb, xbb, ybb, z, 0, b);
+            tma_load_4d(d, &mx, xb, yb, z, 0, b);
+            tma_load_4d(d + L::PBX, &mb, xbb, ybb, z, 0, b);
         } else {
             tma_reject(b, err, 5);
         }
     };
-    auto wait_q = [&](int q) -> bool { return threadIdx.x >= 32 || mbar_wait(bar + (q % NS), (q / NS) & 1, err); };
+    auto wait_s = [&](int s, int parity) -> bool { return threadIdx.x >= 32 || mbar_wait(bar + s, parity, err); };
     if (threadIdx.x == 0) {
         prefetch_tmap(&mx); prefetch_tmap(&mb);
         for (int s = 0; s < NS; s++) mbar_init(bar + s, 1);
         mbar_fence_init();
     }
+    // the chunk's z coefficients
+    for (int q = threadIdx.x; q < nplanes; q += blockDim.x) {
+        const int kz = min(max(P0 + q, 0), g.sz - 1);
+        ztab[q] = make_float4(ldg(tb.cm[2] + kz), ldg(tb.cp[2] + kz), -ldg(tb.up[2] + kz), -ldg(tb.um[2] + kz));
+    }
     __syncthreads();
     int issued = min(NS, nplanes), waited = 0;
     if (threadIdx.x == 0)
-        for (int q = 0; q < issued; q++) issue(q);
+        for (int q = 0; q < issued; q++) issue(q, q % NS);
     const long long sxy = (long long)g.sx * g.sy;
     // write-out: this thread's cell pairs w = t and t + NT of the tile (14 pairs
     // per row): offsets in the x box and in a plane of x_out, -1 when outside
@@ -375,57 +392,26 @@ __global__ void __launch_bounds__(RB2Tile<T>::NT, 4) k_sor_rb2_tma(Geom g, int k
         wgo[n] = wy * g.sx + wx;
         wpair[n] = wx + 1 < ihi;
     }
-    // z coefficients of planes q-1 .. q-H as lane pairs (ab, at; -up, -um)
-    float2 zab[H], zat[H], zpn[H], zmn[H];
-#pragma unroll
-    for (int h = 0; h < H; h++) zab[h] = zat[h] = zpn[h] = zmn[h] = f2(0.f, 0.f);
     const float2 sc2 = f2(tb.scale, tb.scale), om2 = f2(omega, omega);
-    for (int q0 = 0; q0 < nplanes; q0 += NS) {
+    const int nit = nplanes + H;   // the last tile plane, nplanes - H - 1, is written out at iteration nplanes + H - 1
+    for (int q0 = 0, ph = 0; q0 < nit; q0 += NS, ph ^= 1) {
 #pragma unroll
         for (int u = 0; u < NS; u++) {
             const int q = q0 + u;
-            if (q >= nplanes) break;
+            if (q >= nit) break;
             // slot of plane q - m (a constant once unrolled)
             auto sl = [&](int m) { return smem + ((u - m + 2 * NS) % NS) * L::SLOT; };
-#pragma unroll
-            for (int h = H - 1; h > 0; h--) { zab[h] = zab[h - 1]; zat[h] = zat[h - 1]; zpn[h] = zpn[h - 1]; zmn[h] = zmn[h - 1]; }
-            {
-                const int kz = min(max(P0 + q - 1, 0), g.sz - 1);
-                const float vab = ldg(tb.cm[2] + kz), vat = ldg(tb.cp[2] + kz), vup = ldg(tb.up[2] + kz), vum = ldg(tb.um[2] + kz);
-                zab[0] = f2(vab, vab); zat[0] = f2(vat, vat); zpn[0] = f2(-vup, -vup); zmn[0] = f2(-vum, -vum);
+            bool fail = false;
+            if (q < nplanes) {
+                fail = !wait_s(u, ph);
+                waited = q + 1;
             }
-            bool fail = !wait_q(q);
-            waited = q + 1;
             if (__syncthreads_or(fail)) goto drain;
-#pragma unroll
-            for (int h = 1; h <= H; h++) {
-                const int p = q - h, kp = P0 + p, ring = H - h;
-                if (p >= 1 && kp >= max(klo, k0 - ring) && kp < min(khi, k1 + ring)) {
-                    const int color = (c1 + h - 1) & 1;
-                    const int e = (color ^ par0 ^ kp) & 1;   // the pairs' cell of this colour (both row sets)
-                    const unsigned l0 = (live >> (3 * e + h - 1)) & 1u, l1 = (live >> (3 * (2 + e) + h - 1)) & 1u;
-                    if (l0 | l1) {
-                        float *X0 = (float *)sl(h);
-                        const float *Xm = (const float *)sl(h + 1), *Xp = (const float *)sl(h - 1);
-                        const float *B0 = (const float *)(sl(h) + L::PBX);
-                        const int o0 = ox[0] + e, o1 = ox[1] + e;
-                        const float2 ac = __fmul2_rn(__fadd2_rn(__fadd2_rn(e ? dxy2[1] : dxy2[0], zpn[h - 1]), zmn[h - 1]), sc2);
-                        const float2 xc = f2(X0[o0], X0[o1]);
-                        const float2 r = sor_point2(ac, e ? ae2[1] : ae2[0], e ? aw2[1] : aw2[0], an2, as2, zat[h - 1], zab[h - 1], xc,
-                                                    f2(X0[o0 + 1], X0[o1 + 1]), f2(X0[o0 - 1], X0[o1 - 1]),
-                                                    f2(X0[o0 + L::BX], X0[o1 + L::BX]), f2(X0[o0 - L::BX], X0[o1 - L::BX]),
-                                                    f2(Xp[o0], Xp[o1]), f2(Xm[o0], Xm[o1]), f2(B0[ob[0] + e], B0[ob[1] + e]), om2);
-                        if (l0) X0[o0] = r.x;
-                        if (l1) X0[o1] = r.y;
-                    }
-                }
-                __syncthreads();
-            }
-            // the tile of plane q-H is final: pairs of cells out
+            // plane q - 2H is final (its last half sweep ran at iteration q - 1): write it out
             {
-                const int kp = P0 + q - H;
+                const int kp = P0 + q - 2 * H;
                 if (kp >= k0 && kp < k1) {
-                    const float *Xf = (const float *)sl(H);
+                    const float *Xf = (const float *)sl(2 * H);
                     float *plane = xout + (long long)kp * sxy;
 #pragma unroll
                     for (int n = 0; n < NW; n++) {
@@ -436,18 +422,43 @@ __global__ void __launch_bounds__(RB2Tile<T>::NT, 4) k_sor_rb2_tma(Geom g, int k
                     }
                 }
             }
+            // the slot of plane q - 2H - 1 was last read in iteration q - 1: refill it
             {
-                const int qn = q - H - 1 + NS;
-                if (q - H - 1 >= 0 && qn < nplanes) {
-                    if (threadIdx.x == 0) { fence_proxy_async(); issue(qn); }
+                const int qn = q - 2 * H - 1 + NS;
+                if (q - 2 * H - 1 >= 0 && qn < nplanes) {
+                    if (threadIdx.x == 0) { fence_proxy_async(); issue(qn, (u + NS - 2 * H - 1) % NS); }
                     issued = qn + 1;
+                }
+            }
+            // half sweeps h = 1..H on planes q - (2h - 1), no barrier between them
+#pragma unroll
+            for (int h = 1; h <= H; h++) {
+                const int p = q - (2 * h - 1), kp = P0 + p, ring = H - h;
+                if (p >= 1 && p + 1 < nplanes && kp >= max(klo, k0 - ring) && kp < min(khi, k1 + ring)) {
+                    const int color = (c1 + h - 1) & 1;
+                    const int e = (color ^ par0 ^ kp) & 1;   // the pairs' cell of this colour (both row sets)
+                    const unsigned l0 = (live >> (3 * e + h - 1)) & 1u, l1 = (live >> (3 * (2 + e) + h - 1)) & 1u;
+                    if (l0 | l1) {
+                        float *X0 = (float *)sl(2 * h - 1);
+                        const float *Xm = (const float *)sl(2 * h), *Xp = (const float *)sl(2 * h - 2);
+                        const float *B0 = (const float *)(sl(2 * h - 1) + L::PBX);
+                        const float4 z = ztab[p];
+                        const int o0 = ox[0] + e, o1 = ox[1] + e;
+                        const float2 ac = __fmul2_rn(__fadd2_rn(__fadd2_rn(e ? dxy2[1] : dxy2[0], f2(z.z, z.z)), f2(z.w, z.w)), sc2);
+                        const float2 r = sor_point2(ac, e ? ae2[1] : ae2[0], e ? aw2[1] : aw2[0], an2, as2, f2(z.y, z.y), f2(z.x, z.x), f2(X0[o0], X0[o1]),
+                                                    f2(X0[o0 + 1], X0[o1 + 1]), f2(X0[o0 - 1], X0[o1 - 1]),
+                                                    f2(X0[o0 + L::BX], X0[o1 + L::BX]), f2(X0[o0 - L::BX], X0[o1 - L::BX]),
+                                                    f2(Xp[o0], Xp[o1]), f2(Xm[o0], Xm[o1]), f2(B0[ob[0] + e], B0[ob[1] + e]), om2);
+                        if (l0) X0[o0] = r.x;
+                        if (l1) X0[o1] = r.y;
+                    }
                 }
             }
         }
     }
     return;
 drain:
-    for (int q = waited; q < issued; q++) wait_q(q);
+    for (int q = waited; q < issued; q++) wait_s(q % NS, (q / NS) & 1);
 }
 
 }  // namespace fb

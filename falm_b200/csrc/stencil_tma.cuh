@@ -47,8 +47,6 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_pseudo_u_tma(Ge
     const int i = i0 + tx, j = j0 + ty;
     bool active = i < g.sx - g.gc && j < g.sy - g.gc;
     const int P0 = k0 - 2, nplanes = (k1 + 2) - P0;
-    long long cc = g.id(i, j, P0 + 2);   // cell of the first computed plane, advanced per plane
-    const long long sxy = (long long)g.sx * g.sy;
     // box origin (tile minus the halo of 2), kept inside the tensor when it is wide enough
     const int xb = box_origin(i0 - 2, L::BX, g.sx, 16 / (int)sizeof(T)), yb = box_origin(j0 - 2, L::BY, g.sy, 1);
     const int ox = min(i, g.sx - g.gc - 1) - xb, oy = min(j, g.sy - g.gc - 1) - yb;
@@ -140,13 +138,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_pseudo_u_tma(Ge
             issued = upto + 1;
         }
     }
-    // the march, unrolled over the slots: plane q = q0 + u is in slot u
-    for (int q0 = 0; q0 < nplanes - 2; q0 += NS) {
-#pragma unroll
-      for (int u = 0; u < NS; u++) {
-        const int q = q0 + u;
-        if (q < 2) continue;
-        if (q >= nplanes - 2) break;
+    for (int q = 2; q < nplanes - 2; q++) {
         // planes q (= k), q+1, q+2 must be resident; q+2 is the new one
         fail = !wait_q(q + 2);
         waited = q + 3;
@@ -162,12 +154,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_pseudo_u_tma(Ge
             }
         }
         const int k = P0 + q;
-        unsigned char *const s0 = smem + u * L::SLOT, *const s1 = smem + ((u + 1) % NS) * L::SLOT, *const s2 = smem + ((u + 2) % NS) * L::SLOT;
-        const T *U0 = (const T *)s0, *UU0 = (const T *)(s0 + L::U_BYTES), *N0 = (const T *)(s0 + 2 * L::U_BYTES);
-        const T *U1 = (const T *)s1, *N1 = (const T *)(s1 + 2 * L::U_BYTES);
-        const T *U2 = (const T *)s2;
+        const T *U0 = (const T *)slot(q), *UU0 = (const T *)(slot(q) + L::U_BYTES), *N0 = (const T *)(slot(q) + 2 * L::U_BYTES);
+        const T *U1 = (const T *)slot(q + 1), *N1 = (const T *)(slot(q + 1) + 2 * L::U_BYTES);
+        const T *U2 = (const T *)slot(q + 2);
         const T hzt = ldg(mv.m.h[2] + k + 1), kzt = ldg(mv.m.k[2] + k + 1);
         if (active) {
+            const long long cc = g.id(i, j, k);
             const T hzkz2 = hzk * (kzk * kzk);
             const T Bzt = hzkz2 + hzt * (kzt * kzt), Bzb = hzkz2 + hzb * (kzb * kzb);
             // the scheme's divisions by the Jacobian become multiplications by 1/ja
@@ -249,8 +241,6 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_pseudo_u_tma(Ge
         for (int d = 0; d < 3; d++) { um2[d] = um1[d]; um1[d] = U0[d * L::PE + o]; }
         nutm1 = N0[o];
         uu2m1 = UU0[2 * L::PE + o];
-        cc += sxy;
-      }
     }
     return;
 drain:
