@@ -235,7 +235,7 @@ struct RB2Tile {
     static constexpr int BXB = 32, BYB = TY + 2 * R, PEB = BXB * BYB;    // right-hand side box from i0 - 2
     static constexpr int PBX = (PE * (int)sizeof(T) + 127) / 128 * 128, PBB = (PEB * (int)sizeof(T) + 127) / 128 * 128;
     static constexpr int SLOT = PBX + PBB;
-    static constexpr int NS = 10;                                         // 7 resident planes + 3 in flight
+    static constexpr int NS = 9;                                          // 7 resident planes + 2 in flight
     static constexpr int ZMAX = 72;                                       // z coefficient planes staged (kc <= ZMAX - 2H)
     static constexpr int PX = 16, PY = TY + 2 * R, HALF = PY / 2;        // pairs per row, rows, rows per set
     static constexpr int NT = PX * HALF;                                  // threads
@@ -264,7 +264,7 @@ __device__ __forceinline__ float2 sor_point2(float2 ac, float2 ae, float2 aw, fl
 }
 
 template <typename T>
-__global__ void __launch_bounds__(RB2Tile<T>::NT, 3) k_sor_rb2_tma(Geom g, int kc, const __grid_constant__ CUtensorMap mx,
+__global__ void __launch_bounds__(RB2Tile<T>::NT, 4) k_sor_rb2_tma(Geom g, int kc, const __grid_constant__ CUtensorMap mx,
                                                                  const __grid_constant__ CUtensorMap mb, PoissonTables<T> tb,
                                                                  T *__restrict__ xout, T omega, int c1, const SolverScalars *sc,
                                                                  int *err) {

@@ -47,6 +47,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_pseudo_u_tma(Ge
     const int i = i0 + tx, j = j0 + ty;
     bool active = i < g.sx - g.gc && j < g.sy - g.gc;
     const int P0 = k0 - 2, nplanes = (k1 + 2) - P0;
+    // slots of planes q, q+1, q+2 and the barrier parity of plane q+2, rolled
+    // along the march from q = 2 (NS need not be a power of two)
+    int s0 = 2 % NS, s1 = 3 % NS, s2 = 4 % NS, ph2 = (4 / NS) & 1;
     // box origin (tile minus the halo of 2), kept inside the tensor when it is wide enough
     const int xb = box_origin(i0 - 2, L::BX, g.sx, 16 / (int)sizeof(T)), yb = box_origin(j0 - 2, L::BY, g.sy, 1);
     const int ox = min(i, g.sx - g.gc - 1) - xb, oy = min(j, g.sy - g.gc - 1) - yb;
@@ -140,7 +143,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_pseudo_u_tma(Ge
     }
     for (int q = 2; q < nplanes - 2; q++) {
         // planes q (= k), q+1, q+2 must be resident; q+2 is the new one
-        fail = !wait_q(q + 2);
+        fail = !(threadIdx.x >= 32 || mbar_wait(bar + s2, ph2, err));
         waited = q + 3;
         if (__syncthreads_or(fail)) goto drain;
         {   // planes up to q-1 are no longer read (held in registers): refill their slots
@@ -154,9 +157,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_pseudo_u_tma(Ge
             }
         }
         const int k = P0 + q;
-        const T *U0 = (const T *)slot(q), *UU0 = (const T *)(slot(q) + L::U_BYTES), *N0 = (const T *)(slot(q) + 2 * L::U_BYTES);
-        const T *U1 = (const T *)slot(q + 1), *N1 = (const T *)(slot(q + 1) + 2 * L::U_BYTES);
-        const T *U2 = (const T *)slot(q + 2);
+        unsigned char *const sp0 = smem + s0 * L::SLOT, *const sp1 = smem + s1 * L::SLOT, *const sp2 = smem + s2 * L::SLOT;
+        const T *U0 = (const T *)sp0, *UU0 = (const T *)(sp0 + L::U_BYTES), *N0 = (const T *)(sp0 + 2 * L::U_BYTES);
+        const T *U1 = (const T *)sp1, *N1 = (const T *)(sp1 + 2 * L::U_BYTES);
+        const T *U2 = (const T *)sp2;
         const T hzt = ldg(mv.m.h[2] + k + 1), kzt = ldg(mv.m.k[2] + k + 1);
         if (active) {
             const long long cc = g.id(i, j, k);
@@ -241,6 +245,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_pseudo_u_tma(Ge
         for (int d = 0; d < 3; d++) { um2[d] = um1[d]; um1[d] = U0[d * L::PE + o]; }
         nutm1 = N0[o];
         uu2m1 = UU0[2 * L::PE + o];
+        s0 = s1; s1 = s2;
+        if (++s2 == NS) { s2 = 0; ph2 ^= 1; }
     }
     return;
 drain:
