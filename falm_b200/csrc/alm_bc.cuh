@@ -186,21 +186,21 @@ __global__ void __launch_bounds__(256) k_alm_box(AlmDev a, const double *xc, con
     const double eps = a.euler_eps, sq = sqrt(3.14159265358979323846) * eps, eta = 1. / (sq * sq * sq);
     const double *bb = a.scal->bbox;
     const double b0 = bb[0], b1 = bb[1], b2 = bb[2], b3 = bb[3], b4 = bb[4], b5 = bb[5];
-    const long long tot = a.bs.total;
+    // force boxes hold far fewer than 2^31 cells: 32-bit index arithmetic
+    const int tot = (int)a.bs.total;
     T *f = (T *)a.fbox;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
-        int l0 = 0, l1 = 0, l2 = 0, e0 = 1, e1 = 1;
-        long long o = 0;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) {
+        int l0 = 0, l1 = 0, l2 = 0, e0 = 1, e1 = 1, o = 0;
 #pragma unroll
         for (int s = 0; s < kMaxTurbines; s++)
             if (s < a.bs.n && q >= a.bs.off[s]) {
                 l0 = a.bs.lo[s][0]; l1 = a.bs.lo[s][1]; l2 = a.bs.lo[s][2];
-                e0 = a.bs.ext[s][0]; e1 = a.bs.ext[s][1]; o = a.bs.off[s];
+                e0 = a.bs.ext[s][0]; e1 = a.bs.ext[s][1]; o = (int)a.bs.off[s];
             }
-        long long r = q - o;
-        const int i = l0 + (int)(r % e0);
+        int r = q - o;
+        const int i = l0 + r % e0;
         r /= e0;
-        const int j = l1 + (int)(r % e1), k = l2 + (int)(r / e1);
+        const int j = l1 + r % e1, k = l2 + r / e1;
         const double cxd = xc[i], cyd = yc[j], czd = zc[k];
         T fx = 0, fy = 0, fz = 0;
         if (box_dist2(cxd, b0, b1) + box_dist2(cyd, b2, b3) + box_dist2(czd, b4, b5) < a.rcut2) {
@@ -237,14 +237,15 @@ struct UPrev {
 
 template <typename T>
 __global__ void k_save_outlet(Geom g, const T *__restrict__ u, T *__restrict__ out) {
-    long long tot = 9LL * g.sy * g.sz;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
-        int j = (int)(q % g.sy);
-        long long r = q / g.sy;
-        int k = (int)(r % g.sz);
-        int dp = (int)(r / g.sz);
-        int d = dp / 3, pl = dp % 3;
-        out[q] = u[g.id(g.sx - g.gc - 2 + pl, j, k) + d * g.n];
+    // one thread per (j, k, d): the three outlet-side cells are adjacent in x
+    const int ns = g.sy * g.sz, tot = 3 * ns;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) {
+        const int d = q / ns, jk = q - d * ns;
+        const int j = jk % g.sy, k = jk / g.sy;
+        const T *src = u + g.id(g.sx - g.gc - 2, j, k) + d * g.n;
+        const T v0 = src[0], v1 = src[1], v2 = src[2];
+        T *o = out + (long long)(3 * d) * ns + jk;
+        o[0] = v0; o[ns] = v1; o[2 * ns] = v2;
     }
 }
 
@@ -265,8 +266,8 @@ __global__ void k_ubc(Geom g, int kind, T *u, UPrev<T> up, const double *xc, dou
     const int pair = blockIdx.y;
     const int na = pair == 0 ? sy - 2 * gc : sx - 2 * gc;
     const int nb = pair == 2 ? sy - 2 * gc : sz - 2 * gc;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < (long long)na * nb; q += (long long)gridDim.x * blockDim.x) {
-        int a = (int)(q % na) + gc, b = (int)(q / na) + gc;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < na * nb; q += gridDim.x * blockDim.x) {
+        const int a = q % na + gc, b = q / na + gc;
         if (kind == FALM_BC_CHANNEL) {
             if (pair == 0) {
                 int j = a, k = b;
@@ -349,8 +350,8 @@ __global__ void k_pbc(Geom g, int kind, T *p) {
     const int pair = blockIdx.y;
     const int na = pair == 0 ? sy - 2 * gc : sx - 2 * gc;
     const int nb = pair == 2 ? sy - 2 * gc : sz - 2 * gc;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < (long long)na * nb; q += (long long)gridDim.x * blockDim.x) {
-        int a = (int)(q % na) + gc, b = (int)(q / na) + gc;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < na * nb; q += gridDim.x * blockDim.x) {
+        const int a = q % na + gc, b = q / na + gc;
         if (pair == 0) {
             p[g.id(gc - 1, a, b)] = p[g.id(gc, a, b)];
             p[g.id(sx - gc, a, b)] = kind == FALM_BC_CHANNEL ? T(0.0) : p[g.id(sx - gc - 1, a, b)];
@@ -371,8 +372,8 @@ __global__ void k_uubc(Geom g, T *uu) {
     const int pair = blockIdx.y;
     const int na = pair == 0 ? sy - 2 * gc : sx - 2 * gc;
     const int nb = pair == 2 ? sy - 2 * gc : sz - 2 * gc;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < (long long)na * nb; q += (long long)gridDim.x * blockDim.x) {
-        int a = (int)(q % na) + gc, b = (int)(q / na) + gc;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < na * nb; q += gridDim.x * blockDim.x) {
+        const int a = q % na + gc, b = q / na + gc;
         if (pair == 0) { uu[g.id(gc - 1, a, b)] = T(0); uu[g.id(sx - gc - 1, a, b)] = T(0); }
         else if (pair == 1) { uu[g.id(a, gc - 1, b) + g.n] = T(0); uu[g.id(a, sy - gc - 1, b) + g.n] = T(0); }
         else { uu[g.id(a, b, gc - 1) + 2 * g.n] = T(0); uu[g.id(a, b, sz - gc - 1) + 2 * g.n] = T(0); }

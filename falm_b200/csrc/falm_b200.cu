@@ -15,6 +15,7 @@
 #include <mutex>
 #include <unordered_map>
 #include <map>
+#include <climits>
 #include <tuple>
 #include "falm_internal.cuh"
 #include "common.cuh"
@@ -146,6 +147,14 @@ int chunk_len(const falm_ctx *ctx, long long blocks_xy, int nz, int per_sm, int 
         if (best_t < 0 || t < best_t) { best_t = t; best = kc; }
     }
     return std::max(1, best);
+}
+
+// blocks along x of a face-pair kernel (blockIdx.y = pair): the largest face's
+// cells at one per thread, at most four blocks per SM
+int face_blocks(const falm_ctx *ctx) {
+    const Geom &g = ctx->geo;
+    const long long mx = std::max({(long long)g.ny * g.nz, (long long)g.nx * g.nz, (long long)g.nx * g.ny});
+    return (int)std::max(1LL, std::min((mx + 255) / 256, (long long)ctx->sm_count * 4));
 }
 
 int row_grid(const falm_ctx *ctx, const Region3 &R) {
@@ -644,7 +653,7 @@ template <typename T>
 int ubc_t(falm_ctx *ctx, T *u, UPrev<T> up, double dt, double t, cudaStream_t st) {
     Inflow inf{ctx->inflow_box, ctx->inflow_nb, ctx->inflow_dx, ctx->inlet_plane_valid ? ctx->inlet_plane : nullptr};
     ctx->inlet_plane_valid = 0;
-    dim3 grid(64, 3);
+    dim3 grid(face_blocks(ctx), 3);
     LAUNCH(FALM_K_UBC, st, k_ubc<T><<<grid, 256, 0, st>>>(ctx->geo, ctx->bc_kind, u, up, ctx->m64.x[0], dt, t, ctx->u_inlet, inf));
     return FALM_OK;
 }
@@ -671,7 +680,7 @@ int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_
         const Region3 R = facemap(g);
         T scale = (T)(1.0 / (dt * ctx->maxdiag));
         // the guide layer of ua takes the previous velocity (the reference's aliased u)
-        LAUNCH(FALM_K_OTHER, st, k_copy_shell<T><<<ctx->sm_count * 2, 256, 0, st>>>(g, u, ua));
+        LAUNCH(FALM_K_OTHER, st, k_copy_shell<T><<<ctx->sm_count * 8, 256, 0, st>>>(g, u, ua));
         if (chan)
             P3_OR(FALM_K_UTOUU_RHS, st, T, 1, 0, R, 1, FB_ARR(ua), FB_ARR(3), (UtoUUBody<T, true, false>{g, mview<T>(ctx), uu, rhs, scale}),
                   (k_utouu<T, true, false><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), ua, u, uu, rhs, scale)));
@@ -686,9 +695,9 @@ int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_
     int solve_status = ctx->scal_host->status;
     if (rc) return rc;
     // 5. pbc
-    LAUNCH(FALM_K_PBC, st, k_pbc<T><<<dim3(64, 3), 256, 0, st>>>(g, ctx->bc_kind, p));
+    LAUNCH(FALM_K_PBC, st, k_pbc<T><<<dim3(face_blocks(ctx), 3), 256, 0, st>>>(g, ctx->bc_kind, p));
     // 6. keep the previous velocity at the outlet planes, then project
-    if (chan) { LAUNCH(FALM_K_OTHER, st, k_save_outlet<T><<<64, 256, 0, st>>>(g, u, (T *)ctx->w_outlet)); }
+    if (chan) { LAUNCH(FALM_K_OTHER, st, k_save_outlet<T><<<std::min(ctx->sm_count * 4, (3 * g.sy * g.sz + 255) / 256), 256, 0, st>>>(g, u, (T *)ctx->w_outlet)); }
     {
         const Region3 R = facemap(g);
         P3_OR(FALM_K_PROJECT, st, T, 1, 0, R, 1, FB_ARR(p), FB_ARR(1), (ProjectBody<T>{g, mview<T>(ctx), u, ua, uu, uu, (T)dt}),
@@ -1105,7 +1114,7 @@ int falm_bc_pbc(falm_ctx *ctx, void *p, void *stream) {
     if (!ctx || !p) return FALM_ERR_ARG;
     return dispatch(ctx, [&](auto z) {
         using T = decltype(z);
-        LAUNCH(FALM_K_PBC, S(stream), k_pbc<T><<<dim3(64, 3), 256, 0, S(stream)>>>(ctx->geo, ctx->bc_kind, (T *)p));
+        LAUNCH(FALM_K_PBC, S(stream), k_pbc<T><<<dim3(face_blocks(ctx), 3), 256, 0, S(stream)>>>(ctx->geo, ctx->bc_kind, (T *)p));
         return (int)FALM_OK;
     });
 }
@@ -1115,7 +1124,7 @@ int falm_bc_uubc(falm_ctx *ctx, void *uu, void *stream) {
     if (ctx->bc_kind != FALM_BC_CAVITY) return FALM_OK;
     return dispatch(ctx, [&](auto z) {
         using T = decltype(z);
-        LAUNCH(FALM_K_OTHER, S(stream), k_uubc<T><<<dim3(64, 3), 256, 0, S(stream)>>>(ctx->geo, (T *)uu));
+        LAUNCH(FALM_K_OTHER, S(stream), k_uubc<T><<<dim3(face_blocks(ctx), 3), 256, 0, S(stream)>>>(ctx->geo, (T *)uu));
         return (int)FALM_OK;
     });
 }
@@ -1228,6 +1237,7 @@ int falm_alm_init(falm_ctx *ctx, const falm_alm_desc *d) {
             bs.off[t] = off;
             off += cells;
         }
+        if (off > (long long)INT_MAX / 3) return fail(ctx, FALM_ERR_ARG, "alm_init: force boxes hold more than 2^31 / 3 cells");
         bs.n = nt;
         bs.total = off;
         if (a.fbox) { cudaFree(a.fbox); a.fbox = nullptr; }
