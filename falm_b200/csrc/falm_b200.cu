@@ -524,26 +524,31 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
     };
     auto first_target = [&](T *z) -> T * { return (pct == FALM_LS_JACOBI && ((m - 1) & 1)) ? xp : z; };
     for (outer = 0; outer < max_outer; outer++) {
-        // outer > 0: true residual in FP64; stop when it meets the tolerance.
-        // The first pass stores the residual in rr only (r equals rr until the
-        // pass's first k_bicg_xr, which writes r; the iteration reads rr before)
-        S7_OR(FALM_K_RES, st, T, 2, x, (ResBody<T>{op, b, outer > 0 ? r : nullptr, rr, sc, outer > 0 ? 1 : 0}),
+        // outer > 0: true residual in FP64; stop when it meets the tolerance
+        // (a check that stores nothing; a pass that follows recomputes it into
+        // rr). A pass stores its residual in rr only: r equals rr until the
+        // pass's first k_bicg_xr, which writes r, and the iteration reads rr before.
+        S7_OR(FALM_K_RES, st, T, 2, x, (ResBody<T>{op, b, nullptr, outer > 0 ? nullptr : rr, sc, outer > 0 ? 1 : 0}),
               (k_res<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, r, rr, ctx->red, sc, outer > 0 ? 1 : 0)));
         if (outer > 0) {
             CK(cudaMemcpyAsync(ctx->scal_host, sc, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             if (ctx->scal_host->done) break;
+            S7_OR(FALM_K_RES, st, T, 2, x, (ResBody<T>{op, b, nullptr, rr, sc, 0}),
+                  (k_res<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, r, rr, ctx->red, sc, 0)));
             // restart the iteration count of this pass
             int zero = 0;
             CK(cudaMemcpyAsync(&sc->it, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
             CK(cudaStreamSynchronize(st));
         }
-        bool first_it = true;
-        for (;;) {
-            const T *rin = first_it ? rr : r;
-            first_it = false;
-            LAUNCH(FALM_K_BICG_P, st, k_bicg_p<T><<<grid_p, kRowThreads, 0, st>>>(g, R, op, p, q, rin, first_target(pp), pct, pcw, sc));
-            if ((rc = precondition_rest(pp, p))) return rc;
+        // iteration itp of the pass: r equals rr until the first k_bicg_xr, and
+        // the first iteration's p equals r, so it reads rr in their place
+        for (int itp = 0;; itp++) {
+            const T *rin = itp == 0 ? rr : r;
+            T *pout = itp == 0 ? nullptr : p;
+            const T *pin = itp == 1 ? rr : p, *pv = itp == 0 ? rr : p;
+            LAUNCH(FALM_K_BICG_P, st, k_bicg_p<T><<<grid_p, kRowThreads, 0, st>>>(g, R, op, pout, pin, q, rin, first_target(pp), pct, pcw, sc));
+            if ((rc = precondition_rest(pp, pv))) return rc;
             S7_OR(FALM_K_MV_DOT1, st, T, 1, pp, (MvDot1Body<T>{op, q, rr, sc}),
                   (k_mv_dot1<T><<<grid, kRowThreads, 0, st>>>(g, R, op, pp, q, rr, ctx->red, sc)));
             LAUNCH(FALM_K_BICG_S, st, k_bicg_s<T><<<grid_s, kRowThreads, 0, st>>>(g, R, op, s, q, rin, first_target(ss), pct, pcw, sc));

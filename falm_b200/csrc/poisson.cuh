@@ -253,8 +253,10 @@ __device__ __forceinline__ T pc_first(int pc_type, int i, int j, int k, T v, T a
 constexpr int kRowILP = 4;
 
 // ---------------------------------------------------------------- BiCGStab steps
+// p_in: the previous p (read unless first); p_out: the new p, or null when the
+// caller reads r in its place (first iteration, p = r)
 template <typename T>
-__global__ void __launch_bounds__(kRowThreads) k_bicg_p(Geom g, Region3 R, Op7<T> op, T *__restrict__ p,
+__global__ void __launch_bounds__(kRowThreads) k_bicg_p(Geom g, Region3 R, Op7<T> op, T *p_out, const T *p_in,
     const T *__restrict__ q, const T *__restrict__ r, T *__restrict__ pp, int pc_type, T pc_omega, const SolverScalars *sc) {
     if (sc->done) return;
     const int first = sc->first;
@@ -270,7 +272,7 @@ __global__ void __launch_bounds__(kRowThreads) k_bicg_p(Geom g, Region3 R, Op7<T
                 rv[u] = pv[u] = qv[u] = T(0);
                 if (i < R.i1) {
                     rv[u] = r[c0 + i];
-                    if (!first) { pv[u] = p[c0 + i]; qv[u] = q[c0 + i]; }
+                    if (!first) { pv[u] = p_in[c0 + i]; qv[u] = q[c0 + i]; }
                 }
             }
 #pragma unroll
@@ -279,7 +281,7 @@ __global__ void __launch_bounds__(kRowThreads) k_bicg_p(Geom g, Region3 R, Op7<T
                 if (i < R.i1) {
                     const long long c = c0 + i;
                     const T v = first ? rv[u] : rv[u] + beta * (pv[u] - omega * qv[u]);   // src/dev/FalmEqDevCall.cu:261
-                    p[c] = v;
+                    if (p_out) p_out[c] = v;
                     pp[c] = pc_first<T>(pc_type, i, j, k, v, op.diag_row(rd, i, c), pc_omega);
                 }
             }

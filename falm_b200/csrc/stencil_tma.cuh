@@ -11,9 +11,42 @@
 // halo columns are re-read by the neighbouring CTAs, mostly from L2.
 #pragma once
 #include "cfd.cuh"
+#include "pair.cuh"
 #include "tma.cuh"
 
 namespace fb {
+
+// axis4r (one axis of the 4th-order schemes) with its operations spelled out,
+// on one lane or on a lane pair (two axes of a component); each lane rounds as
+// the scalar version
+template <typename T>
+__device__ __forceinline__ T axis4e(T ucc, T up1, T up2, T um1, T um2, T Ua, T JP, T JM, T c) {
+    T dl = fma(T(27), up1, -up2);
+    dl = fma(T(-27), ucc, dl) + um1;
+    T dr = fma(T(27), ucc, -up1);
+    dr = fma(T(-27), um1, dr) + um2;
+    T d4 = fma(T(-4), up1, up2);
+    d4 = fma(T(6), ucc, d4);
+    d4 = fma(T(-4), um1, d4) + um2;
+    T r = JP * dl;
+    r = fma(JM, dr, r) * c;
+    return fma(Ua, d4, r);
+}
+template <typename T2>
+__device__ __forceinline__ T2 axis4p(T2 ucc, T2 up1, T2 up2, T2 um1, T2 um2, T2 Ua, T2 JP, T2 JM, T2 c) {
+    using S = decltype(ucc.x);
+    const T2 k27 = mk2(S(27), S(27)), m27 = mk2(S(-27), S(-27)), m4 = mk2(S(-4), S(-4)), k6 = mk2(S(6), S(6));
+    T2 dl = fma2(k27, up1, mk2(-up2.x, -up2.y));
+    dl = add2(fma2(m27, ucc, dl), um1);
+    T2 dr = fma2(k27, ucc, mk2(-up1.x, -up1.y));
+    dr = add2(fma2(m27, um1, dr), um2);
+    T2 d4 = fma2(m4, up1, up2);
+    d4 = fma2(k6, ucc, d4);
+    d4 = add2(fma2(m4, um1, d4), um2);
+    T2 r = mul2(JP, dl);
+    r = mul2(fma2(JM, dr, r), c);
+    return fma2(Ua, d4, r);
+}
 
 __host__ __device__ constexpr int round128(int b) { return (b + 127) / 128 * 128; }
 
@@ -202,12 +235,17 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_pseudo_u_tma(Ge
             const T alpha = adv == FALM_ADV_UTOPIA ? T(1. / 12.) : (adv == FALM_ADV_KK ? T(1. / 4.) : T(1. / 24.));
             const T Ua = fabs(U0[o] * kxc) * alpha, Va = fabs(U0[L::PE + o] * kyc) * alpha, Wa = fabs(U0[2 * L::PE + o] * kzk) * alpha;
             const T c4 = T(0.5 / 24.) * ij;
+            // the x and y axes of a component run as one lane pair
+            using T2 = P2<T>;
+            const T2 JP2 = mk2(UE, VN), JM2 = mk2(UW, VS), UA2 = mk2(Ua, Va), C42 = mk2(c4, c4);
+            const T2 CP2 = mk2(ce, cn), CM2 = mk2(cw, cs);
 #pragma unroll
             for (int d = 0; d < 3; d++) {
                 const T *Ud = U0 + d * L::PE;
                 const T ucc = Ud[o];
                 const T ue1 = Ud[o + 1], uw1 = Ud[o - 1], un1 = Ud[o + L::BX], us1 = Ud[o - L::BX];
                 const T ut1 = U1[d * L::PE + o], ub1 = um1[d];
+                const T2 cc2 = mk2(ucc, ucc), p1 = mk2(ue1, un1), m1 = mk2(uw1, us1);
                 T adv_v;
                 if constexpr (adv == FALM_ADV_UPWIND1) {
                     adv_v = T(0);
@@ -228,12 +266,14 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 3) k_pseudo_u_tma(Ge
                         axis_quick(adv_v, ucc, ut1, ut2, ub1, ub2, WT, WB);
                         adv_v *= T(1. / 16.) * ij;
                     } else {
-                        adv_v = axis4r(ucc, ue1, ue2, uw1, uw2, Ua, UE, UW, c4);
-                        adv_v += axis4r(ucc, un1, un2, us1, us2, Va, VN, VS, c4);
-                        adv_v += axis4r(ucc, ut1, ut2, ub1, ub2, Wa, WT, WB, c4);
+                        const T2 axy = axis4p(cc2, p1, mk2(ue2, un2), m1, mk2(uw2, us2), UA2, JP2, JM2, C42);
+                        adv_v = axy.x + axy.y;
+                        adv_v += axis4e(ucc, ut1, ut2, ub1, ub2, Wa, WT, WB, c4);
                     }
                 }
-                T vis = ce * (ue1 - ucc) - cw * (ucc - uw1) + cn * (un1 - ucc) - cs * (ucc - us1) + ct * (ut1 - ucc) - cb * (ucc - ub1);
+                // diffusion: the (e, n) and (w, s) face terms as lane pairs
+                const T2 dxy = sub2(mul2(CP2, sub2(p1, cc2)), mul2(CM2, sub2(cc2, m1)));
+                T vis = (dxy.x + dxy.y) + (ct * (ut1 - ucc) - cb * (ucc - ub1));
                 vis *= vscale;
                 const T unv = un_is_u ? ucc : un[cc + d * N];
                 ua[cc + d * N] = unv + dt * (-adv_v + vis + fvec[d]);
