@@ -146,7 +146,9 @@ int falm_eq_poisson_operator(falm_ctx *ctx, int bc_kind, double *maxdiag_out);
 int falm_eq_set_matrix(falm_ctx *ctx, const void *A);
 /* FalmEq::Solve (src/FalmEq.h:56-64) -> PBiCGStab (src/FalmEq.cpp:305-410).  In FALM_MIXED the
    iteration runs in FP32 storage with FP64 inner products and is wrapped in an FP64
-   true-residual refinement loop.  it/err as FalmEq::it/err (src/FalmEqDevCall.h:27-30). */
+   true-residual refinement loop.  it/err as FalmEq::it/err (src/FalmEqDevCall.h:27-30).
+   r is work storage; on return it holds the last iteration's updated residual (as the
+   reference's r), or the true residual when the refinement ran out of passes. */
 int falm_eq_solve(falm_ctx *ctx, void *x, const void *b, void *r, void *stream, int *it_out, double *err_out);
 /* FalmEq::Res (src/FalmEq.cpp:45-78) */
 int falm_eq_res(falm_ctx *ctx, const void *x, const void *b, void *r, void *stream);
