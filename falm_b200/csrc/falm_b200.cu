@@ -528,14 +528,24 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
         // (a check that stores nothing; a pass that follows recomputes it into
         // rr). A pass stores its residual in rr only: r equals rr until the
         // pass's first k_bicg_xr, which writes r, and the iteration reads rr before.
-        S7_OR(FALM_K_RES, st, T, 2, x, (ResBody<T>{op, b, nullptr, outer > 0 ? nullptr : rr, sc, outer > 0 ? 1 : 0}),
-              (k_res<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, r, rr, ctx->red, sc, outer > 0 ? 1 : 0)));
+        // a pass's residual also gives the first iteration's first preconditioner
+        // sweep (pp_ready: the stream kernel stored it, so k_bicg_p is skipped)
+        bool pp_ready = false;
+        auto res_pass = [&](int check) -> int {
+            ResBody<T> body{op, b, nullptr, check ? nullptr : rr, sc, check};
+            if (!check) { body.pp = first_target(pp); body.pc_type = pct; body.pc_omega = pcw; }
+            const int s7 = s7_launch<T, 2>(ctx, FALM_K_RES, st, x, body);
+            if (s7 < 0) return -s7;
+            if (s7 == 0) LAUNCH(FALM_K_RES, st, (k_res<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, r, rr, ctx->red, sc, check)));
+            pp_ready = !check && s7 == 1;
+            return FALM_OK;
+        };
+        if ((rc = res_pass(outer > 0 ? 1 : 0))) return rc;
         if (outer > 0) {
             CK(cudaMemcpyAsync(ctx->scal_host, sc, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             if (ctx->scal_host->done) break;
-            S7_OR(FALM_K_RES, st, T, 2, x, (ResBody<T>{op, b, nullptr, rr, sc, 0}),
-                  (k_res<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, r, rr, ctx->red, sc, 0)));
+            if ((rc = res_pass(0))) return rc;
             // restart the iteration count of this pass
             int zero = 0;
             CK(cudaMemcpyAsync(&sc->it, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
@@ -547,7 +557,8 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
             const T *rin = itp == 0 ? rr : r;
             T *pout = itp == 0 ? nullptr : p;
             const T *pin = itp == 1 ? rr : p, *pv = itp == 0 ? rr : p;
-            LAUNCH(FALM_K_BICG_P, st, k_bicg_p<T><<<grid_p, kRowThreads, 0, st>>>(g, R, op, pout, pin, q, rin, first_target(pp), pct, pcw, sc));
+            if (!(itp == 0 && pp_ready))
+                LAUNCH(FALM_K_BICG_P, st, k_bicg_p<T><<<grid_p, kRowThreads, 0, st>>>(g, R, op, pout, pin, q, rin, first_target(pp), pct, pcw, sc));
             if ((rc = precondition_rest(pp, pv))) return rc;
             S7_OR(FALM_K_MV_DOT1, st, T, 1, pp, (MvDot1Body<T>{op, q, rr, sc}),
                   (k_mv_dot1<T><<<grid, kRowThreads, 0, st>>>(g, R, op, pp, q, rr, ctx->red, sc)));

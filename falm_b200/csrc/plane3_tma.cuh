@@ -54,12 +54,15 @@ struct ColMet {
     }
 };
 
-// pointwise operands of a body that has none
+// pointwise operands (or per-column / per-plane state) of a body that has none
 struct NoPW {};
 
 // Body: bool skip() const; MetricView<T> mv; type PW (the cell's pointwise
-//       operands) and PW pw_load(i, j, k, cc) const;
-//       void cell(i, j, k, cc, const P3View&, const ColMet&, const PW&, acc); void finish(tot)
+//       operands) and PW pw_load(i, j, k, cc) const; types CS, ZS (state of a
+//       column and of a plane) with CS col_state(i, j) const, ZS plane_state(k)
+//       const, evaluated once per thread and row, and once per plane;
+//       void cell(i, j, k, cc, const P3View&, const ColMet&, const PW&, const CS&,
+//       const ZS&, acc); void finish(tot)
 // The pointwise operands of a plane are loaded before the wait for the plane
 // ahead, for every row of the thread, so their latency overlaps the wait.
 template <typename T, int NF, int NS, int NV, class Body>
@@ -101,6 +104,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_plane3_tma(Geom
     for (int d = 0; d < (NV > 0 ? NV : 1); d++) acc[d] = 0.0;
     // column metric factors (x shared by the rows, y per row); z rolled per plane below
     ColMet<T> cm[RY];
+    typename Body::CS cst[RY];
+#pragma unroll
+    for (int r = 0; r < RY; r++) cst[r] = body.col_state(min(i, R.i1 - 1), min(jr[r], R.j1 - 1));
     const MetricView<T> &mv = body.mv;
     {
 #pragma unroll
@@ -180,6 +186,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_plane3_tma(Geom
                     if (threadIdx.x == 0) { fence_proxy_async(); issue(q - 2 + NS, (u + NS - 2) % NS); }
                     issued = q - 2 + NS + 1;
                 }
+                const typename Body::ZS zst = body.plane_state(k);
                 v.pl[0] = (const T *)(smem + ((u + NS - 1) % NS) * SLOTB);
                 v.pl[1] = (const T *)(smem + u * SLOTB);
                 v.pl[2] = (const T *)(smem + ((u + 1) % NS) * SLOTB);
@@ -189,7 +196,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_plane3_tma(Geom
                         v.o = orr[r];
                         cm[r].hz[0] = hz0; cm[r].hz[1] = hz1; cm[r].hz[2] = hz2;
                         cm[r].kz[0] = kz0; cm[r].kz[1] = kz1; cm[r].kz[2] = kz2;
-                        body.cell(i, jr[r], k, ccr[r], v, cm[r], pwv[r], acc);
+                        body.cell(i, jr[r], k, ccr[r], v, cm[r], pwv[r], cst[r], zst, acc);
                     }
                     ccr[r] += sxy;
                 }
@@ -224,8 +231,12 @@ struct UtoUUBody {
     T scale;
     static constexpr int NC0 = 3, NC1 = 0;   // field: the velocity to interpolate
     using PW = NoPW;
+    using CS = NoPW;
+    using ZS = NoPW;
     __device__ bool skip() const { return false; }
     __device__ PW pw_load(int, int, int, long long) const { return PW{}; }
+    __device__ CS col_state(int, int) const { return CS{}; }
+    __device__ ZS plane_state(int) const { return ZS{}; }
     __device__ __forceinline__ T ucv(const P3View<T, 1> &v, const ColMet<T> &cm, int d, int dx, int dy, int dz) const {
         return cm.ja(dx, dy, dz) * cm.k(d, dx, dy, dz) * v.at(0, d, dz, dx, dy);
     }
@@ -244,8 +255,8 @@ struct UtoUUBody {
         T b = ucv(v, cm, d, dx + (d == 0), dy + (d == 1), dz + (d == 2));
         return T(0.5) * (a + b);
     }
-    __device__ void cell(int i, int j, int k, long long c, const P3View<T, 1> &v, const ColMet<T> &cm, const PW &,
-                         double (&)[1]) const {
+    __device__ void cell(int i, int j, int k, long long c, const P3View<T, 1> &v, const ColMet<T> &cm, const PW &, const CS &,
+                         const ZS &, double (&)[1]) const {
         const T UE = face(v, cm, 0, i, j, k, 0, 0, 0), VN = face(v, cm, 1, i, j, k, 0, 0, 0), WT = face(v, cm, 2, i, j, k, 0, 0, 0);
         uu[c] = UE; uu[c + g.n] = VN; uu[c + 2 * g.n] = WT;
         if (RHS && i >= g.gc && j >= g.gc && k >= g.gc) {
@@ -273,7 +284,11 @@ struct ProjectBody {
     static constexpr int NC0 = 1, NC1 = 0;   // field: the pressure
     // face velocity (f) and cell velocity (a, interior cells only) before the correction
     struct PW { T f0, f1, f2, a0, a1, a2; };
+    using CS = NoPW;
+    using ZS = NoPW;
     __device__ bool skip() const { return false; }
+    __device__ CS col_state(int, int) const { return CS{}; }
+    __device__ ZS plane_state(int) const { return ZS{}; }
     __device__ PW pw_load(int i, int j, int k, long long cc) const {
         const long long N = g.n;
         PW w;
@@ -282,8 +297,8 @@ struct ProjectBody {
         if (i >= g.gc && j >= g.gc && k >= g.gc) { w.a0 = ua[cc]; w.a1 = ua[cc + N]; w.a2 = ua[cc + 2 * N]; }
         return w;
     }
-    __device__ void cell(int i, int j, int k, long long cc, const P3View<T, 1> &v, const ColMet<T> &cm, const PW &w,
-                         double (&)[1]) const {
+    __device__ void cell(int i, int j, int k, long long cc, const P3View<T, 1> &v, const ColMet<T> &cm, const PW &w, const CS &,
+                         const ZS &, double (&)[1]) const {
         const long long N = g.n;
         const T pcc = v.at(0, 0, 0), pe = v.at(0, 0, 0, 1, 0), pn = v.at(0, 0, 0, 0, 1), pt = v.at(0, 0, 1);
         const T dpx = T(0.5) * (cm.g(0, 0, 0, 0) + cm.g(0, 1, 0, 0)) * (pe - pcc);
@@ -319,10 +334,18 @@ struct SgsDivBody {
     double *divsum;
     static constexpr int NC0 = 3, NC1 = 3;   // fields: the cell velocity, the face velocity
     using PW = NoPW;
+    // filter width (cube root of the volume, as cbrt(hx) cbrt(hy) cbrt(hz)) and
+    // the FP64 inverse widths, split into column and plane factors
+    struct CS { T cbxy; double kxy; };
+    struct ZS { T cbz; double kz; };
     __device__ bool skip() const { return false; }
     __device__ PW pw_load(int, int, int, long long) const { return PW{}; }
-    __device__ void cell(int i, int j, int k, long long cc, const P3View<T, 2> &v, const ColMet<T> &cm, const PW &,
-                         double (&acc)[1]) const {
+    __device__ CS col_state(int i, int j) const {
+        return CS{cbrt(ldg(mv.m.h[0] + i)) * cbrt(ldg(mv.m.h[1] + j)), ldg(m64.k[0] + i) * ldg(m64.k[1] + j)};
+    }
+    __device__ ZS plane_state(int k) const { return ZS{cbrt(ldg(mv.m.h[2] + k)), ldg(m64.k[2] + k)}; }
+    __device__ void cell(int i, int j, int k, long long cc, const P3View<T, 2> &v, const ColMet<T> &cm, const PW &, const CS &cs,
+                         const ZS &zs, double (&acc)[1]) const {
         if (sgs != FALM_SGS_EMPTY) {
             const T kxx = cm.kx[1], kxy = cm.ky[1], kxz = cm.kz[1];
             T dd[3][3];
@@ -338,7 +361,7 @@ struct SgsDivBody {
             T d1 = T(2) * (dux * dux), d2 = T(2) * (dvy * dvy), d3 = T(2) * (dwz * dwz);
             T d4 = (duy + dvx) * (duy + dvx), d5 = (dvz + dwy) * (dvz + dwy), d6 = (duz + dwx) * (duz + dwx);
             T Du = sqrt(d1 + d2 + d3 + d4 + d5 + d6);
-            T De = cbrt(cm.ja(0, 0, 0));
+            T De = cs.cbxy * zs.cbz;
             if (sgs == FALM_SGS_SMAGORINSKY) {
                 T lc = Cs * De;
                 nut[cc] = (lc * lc) * Du;
@@ -361,7 +384,7 @@ struct SgsDivBody {
             double WT = to_d(v.at(1, 2, 0)), WB = to_d(v.at(1, 2, -1));
             // 1/ja as the product of the three FP64 inverse widths (one rounding
             // step per factor instead of a division)
-            const double ija = ldg(m64.k[0] + i) * ldg(m64.k[1] + j) * ldg(m64.k[2] + k);
+            const double ija = cs.kxy * zs.kz;
             double dv = (UE - UW + VN - VS + WT - WB) * ija;
             if (div_out) div_out[cc] = (T)dv;
             acc[0] += dv * dv;

@@ -299,7 +299,9 @@ struct MvDot2Body {
     }
 };
 
-// r = b - A x (FP64 arithmetic), rr = r, solver start (see k_res)
+// r = b - A x (FP64 arithmetic), rr = r, solver start (see k_res); with pp,
+// also the pointwise first preconditioner sweep from zero of the new r (what
+// k_bicg_p computes in a pass's first iteration, where p = r)
 template <typename T>
 struct ResBody {
     using V = double;
@@ -308,6 +310,9 @@ struct ResBody {
     T *r, *rr;
     SolverScalars *sc;
     int check_tol;
+    T *pp = nullptr;
+    int pc_type = 0;
+    T pc_omega = T(0);
     __device__ bool skip() const { return false; }
     __device__ const T *pw() const { return b; }
     __device__ const Op7<T> &op_() const { return op; }
@@ -318,6 +323,8 @@ struct ResBody {
         const P2<T> rt = mk2((T)r0, (T)r1);
         if (r) st2(r + c, rt);
         if (rr) st2(rr + c, rt);
+        if (pp) st2(pp + c, mk2(pc_first<T>(pc_type, i, j, k, rt.x, (T)a.ac.x, pc_omega),
+                                pc_first<T>(pc_type, i + 1, j, k, rt.y, (T)a.ac.y, pc_omega)));
         acc[0] += r0 * r0;
         acc[0] += r1 * r1;
         acc[1] += to_d(rt.x) * to_d(rt.x);
