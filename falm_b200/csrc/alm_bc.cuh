@@ -45,9 +45,23 @@ __device__ inline int find_index(const double *seq, double v, int n) {
 // UpdateAPX (:63-129), CalcAPForce (:131-253), then CalcTorqueAndThrust
 // (:362-370) and the AP bounding box used to truncate the projection.
 // FP64 arithmetic in both precision modes (O(apcount) work).
+// The cell-centre coordinates are staged in shared memory when `stage` (the
+// bisections then run there), and the per-AP results the block reduces at the
+// end are kept in shared memory too (up to kMaxFusedAp points).
 template <typename T>
-__global__ void __launch_bounds__(256) k_alm_force(Geom g, AlmDev a, const double *xc, const double *yc, const double *zc,
-                                                 const T *__restrict__ u, double t) {
+__global__ void __launch_bounds__(256) k_alm_force(Geom g, AlmDev a, const double *xc_g, const double *yc_g, const double *zc_g,
+                                                 const T *__restrict__ u, double t, int stage) {
+    extern __shared__ double s_coord[];
+    __shared__ double s_xyz[3 * kMaxFusedAp], s_tq[kMaxFusedAp], s_th[kMaxFusedAp];
+    const bool keep = a.apcount <= kMaxFusedAp;
+    const double *xc = xc_g, *yc = yc_g, *zc = zc_g;
+    if (stage) {
+        for (int q = threadIdx.x; q < g.sx; q += blockDim.x) s_coord[q] = xc_g[q];
+        for (int q = threadIdx.x; q < g.sy; q += blockDim.x) s_coord[g.sx + q] = yc_g[q];
+        for (int q = threadIdx.x; q < g.sz; q += blockDim.x) s_coord[g.sx + g.sy + q] = zc_g[q];
+        __syncthreads();
+        xc = s_coord; yc = s_coord + g.sx; zc = s_coord + g.sx + g.sy;
+    }
     const long long N = g.n;
     const int nappt = a.n_ap_per_blade * a.n_blade;
     const double dr = (a.radius - a.hub_radius) / a.n_ap_per_blade;
@@ -70,12 +84,14 @@ __global__ void __launch_bounds__(256) k_alm_force(Geom g, AlmDev a, const doubl
         rot(c1, nang, at, c0);
         for (int d = 0; d < 3; d++) c0[d] += a.base[3 * tid + d];
         for (int d = 0; d < 3; d++) a.ap_xyz[3 * ap + d] = c0[d];
+        if (keep) for (int d = 0; d < 3; d++) s_xyz[3 * ap + d] = c0[d];
         int I = find_index(xc, c0[0], g.sx), J = find_index(yc, c0[1], g.sy), K = find_index(zc, c0[2], g.sz);
         bool inside = I >= g.gc - 1 && I < g.sx - g.gc - 1 && J >= g.gc - 1 && J < g.sy - g.gc - 1 &&
                       K >= g.gc - 1 && K < g.sz - g.gc - 1;
         if (!inside) {
             for (int d = 0; d < 3; d++) a.ap_force[3 * ap + d] = 0;
             a.ap_torque[ap] = 0; a.ap_thrust[ap] = 0;
+            if (keep) { s_tq[ap] = 0; s_th[ap] = 0; }
             continue;
         }
         double xd = fabs(c0[0] - xc[I]) / fabs(xc[I + 1] - xc[I]);
@@ -124,19 +140,21 @@ __global__ void __launch_bounds__(256) k_alm_force(Geom g, AlmDev a, const doubl
         rot(ftt, nang, at, a.ap_force + 3 * ap);
         a.ap_torque[ap] = fabs(ft) * apr;
         a.ap_thrust[ap] = fx;
+        if (keep) { s_tq[ap] = fabs(ft) * apr; s_th[ap] = fx; }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
+        const double *pxyz = keep ? s_xyz : a.ap_xyz, *ptq = keep ? s_tq : a.ap_torque, *pth = keep ? s_th : a.ap_thrust;
         double bb[6] = {1e300, -1e300, 1e300, -1e300, 1e300, -1e300};
         for (int ap = 0; ap < a.apcount; ap++)
             for (int d = 0; d < 3; d++) {
-                bb[2 * d] = fmin(bb[2 * d], a.ap_xyz[3 * ap + d]);
-                bb[2 * d + 1] = fmax(bb[2 * d + 1], a.ap_xyz[3 * ap + d]);
+                bb[2 * d] = fmin(bb[2 * d], pxyz[3 * ap + d]);
+                bb[2 * d + 1] = fmax(bb[2 * d + 1], pxyz[3 * ap + d]);
             }
         for (int q = 0; q < 6; q++) a.scal->bbox[q] = bb[q];
         for (int tid = 0; tid < a.n_turbine && tid < kMaxTurbines; tid++) {
             double tq = 0, th = 0;
-            for (int q = 0; q < nappt; q++) { tq += a.ap_torque[tid * nappt + q]; th += a.ap_thrust[tid * nappt + q]; }
+            for (int q = 0; q < nappt; q++) { tq += ptq[tid * nappt + q]; th += pth[tid * nappt + q]; }
             a.scal->torque[tid] = tq;
             a.scal->thrust[tid] = th;
         }

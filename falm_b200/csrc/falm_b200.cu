@@ -552,7 +552,11 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
             CK(cudaStreamSynchronize(st));
         }
         // iteration itp of the pass: r equals rr until the first k_bicg_xr, and
-        // the first iteration's p equals r, so it reads rr in their place
+        // the first iteration's p equals r, so it reads rr in their place.
+        // Iterations are queued in batches of 1, 2, 4, 8, 8, ... between host
+        // checks of the convergence flag; every kernel of an iteration queued
+        // after convergence returns at once.
+        int batch = 1, queued = 0;
         for (int itp = 0;; itp++) {
             const T *rin = itp == 0 ? rr : r;
             T *pout = itp == 0 ? nullptr : p;
@@ -567,9 +571,12 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
             S7_OR(FALM_K_MV_DOT2, st, T, 2, ss, (MvDot2Body<T>{op, t, s, sc}),
                   (k_mv_dot2<T><<<grid, kRowThreads, 0, st>>>(g, R, op, ss, t, s, ctx->red, sc)));
             LAUNCH(FALM_K_BICG_XR, st, k_bicg_xr<T><<<grid_xr, kRowThreads, 0, st>>>(g, R, x, pp, ss, r, s, t, rr, ctx->red, sc));
+            if (++queued < batch) continue;
             CK(cudaMemcpyAsync(ctx->scal_host, sc, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             if (ctx->scal_host->done) break;
+            queued = 0;
+            batch = std::min(2 * batch, 8);
         }
         total_it += ctx->scal_host->it;
         if (ctx->scal_host->status == FALM_ERR_NAN) break;
@@ -653,7 +660,11 @@ int pseudo_u_t(falm_ctx *ctx, const T *un, const T *u, const T *uu, T *ua, const
 
 template <typename T>
 int alm_run_t(falm_ctx *ctx, const T *u, T *ff, double t, cudaStream_t st) {
-    LAUNCH(FALM_K_ALM, st, k_alm_force<T><<<1, 256, 0, st>>>(ctx->geo, ctx->alm, ctx->m64.x[0], ctx->m64.x[1], ctx->m64.x[2], u, t));
+    // stage the coordinate tables in shared memory when they fit in 96 KB
+    const int csm = (ctx->geo.sx + ctx->geo.sy + ctx->geo.sz) * (int)sizeof(double);
+    const int stage = csm <= 96 * 1024 ? 1 : 0;
+    if (stage && csm > 32 * 1024) cudaFuncSetAttribute(k_alm_force<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
+    LAUNCH(FALM_K_ALM, st, k_alm_force<T><<<1, 256, stage ? csm : 0, st>>>(ctx->geo, ctx->alm, ctx->m64.x[0], ctx->m64.x[1], ctx->m64.x[2], u, t, stage));
     if (ff) {
         const Region3 R = interior(ctx->geo);
         LAUNCH(FALM_K_ALM, st, k_alm_project<T><<<row_grid(ctx, R), kRowThreads, 0, st>>>(ctx->geo, R, mview<T>(ctx), ctx->alm, ff));
