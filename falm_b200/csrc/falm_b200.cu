@@ -523,34 +523,45 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
         return FALM_OK;
     };
     auto first_target = [&](T *z) -> T * { return (pct == FALM_LS_JACOBI && ((m - 1) & 1)) ? xp : z; };
+    // a pass's residual also gives the first iteration's first preconditioner
+    // sweep (pp_ready: the stream kernel stored it, so k_bicg_p is skipped)
+    bool pp_ready = false;
+    auto res_pass = [&](int check) -> int {
+        ResBody<T> body{op, b, nullptr, check ? nullptr : rr, sc, check};
+        if (!check) { body.pp = first_target(pp); body.pc_type = pct; body.pc_omega = pcw; }
+        const int s7 = s7_launch<T, 2>(ctx, FALM_K_RES, st, x, body);
+        if (s7 < 0) return -s7;
+        if (s7 == 0) LAUNCH(FALM_K_RES, st, (k_res<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, r, rr, ctx->red, sc, check)));
+        pp_ready = !check && s7 == 1;
+        return FALM_OK;
+    };
+    auto zero_it = [&]() -> int {
+        static const int zero = 0;
+        CK(cudaMemcpyAsync(&sc->it, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
+        return FALM_OK;
+    };
+    // In mixed precision each pass but the last is followed by a check of the
+    // true residual in FP64 (stop when it meets the tolerance; the check stores
+    // nothing). The check is queued behind the pass's iterations and runs only
+    // once the pass has stopped, so one host synchronisation serves both; where
+    // the stream kernel is not available it runs at the start of the next pass.
+    // A pass stores its residual in rr only: r equals rr until the pass's first
+    // k_bicg_xr, which writes r, and the iteration reads rr before.
+    bool explicit_check = false, pass_queued = false;
     for (outer = 0; outer < max_outer; outer++) {
-        // outer > 0: true residual in FP64; stop when it meets the tolerance
-        // (a check that stores nothing; a pass that follows recomputes it into
-        // rr). A pass stores its residual in rr only: r equals rr until the
-        // pass's first k_bicg_xr, which writes r, and the iteration reads rr before.
-        // a pass's residual also gives the first iteration's first preconditioner
-        // sweep (pp_ready: the stream kernel stored it, so k_bicg_p is skipped)
-        bool pp_ready = false;
-        auto res_pass = [&](int check) -> int {
-            ResBody<T> body{op, b, nullptr, check ? nullptr : rr, sc, check};
-            if (!check) { body.pp = first_target(pp); body.pc_type = pct; body.pc_omega = pcw; }
-            const int s7 = s7_launch<T, 2>(ctx, FALM_K_RES, st, x, body);
-            if (s7 < 0) return -s7;
-            if (s7 == 0) LAUNCH(FALM_K_RES, st, (k_res<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, r, rr, ctx->red, sc, check)));
-            pp_ready = !check && s7 == 1;
-            return FALM_OK;
-        };
-        if ((rc = res_pass(outer > 0 ? 1 : 0))) return rc;
-        if (outer > 0) {
+        if (outer > 0 && explicit_check) {
+            if ((rc = res_pass(1))) return rc;
             CK(cudaMemcpyAsync(ctx->scal_host, sc, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             if (ctx->scal_host->done) break;
-            if ((rc = res_pass(0))) return rc;
-            // restart the iteration count of this pass
-            int zero = 0;
-            CK(cudaMemcpyAsync(&sc->it, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
-            CK(cudaStreamSynchronize(st));
         }
+        if (!pass_queued) {
+            if ((rc = res_pass(0))) return rc;
+            if (outer > 0 && (rc = zero_it())) return rc;
+        }
+        pass_queued = false;
+        const bool want_check = mixed && outer + 1 < max_outer && !explicit_check;
+        bool checked = false;
         // iteration itp of the pass: r equals rr until the first k_bicg_xr, and
         // the first iteration's p equals r, so it reads rr in their place.
         // Iterations are queued in batches of 1, 2, 4, 8, 8, ... between host
@@ -572,14 +583,28 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
                   (k_mv_dot2<T><<<grid, kRowThreads, 0, st>>>(g, R, op, ss, t, s, ctx->red, sc)));
             LAUNCH(FALM_K_BICG_XR, st, k_bicg_xr<T><<<grid_xr, kRowThreads, 0, st>>>(g, R, x, pp, ss, r, s, t, rr, ctx->red, sc));
             if (++queued < batch) continue;
+            if (want_check && !explicit_check) {
+                ResBody<T> cb{op, b, nullptr, nullptr, sc, 1};
+                cb.queued_check = 1;
+                const int s7 = s7_launch<T, 2>(ctx, FALM_K_RES, st, x, cb);
+                if (s7 < 0) return -s7;
+                if (s7 == 0) explicit_check = true;
+            }
             CK(cudaMemcpyAsync(ctx->scal_host, sc, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
+            if (want_check && !explicit_check && ctx->scal_host->checked) { checked = true; break; }
             if (ctx->scal_host->done) break;
             queued = 0;
             batch = std::min(2 * batch, 8);
         }
         total_it += ctx->scal_host->it;
         if (ctx->scal_host->status == FALM_ERR_NAN) break;
+        if (checked) {
+            if (ctx->scal_host->done) break;   // the true residual meets the tolerance
+            if ((rc = res_pass(0))) return rc;
+            if ((rc = zero_it())) return rc;
+            pass_queued = true;
+        }
     }
     if (mixed && outer >= max_outer) {
         // report the true residual of the final iterate

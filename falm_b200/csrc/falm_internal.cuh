@@ -55,7 +55,8 @@ struct SolverScalars {
     int it, maxit, done, status;
     int first;          // 1 before the first BiCGStab iteration of a solve
     int kerr;           // bounded device-side wait gave up (FALM_ERR_TIMEOUT)
-    int pad[2];
+    int checked;        // the queued outer check of the true residual ran (mixed precision)
+    int pad;
 };
 
 struct AlmScalars {

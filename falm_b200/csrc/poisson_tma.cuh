@@ -313,7 +313,10 @@ struct ResBody {
     T *pp = nullptr;
     int pc_type = 0;
     T pc_omega = T(0);
-    __device__ bool skip() const { return false; }
+    // a check queued behind a pass's iterations: it runs only once the pass has
+    // stopped without a non-finite scalar, and records that it ran
+    int queued_check = 0;
+    __device__ bool skip() const { return queued_check && !(sc->done && sc->status != FALM_ERR_NAN && !sc->checked); }
     __device__ const T *pw() const { return b; }
     __device__ const Op7<T> &op_() const { return op; }
     __device__ void cell2(int i, int j, int k, long long c, const Coef7<double2> &a, double2 xc, double2 xe, double2 xw, double2 xn,
@@ -338,6 +341,7 @@ struct ResBody {
         sc->rrho = 1.0; sc->alpha = 0.0; sc->omega = 1.0; sc->beta = 0.0;
         sc->first = 1;
         sc->done = 0;
+        sc->checked = queued_check;
         if (!isfinite(err)) { sc->done = 1; sc->status = FALM_ERR_NAN; }
         else if (check_tol && err <= sc->tol) { sc->done = 1; sc->status = FALM_OK; }
         else if (fabs(tot[1]) < FLT_MIN) {
