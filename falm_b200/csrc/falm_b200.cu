@@ -527,9 +527,14 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
     // sweep (pp_ready: the stream kernel stored it, so k_bicg_p is skipped)
     bool pp_ready = false;
     auto res_pass = [&](int check) -> int {
-        ResBody<T> body{op, b, nullptr, check ? nullptr : rr, sc, check};
-        if (!check) { body.pp = first_target(pp); body.pc_type = pct; body.pc_omega = pcw; }
-        const int s7 = s7_launch<T, 2>(ctx, FALM_K_RES, st, x, body);
+        int s7;
+        if (check) {
+            s7 = s7_launch<T, 2>(ctx, FALM_K_RES, st, x, ResBody<T, true>{op, b, nullptr, nullptr, sc, 1});
+        } else {
+            ResBody<T> body{op, b, nullptr, rr, sc, 0};
+            body.pp = first_target(pp); body.pc_type = pct; body.pc_omega = pcw;
+            s7 = s7_launch<T, 2>(ctx, FALM_K_RES, st, x, body);
+        }
         if (s7 < 0) return -s7;
         if (s7 == 0) LAUNCH(FALM_K_RES, st, (k_res<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, r, rr, ctx->red, sc, check)));
         pp_ready = !check && s7 == 1;
@@ -584,7 +589,7 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
             LAUNCH(FALM_K_BICG_XR, st, k_bicg_xr<T><<<grid_xr, kRowThreads, 0, st>>>(g, R, x, pp, ss, r, s, t, rr, ctx->red, sc));
             if (++queued < batch) continue;
             if (want_check && !explicit_check) {
-                ResBody<T> cb{op, b, nullptr, nullptr, sc, 1};
+                ResBody<T, true> cb{op, b, nullptr, nullptr, sc, 1};
                 cb.queued_check = 1;
                 const int s7 = s7_launch<T, 2>(ctx, FALM_K_RES, st, x, cb);
                 if (s7 < 0) return -s7;

@@ -31,9 +31,10 @@ template <> struct S7Conf<double> { static constexpr int NS = 6; };
 template <> struct S7Conf<float> { static constexpr int NS = 8; };
 
 // resident CTAs per SM asked of the register allocator: 3 for FP32 arithmetic
-// on an FP32 field (at most 85 registers), 2 where the body works in FP64
+// on an FP32 field (at most 85 registers) and for the store-free FP64 residual
+// check, 2 where the body works in FP64 and stores
 template <typename T, class Body>
-constexpr int s7_minb() { return (sizeof(T) == 4 && sizeof(typename Body::V) == 4) ? 3 : 2; }
+constexpr int s7_minb() { return (sizeof(T) == 4 && (sizeof(typename Body::V) == 4 || Body::kLean)) ? 3 : 2; }
 
 template <typename T>
 constexpr int s7_smem() { return S7Conf<T>::NS * S7Tile<T>::SLOT + 128 + 128; }
@@ -210,6 +211,7 @@ reduce:
 template <typename T>
 struct SorBody {
     using V = T;
+    static constexpr bool kLean = false;
     Op7<T> op;
     T *x;
     const T *b;
@@ -234,6 +236,7 @@ struct SorBody {
 template <typename T>
 struct MvBody {
     using V = T;
+    static constexpr bool kLean = false;
     Op7<T> op;
     T *ax;
     __device__ bool skip() const { return false; }
@@ -250,6 +253,7 @@ struct MvBody {
 template <typename T>
 struct MvDot1Body {
     using V = T;
+    static constexpr bool kLean = false;
     Op7<T> op;
     T *q;
     const T *rr;
@@ -275,6 +279,7 @@ struct MvDot1Body {
 template <typename T>
 struct MvDot2Body {
     using V = T;
+    static constexpr bool kLean = false;
     Op7<T> op;
     T *t;
     const T *s;
@@ -301,10 +306,12 @@ struct MvDot2Body {
 
 // r = b - A x (FP64 arithmetic), rr = r, solver start (see k_res); with pp,
 // also the pointwise first preconditioner sweep from zero of the new r (what
-// k_bicg_p computes in a pass's first iteration, where p = r)
-template <typename T>
+// k_bicg_p computes in a pass's first iteration, where p = r).  CHECK: the
+// outer check of the true residual, which stores nothing.
+template <typename T, bool CHECK = false>
 struct ResBody {
     using V = double;
+    static constexpr bool kLean = CHECK;
     Op7<T> op;
     const T *b;
     T *r, *rr;
@@ -324,9 +331,9 @@ struct ResBody {
         const double2 ax = dot7p(a.ac, a.ae, a.aw, a.an, a.as, a.at, a.ab, xc, xe, xw, xn, xs, xt, xb);
         const double r0 = to_d(bv.x) - ax.x, r1 = to_d(bv.y) - ax.y;
         const P2<T> rt = mk2((T)r0, (T)r1);
-        if (r) st2(r + c, rt);
-        if (rr) st2(rr + c, rt);
-        if (pp) st2(pp + c, mk2(pc_first<T>(pc_type, i, j, k, rt.x, (T)a.ac.x, pc_omega),
+        if (!CHECK && r) st2(r + c, rt);
+        if (!CHECK && rr) st2(rr + c, rt);
+        if (!CHECK && pp) st2(pp + c, mk2(pc_first<T>(pc_type, i, j, k, rt.x, (T)a.ac.x, pc_omega),
                                 pc_first<T>(pc_type, i + 1, j, k, rt.y, (T)a.ac.y, pc_omega)));
         acc[0] += r0 * r0;
         acc[0] += r1 * r1;
