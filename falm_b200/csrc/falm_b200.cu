@@ -529,7 +529,7 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
     auto res_pass = [&](int check) -> int {
         int s7;
         if (check) {
-            s7 = s7_launch<T, 2>(ctx, FALM_K_RES, st, x, ResBody<T, true>{op, b, nullptr, nullptr, sc, 1});
+            s7 = s7_launch<T, 1>(ctx, FALM_K_RES, st, x, ResBody<T, true>{op, b, nullptr, nullptr, sc, 1});
         } else {
             ResBody<T> body{op, b, nullptr, rr, sc, 0};
             body.pp = first_target(pp); body.pc_type = pct; body.pc_omega = pcw;
@@ -591,7 +591,7 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
             if (want_check && !explicit_check) {
                 ResBody<T, true> cb{op, b, nullptr, nullptr, sc, 1};
                 cb.queued_check = 1;
-                const int s7 = s7_launch<T, 2>(ctx, FALM_K_RES, st, x, cb);
+                const int s7 = s7_launch<T, 1>(ctx, FALM_K_RES, st, x, cb);
                 if (s7 < 0) return -s7;
                 if (s7 == 0) explicit_check = true;
             }

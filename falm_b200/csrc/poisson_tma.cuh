@@ -326,8 +326,9 @@ struct ResBody {
     __device__ bool skip() const { return queued_check && !(sc->done && sc->status != FALM_ERR_NAN && !sc->checked); }
     __device__ const T *pw() const { return b; }
     __device__ const Op7<T> &op_() const { return op; }
+    static constexpr int NV = CHECK ? 1 : 2;   // the check reduces only the norm
     __device__ void cell2(int i, int j, int k, long long c, const Coef7<double2> &a, double2 xc, double2 xe, double2 xw, double2 xn,
-                          double2 xs, double2 xt, double2 xb, P2<T> bv, double (&acc)[2]) const {
+                          double2 xs, double2 xt, double2 xb, P2<T> bv, double (&acc)[NV]) const {
         const double2 ax = dot7p(a.ac, a.ae, a.aw, a.an, a.as, a.at, a.ab, xc, xe, xw, xn, xs, xt, xb);
         const double r0 = to_d(bv.x) - ax.x, r1 = to_d(bv.y) - ax.y;
         const P2<T> rt = mk2((T)r0, (T)r1);
@@ -337,22 +338,27 @@ struct ResBody {
                                 pc_first<T>(pc_type, i + 1, j, k, rt.y, (T)a.ac.y, pc_omega)));
         acc[0] += r0 * r0;
         acc[0] += r1 * r1;
-        acc[1] += to_d(rt.x) * to_d(rt.x);
-        acc[1] += to_d(rt.y) * to_d(rt.y);
+        if constexpr (!CHECK) {
+            acc[NV - 1] += to_d(rt.x) * to_d(rt.x);
+            acc[NV - 1] += to_d(rt.y) * to_d(rt.y);
+        }
     }
-    __device__ void finish(const double (&tot)[2]) const {
+    __device__ void finish(const double (&tot)[NV]) const {
         if (!sc) return;
         double err = sqrt(tot[0]) / sc->gsize;
         sc->err = err;
-        sc->rho = tot[1];
+        // a check that passes ends the solve; one that fails is followed by a
+        // pass residual, which sets the iteration's scalars
+        const double rho = tot[NV - 1];
+        sc->rho = rho;
         sc->rrho = 1.0; sc->alpha = 0.0; sc->omega = 1.0; sc->beta = 0.0;
         sc->first = 1;
         sc->done = 0;
         sc->checked = queued_check;
         if (!isfinite(err)) { sc->done = 1; sc->status = FALM_ERR_NAN; }
         else if (check_tol && err <= sc->tol) { sc->done = 1; sc->status = FALM_OK; }
-        else if (fabs(tot[1]) < FLT_MIN) {
-            sc->err = tot[1];
+        else if (!CHECK && fabs(rho) < FLT_MIN) {
+            sc->err = rho;
             sc->done = 1;
             sc->status = (err <= sc->tol) ? FALM_OK : FALM_ERR_BREAKDOWN;
         }
