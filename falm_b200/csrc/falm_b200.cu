@@ -467,8 +467,21 @@ int build_poisson(falm_ctx *ctx, int kind) {
 }
 
 // ---------------------------------------------------------------- solver driver
+// solver scalars at the start of a solve
+int solver_init(falm_ctx *ctx, cudaStream_t st) {
+    const Geom &g = ctx->geo;
+    SolverScalars init;
+    memset(&init, 0, sizeof(init));
+    init.gsize = (double)g.nx * g.ny * g.nz;
+    init.tol = ctx->tol;
+    init.maxit = ctx->maxit;
+    CK(cudaMemcpyAsync(ctx->scal, &init, sizeof(init), cudaMemcpyHostToDevice, st));
+    return FALM_OK;
+}
+
 template <typename T>
-int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out, double *err_out, int *outer_out) {
+int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out, double *err_out, int *outer_out,
+            bool first_res_done = false) {
     int rc = ensure_work(ctx);
     if (rc) return rc;
     if (!ctx->op_ready && !ctx->A_explicit) return fail(ctx, FALM_ERR_STATE, "solve: no operator (call falm_eq_poisson_operator or falm_eq_set_matrix)");
@@ -481,12 +494,10 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
     const Op7<T> op = op7<T>(ctx);
     T *rr = (T *)ctx->w_rr, *p = (T *)ctx->w_p, *q = (T *)ctx->w_q, *s = (T *)ctx->w_s, *pp = (T *)ctx->w_pp;
     T *ss = (T *)ctx->w_ss, *t = (T *)ctx->w_t, *xp = (T *)ctx->w_xp;
-    SolverScalars init;
-    memset(&init, 0, sizeof(init));
-    init.gsize = (double)g.nx * g.ny * g.nz;
-    init.tol = ctx->tol;
-    init.maxit = ctx->maxit;
-    CK(cudaMemcpyAsync(ctx->scal, &init, sizeof(init), cudaMemcpyHostToDevice, st));
+    // first_res_done: the caller initialised the scalars (solver_init) and a
+    // kernel of its own already computed the first pass's residual into rr with
+    // the first preconditioner sweep into pp (the step's face-velocity kernel)
+    if (!first_res_done && (rc = solver_init(ctx, st))) return rc;
     const T pcw = (T)ctx->pc_relax;
     const int pct = ctx->pc_type, m = ctx->pc_maxit;
     SolverScalars *sc = ctx->scal;
@@ -525,7 +536,7 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
     auto first_target = [&](T *z) -> T * { return (pct == FALM_LS_JACOBI && ((m - 1) & 1)) ? xp : z; };
     // a pass's residual also gives the first iteration's first preconditioner
     // sweep (pp_ready: the stream kernel stored it, so k_bicg_p is skipped)
-    bool pp_ready = false;
+    bool pp_ready = first_res_done;
     auto res_pass = [&](int check) -> int {
         int s7;
         if (check) {
@@ -552,7 +563,7 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
     // the stream kernel is not available it runs at the start of the next pass.
     // A pass stores its residual in rr only: r equals rr until the pass's first
     // k_bicg_xr, which writes r, and the iteration reads rr before.
-    bool explicit_check = false, pass_queued = false;
+    bool explicit_check = false, pass_queued = first_res_done;
     for (outer = 0; outer < max_outer; outer++) {
         if (outer > 0 && explicit_check) {
             if ((rc = res_pass(1))) return rc;
@@ -726,6 +737,7 @@ int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_
     T *u = (T *)f->u, *uu = (T *)f->uu, *p = (T *)f->p, *nut = (T *)f->nut, *ff = (T *)f->ff;
     T *ua = (T *)ctx->w_ua, *rhs = (T *)ctx->w_rhs, *r = (T *)ctx->w_r;
     const bool chan = ctx->bc_kind == FALM_BC_CHANNEL;
+    bool fused_res = false;
     // 1. ALM (src/alm/alm.h:66-77) at the previous velocity
     if (ctx->alm_on) {
         if ((rc = alm_run_t<T>(ctx, u, ff, t, st))) return rc;
@@ -738,17 +750,39 @@ int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_
         T scale = (T)(1.0 / (dt * ctx->maxdiag));
         // the guide layer of ua takes the previous velocity (the reference's aliased u)
         LAUNCH(FALM_K_OTHER, st, k_copy_shell<T><<<ctx->sm_count * 8, 256, 0, st>>>(g, u, ua));
-        if (chan)
-            P3_OR(FALM_K_UTOUU_RHS, st, T, 1, 0, R, 1, FB_ARR(ua), FB_ARR(3), (UtoUUBody<T, true, false>{g, mview<T>(ctx), uu, rhs, scale}),
-                  (k_utouu<T, true, false><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), ua, u, uu, rhs, scale)));
-        else
-            P3_OR(FALM_K_UTOUU_RHS, st, T, 1, 0, R, 1, FB_ARR(ua), FB_ARR(3), (UtoUUBody<T, true, true>{g, mview<T>(ctx), uu, rhs, scale}),
-                  (k_utouu<T, true, true><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), ua, u, uu, rhs, scale)));
+        // the plane stream also computes the solve's first residual (rr) and
+        // first preconditioner sweep (pp) from the pressure p, the initial guess
+        fused_res = false;
+        if (!ctx->A_explicit && (ctx->pc_type == FALM_LS_SOR || ctx->pc_type == FALM_LS_JACOBI)) {
+            if ((rc = ensure_work(ctx)) || (rc = solver_init(ctx, st))) return rc;
+            T *ppt = (ctx->pc_type == FALM_LS_JACOBI && ((ctx->pc_maxit - 1) & 1)) ? (T *)ctx->w_xp : (T *)ctx->w_pp;
+            const void *const fp[2] = {ua, p};
+            const int nc[2] = {3, 1};
+            int s3;
+            if (chan)
+                s3 = p3_launch<T, 2, 2>(ctx, FALM_K_UTOUU_RHS, st, R, 1, fp, nc,
+                                        UtoUUResBody<T, false>{UtoUUBody<T, true, false>{g, mview<T>(ctx), uu, rhs, scale}, mview<T>(ctx),
+                                                               op7<T>(ctx), (T *)ctx->w_rr, ppt, ctx->pc_type, (T)ctx->pc_relax, ctx->scal});
+            else
+                s3 = p3_launch<T, 2, 2>(ctx, FALM_K_UTOUU_RHS, st, R, 1, fp, nc,
+                                        UtoUUResBody<T, true>{UtoUUBody<T, true, true>{g, mview<T>(ctx), uu, rhs, scale}, mview<T>(ctx),
+                                                              op7<T>(ctx), (T *)ctx->w_rr, ppt, ctx->pc_type, (T)ctx->pc_relax, ctx->scal});
+            if (s3 < 0) return -s3;
+            fused_res = s3 == 1;
+        }
+        if (!fused_res) {
+            if (chan)
+                P3_OR(FALM_K_UTOUU_RHS, st, T, 1, 0, R, 1, FB_ARR(ua), FB_ARR(3), (UtoUUBody<T, true, false>{g, mview<T>(ctx), uu, rhs, scale}),
+                      (k_utouu<T, true, false><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), ua, u, uu, rhs, scale)));
+            else
+                P3_OR(FALM_K_UTOUU_RHS, st, T, 1, 0, R, 1, FB_ARR(ua), FB_ARR(3), (UtoUUBody<T, true, true>{g, mview<T>(ctx), uu, rhs, scale}),
+                      (k_utouu<T, true, true><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), ua, u, uu, rhs, scale)));
+        }
     }
     // 4. Poisson
     int it = 0, outer = 1;
     double err = 0;
-    rc = solve_t<T>(ctx, p, rhs, r, st, &it, &err, &outer);
+    rc = solve_t<T>(ctx, p, rhs, r, st, &it, &err, &outer, fused_res);
     int solve_status = ctx->scal_host->status;
     if (rc) return rc;
     // 5. pbc

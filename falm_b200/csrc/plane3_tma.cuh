@@ -11,7 +11,9 @@
 //   face-map kernels: tile i0 = gc - 1 + 32 bx, box x = i0 - 1  (org 1)
 // (both start at 32 bx for gc = 2).
 #pragma once
+#include <type_traits>
 #include "common.cuh"
+#include "poisson.cuh"
 #include "tma.cuh"
 
 namespace fb {
@@ -57,6 +59,14 @@ struct ColMet {
 // pointwise operands (or per-column / per-plane state) of a body that has none
 struct NoPW {};
 
+// resident CTAs per SM asked of the register allocator: 4 in FP32 (at most 64
+// registers), 2 in FP64, or the body's own kMinBlocks
+template <typename T, class Body, class = void> struct P3MinB { static constexpr int v = sizeof(T) == 4 ? 4 : 2; };
+template <typename T, class Body> struct P3MinB<T, Body, std::void_t<decltype(Body::kMinBlocks)>> {
+    static constexpr int v = sizeof(T) == 4 ? Body::kMinBlocks : 2;
+};
+template <typename T, class Body> constexpr int p3_minb() { return P3MinB<T, Body>::v; }
+
 // Body: bool skip() const; MetricView<T> mv; type PW (the cell's pointwise
 //       operands) and PW pw_load(i, j, k, cc) const; types CS, ZS (state of a
 //       column and of a plane) with CS col_state(i, j) const, ZS plane_state(k)
@@ -66,7 +76,7 @@ struct NoPW {};
 // The pointwise operands of a plane are loaded before the wait for the plane
 // ahead, for every row of the thread, so their latency overlaps the wait.
 template <typename T, int NF, int NS, int NV, class Body>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_plane3_tma(Geom g, Region3 R, int org, int kc, const __grid_constant__ MapSet<NF> maps,
+__global__ void __launch_bounds__(256, (p3_minb<T, Body>())) k_plane3_tma(Geom g, Region3 R, int org, int kc, const __grid_constant__ MapSet<NF> maps,
                                                   Body body, RedWork rw, int *err) {
     using L = P3Layout<T, NF>;
     extern __shared__ unsigned char smem_raw[];
@@ -317,6 +327,81 @@ struct ProjectBody {
         if (in) { u[cc] = a0 - dt * gx; u[cc + N] = a1 - dt * gy; u[cc + 2 * N] = a2 - dt * gz; }
     }
     __device__ void finish(const double (&)[1]) const {}
+};
+
+// ---------------------------------------------------------------- face velocity + RHS + first residual
+// UtoUUBody (RHS) fused with the residual that starts the Poisson solve (the
+// pass residual of ResBody): r = rhs - A p in FP64 at interior cells, stored
+// to rr with the first preconditioner sweep into pp, and the norms reduced
+// into the solver scalars.  Fields: 0 the velocity to interpolate (3 comps),
+// 1 the pressure (the solve's initial guess).
+template <typename T, bool CAVITY>
+struct UtoUUResBody {
+    UtoUUBody<T, true, CAVITY> uub;
+    MetricView<T> mv;
+    Op7<T> op;
+    T *rr, *pp;
+    int pc_type;
+    T pc_omega;
+    SolverScalars *sc;
+    static constexpr int NC0 = 3, NC1 = 1;
+    static constexpr int kMinBlocks = 2;   // FP32: at most 128 registers (fewer spills than 3 CTAs per SM)
+    using PW = NoPW;
+    using CS = typename Op7<T>::Col;
+    using ZS = typename Op7<T>::ZPl;
+    __device__ bool skip() const { return false; }
+    __device__ PW pw_load(int, int, int, long long) const { return PW{}; }
+    __device__ CS col_state(int i, int j) const { return op.column(i, j); }
+    __device__ ZS plane_state(int k) const { return op.zplane(k); }
+    __device__ void cell(int i, int j, int k, long long c, const P3View<T, 2> &v, const ColMet<T> &cm, const PW &, const CS &cs,
+                         const ZS &zs, double (&acc)[2]) const {
+        const Geom &g = uub.g;
+        // the face velocity and, at interior cells, the RHS (UtoUUBody's expressions)
+        P3View<T, 1> v1;
+        v1.pl[0] = v.pl[0]; v1.pl[1] = v.pl[1]; v1.pl[2] = v.pl[2];
+        v1.foff[0] = v.foff[0];
+        v1.o = v.o;
+        const T UE = uub.face(v1, cm, 0, i, j, k, 0, 0, 0), VN = uub.face(v1, cm, 1, i, j, k, 0, 0, 0), WT = uub.face(v1, cm, 2, i, j, k, 0, 0, 0);
+        uub.uu[c] = UE; uub.uu[c + g.n] = VN; uub.uu[c + 2 * g.n] = WT;
+        if (i >= g.gc && j >= g.gc && k >= g.gc) {
+            const T UW = uub.face(v1, cm, 0, i, j, k, -1, 0, 0), VS = uub.face(v1, cm, 1, i, j, k, 0, -1, 0),
+                    WB = uub.face(v1, cm, 2, i, j, k, 0, 0, -1);
+            const T div = (UE - UW + VN - VS + WT - WB) * ((cm.kx[1] * cm.ky[1]) * cm.kz[1]);
+            const T bv = div * uub.scale;
+            uub.rhs[c] = bv;
+            // r = b - A p in FP64, the 7-point products accumulated in ResBody's order
+            const T ac = op.ac_col(cs, zs);
+            double ax = (double)ac * (double)v.at(1, 0, 0);
+            ax = fma((double)cs.ae, (double)v.at(1, 0, 0, 1, 0), ax);
+            ax = fma((double)cs.aw, (double)v.at(1, 0, 0, -1, 0), ax);
+            ax = fma((double)cs.an, (double)v.at(1, 0, 0, 0, 1), ax);
+            ax = fma((double)cs.as, (double)v.at(1, 0, 0, 0, -1), ax);
+            ax = fma((double)zs.at, (double)v.at(1, 0, 1), ax);
+            ax = fma((double)zs.ab, (double)v.at(1, 0, -1), ax);
+            const double rv = (double)bv - ax;
+            const T rt = (T)rv;
+            rr[c] = rt;
+            pp[c] = pc_first<T>(pc_type, i, j, k, rt, ac, pc_omega);
+            acc[0] += rv * rv;
+            acc[1] += (double)rt * (double)rt;
+        }
+    }
+    __device__ void finish(const double (&tot)[2]) const {
+        // ResBody::finish of a pass residual
+        const double err = sqrt(tot[0]) / sc->gsize;
+        sc->err = err;
+        sc->rho = tot[1];
+        sc->rrho = 1.0; sc->alpha = 0.0; sc->omega = 1.0; sc->beta = 0.0;
+        sc->first = 1;
+        sc->done = 0;
+        sc->checked = 0;
+        if (!isfinite(err)) { sc->done = 1; sc->status = FALM_ERR_NAN; }
+        else if (fabs(tot[1]) < FLT_MIN) {
+            sc->err = tot[1];
+            sc->done = 1;
+            sc->status = (err <= sc->tol) ? FALM_OK : FALM_ERR_BREAKDOWN;
+        }
+    }
 };
 
 // ---------------------------------------------------------------- SGS + divergence body
