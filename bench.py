@@ -163,8 +163,8 @@ def step_bytes(S, n, it, m=2):
 # each operand once): used for the per-kernel achieved bandwidth
 KERNEL_VALUES = {
     "pseudo_u": 10,     # u(3) uu(3) nut(1) in, ua(3) out (ALM force evaluated in-kernel)
-    "utouu_rhs": 7,     # ua(3) in, uu(3) rhs(1) out
-    "res": 3,           # pass residual: x b in, rr pp out (4); outer check: x b in (2); mean of the two launches
+    "utouu_rhs": 10,    # ua(3) p(1) in, uu(3) rhs(1) rr(1) pp(1) out (the solve's first residual fused in)
+    "res": 2,           # the mixed-precision outer check: x b in (a pass residual after a failed check: 4)
     "bicg_p": 5,        # r p q in, p pp out (from a pass's second iteration on)
     "sor": 3,           # x b in, x out (three red-black half sweeps per launch, one HBM pass)
     "mv_dot1": 3,       # pp rr in, q out

@@ -71,6 +71,43 @@ def test_step_fp64_fixed_iterations(oracle, lib_built, name):
             assert x == pytest.approx(y, rel=1e-10)
 
 
+def oracle_spread(oracle, case, steps, eps=1e-15, seed=1):
+    """How far the oracle's own fields move when its initial velocity is scaled
+    by (1 + eps * N(0, 1)) cell by cell: the rounding sensitivity of the
+    fixed-iteration step map for this case."""
+    from oracle.oracle import CaseStruct
+    cs = CaseStruct(case, maxit=6, tol=0.0)
+    m = oracle.setup(cs)
+    st = cases.initial_state(case)
+    st["u"] = st["u"] * (1 + eps * np.random.default_rng(seed).standard_normal(st["u"].shape))
+    oracle.init_state(cs, m, st)
+    for it in range(steps):
+        oracle.step(cs, st, m, (it + 1) * case.dt)
+    return st
+
+
+@pytest.mark.parametrize("pc_maxit", [2, 3, 4])
+def test_step_fp64_fixed_iterations_jacobi(oracle, lib_built, pc_maxit):
+    """Jacobi preconditioning through the step: the face-velocity kernel's fused
+    first residual writes the first sweep into the buffer from which the sweeps
+    ping-pong to pp (xp for an even sweep count, pp for an odd one).
+
+    With 3 sweeps this case's BiCGStab runs close to a breakdown: a 1e-15
+    relative perturbation of the oracle's own input moves its pressure by about
+    6e-8 (against 2e-15 at 2 or 4 sweeps). There the bound is that measured
+    spread of the oracle itself, otherwise 1e-10."""
+    case = small_cases()["wide"]
+    case.pc, case.pc_maxit = "Jacobi", pc_maxit
+    ref, rs = run_oracle(oracle, case, 5, maxit=6, tol=0.0)
+    got, gs, _ = run_gpu(case, 5, maxit=6, tol=0.0)
+    err = compare(case, got, ref)
+    spread = compare(case, oracle_spread(oracle, case, 5), ref)
+    for k, v in err.items():
+        assert v < max(1e-10, spread[k]), (k, v, err, spread)
+    for a, b in zip(gs, rs):
+        assert a["it"] == b["it"]
+
+
 @pytest.mark.parametrize("name", ["channel", "cavity"])
 def test_step_fp64_converged(oracle, lib_built, name):
     case = small_cases()[name]
