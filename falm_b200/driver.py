@@ -36,6 +36,17 @@ class Simulation:
         self.it += 1
         return self.ctx.step(self.u, self.uu, self.p, self.nut, self.ff, self.case.dt, self.t())
 
+    def snapshot(self):
+        """keep a device copy of the state (fields and step counter) for restore()"""
+        self._snap = ({k: getattr(self, k).clone() for k in ("u", "uu", "p", "nut")}, self.it)
+
+    def restore(self):
+        """return to the last snapshot (device-to-device copies on the current stream)"""
+        fields, it = self._snap
+        for k, v in fields.items():
+            getattr(self, k).copy_(v)
+        self.it = it
+
     def inlet_plane(self, it):
         """inlet velocity of step `it` sampled from the case's inflow box (as the
         library samples it): 3 x nz x ny, float64"""

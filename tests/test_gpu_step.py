@@ -157,6 +157,42 @@ def test_step_cavity_mixed(oracle, lib_built):
     assert err["u"] < 2e-4, err
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_streamed_inlet_planes_match_inflow_box(lib_built, precision):
+    """falm_bc_set_inlet_plane: run b takes, as a pinned host plane copied before
+    each step, the inlet plane that run a's step sampled from the inflow box on
+    the device (read back from a's inlet ghost layer), and makes the same steps
+    bit for bit. A plane set twice before a step is replaced by the second call;
+    a step without a plane samples the box again."""
+    import torch
+    from falm_b200.driver import Simulation
+    case = small_cases()["channel"]
+    g = case.grid
+    sx, sy, sz, gc = g.sx, g.sy, g.sz, g.gc
+    a, b = Simulation(case, precision), Simulation(case, precision)
+
+    def inlet(sim):
+        u = host(sim.u).reshape(3, sz, sy, sx)
+        return np.ascontiguousarray(u[:, gc:sz - gc, gc:sy - gc, gc - 1])
+
+    keep = []
+    for q in range(5):
+        sa = a.step()
+        plane = torch.from_numpy(inlet(a)).pin_memory()
+        keep.append(plane)
+        if q == 2:
+            wrong = torch.zeros_like(plane).pin_memory()
+            keep.append(wrong)
+            b.ctx.set_inlet_plane(wrong)
+        b.ctx.set_inlet_plane(plane)
+        sb = b.step()
+        assert sa["it"] == sb["it"]
+        for x, y in ((a.u, b.u), (a.p, b.p), (a.uu, b.uu), (a.nut, b.nut)):
+            assert np.array_equal(host(x), host(y)), q
+    a.step(), b.step()
+    assert np.array_equal(host(a.u), host(b.u))
+
+
 def test_step_launch_count_and_statuses(lib_built):
     case = small_cases()["channel"]
     got, gs, ctx = run_gpu(case, 2)
