@@ -479,13 +479,68 @@ int solver_init(falm_ctx *ctx, cudaStream_t st) {
     return FALM_OK;
 }
 
+// The plain solvers of FalmEq::Solve (src/FalmEq.h:56-64): Jacobi
+// (src/FalmEq.cpp:80-127) and red-black SOR (:173-240, the Black half sweep then
+// the Red one, with the solver's relaxation factor).  Each iteration ends with
+// the residual r = b - A x and the loop test (k_res_plain).  Iterations are
+// queued in batches of 1, 2, 4, 8, 8, ... between host checks of the stop
+// flag, and every kernel of an iteration queued after the stop returns at once.
+// Jacobi alternates between x and the work vector xp instead of copying x to
+// xp each iteration: after one copy of x (ghosts included) the ghost cells of
+// both agree, iteration n reads {x, xp}[n % 2] and writes the other, and an odd
+// final count copies the result back into x.
+template <typename T>
+int plain_solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out, double *err_out, int *outer_out) {
+    int rc = solver_init(ctx, st);
+    if (rc) return rc;
+    const Geom &g = ctx->geo;
+    const Region3 R = interior(g);
+    const int grid = row_grid(ctx, R);
+    const Op7<T> op = op7<T>(ctx);
+    SolverScalars *sc = ctx->scal;
+    T *xp = (T *)ctx->w_xp;
+    const bool jac = ctx->ls_type == FALM_LS_JACOBI;
+    const T w = (T)ctx->relax;
+    if (jac) CK(cudaMemcpyAsync(xp, x, (size_t)g.n * sizeof(T), cudaMemcpyDeviceToDevice, st));
+    int batch = 1, queued = 0;
+    for (int n = 0;; n++) {
+        T *dst = x;
+        if (jac) {
+            const T *src = (n & 1) ? xp : x;
+            dst = (n & 1) ? x : xp;
+            LAUNCH(FALM_K_SOR, st, k_jacobi<T><<<grid, kRowThreads, 0, st>>>(g, R, op, dst, src, b, sc));
+        } else {
+            for (int color = 0; color < 2; color++)
+                S7_OR(FALM_K_SOR, st, T, 0, x, (SorBody<T>{op, x, b, w, color, sc}),
+                      (k_sor<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, w, color, sc)));
+        }
+        LAUNCH(FALM_K_RES, st, k_res_plain<T><<<grid, kRowThreads, 0, st>>>(g, R, op, dst, b, r, ctx->red, sc));
+        if (++queued < batch) continue;
+        CK(cudaMemcpyAsync(ctx->scal_host, sc, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (ctx->scal_host->done) break;
+        queued = 0;
+        batch = std::min(2 * batch, 8);
+    }
+    const int it = ctx->scal_host->it;
+    if (jac && (it & 1)) CK(cudaMemcpyAsync(x, xp, (size_t)g.n * sizeof(T), cudaMemcpyDeviceToDevice, st));
+    if (it_out) *it_out = it;
+    if (err_out) *err_out = ctx->scal_host->err;
+    if (outer_out) *outer_out = 1;
+    return ctx->scal_host->status == FALM_ERR_NAN ? fail(ctx, FALM_ERR_NAN, "solve: non-finite residual") : FALM_OK;
+}
+
 template <typename T>
 int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out, double *err_out, int *outer_out,
             bool first_res_done = false) {
     int rc = ensure_work(ctx);
     if (rc) return rc;
     if (!ctx->op_ready && !ctx->A_explicit) return fail(ctx, FALM_ERR_STATE, "solve: no operator (call falm_eq_poisson_operator or falm_eq_set_matrix)");
-    if (ctx->ls_type != FALM_LS_PBICGSTAB) return fail(ctx, FALM_ERR_ARG, "solve: only PBiCGStab is implemented");
+    if (ctx->ls_type == FALM_LS_JACOBI || ctx->ls_type == FALM_LS_SOR) {
+        if (first_res_done) return fail(ctx, FALM_ERR_STATE, "solve: a BiCGStab start was prepared for a plain solver");
+        return plain_solve_t<T>(ctx, x, b, r, st, it_out, err_out, outer_out);
+    }
+    if (ctx->ls_type != FALM_LS_PBICGSTAB) return fail(ctx, FALM_ERR_ARG, "solve: unknown linear solver type");
     const Geom &g = ctx->geo;
     const Region3 R = interior(g);
     const int grid = row_grid(ctx, R);
@@ -753,7 +808,7 @@ int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_
         // the plane stream also computes the solve's first residual (rr) and
         // first preconditioner sweep (pp) from the pressure p, the initial guess
         fused_res = false;
-        if (!ctx->A_explicit && (ctx->pc_type == FALM_LS_SOR || ctx->pc_type == FALM_LS_JACOBI)) {
+        if (!ctx->A_explicit && ctx->ls_type == FALM_LS_PBICGSTAB && (ctx->pc_type == FALM_LS_SOR || ctx->pc_type == FALM_LS_JACOBI)) {
             if ((rc = ensure_work(ctx)) || (rc = solver_init(ctx, st))) return rc;
             T *ppt = (ctx->pc_type == FALM_LS_JACOBI && ((ctx->pc_maxit - 1) & 1)) ? (T *)ctx->w_xp : (T *)ctx->w_pp;
             const void *const fp[2] = {ua, p};
@@ -1042,7 +1097,8 @@ int falm_cfd_sgs(falm_ctx *ctx, const void *u, void *nut, void *stream) {
 // ---------------------------------------------------------------- FalmEq
 int falm_eq_init(falm_ctx *ctx, int type, int maxit, double tol, double relax, int pc_type, int pc_maxit, double pc_relax) {
     if (!ctx || maxit < 1 || pc_maxit < 1 || !(tol >= 0)) return FALM_ERR_ARG;
-    if (type != FALM_LS_PBICGSTAB) return fail(ctx, FALM_ERR_ARG, "eq_init: only PBiCGStab (4) is implemented");
+    if (type != FALM_LS_PBICGSTAB && type != FALM_LS_SOR && type != FALM_LS_JACOBI)
+        return fail(ctx, FALM_ERR_ARG, "eq_init: solver must be Jacobi (1), SOR (2) or PBiCGStab (4)");
     if (pc_type != FALM_LS_SOR && pc_type != FALM_LS_JACOBI) return fail(ctx, FALM_ERR_ARG, "eq_init: preconditioner must be SOR (2) or Jacobi (1)");
     ctx->ls_type = type; ctx->maxit = maxit; ctx->tol = tol; ctx->relax = relax;
     ctx->pc_type = pc_type; ctx->pc_maxit = pc_maxit; ctx->pc_relax = pc_relax;
@@ -1611,6 +1667,8 @@ extern "C" int falm_step_adjoint(falm_ctx *ctx, const falm_fields *f0, const fal
         LAUNCH(FALM_K_OTHER, st, k_scale<double><<<grid, 256, 0, st>>>(w.ap, (long long)n, 1.0 / apn));
         const void *a_saved = ctx->A_explicit;
         const double tol_saved = ctx->tol;
+        const int ls_saved = ctx->ls_type;
+        ctx->ls_type = FALM_LS_PBICGSTAB;   // whatever solver the forward step uses
         if (!use_tables) ctx->A_explicit = w.AT;
         LAUNCH(FALM_K_OTHER, st, k_adj_extrapolate<<<grid, 256, 0, st>>>(w.arhs, w.arhs1, (long long)n));
         // relative residual 1e-6 (1e-12 when the context's tolerance is below 1e-12):
@@ -1621,6 +1679,7 @@ extern "C" int falm_step_adjoint(falm_ctx *ctx, const falm_fields *f0, const fal
         rc = solve_t<double>(ctx, w.arhs, w.ap, w.r, st, &it, &err, &outer);
         ctx->A_explicit = a_saved;
         ctx->tol = tol_saved;
+        ctx->ls_type = ls_saved;
         if (rc) return rc;
     }
     const double scale = apn / (dt * ctx->maxdiag);   // arhs holds the solution for the normalised right-hand side

@@ -201,6 +201,32 @@ __global__ void __launch_bounds__(kRowThreads) k_res(Geom g, Region3 R, Op7<T> o
     }
 }
 
+// residual of a plain Jacobi / SOR iteration and the loop test of
+// src/FalmEq.cpp:121-126 (and :236-239): r = b - A x, err = ||r||_2 / N in
+// FP64, it++, stop when err <= tol or it == maxit.  Every block returns at once
+// once the solve has stopped (queued iterations).
+template <typename T>
+__global__ void __launch_bounds__(kRowThreads) k_res_plain(Geom g, Region3 R, Op7<T> op, const T *__restrict__ x,
+    const T *__restrict__ b, T *__restrict__ r, RedWork rw, SolverScalars *sc) {
+    if (sc->done) return;
+    double acc[1] = {0.0};
+    FB_FOR_ROWS(R, j, k) FB_FOR_I(R, i) {
+        long long c = g.id(i, j, k);
+        double rv = to_d(b[c]) - apply7<T, double>(op, g, i, j, k, c, x);
+        r[c] = (T)rv;
+        acc[0] += rv * rv;
+    }
+    double tot[1];
+    if (grid_sum<1>(acc, rw, tot) && threadIdx.x == 0) {
+        const double err = sqrt(tot[0]) / sc->gsize;
+        sc->err = err;
+        sc->it += 1;
+        if (!isfinite(err)) { sc->done = 1; sc->status = FALM_ERR_NAN; }
+        else if (err <= sc->tol) { sc->done = 1; sc->status = FALM_OK; }
+        else if (sc->it >= sc->maxit) { sc->done = 1; sc->status = FALM_ERR_MAXIT; }
+    }
+}
+
 // ---------------------------------------------------------------- preconditioner sweeps
 // red-black SOR half sweep, colour (i+j+k)%2 (src/dev/FalmEqDevCall.cu:175-211)
 template <typename T>

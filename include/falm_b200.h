@@ -134,7 +134,9 @@ int falm_cfd_sgs(falm_ctx *ctx, const void *u, void *nut, void *stream);
 int falm_cfd_divergence(falm_ctx *ctx, const void *uu, void *div, void *stream);
 
 /* ---------------- FalmEq (src/FalmEq.h:14-76) -------------------------------------------- */
-/* FalmEq::init (src/FalmEq.h:23-25) */
+/* FalmEq::init (src/FalmEq.h:23-25).  type: FALM_LS_PBICGSTAB, or the plain FALM_LS_JACOBI /
+   FALM_LS_SOR solvers (relax is the SOR relaxation factor); pc_type (SOR or Jacobi) is used
+   by PBiCGStab only. */
 int falm_eq_init(falm_ctx *ctx, int type, int maxit, double tol, double relax,
                  int pc_type, int pc_maxit, double pc_relax);
 /* Poisson operator of the application drivers (app/nedo/main.cpp:25-100,
@@ -144,7 +146,10 @@ int falm_eq_poisson_operator(falm_ctx *ctx, int bc_kind, double *maxdiag_out);
 /* Use an explicit caller-owned 7-column matrix (columns c,w,e,s,n,b,t,
    src/dev/FalmEqDevCall.cu:69-75) instead; NULL returns to the Poisson tables. */
 int falm_eq_set_matrix(falm_ctx *ctx, const void *A);
-/* FalmEq::Solve (src/FalmEq.h:56-64) -> PBiCGStab (src/FalmEq.cpp:305-410).  In FALM_MIXED the
+/* FalmEq::Solve (src/FalmEq.h:56-64) -> Jacobi (src/FalmEq.cpp:80-127), SOR (:173-240; Black
+   then Red half sweep, then the residual, per iteration) or PBiCGStab (:305-410).  For the plain
+   solvers r holds the residual of the final iterate; both iterate in the storage type with
+   FP64 residual norms.  For PBiCGStab in FALM_MIXED the
    iteration runs in FP32 storage with FP64 inner products and is wrapped in an FP64
    true-residual refinement loop.  it/err as FalmEq::it/err (src/FalmEqDevCall.h:27-30).
    r is work storage; on return it holds the last iteration's updated residual (as the

@@ -587,6 +587,48 @@ void oracle_pbicgstab(const or_case *c, const double *A, double *x, const double
     *err_out = err;
 }
 
+/* The plain solvers of FalmEq::Solve: src/FalmEq.cpp:80-127 (Jacobi: xp = x
+ * including ghosts, one sweep x = xp + (b - A xp)/ac as
+ * src/dev/FalmEqDevCall.cu:101-132) and :173-240 (SOR: the Black half sweep,
+ * then the Red one, with the solver's relaxation factor).  After each
+ * iteration r = b - A x and err = ||r||_2 / N; the loop runs while
+ * it < maxit && err > tol. */
+void oracle_plain_solve(const or_case *c, int ls_type, double relax, const double *A, double *x,
+                        const double *bvec, double *r, int *it_out, double *err_out) {
+    Box b(c);
+    const long N = b.n;
+    const double gsize = (double)(b.sx - 2 * b.gc) * (b.sy - 2 * b.gc) * (b.sz - 2 * b.gc);
+    std::vector<double> xp(N);
+    int it = 0;
+    double err = 0.0;
+    do {
+        if (ls_type == OR_PC_JACOBI) {
+            memcpy(xp.data(), x, sizeof(double) * N);
+            const double *v = xp.data();
+#pragma omp parallel for schedule(static)
+            for (int k = b.gc; k < b.sz - b.gc; k++)
+                for (int j = b.gc; j < b.sy - b.gc; j++)
+                    for (int i = b.gc; i < b.sx - b.gc; i++) {
+                        long cc = b.id(i, j, k);
+                        double ac = A[cc], aw = A[cc + N], ae = A[cc + 2 * N], as = A[cc + 3 * N];
+                        double an = A[cc + 4 * N], ab = A[cc + 5 * N], at = A[cc + 6 * N];
+                        double xc = v[cc], xe = v[b.id(i + 1, j, k)], xw = v[b.id(i - 1, j, k)];
+                        double xn = v[b.id(i, j + 1, k)], xs = v[b.id(i, j - 1, k)];
+                        double xt = v[b.id(i, j, k + 1)], xb = v[b.id(i, j, k - 1)];
+                        x[cc] = xc + (bvec[cc] - (ac * xc + ae * xe + aw * xw + an * xn + as * xs + at * xt + ab * xb)) / ac;
+                    }
+        } else {
+            oracle_sor_sweep(c, A, x, bvec, relax, 0);
+            oracle_sor_sweep(c, A, x, bvec, relax, 1);
+        }
+        oracle_res(c, A, x, bvec, r);
+        err = sqrt(oracle_normsq(c, r, 1)) / gsize;
+        it++;
+    } while (it < c->ls_maxit && err > c->ls_tol);
+    *it_out = it;
+    *err_out = err;
+}
+
 /* velocity ghost fill.  Channel: app/nedo/bcdevcall.cu:8-151 (inlet value
  * u_inlet as app/windtunnel/bcdevcall.cu:8-22, optionally perturbed by the
  * seeded inflow box); cavity: app/lid3d/bcdev.cu:11-105 (lid on y+). */

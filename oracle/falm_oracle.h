@@ -86,6 +86,10 @@ void   oracle_res(const or_case *c, const double *A, const double *x, const doub
 void   oracle_sor_sweep(const or_case *c, const double *A, double *x, const double *b, double omega, int color);
 void   oracle_pbicgstab(const or_case *c, const double *A, double *x, const double *b, double *r,
                         int *it_out, double *err_out);
+/* plain Jacobi (ls_type 1) or red-black SOR (ls_type 2, relaxation `relax`) solver with
+   c->ls_maxit and c->ls_tol */
+void   oracle_plain_solve(const or_case *c, int ls_type, double relax, const double *A, double *x,
+                          const double *b, double *r, int *it_out, double *err_out);
 /* ---- boundary conditions (application drivers) ---------------------------------- */
 void oracle_ubc(const or_case *c, double *u, const double *uprev, double t);
 void oracle_pbc(const or_case *c, double *p);

@@ -107,6 +107,7 @@ class Oracle:
             "oracle_mv": [C, dp, dp, dp], "oracle_dot": [C, dp, dp], "oracle_normsq": [C, dp, I],
             "oracle_res": [C, dp, dp, dp, dp], "oracle_sor_sweep": [C, dp, dp, dp, D, I],
             "oracle_pbicgstab": [C, dp, dp, dp, dp, ip, dp], "oracle_ubc": [C, dp, dp, D],
+            "oracle_plain_solve": [C, I, D, dp, dp, dp, dp, ip, dp],
             "oracle_pbc": [C, dp], "oracle_uubc": [C, dp],
             "oracle_build_aps": [I, dp, dp, dp, dp, dp, I, I, I, D, D, dp, dp, dp, dp, dp],
             "oracle_alm": [C, dp, dp, D, dp, dp, dp, dp, dp, dp],
@@ -122,7 +123,7 @@ class Oracle:
             getattr(L, k).restype = ctypes.c_double
         for k in ("oracle_metrics", "oracle_pseudo_u", "oracle_utouu", "oracle_divergence", "oracle_poisson_rhs",
                   "oracle_project_p", "oracle_sgs", "oracle_mv", "oracle_res", "oracle_sor_sweep",
-                  "oracle_pbicgstab", "oracle_ubc", "oracle_pbc", "oracle_uubc", "oracle_build_aps",
+                  "oracle_pbicgstab", "oracle_plain_solve", "oracle_ubc", "oracle_pbc", "oracle_uubc", "oracle_build_aps",
                   "oracle_alm", "oracle_step", "oracle_transpose_matrix"):
             getattr(L, k).restype = None
 
@@ -154,6 +155,13 @@ class Oracle:
     def pbicgstab(self, cs, A, x, b, r):
         it, err = ctypes.c_int(), ctypes.c_double()
         self.L.oracle_pbicgstab(ctypes.byref(cs.c), _p(A), _p(x), _p(b), _p(r), ctypes.byref(it), ctypes.byref(err))
+        return it.value, err.value
+
+    def plain_solve(self, cs, ls, relax, A, x, b, r):
+        """FalmEq::Jacobi / FalmEq::SOR (ls "Jacobi" or "SOR") with the case's maxit and tol"""
+        it, err = ctypes.c_int(), ctypes.c_double()
+        self.L.oracle_plain_solve(ctypes.byref(cs.c), PC[ls], relax, _p(A), _p(x), _p(b), _p(r), ctypes.byref(it),
+                                  ctypes.byref(err))
         return it.value, err.value
 
     def power(self, cs, stats):

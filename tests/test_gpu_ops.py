@@ -226,6 +226,95 @@ def test_pbicgstab_converged(oracle, lib_built):
     assert rel_l2(interior(host(xd), g), interior(xo, g)) < 1e-7
 
 
+@pytest.mark.parametrize("ls", ["Jacobi", "SOR"])
+@pytest.mark.parametrize("maxit", [4, 7])
+@pytest.mark.parametrize("shape", [(24, 16, 12), (72, 20, 16)])
+def test_plain_solvers_fixed_iterations(oracle, lib_built, ls, maxit, shape):
+    """FalmEq::Jacobi / FalmEq::SOR (src/FalmEq.cpp:80-127, :173-240) in
+    fixed-iteration mode (tol 0): the oracle's iterate, residual and err. An even
+    and an odd count end the Jacobi alternation in either buffer; nx = 72 runs
+    the SOR half sweeps on the 7-point plane stream."""
+    case = cases.small_channel(*shape, intensity=0.05).with_inflow(nb=8)
+    case.tol, case.maxit = 0.0, maxit
+    cs, m = _setup(oracle, case)
+    g = case.grid
+    rng = np.random.default_rng(21)
+    b = np.zeros(g.n)
+    interior(b, g)[...] = rng.standard_normal(interior(b, g).shape)
+    x0 = 0.1 * rng.standard_normal(g.n)
+    xo, ro = x0.copy(), np.zeros(g.n)
+    it_o, err_o = oracle.plain_solve(cs, ls, 1.3, m["A"], xo, b, ro)
+    ctx = make_ctx(case)
+    ctx.eq_init(maxit, 0.0, case.pc, case.pc_maxit, case.pc_relax, ls=ls, relax=1.3)
+    xd, bd, rd = dev(ctx, x0), dev(ctx, b), ctx.field(1)
+    it, err, rc = ctx.solve(xd, bd, rd)
+    assert it == it_o == maxit and rc == 5          # FALM_ERR_MAXIT: tol 0 is never met
+    assert err == pytest.approx(err_o, rel=1e-10)
+    assert rel_l2(interior(host(xd), g), interior(xo, g)) < 1e-12
+    assert rel_l2(interior(host(rd), g), interior(ro, g)) < 1e-10
+    # the ghost cells of x are the caller's
+    np.testing.assert_array_equal(host(xd)[:g.sx * g.sy], x0[:g.sx * g.sy])
+
+
+@pytest.mark.parametrize("ls,relax", [("Jacobi", 1.0), ("SOR", 1.5)])
+def test_plain_solvers_converged(oracle, lib_built, ls, relax):
+    """Convergence mode: the loop stops at the first iterate with ||r||/N <= tol
+    (iteration counts within 1 of the oracle's: about 6800 Jacobi and 1200 SOR
+    iterations), FP64 and mixed precision (FP32 iterate, FP64 residual norm).
+    The channel's p = 0 outlet makes the operator nonsingular; on the
+    all-Neumann cavity plain Jacobi does not converge (its iteration matrix has
+    the eigenvalue -1 of the checkerboard mode)."""
+    case = cases.small_channel(16, 12, 12, intensity=0.0)
+    case.tol, case.maxit = 1e-8, 20000
+    cs, m = _setup(oracle, case)
+    g = case.grid
+    rng = np.random.default_rng(5)
+    b = np.zeros(g.n)
+    interior(b, g)[...] = rng.standard_normal(interior(b, g).shape)
+    xo, ro = np.zeros(g.n), np.zeros(g.n)
+    it_o, err_o = oracle.plain_solve(cs, ls, relax, m["A"], xo, b, ro)
+    assert err_o <= case.tol and it_o < case.maxit
+    ctx = make_ctx(case)
+    ctx.eq_init(case.maxit, case.tol, case.pc, case.pc_maxit, case.pc_relax, ls=ls, relax=relax)
+    xd, rd = ctx.field(1), ctx.field(1)
+    it, err, rc = ctx.solve(xd, dev(ctx, b), rd)
+    assert rc == 0 and err <= case.tol and abs(it - it_o) <= 1
+    assert rel_l2(interior(host(xd), g), interior(xo, g)) < 1e-8
+    ctx32 = make_ctx(case, "mixed")
+    ctx32.eq_init(case.maxit, 1e-5, case.pc, case.pc_maxit, case.pc_relax, ls=ls, relax=relax)
+    x32, r32 = ctx32.field(1), ctx32.field(1)
+    it32, err32, rc32 = ctx32.solve(x32, dev(ctx32, b), r32)
+    assert rc32 == 0 and err32 <= 1e-5
+    # the FP64 residual of the FP32 iterate, by the oracle, meets the tolerance
+    r64, xh = np.zeros(g.n), host(x32)
+    oracle.L.oracle_res(ctypes.byref(cs.c), _p(m["A"]), _p(xh), _p(b), _p(r64))
+    assert np.sqrt(oracle.L.oracle_normsq(ctypes.byref(cs.c), _p(r64), 1)) / g.n_interior <= 1.01e-5
+
+
+def test_step_with_plain_sor_solver(lib_built):
+    """A whole step with the plain SOR Poisson solver: the step skips the
+    BiCGStab start fused into the face-velocity kernel, runs the solver's
+    iterations and gives another pressure than PBiCGStab does."""
+    case = CASES["channel"]()
+    ctx = make_ctx(case)
+    ctx.eq_init(5, 0.0, case.pc, case.pc_maxit, case.pc_relax, ls="SOR", relax=1.2)
+    st0 = cases.initial_state(case)
+    u, uu, p, nut = dev(ctx, st0["u"]), ctx.field(3), ctx.field(1), ctx.field(1)
+    ctx.utouu(u, uu)
+    ctx.sgs(u, nut)
+    s = ctx.step(u, uu, p, nut, None, case.dt, case.dt)
+    assert s["it"] == 5
+    # the same step with PBiCGStab gives a different pressure: the solver switch took effect
+    ctx2 = make_ctx(case)
+    ctx2.eq_init(5, 0.0, case.pc, case.pc_maxit, case.pc_relax)
+    u2, uu2, p2, nut2 = dev(ctx2, st0["u"]), ctx2.field(3), ctx2.field(1), ctx2.field(1)
+    ctx2.utouu(u2, uu2)
+    ctx2.sgs(u2, nut2)
+    ctx2.step(u2, uu2, p2, nut2, None, case.dt, case.dt)
+    assert rel_l2(host(p), host(p2)) > 1e-6
+    assert np.isfinite(host(u)).all()
+
+
 def test_heat1d_explicit_matrix(lib_built):
     """test/heat1d2.cpp:217 on the GPU through falm_eq_set_matrix"""
     from tests.test_oracle_kat import _box_case, heat1d_system

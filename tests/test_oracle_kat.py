@@ -83,6 +83,25 @@ def test_heat1d_linear_profile(oracle):
     assert rel_l2(x, exact) < 1e-7
 
 
+@pytest.mark.parametrize("ls,relax", [("Jacobi", 1.0), ("SOR", 1.8)])
+def test_heat1d_plain_solvers(oracle, ls, relax):
+    """FalmEq::Jacobi / FalmEq::SOR (src/FalmEq.cpp:80-127, :173-240) on the
+    test/heat1d2.cpp system (20 cells) reproduce the linear Dirichlet profile,
+    and the loop stops at the first iterate with ||r||/N <= tol."""
+    from oracle.oracle import CaseStruct
+    shape, A, b, exact = heat1d_system(nx=20)
+    case = _box_case(shape, 2, h=0.05)
+    case.maxit, case.tol = 100000, 1e-10
+    x, r = np.zeros_like(b), np.zeros_like(b)
+    it, err = oracle.plain_solve(CaseStruct(case), ls, relax, A, x, b, r)
+    assert err <= 1e-10 and it < case.maxit
+    assert rel_l2(x, exact) < 1e-6
+    case.maxit = it - 1
+    x2 = np.zeros_like(b)
+    it2, err2 = oracle.plain_solve(CaseStruct(case), ls, relax, A, x2, b, r)
+    assert it2 == it - 1 and err2 > 1e-10
+
+
 def test_red_black_colouring(oracle):
     """src/dev/FalmEqDevCall.cu:206 and test/coloridx.py: colour (i+j+k+offset)%2,
     the black (0) half-sweep touches only colour-0 cells and leaves the others."""
