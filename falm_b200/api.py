@@ -229,6 +229,69 @@ class Context:
                     "step_adjoint")
 
 
+    # ------------------------------------------------------------ output (FalmIO, TAvg)
+    def tavg(self, avg, f, count):
+        """FalmSolver::TAvg (src/falm.h:433-444): avg = (1 - 1/count) avg + f/count"""
+        ncol = f.numel() // self.grid.n
+        self._check(self.lib.falm_tavg(self.h, _ptr(avg), _ptr(f), ncol, count, self.stream()), "tavg")
+
+    def write_vector_file(self, path, fields, step, time, as_fp64=False):
+        """FalmIO::writeVectorFile of the columns of `fields` (device tensors) in order;
+        returns before the file is written (see io_wait)"""
+        ptrs = (L.P * len(fields))(*[f.data_ptr() for f in fields])
+        ncols = (ctypes.c_int * len(fields))(*[f.numel() // self.grid.n for f in fields])
+        self._check(self.lib.falm_io_write_vector_file(self.h, str(path).encode(), ptrs, ncols, len(fields), int(step),
+                                                       float(time), 1 if as_fp64 else 0, self.stream()),
+                    "write_vector_file")
+
+    def io_wait(self):
+        """wait for every queued snapshot file"""
+        self._check(self.lib.falm_io_wait(self.h), "io_wait")
+
+    def write_cv_file(self, path):
+        """FalmIO::writeControlVolumeFile of this grid"""
+        self._check(self.lib.falm_io_write_cv_file(self.h, str(path).encode()), "write_cv_file")
+
+
+def write_index_file(path, interior, gc, snapshots, dsize=8):
+    """FalmIO::writeIndexFile (src/FalmIO.h:25-67); snapshots: [(step, time, tavg), ...]"""
+    lib = L.load()
+    n = len(snapshots)
+    steps = (ctypes.c_ulonglong * max(n, 1))(*[int(s[0]) for s in snapshots])
+    times = np.ascontiguousarray([float(s[1]) for s in snapshots] or [0.0], dtype=np.float64)
+    tav = (ctypes.c_int * max(n, 1))(*[1 if s[2] else 0 for s in snapshots])
+    rc = lib.falm_io_write_index_file(str(path).encode(), interior[0], interior[1], interior[2], gc, steps, _dp(times),
+                                      tav, n, dsize)
+    if rc != 0:
+        raise L.FalmError(rc, "write_index_file")
+
+
+def read_cv_file(path):
+    """FalmIO::readControlVolumeFile (src/FalmIO.h:99-116): (dims (sx, sy, sz, gc), x, hx, y, hy, z, hz)"""
+    lib = L.load()
+    dims = (ctypes.c_int * 4)()
+    rc = lib.falm_io_read_cv_file(str(path).encode(), dims, None, None, None, None, None, None)
+    if rc != 0:
+        raise L.FalmError(rc, "read_cv_file")
+    arr = [np.zeros(dims[d // 2]) for d in range(6)]
+    rc = lib.falm_io_read_cv_file(str(path).encode(), dims, *[_dp(a) for a in arr])
+    if rc != 0:
+        raise L.FalmError(rc, "read_cv_file")
+    return tuple(dims), arr[0], arr[1], arr[2], arr[3], arr[4], arr[5]
+
+
+def read_vector_file(path):
+    """a FalmIO vector file: (header dict, array [ncol, kmax, jmax, imax])"""
+    with open(path, "rb") as f:
+        head = np.frombuffer(f.read(48), dtype=np.uint64)
+        time = np.frombuffer(f.read(8), dtype=np.float64)[0]
+        dsize = int(np.frombuffer(f.read(8), dtype=np.uint64)[0])
+        imax, jmax, kmax, ncol, gc, step = (int(v) for v in head)
+        data = np.frombuffer(f.read(), dtype=np.float64 if dsize == 8 else np.float32)
+    hd = {"imax": imax, "jmax": jmax, "kmax": kmax, "ncol": ncol, "gc": gc, "step": step, "time": float(time), "dsize": dsize}
+    return hd, data.reshape(ncol, kmax, jmax, imax)
+
+
 def build_aps(stations, n_turbine, n_blade, n_ap_per_blade, radius, hub_radius):
     """BladeHandler::buildAP (src/alm/bladeHandler.h:16-104) through the C ABI (host only)."""
     lib = L.load()

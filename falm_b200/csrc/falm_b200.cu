@@ -25,6 +25,7 @@
 #include "stencil_tma.cuh"
 #include "poisson_tma.cuh"
 #include "plane3_tma.cuh"
+#include "falm_io.cuh"
 #include "sor_rb_tma.cuh"
 #include "adjoint.cuh"
 #include <cudaTypedefs.h>
@@ -986,6 +987,7 @@ int falm_create(const falm_grid *grid, int precision, falm_ctx **out) {
 
 int falm_destroy(falm_ctx *ctx) {
     if (!ctx) return FALM_ERR_ARG;
+    delete ctx->io;   // writes the queued snapshots, then stops its thread
     cudaFree(ctx->metric_mem);
     cudaFree(ctx->op_mem);
     cudaFree(ctx->work_mem);
@@ -1096,10 +1098,17 @@ int falm_cfd_sgs(falm_ctx *ctx, const void *u, void *nut, void *stream) {
 
 // ---------------------------------------------------------------- FalmEq
 int falm_eq_init(falm_ctx *ctx, int type, int maxit, double tol, double relax, int pc_type, int pc_maxit, double pc_relax) {
-    if (!ctx || maxit < 1 || pc_maxit < 1 || !(tol >= 0)) return FALM_ERR_ARG;
+    if (!ctx || maxit < 1 || !(tol >= 0)) return FALM_ERR_ARG;
     if (type != FALM_LS_PBICGSTAB && type != FALM_LS_SOR && type != FALM_LS_JACOBI)
         return fail(ctx, FALM_ERR_ARG, "eq_init: solver must be Jacobi (1), SOR (2) or PBiCGStab (4)");
+    const bool plain = type != FALM_LS_PBICGSTAB;
+    if (plain && pc_type == FALM_LS_EMPTY) {
+        // a plain solver has no preconditioner; the adjoint's transposed solve
+        // (always PBiCGStab) then uses the drivers' SOR x2, omega 1.2
+        pc_type = FALM_LS_SOR; pc_maxit = 2; pc_relax = 1.2;
+    }
     if (pc_type != FALM_LS_SOR && pc_type != FALM_LS_JACOBI) return fail(ctx, FALM_ERR_ARG, "eq_init: preconditioner must be SOR (2) or Jacobi (1)");
+    if (pc_maxit < 1) return FALM_ERR_ARG;
     ctx->ls_type = type; ctx->maxit = maxit; ctx->tol = tol; ctx->relax = relax;
     ctx->pc_type = pc_type; ctx->pc_maxit = pc_maxit; ctx->pc_relax = pc_relax;
     return FALM_OK;
@@ -1223,9 +1232,171 @@ int falm_mv_axby(falm_ctx *ctx, double a, const void *x, double b, const void *y
     if (!ctx || !x || !y || !result || n < 0) return FALM_ERR_ARG;
     return dispatch(ctx, [&](auto z) {
         using T = decltype(z);
-        LAUNCH(FALM_K_OTHER, (cudaStream_t)0, k_axby<T><<<ctx->sm_count * 4, 256, 0, S(stream)>>>((T)a, (const T *)x, (T)b, (const T *)y, (T *)result, n));
+        LAUNCH(FALM_K_OTHER, S(stream), k_axby<T><<<ctx->sm_count * 4, 256, 0, S(stream)>>>((T)a, (const T *)x, (T)b, (const T *)y, (T *)result, n));
         return (int)FALM_OK;
     });
+}
+
+// ---------------------------------------------------------------- FalmIO + TAvg
+int falm_tavg(falm_ctx *ctx, void *avg, const void *f, int ncol, long long count, void *stream) {
+    if (!ctx || !avg || !f || ncol < 1 || count < 1) return FALM_ERR_ARG;
+    const double b = 1.0 / (double)count, a = 1.0 - b;
+    return falm_mv_axby(ctx, a, avg, b, f, avg, (long long)ncol * ctx->geo.n, stream);
+}
+
+int falm_io_write_vector_file(falm_ctx *ctx, const char *path, const void *const *fields, const int *ncols, int nfields,
+                              unsigned long long step, double time, int as_fp64, void *stream) {
+    if (!ctx || !path || !fields || !ncols || nfields < 1) return FALM_ERR_ARG;
+    long long cols = 0;
+    for (int q = 0; q < nfields; q++) {
+        if (!fields[q] || ncols[q] < 1) return FALM_ERR_ARG;
+        cols += ncols[q];
+    }
+    const Geom &g = ctx->geo;
+    const size_t n = (size_t)g.n, es = ctx->esize;
+    const bool cast = as_fp64 && es == sizeof(float);
+    const size_t ds = cast ? sizeof(double) : es, bytes = (size_t)cols * n * ds;
+    if (!ctx->io) {
+        ctx->io = new IoWriter();
+        ctx->io->device = ctx->device;
+        IoWriter *w = ctx->io;
+        ctx->io->worker = std::thread([w] { w->run(); });
+    }
+    IoWriter &w = *ctx->io;
+    int bi = -1;
+    {
+        std::unique_lock<std::mutex> lk(w.m);
+        w.cv.wait(lk, [&] { return !w.bufs[0].in_use || !w.bufs[1].in_use; });
+        bi = w.bufs[0].in_use ? 1 : 0;
+        w.bufs[bi].in_use = true;
+    }
+    IoBuf &b = w.bufs[bi];
+    auto release = [&](int rc, const char *msg) {
+        { std::lock_guard<std::mutex> lk(w.m); b.in_use = false; }
+        w.cv.notify_all();
+        return fail(ctx, rc, msg);
+    };
+    if (b.cap < bytes) {
+        if (b.host) cudaFreeHost(b.host);
+        b.host = nullptr; b.cap = 0;
+        if (cudaHostAlloc(&b.host, bytes, cudaHostAllocDefault) != cudaSuccess) { cudaGetLastError(); return release(FALM_ERR_ALLOC, "io: pinned staging buffer"); }
+        b.cap = bytes;
+    }
+    if (cast && b.dcap < bytes) {
+        if (b.dev) cudaFree(b.dev);
+        b.dev = nullptr; b.dcap = 0;
+        if (cudaMalloc(&b.dev, bytes) != cudaSuccess) { cudaGetLastError(); return release(FALM_ERR_ALLOC, "io: device staging buffer"); }
+        b.dcap = bytes;
+    }
+    if (!b.ready && cudaEventCreateWithFlags(&b.ready, cudaEventDisableTiming) != cudaSuccess) return release(FALM_ERR_CUDA, "io: event");
+    // the columns, field after field: the reference's uvwp layout (u's 3, then p's 1)
+    cudaStream_t st = S(stream);
+    size_t off = 0;
+    for (int q = 0; q < nfields; q++) {
+        const size_t len = (size_t)ncols[q] * n;
+        if (cast) {
+            LAUNCH(FALM_K_OTHER, st, k_cast_f64<<<ctx->sm_count * 4, 256, 0, st>>>((const float *)fields[q], (double *)b.dev + off, (long long)len));
+        } else if (cudaMemcpyAsync((char *)b.host + off * ds, fields[q], len * ds, cudaMemcpyDeviceToHost, st) != cudaSuccess) {
+            return release(FALM_ERR_CUDA, "io: snapshot copy");
+        }
+        off += len;
+    }
+    if (cast && cudaMemcpyAsync(b.host, b.dev, bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess) return release(FALM_ERR_CUDA, "io: snapshot copy");
+    if (cudaEventRecord(b.ready, st) != cudaSuccess) return release(FALM_ERR_CUDA, "io: event record");
+    IoJob job;
+    job.path = path;
+    job.head[0] = (uint64_t)g.sx; job.head[1] = (uint64_t)g.sy; job.head[2] = (uint64_t)g.sz;
+    job.head[3] = (uint64_t)cols; job.head[4] = (uint64_t)g.gc; job.head[5] = (uint64_t)step;
+    job.time = time;
+    job.dsize = ds;
+    job.bytes = bytes;
+    job.buf = bi;
+    {
+        std::lock_guard<std::mutex> lk(w.m);
+        w.jobs.push_back(job);
+        w.pending++;
+    }
+    w.cv.notify_all();
+    return FALM_OK;
+}
+
+int falm_io_wait(falm_ctx *ctx) {
+    if (!ctx) return FALM_ERR_ARG;
+    if (!ctx->io) return FALM_OK;
+    IoWriter &w = *ctx->io;
+    std::unique_lock<std::mutex> lk(w.m);
+    w.cv.wait(lk, [&] { return w.pending == 0; });
+    const int rc = w.error;
+    const std::string msg = w.error_msg;
+    w.error = 0;
+    w.error_msg.clear();
+    lk.unlock();
+    return rc ? fail(ctx, rc, msg.c_str()) : FALM_OK;
+}
+
+int falm_io_write_index_file(const char *path, int nx, int ny, int nz, int gc, const unsigned long long *steps,
+                             const double *times, const int *tavg, int nsnap, int dsize) {
+    if (!path || nx < 1 || ny < 1 || nz < 1 || gc < 0 || nsnap < 0 || (nsnap > 0 && (!steps || !times))) return FALM_ERR_ARG;
+    if (dsize != 4 && dsize != 8) return FALM_ERR_ARG;
+    for (int q = 0; q < nsnap; q++)
+        if (!std::isfinite(times[q])) return FALM_ERR_ARG;
+    // nlohmann::json's dump(2) of the reference's index object: keys in
+    // lexicographic order, two-space indent, every array element on a line of
+    // its own, no newline at the end
+    std::string o = "{\n";
+    o += std::string("  \"dataType\": \"") + (dsize == 4 ? "float32" : "float64") + "\",\n";
+    o += "  \"global\": [\n    " + std::to_string(nx) + ",\n    " + std::to_string(ny) + ",\n    " + std::to_string(nz) + "\n  ],\n";
+    o += "  \"guidePoint\": " + std::to_string(gc) + ",\n";
+    if (nsnap > 0) {
+        o += "  \"outputSteps\": [\n";
+        for (int q = 0; q < nsnap; q++) {
+            o += "    {\n      \"step\": " + std::to_string(steps[q]) + ",\n      \"time\": " + json_double(times[q]);
+            if (tavg && tavg[q]) o += ",\n      \"timeAvg\": 1";
+            o += std::string("\n    }") + (q + 1 < nsnap ? "," : "") + "\n";
+        }
+        o += "  ],\n";
+    }
+    o += "  \"ranks\": [\n    {\n      \"offset\": [\n        0,\n        0,\n        0\n      ],\n      \"rank\": 0,\n";
+    o += "      \"voxel\": [\n        " + std::to_string(nx) + ",\n        " + std::to_string(ny) + ",\n        " + std::to_string(nz) +
+         "\n      ]\n    }\n  ],\n";
+    o += "  \"variables\": [\n    \"u\",\n    \"v\",\n    \"w\",\n    \"p\"\n  ]\n}";
+    FILE *f = fopen(path, "wb");
+    if (!f) return FALM_ERR_ARG;
+    const bool ok = fwrite(o.data(), 1, o.size(), f) == o.size();
+    return (fclose(f) == 0 && ok) ? FALM_OK : FALM_ERR_ARG;
+}
+
+int falm_io_write_cv_file(falm_ctx *ctx, const char *path) {
+    if (!ctx || !path || !ctx->xc || !ctx->hx) return FALM_ERR_ARG;
+    FILE *f = fopen(path, "w");
+    if (!f) return fail(ctx, FALM_ERR_ARG, "io: cannot open the control-volume file");
+    const Geom &g = ctx->geo;
+    fprintf(f, "%d %d %d %d\n", g.sx, g.sy, g.sz, g.gc);
+    const std::vector<double> *c[3] = {ctx->xc, ctx->yc, ctx->zc}, *h[3] = {ctx->hx, ctx->hy, ctx->hz};
+    for (int d = 0; d < 3; d++)
+        for (size_t q = 0; q < c[d]->size(); q++) fprintf(f, "\t%.15e\t%.15e\n", (*c[d])[q], (*h[d])[q]);
+    return fclose(f) == 0 ? FALM_OK : fail(ctx, FALM_ERR_ARG, "io: control-volume write");
+}
+
+int falm_io_read_cv_file(const char *path, int dims[4], double *x, double *hx, double *y, double *hy, double *z, double *hz) {
+    if (!path || !dims) return FALM_ERR_ARG;
+    FILE *f = fopen(path, "r");
+    if (!f) return FALM_ERR_ARG;
+    int d4[4];
+    if (fscanf(f, "%d %d %d %d", &d4[0], &d4[1], &d4[2], &d4[3]) != 4 || d4[0] < 1 || d4[1] < 1 || d4[2] < 1 || d4[3] < 0) {
+        fclose(f);
+        return FALM_ERR_ARG;
+    }
+    for (int q = 0; q < 4; q++) dims[q] = d4[q];
+    double *c[3] = {x, y, z}, *h[3] = {hx, hy, hz};
+    int rc = FALM_OK;
+    if (x && hx && y && hy && z && hz) {
+        for (int d = 0; d < 3 && rc == FALM_OK; d++)
+            for (int q = 0; q < d4[d]; q++)
+                if (fscanf(f, "%lf %lf", &c[d][q], &h[d][q]) != 2) { rc = FALM_ERR_ARG; break; }
+    }
+    fclose(f);
+    return rc;
 }
 
 // ---------------------------------------------------------------- boundary conditions

@@ -95,6 +95,7 @@ struct AlmDev {
     AlmScalars *scal;
 };
 
+struct IoWriter;
 }  // namespace fb
 
 // host-side context
@@ -163,4 +164,5 @@ struct falm_ctx {
     int sor_v1;                             // FP32 blocked SOR on the 32 x 8 tile kernel (tests)
     int check_sync;                         // synchronise after every launch (fault location)
     std::string *last_error;
+    fb::IoWriter *io;                       // snapshot writer (falm_io.cuh), created on first use
 };

@@ -136,7 +136,7 @@ int falm_cfd_divergence(falm_ctx *ctx, const void *uu, void *div, void *stream);
 /* ---------------- FalmEq (src/FalmEq.h:14-76) -------------------------------------------- */
 /* FalmEq::init (src/FalmEq.h:23-25).  type: FALM_LS_PBICGSTAB, or the plain FALM_LS_JACOBI /
    FALM_LS_SOR solvers (relax is the SOR relaxation factor); pc_type (SOR or Jacobi) is used
-   by PBiCGStab only. */
+   by PBiCGStab only, and a plain solver also accepts FALM_LS_EMPTY. */
 int falm_eq_init(falm_ctx *ctx, int type, int maxit, double tol, double relax,
                  int pc_type, int pc_maxit, double pc_relax);
 /* Poisson operator of the application drivers (app/nedo/main.cpp:25-100,
@@ -212,6 +212,34 @@ int falm_step(falm_ctx *ctx, const falm_fields *f, double dt, double t, void *st
    `stream` (pass pinned memory).  Takes precedence over the inflow box for that one call.
    No reference counterpart (the reference has uniform inflow only). */
 int falm_bc_set_inlet_plane(falm_ctx *ctx, const double *plane, void *stream);
+
+/* ---------------- FalmIO (src/FalmIO.h) and time averaging (src/falm.h:433-478) ----------- */
+/* FalmSolver::TAvg (src/falm.h:433-444): avg = (1 - 1/count) avg + (1/count) f over the whole
+   arrays (ncol columns of the context's grid, guide cells included), count = it - start + 1. */
+int falm_tavg(falm_ctx *ctx, void *avg, const void *f, int ncol, long long count, void *stream);
+/* FalmIO::writeVectorFile (src/FalmIO.h:69-97) as outputUVWP calls it (src/falm.h:446-475): the
+   header imax, jmax, kmax, ncol, gc, step (8-byte unsigned each), time (double), dsize (8-byte),
+   then the columns of the whole array (guide cells included, i fastest, then j, k), column after
+   column.  The columns are those of `nfields` device fields of ncols[q] columns each, in order
+   (the drivers' uvwp: u then p).  dsize is the context's storage size, or 8 with as_fp64 (an FP32
+   context's values cast on the device).  The copies run on `stream` into one of two pinned
+   staging buffers and a host thread of the context writes the file, so the call returns before
+   the file exists (a third call waits for a free buffer); falm_io_wait waits for every queued
+   file and returns the first write error since its last call. */
+int falm_io_write_vector_file(falm_ctx *ctx, const char *path, const void *const *fields, const int *ncols, int nfields,
+                              unsigned long long step, double time, int as_fp64, void *stream);
+int falm_io_wait(falm_ctx *ctx);
+/* FalmIO::writeIndexFile (src/FalmIO.h:25-67) for one rank: nlohmann::json's dump(2) of
+   {dataType, global, guidePoint, outputSteps[{step, time, timeAvg}], ranks, variables}, byte for
+   byte (the reference spells the float32 key "dateType"; this writes "dataType" for both).
+   nx, ny, nz are interior sizes; tavg may be NULL; dsize 4 or 8. */
+int falm_io_write_index_file(const char *path, int nx, int ny, int nz, int gc, const unsigned long long *steps,
+                             const double *times, const int *tavg, int nsnap, int dsize);
+/* FalmIO::writeControlVolumeFile (src/FalmIO.h:118-135) of the context's grid ("sx sy sz gc",
+   then x hx, y hy, z hz per line as "\t%.15e\t%.15e") and FalmIO::readControlVolumeFile
+   (:99-116): dims = {sx, sy, sz, gc}; with all six arrays NULL only dims is read. */
+int falm_io_write_cv_file(falm_ctx *ctx, const char *path);
+int falm_io_read_cv_file(const char *path, int dims[4], double *x, double *hx, double *y, double *hy, double *z, double *hz);
 
 /* ---------------- discrete adjoint of the step ---------------------------------------------- */
 /* No reference counterpart.  Adjoint of falm_step for FP64 contexts (Upwind3/UTOPIA/KK advection,

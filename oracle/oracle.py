@@ -232,6 +232,11 @@ class RefStep:
         L.ref_op.argtypes = [P, ctypes.c_int, ctypes.c_double, ctypes.POINTER(OrStats)]
         L.ref_step.argtypes = [P, ctypes.c_double, ctypes.POINTER(OrStats)]
         L.ref_get_aps.argtypes = [P, dp, dp, dp, dp]
+        L.ref_plain_solve.argtypes = [P, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.POINTER(OrStats)]
+        L.ref_write_uvwp.argtypes = [P, ctypes.c_char_p, ctypes.c_ulonglong, ctypes.c_double]
+        L.ref_write_index.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_ulonglong), dp,
+                                      ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+        L.ref_write_cv.argtypes = [P, ctypes.c_char_p]
         self.cs = cs
         self.n = cs.case.grid.n
         st = cs.case.alm.stations if cs.case.alm is not None else None
@@ -287,3 +292,29 @@ class RefStep:
 
     def maxdiag(self):
         return self.L.ref_maxdiag(self.h)
+
+    def plain_solve(self, ls, relax, maxit, tol):
+        """FalmEq::Solve with the plain Jacobi / SOR solver on the harness's P, RHS, RES"""
+        s = OrStats()
+        rc = self.L.ref_plain_solve(self.h, PC[ls], relax, maxit, tol, ctypes.byref(s))
+        if rc:
+            raise RuntimeError(f"ref_plain_solve: {rc}")
+        return s.it, s.err
+
+    def write_uvwp(self, path, step, time):
+        """FalmIO::writeVectorFile of u and p, as the drivers' outputUVWP"""
+        rc = self.L.ref_write_uvwp(self.h, str(path).encode(), int(step), float(time))
+        if rc:
+            raise RuntimeError(f"ref_write_uvwp: {rc}")
+
+    def write_index(self, path, snapshots):
+        """FalmIO::writeIndexFile; snapshots: [(step, time, tavg), ...]"""
+        n = len(snapshots)
+        steps = (ctypes.c_ulonglong * max(n, 1))(*[int(q[0]) for q in snapshots])
+        times = np.ascontiguousarray([float(q[1]) for q in snapshots] or [0.0])
+        tav = (ctypes.c_int * max(n, 1))(*[1 if q[2] else 0 for q in snapshots])
+        self.L.ref_write_index(self.h, str(path).encode(), steps, _p(times), tav, n)
+
+    def write_cv(self, path):
+        """FalmIO::writeControlVolumeFile of the case grid"""
+        self.L.ref_write_cv(self.h, str(path).encode())

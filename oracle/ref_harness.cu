@@ -26,6 +26,7 @@
 #include "alm/alm.h"
 #include "windtunnel/bcdevcall.h"
 #include "lid3d/bcdev.h"
+#include "FalmIO.h"
 #include "falm_oracle.h"
 
 using namespace Falm;
@@ -354,6 +355,58 @@ int ref_op(void *h, int op, double t, or_stats *st) {
     default: return 1;
     }
     return (int)cudaDeviceSynchronize();
+}
+
+/* FalmEq::Solve with the plain Jacobi (ls_type 1) or red-black SOR (2) solver
+ * (src/FalmEq.cpp:80-127, :173-240) on the harness's p (initial guess, then
+ * solution), rhs and res */
+int ref_plain_solve(void *h, int ls_type, double relax, int maxit, double tol, or_stats *st) {
+    RefCase *R = (RefCase *)h;
+    FalmEq eq;
+    eq.init(ls_type == OR_PC_JACOBI ? LSType::Jacobi : LSType::SOR, maxit, tol, relax, LSType::Empty, 1, 1.0);
+    eq.alloc(R->cpm.pdm_list[0].shape);
+    eq.Solve(R->poi_a, R->p, R->rhs, R->res, R->cpm, R->block, R->streams);
+    if (st) { st->it = eq.it; st->err = eq.err; }
+    eq.release();
+    return (int)cudaDeviceSynchronize();
+}
+
+/* FalmIO::writeVectorFile of the drivers' uvwp buffer (u, then p), as
+ * FalmSolver::outputUVWP fills it (src/falm.h:446-460) */
+int ref_write_uvwp(void *h, const char *path, unsigned long long step, double time) {
+    RefCase *R = (RefCase *)h;
+    Int3 shape = R->cpm.pdm_list[0].shape;
+    Matrix<Real> uvwp;
+    uvwp.alloc(shape, 4, HDC::Host, "uvwp");
+    const size_t n = (size_t)PRODUCT3(shape);
+    cudaMemcpy(&uvwp(0, 0), &R->u.dev(0), sizeof(Real) * n * 3, cudaMemcpyDeviceToHost);
+    cudaMemcpy(&uvwp(0, 3), &R->p.dev(0), sizeof(Real) * n, cudaMemcpyDeviceToHost);
+    FalmIO::writeVectorFile(path, R->cpm, uvwp, (size_t)step, time);
+    uvwp.release();
+    return (int)cudaDeviceSynchronize();
+}
+
+/* FalmIO::writeIndexFile for the harness's one-rank partition */
+int ref_write_index(void *h, const char *path, const unsigned long long *steps, const double *times, const int *tavg, int n) {
+    RefCase *R = (RefCase *)h;
+    std::vector<FalmSnapshotInfo> list;
+    for (int q = 0; q < n; q++) list.push_back(FalmSnapshotInfo{(size_t)steps[q], times[q], tavg && tavg[q] != 0});
+    FalmIO::writeIndexFile(path, R->cpm, list);
+    return 0;
+}
+
+/* FalmIO::writeControlVolumeFile of the case's grid */
+int ref_write_cv(void *h, const char *path) {
+    RefCase *R = (RefCase *)h;
+    FalmBaseMesh mesh;
+    mesh.alloc(R->c.sx, R->c.sy, R->c.sz, HDC::Host);
+    for (int i = 0; i < R->c.sx; i++) { mesh.x(i) = R->c.x[i]; mesh.hx(i) = R->c.hx[i]; }
+    for (int j = 0; j < R->c.sy; j++) { mesh.y(j) = R->c.y[j]; mesh.hy(j) = R->c.hy[j]; }
+    for (int k = 0; k < R->c.sz; k++) { mesh.z(k) = R->c.z[k]; mesh.hz(k) = R->c.hz[k]; }
+    Int3 idmax{{R->c.sx, R->c.sy, R->c.sz}};
+    FalmIO::writeControlVolumeFile(path, mesh, idmax, R->c.gc);
+    mesh.release();
+    return 0;
 }
 
 /* one time step in the drivers' order (app/nedo/main.cpp:150-204;

@@ -61,3 +61,51 @@ def test_inflow_box_statistics():
     np.testing.assert_allclose(box.reshape(3, -1).std(axis=1), 0.05, rtol=1e-12)
     again = cases.inflow_box(24, 20, 0.05, nb=16, corr=8, seed=cases.INFLOW_SEED)
     np.testing.assert_array_equal(box, again)
+
+
+def test_index_file_host_entry_point(lib_built, tmp_path):
+    """falm_io_write_index_file renders FalmIO::writeIndexFile's object as
+    nlohmann::json's dump(2) does: sorted keys, two-space indent, no final
+    newline, and each double as its shortest round-trip digits laid out by the
+    library's rules (fixed point for decimal exponents -4 < n <= 15, ".0" on
+    integral values, else d.ddde+XX)."""
+    import json
+    from falm_b200 import api
+    snaps = [(100, 1.5, False), (200, 3.0, True), (300, 0.1 + 0.2, True), (7, 1e-05, False), (8, 0.0001, False)]
+    api.write_index_file(tmp_path / "a.json", (64, 32, 16), 2, snaps, dsize=4)
+    text = (tmp_path / "a.json").read_text()
+    obj = {"dataType": "float32", "global": [64, 32, 16], "guidePoint": 2,
+           "outputSteps": [dict({"step": s, "time": t}, **({"timeAvg": 1} if a else {})) for s, t, a in snaps],
+           "ranks": [{"offset": [0, 0, 0], "rank": 0, "voxel": [64, 32, 16]}], "variables": ["u", "v", "w", "p"]}
+    assert text == json.dumps(obj, indent=2, sort_keys=True)
+    # the cases where Python's float repr and the library's layout differ, by the rules above
+    cases_ = {1e15: "1e+15", 2.5e15: "2.5e+15", 123456789012345.6: "123456789012345.6", 1e16: "1e+16",
+              5e-324: "5e-324", 1.7976931348623157e308: "1.7976931348623157e+308", -2.0: "-2.0", 0.0: "0.0",
+              100.0: "100.0", 1e-4: "0.0001", 1.25e-5: "1.25e-05", 1e100: "1e+100"}
+    api.write_index_file(tmp_path / "b.json", (4, 4, 4), 2, [(q, v, False) for q, v in enumerate(cases_)])
+    got = [line.split(": ")[1] for line in (tmp_path / "b.json").read_text().splitlines() if '"time"' in line]
+    assert got == list(cases_.values())
+    # an empty snapshot list has no outputSteps key, as the reference's object
+    api.write_index_file(tmp_path / "c.json", (4, 4, 4), 2, [])
+    assert "outputSteps" not in json.loads((tmp_path / "c.json").read_text())
+    lib = _lib.load()
+    assert lib.falm_io_write_index_file(b"/nonexistent/dir/x.json", 4, 4, 4, 2, None, None, None, 0, 8) == 1
+    assert lib.falm_io_write_index_file(str(tmp_path / "d.json").encode(), 4, 4, 4, 2, None, None, None, 0, 2) == 1
+
+
+def test_control_volume_reader_host_entry_point(lib_built, tmp_path):
+    """falm_io_read_cv_file reads FalmIO::writeControlVolumeFile's text layout."""
+    from falm_b200 import api
+    g = cases.stretched_grid(10, 6, 5, 0.1)
+    with open(tmp_path / "g.cv", "w") as f:
+        f.write(f"{g.sx} {g.sy} {g.sz} {g.gc}\n")
+        for c, h in ((g.x, g.hx), (g.y, g.hy), (g.z, g.hz)):
+            for a, b in zip(c, h):
+                f.write("\t%.15e\t%.15e\n" % (a, b))
+    dims, x, hx, y, hy, z, hz = api.read_cv_file(tmp_path / "g.cv")
+    assert dims == (g.sx, g.sy, g.sz, g.gc)
+    for a, b in ((x, g.x), (hx, g.hx), (y, g.y), (hy, g.hy), (z, g.z), (hz, g.hz)):
+        np.testing.assert_allclose(a, b, rtol=1e-14, atol=0)
+    (tmp_path / "bad.cv").write_text("4 4\n")
+    with pytest.raises(_lib.FalmError):
+        api.read_cv_file(tmp_path / "bad.cv")

@@ -291,6 +291,19 @@ def test_plain_solvers_converged(oracle, lib_built, ls, relax):
     assert np.sqrt(oracle.L.oracle_normsq(ctypes.byref(cs.c), _p(r64), 1)) / g.n_interior <= 1.01e-5
 
 
+def test_eq_init_preconditioner_rules(lib_built):
+    """A plain solver needs no preconditioner (FALM_LS_EMPTY is accepted);
+    PBiCGStab needs SOR or Jacobi."""
+    from falm_b200._lib import FalmError
+    case = CASES["channel"]()
+    ctx = make_ctx(case)
+    ctx.eq_init(10, 1e-8, "Empty", 0, 1.0, ls="SOR", relax=1.5)
+    ctx.eq_init(10, 1e-8, "Empty", 0, 1.0, ls="Jacobi")
+    with pytest.raises(FalmError) as e:
+        ctx.eq_init(10, 1e-8, "Empty", 2, 1.0)
+    assert e.value.code == 1
+
+
 def test_step_with_plain_sor_solver(lib_built):
     """A whole step with the plain SOR Poisson solver: the step skips the
     BiCGStab start fused into the face-velocity kernel, runs the solver's

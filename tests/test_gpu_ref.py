@@ -161,3 +161,74 @@ def test_b200_step_matches_reference_converged(lib_built, oracle, name):
         err = compare(case, other, ref)
         assert err["u"] < 1e-9 and err["uu"] < 1e-9 and err["nut"] < 1e-9, err
         assert err["p"] < 1e-6, err
+
+
+@needs_ref
+@pytest.mark.parametrize("ls,relax", [("Jacobi", 1.0), ("SOR", 1.3)])
+def test_plain_solvers_match_reference(oracle, lib_built, ls, relax):
+    """FalmEq::Jacobi / FalmEq::SOR: the reference's own solver, the oracle's
+    restatement and the B200 solver in fixed-iteration mode (tol 0, maxit 6) on
+    the same operator, right-hand side and initial guess."""
+    from oracle.oracle import CaseStruct
+    from tests.helpers import dev, host, make_ctx
+    case = uniform_inflow_cases()["channel"]
+    g = case.grid
+    rng = np.random.default_rng(3)
+    b = np.zeros(g.n)
+    interior(b, g)[...] = rng.standard_normal(interior(b, g).shape)
+    x0 = 0.1 * rng.standard_normal(g.n)
+    ref, _ = ref_for(case)
+    ref.set("RHS", b)
+    ref.set("P", x0)
+    it_r, err_r = ref.plain_solve(ls, relax, 6, 0.0)
+    xr, rr = ref.get("P"), ref.get("RES")
+    ref.close()
+    cs = CaseStruct(case, use_inflow=False, maxit=6, tol=0.0)
+    m = oracle.setup(cs)
+    xo, ro = x0.copy(), np.zeros(g.n)
+    it_o, err_o = oracle.plain_solve(cs, ls, relax, m["A"], xo, b, ro)
+    ctx = make_ctx(case)
+    ctx.eq_init(6, 0.0, case.pc, case.pc_maxit, case.pc_relax, ls=ls, relax=relax)
+    xd, bd, rd = dev(ctx, x0), dev(ctx, b), ctx.field(1)
+    it, err, rc = ctx.solve(xd, bd, rd)
+    assert it_r == it_o == it == 6
+    assert rel_l2(interior(xo, g), interior(xr, g)) < 1e-12
+    assert rel_l2(interior(host(xd), g), interior(xr, g)) < 1e-12
+    assert rel_l2(interior(host(rd), g), interior(rr, g)) < 1e-10
+    assert err_o == pytest.approx(err_r, rel=1e-10) and err == pytest.approx(err_r, rel=1e-10)
+
+
+@needs_ref
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_output_files_match_reference(lib_built, tmp_path, precision):
+    """FalmIO byte for byte against the reference's own writers on the same
+    state: the drivers' u + p vector file (an FP32 context cast to FP64 on the
+    device, from a state exactly representable in FP32), the index file and the
+    control-volume file of a stretched grid."""
+    from falm_b200 import api
+    from tests.helpers import dev, make_ctx
+    case = cases.Case("stretched", cases.stretched_grid(20, 14, 12, 0.1), 0, Re=500.0, dt=0.01, tol=1e-10)
+    g = case.grid
+    st = random_state(case, seed=31)
+    u = st["u"].astype(np.float32).astype(np.float64)
+    p = st["p"].astype(np.float32).astype(np.float64)
+    ref, _ = ref_for(case)
+    ref.set("U", u)
+    ref.set("P", p)
+    ref.write_uvwp(tmp_path / "ref.bin", 1234, 18.51)
+    snaps = [(100, 1.5, False), (200, 0.01 * 200, True), (300, 0.1 + 0.2, True), (7, 1e-05, False), (8, 2.5e15, False)]
+    ref.write_index(tmp_path / "ref.json", snaps)
+    ref.write_cv(tmp_path / "ref.cv")
+    ref.close()
+    ctx = make_ctx(case, precision)
+    ud, pd = dev(ctx, u), dev(ctx, p)
+    ctx.write_vector_file(tmp_path / "b200.bin", [ud, pd], 1234, 18.51, as_fp64=True)
+    ctx.io_wait()
+    api.write_index_file(tmp_path / "b200.json", g.interior, g.gc, snaps)
+    ctx.write_cv_file(tmp_path / "b200.cv")
+    for name in ("bin", "json", "cv"):
+        assert (tmp_path / f"b200.{name}").read_bytes() == (tmp_path / f"ref.{name}").read_bytes(), name
+    dims, x, hx, y, hy, z, hz = api.read_cv_file(tmp_path / "ref.cv")
+    assert dims == (g.sx, g.sy, g.sz, g.gc)
+    for a, b in ((x, g.x), (hx, g.hx), (y, g.y), (hy, g.hy), (z, g.z), (hz, g.hz)):
+        np.testing.assert_allclose(a, b, rtol=1e-14, atol=0)

@@ -220,3 +220,35 @@ def test_step_tma_matches_row_kernels_multichunk(lib_built, monkeypatch, precisi
         {"u": 1e-5, "uu": 1e-5, "p": 1e-3, "nut": 1e-5}
     for k in outs[0]:
         assert rel_l2(outs[1][k], outs[0][k]) < tol[k], (k, rel_l2(outs[1][k], outs[0][k]))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_snapshots_and_time_average(lib_built, tmp_path, precision):
+    """Snapshot files queued during steps (more than the two staging buffers)
+    hold the fields of the step they were taken at, in the context's storage
+    type; TAvg over the steps equals the mean of the snapshots."""
+    from falm_b200 import api
+    from falm_b200.driver import Simulation
+    case = small_cases()["channel"]
+    sim = Simulation(case, precision)
+    ctx = sim.ctx
+    uavg, pavg = ctx.field(3), ctx.field(1)
+    kept = []
+    for q in range(5):
+        sim.step()
+        ctx.tavg(uavg, sim.u, q + 1)
+        ctx.tavg(pavg, sim.p, q + 1)
+        ctx.write_vector_file(tmp_path / f"s{q}.bin", [sim.u, sim.p], sim.it, sim.t())
+        kept.append((host(sim.u), host(sim.p)))
+    ctx.io_wait()
+    g = case.grid
+    for q in range(5):
+        hd, data = api.read_vector_file(tmp_path / f"s{q}.bin")
+        assert (hd["imax"], hd["jmax"], hd["kmax"], hd["ncol"], hd["gc"], hd["step"]) == (g.sx, g.sy, g.sz, 4, g.gc, q + 1)
+        assert hd["time"] == (q + 1) * case.dt and hd["dsize"] == (8 if precision == "fp64" else 4)
+        np.testing.assert_array_equal(data[:3].ravel().astype(np.float64), kept[q][0])
+        np.testing.assert_array_equal(data[3].ravel().astype(np.float64), kept[q][1])
+    tol = 1e-14 if precision == "fp64" else 1e-6
+    assert rel_l2(host(uavg), np.mean([k[0] for k in kept], axis=0)) < tol
+    assert rel_l2(host(pavg), np.mean([k[1] for k in kept], axis=0)) < tol
+    sim.close()
