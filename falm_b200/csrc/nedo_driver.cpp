@@ -1,7 +1,13 @@
 // nedo_driver: the time loop of app/nedo/main.cpp:150-204 written against the
 // reference's class surface (include/falm_b200.hpp), FP64.
 //
-//   nedo_driver <case.bin> <out.bin>
+//   nedo_driver <case.bin> <out.bin> [<prefix> <interval> <tavg_start>]
+//
+// With a prefix the loop also averages u and p from step tavg_start on and
+// writes the drivers' output (src/falm.h:433-475, app/nedo/main.cpp:199-200):
+// every `interval` steps the u + p vector file <prefix>_000000_<it> (and
+// <prefix>_tavg_000000_<it> of the averages while averaging), then
+// <prefix>.json (index) and <prefix>.cv (control volumes) at the end.
 //
 // case.bin (little endian): int32 sx sy sz gc steps maxit pc_maxit adv sgs bc
 // pc_type alm; float64 Re Cs dt tol pc_relax u_inlet; x y z hx hy hz; u (3N);
@@ -11,7 +17,9 @@
 // out.bin: u (3N), uu (3N), p (N), nut (N), then per step: it, err, divnorm, torque, thrust.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <string>
 #include <vector>
 #include "falm_b200.hpp"
 
@@ -31,8 +39,15 @@ struct Reader {
 }  // namespace
 
 int main(int argc, char **argv) {
-    if (argc < 3) {
-        fprintf(stderr, "usage: %s case.bin out.bin\n", argv[0]);
+    if (argc != 3 && argc != 6) {
+        fprintf(stderr, "usage: %s case.bin out.bin [prefix interval tavg_start]\n", argv[0]);
+        return 2;
+    }
+    const bool output = argc == 6;
+    const std::string prefix = output ? argv[3] : "";
+    const int interval = output ? atoi(argv[4]) : 0, tavg_start = output ? atoi(argv[5]) : 0;
+    if (output && interval < 1) {
+        fprintf(stderr, "nedo_driver: interval must be >= 1\n");
         return 2;
     }
     try {
@@ -87,6 +102,13 @@ int main(int argc, char **argv) {
         FILE *out = fopen(argv[2], "wb");
         if (!out) throw Error(1, "cannot open output");
         std::vector<double> stats;
+        Matrix<Real> utavg(shape, 3, "utavg"), ptavg(shape, 1, "ptavg");
+        std::vector<FalmSnapshotInfo> slices;
+        auto name = [&](const std::string &pre, int it) {
+            char buf[64];
+            snprintf(buf, sizeof(buf), "_%06d_%010d", 0, it);
+            return pre + buf;
+        };
         for (int it = 1; it <= steps; it++) {
             const Real t = dt * it;
             // main_loop, app/nedo/main.cpp:150-204 (race-free pseudo-velocity: un = u_previous, ua separate)
@@ -109,6 +131,24 @@ int main(int argc, char **argv) {
             stats.push_back(divnorm);
             stats.push_back(alm_on ? alm.torque[0] : 0.0);
             stats.push_back(alm_on ? alm.thrust[0] : 0.0);
+            if (output) {
+                // FalmSolver::TAvg, then FalmSolver::outputUVWP (src/falm.h:433-475)
+                const bool averaging = it >= tavg_start;
+                if (averaging) {
+                    TAvg(ctx, utavg, u, it - tavg_start + 1);
+                    TAvg(ctx, ptavg, p, it - tavg_start + 1);
+                }
+                if (it % interval == 0) {
+                    FalmIO::writeUVWP(name(prefix, it), ctx, u, p, it, t);
+                    if (averaging) FalmIO::writeUVWP(name(prefix + "_tavg", it), ctx, utavg, ptavg, it, t);
+                    slices.push_back(FalmSnapshotInfo{(size_t)it, t, averaging});
+                }
+            }
+        }
+        if (output) {
+            FalmIO::wait(ctx);
+            FalmIO::writeIndexFile(prefix + ".json", ctx, slices);
+            FalmIO::writeControlVolumeFile(prefix + ".cv", ctx);
         }
         u.sync_to_host(); uu.sync_to_host(); p.sync_to_host(); nut.sync_to_host();
         fwrite(u.host.ptr, sizeof(double), 3 * N, out);

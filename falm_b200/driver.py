@@ -32,9 +32,49 @@ class Simulation:
         return self.it * self.case.dt
 
     def step(self):
-        """one main_loop iteration; returns the step statistics"""
+        """one main_loop iteration (then TAvg and outputUVWP, app/nedo/main.cpp:199-200,
+        when output is enabled); returns the step statistics"""
         self.it += 1
-        return self.ctx.step(self.u, self.uu, self.p, self.nut, self.ff, self.case.dt, self.t())
+        st = self.ctx.step(self.u, self.uu, self.p, self.nut, self.ff, self.case.dt, self.t())
+        out = getattr(self, "_out", None)
+        if out is not None:
+            self._output_step(out)
+        return st
+
+    def enable_output(self, prefix, interval, start=0, end=None, tavg_start=None, tavg_end=None, as_fp64=False):
+        """FalmSolver's output schedule (src/falm.h:83-98, 433-475): after step it,
+        TAvg of u and p while tavg_start <= it <= tavg_end, and when
+        start <= it <= end and it % interval == 0 the u + p vector file
+        <prefix>_000000_<it> (plus <prefix>_tavg_000000_<it> while averaging);
+        finish_output() writes <prefix>.json and <prefix>.cv"""
+        ctx = self.ctx
+        self._out = {"prefix": str(prefix), "interval": int(interval), "start": start,
+                     "end": end if end is not None else 1 << 62,
+                     "tstart": tavg_start, "tend": tavg_end if tavg_end is not None else 1 << 62,
+                     "fp64": as_fp64, "slices": [],
+                     "uavg": ctx.field(3) if tavg_start is not None else None,
+                     "pavg": ctx.field(1) if tavg_start is not None else None}
+
+    def _output_step(self, o):
+        it, ctx = self.it, self.ctx
+        averaging = o["tstart"] is not None and o["tstart"] <= it <= o["tend"]
+        if averaging:
+            ctx.tavg(o["uavg"], self.u, it - o["tstart"] + 1)
+            ctx.tavg(o["pavg"], self.p, it - o["tstart"] + 1)
+        if o["start"] <= it <= o["end"] and it % o["interval"] == 0:
+            ctx.write_vector_file(f"{o['prefix']}_{0:06d}_{it:010d}", [self.u, self.p], it, self.t(), o["fp64"])
+            if averaging:
+                ctx.write_vector_file(f"{o['prefix']}_tavg_{0:06d}_{it:010d}", [o["uavg"], o["pavg"]], it, self.t(), o["fp64"])
+            o["slices"].append((it, self.t(), averaging))
+
+    def finish_output(self):
+        """wait for the queued snapshots, then the index and control-volume files"""
+        from .api import write_index_file
+        o = self._out
+        self.ctx.io_wait()
+        dsize = 8 if (o["fp64"] or self.ctx.precision == "fp64") else 4
+        write_index_file(o["prefix"] + ".json", self.case.grid.interior, self.case.grid.gc, o["slices"], dsize)
+        self.ctx.write_cv_file(o["prefix"] + ".cv")
 
     def snapshot(self):
         """keep a device copy of the state (fields and step counter) for restore()"""

@@ -14,6 +14,10 @@
  *    arguments are accepted and ignored (the library sizes its own launches).
  *  - The reference prints error codes and continues (src/error.h:20-26); here
  *    every call returns the falm_status and a failing call throws Falm::Error.
+ *  - FalmIO takes the Context where the reference takes CPM, writes vector
+ *    files from the device columns of a Matrix on the context's writer thread
+ *    (FalmIO::wait before reading them), and FalmSolver::TAvg is the free
+ *    function TAvg.
  */
 #ifndef FALM_B200_HPP
 #define FALM_B200_HPP
@@ -213,6 +217,64 @@ struct FalmMV {
         cudaDeviceSynchronize();
     }
 };
+
+/* FalmSnapshotInfo (src/typedef.h:35-39) */
+struct FalmSnapshotInfo {
+    size_t step;
+    double time;
+    bool tavg;
+};
+
+/* FalmIO (src/FalmIO.h) */
+struct FalmIO {
+    /* writeVectorFile (src/FalmIO.h:69-97) of the columns of v */
+    template <typename Real>
+    static void writeVectorFile(const std::string &fpath, Context &c, Matrix<Real> &v, size_t step, double time) {
+        const void *f[1] = {v.dev.ptr};
+        const int nc[1] = {(int)v.shape[1]};
+        check(falm_io_write_vector_file(c.h, fpath.c_str(), f, nc, 1, step, time, 0, nullptr), c.h, "FalmIO::writeVectorFile");
+    }
+    /* the drivers' uvwp file (src/falm.h:446-460): the columns of u, then p */
+    template <typename Real>
+    static void writeUVWP(const std::string &fpath, Context &c, Matrix<Real> &u, Matrix<Real> &p, size_t step, double time) {
+        const void *f[2] = {u.dev.ptr, p.dev.ptr};
+        const int nc[2] = {(int)u.shape[1], (int)p.shape[1]};
+        check(falm_io_write_vector_file(c.h, fpath.c_str(), f, nc, 2, step, time, 0, nullptr), c.h, "FalmIO::writeUVWP");
+    }
+    static void wait(Context &c) { check(falm_io_wait(c.h), c.h, "FalmIO::wait"); }
+    /* writeIndexFile (src/FalmIO.h:25-67) */
+    static void writeIndexFile(const std::string &fpath, Context &c, const std::vector<FalmSnapshotInfo> &list, int dsize = 8) {
+        std::vector<unsigned long long> steps;
+        std::vector<double> times;
+        std::vector<int> tavg;
+        for (const auto &s : list) { steps.push_back(s.step); times.push_back(s.time); tavg.push_back(s.tavg ? 1 : 0); }
+        const Int3 &sh = c.cpm.global.shape;
+        const Int gc = c.cpm.gc;
+        check(falm_io_write_index_file(fpath.c_str(), sh[0] - 2 * gc, sh[1] - 2 * gc, sh[2] - 2 * gc, gc, steps.data(), times.data(),
+                                       tavg.data(), (int)list.size(), dsize),
+              c.h, "FalmIO::writeIndexFile");
+    }
+    /* writeControlVolumeFile (src/FalmIO.h:118-135) of the context's grid */
+    static void writeControlVolumeFile(const std::string &path, Context &c) {
+        check(falm_io_write_cv_file(c.h, path.c_str()), c.h, "FalmIO::writeControlVolumeFile");
+    }
+    /* readControlVolumeFile (src/FalmIO.h:99-116): idmax = {sx, sy, sz}, gc and the six tables */
+    static void readControlVolumeFile(const std::string &path, std::vector<double> xyz[3], std::vector<double> h[3], Int3 &idmax, Int &gc) {
+        int d[4];
+        check(falm_io_read_cv_file(path.c_str(), d, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr), nullptr,
+              "FalmIO::readControlVolumeFile");
+        for (int q = 0; q < 3; q++) { idmax[q] = d[q]; xyz[q].assign(d[q], 0.0); h[q].assign(d[q], 0.0); }
+        gc = d[3];
+        check(falm_io_read_cv_file(path.c_str(), d, xyz[0].data(), h[0].data(), xyz[1].data(), h[1].data(), xyz[2].data(), h[2].data()),
+              nullptr, "FalmIO::readControlVolumeFile");
+    }
+};
+
+/* FalmSolver::TAvg (src/falm.h:433-444): avg = (1 - 1/count) avg + f / count */
+template <typename Real>
+void TAvg(Context &c, Matrix<Real> &avg, Matrix<Real> &f, Int count) {
+    check(falm_tavg(c.h, avg.dev.ptr, f.dev.ptr, (int)f.shape[1], count, nullptr), c.h, "TAvg");
+}
 
 /* application boundary routines (app/nedo/bc.h, app/windtunnel/bc.h, app/lid3d/bc.h) */
 template <typename Real>

@@ -67,3 +67,40 @@ def test_cpp_driver_matches_oracle(oracle, lib_built, tmp_path, name):
         assert stats[q, 0] == rs[q]["it"]
         if case.alm is not None:
             assert stats[q, 3] == pytest.approx(rs[q]["torque"][0], rel=1e-10)
+
+
+def test_cpp_driver_output_files(lib_built, tmp_path):
+    """The driver's output path through the shim's FalmIO and TAvg (every step,
+    averaging from step 3): the u + p vector files, the averaged files, the
+    index file and the control-volume file. The last snapshot holds the final
+    fields; the last averaged file is the mean of the snapshots of steps 3..6."""
+    import json
+    from falm_b200 import api
+    case = cases.small_channel(32, 20, 20, intensity=0.0)
+    steps = 6
+    cpath, opath = str(tmp_path / "case.bin"), str(tmp_path / "out.bin")
+    write_case(cpath, case, steps, 6, 0.0)
+    prefix = str(tmp_path / "run")
+    r = subprocess.run([DRIVER, cpath, opath, prefix, "1", "3"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    n, g = case.grid.n, case.grid
+    raw = np.fromfile(opath, dtype="<f8")
+    u_end, p_end = raw[:3 * n], raw[6 * n:7 * n]
+    names = sorted(os.listdir(tmp_path))
+    assert [x for x in names if x.startswith("run_0")] == [f"run_000000_{it:010d}" for it in range(1, 7)]
+    assert [x for x in names if x.startswith("run_tavg")] == [f"run_tavg_000000_{it:010d}" for it in range(3, 7)]
+    snaps = {}
+    for it in range(1, 7):
+        hd, data = api.read_vector_file(tmp_path / f"run_000000_{it:010d}")
+        assert (hd["ncol"], hd["step"], hd["dsize"], hd["time"]) == (4, it, 8, it * case.dt)
+        snaps[it] = data
+    np.testing.assert_array_equal(snaps[6][:3].ravel(), u_end)
+    np.testing.assert_array_equal(snaps[6][3].ravel(), p_end)
+    _, avg6 = api.read_vector_file(tmp_path / "run_tavg_000000_0000000006")
+    mean = np.mean([snaps[it] for it in range(3, 7)], axis=0)
+    assert rel_l2(avg6[:3].ravel(), mean[:3].ravel()) < 1e-13
+    assert rel_l2(avg6[3].ravel(), mean[3].ravel()) < 1e-13
+    idx = json.loads((tmp_path / "run.json").read_text())
+    assert [(s["step"], s.get("timeAvg", 0)) for s in idx["outputSteps"]] == [(1, 0), (2, 0), (3, 1), (4, 1), (5, 1), (6, 1)]
+    assert idx["global"] == list(g.interior) and idx["guidePoint"] == g.gc
+    assert api.read_cv_file(tmp_path / "run.cv")[0] == (g.sx, g.sy, g.sz, g.gc)

@@ -252,3 +252,25 @@ def test_snapshots_and_time_average(lib_built, tmp_path, precision):
     assert rel_l2(host(uavg), np.mean([k[0] for k in kept], axis=0)) < tol
     assert rel_l2(host(pavg), np.mean([k[1] for k in kept], axis=0)) < tol
     sim.close()
+
+
+def test_driver_output_schedule(lib_built, tmp_path):
+    """Simulation.enable_output: the files of FalmSolver's schedule (every second
+    step from step 2 to 6, averaging over steps 3..5) and the index entries."""
+    import json
+    from falm_b200 import api
+    from falm_b200.driver import Simulation
+    case = small_cases()["channel"]
+    sim = Simulation(case, "mixed")
+    sim.enable_output(tmp_path / "o", 2, start=2, end=6, tavg_start=3, tavg_end=5, as_fp64=True)
+    for _ in range(7):
+        sim.step()
+    sim.finish_output()
+    names = sorted(x for x in __import__("os").listdir(tmp_path) if x.startswith("o_"))
+    assert names == ["o_000000_0000000002", "o_000000_0000000004", "o_000000_0000000006", "o_tavg_000000_0000000004"]
+    idx = json.loads((tmp_path / "o.json").read_text())
+    assert [(s["step"], s.get("timeAvg", 0)) for s in idx["outputSteps"]] == [(2, 0), (4, 1), (6, 0)]
+    assert idx["dataType"] == "float64"
+    hd, _ = api.read_vector_file(tmp_path / "o_000000_0000000006")
+    assert hd["dsize"] == 8 and hd["step"] == 6
+    sim.close()
