@@ -98,6 +98,7 @@ SIGNATURES = {
     "falm_io_write_index_file": [ctypes.c_char_p, I, I, I, I, ctypes.POINTER(ctypes.c_ulonglong), c_double_p, c_int_p, I, I],
     "falm_io_write_cv_file": [V, ctypes.c_char_p],
     "falm_io_read_cv_file": [ctypes.c_char_p, c_int_p, c_double_p, c_double_p, c_double_p, c_double_p, c_double_p, c_double_p],
+    "falm_mesh_build": [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, I],
     "falm_profile_enable": [V, I],
     "falm_profile_read": [V, c_double_p, ctypes.POINTER(ctypes.c_longlong), I, I],
 }

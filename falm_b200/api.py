@@ -280,6 +280,13 @@ def read_cv_file(path):
     return tuple(dims), arr[0], arr[1], arr[2], arr[3], arr[4], arr[5]
 
 
+def build_mesh(cvcenter, meshpath, outputfile, gc=2):
+    """Mesher::build_mesh (src/mesher/mesher.hpp:12-260): a control-volume file from node coordinates"""
+    rc = L.load().falm_mesh_build(cvcenter.encode(), str(meshpath).encode(), str(outputfile).encode(), gc)
+    if rc != 0:
+        raise L.FalmError(rc, "build_mesh")
+
+
 def read_vector_file(path):
     """a FalmIO vector file: (header dict, array [ncol, kmax, jmax, imax])"""
     with open(path, "rb") as f:

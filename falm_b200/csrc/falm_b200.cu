@@ -6,6 +6,7 @@
 // tables; the caller owns the fields.  Every call is asynchronous on the given
 // stream except those that return scalars on the host.
 #include <vector>
+#include <fstream>
 #include <string>
 #include <cstring>
 #include <cstdio>
@@ -1376,6 +1377,92 @@ int falm_io_write_cv_file(falm_ctx *ctx, const char *path) {
     for (int d = 0; d < 3; d++)
         for (size_t q = 0; q < c[d]->size(); q++) fprintf(f, "\t%.15e\t%.15e\n", (*c[d])[q], (*h[d])[q]);
     return fclose(f) == 0 ? FALM_OK : fail(ctx, FALM_ERR_ARG, "io: control-volume write");
+}
+
+// Mesher::build_mesh (src/mesher/mesher.hpp:12-260): control volumes from node
+// coordinates.  Each of meshpath/{x,y,z}.txt holds a count, then one
+// coordinate per line; meshpath/mesh.json names them "node" points.
+//  - "cell": the nodes are the cell faces.  A cell's width is the node
+//    spacing and its centre the midpoint; gc guide cells are extrapolated
+//    linearly (constant widths when an axis has fewer than 3 nodes).
+//  - "innerNode": the nodes are the centres of the interior cells plus one
+//    guide cell on each side.  Widths are half the distance between the two
+//    neighbours, the end ones extrapolated.  The upper z guide widths repeat
+//    the last one where the x and y ones extrapolate linearly, as the
+//    reference computes them.
+// Guide-cell centres step outwards by the mean of adjacent widths.
+int falm_mesh_build(const char *cvcenter, const char *meshpath, const char *outputfile, int gc) {
+    if (!cvcenter || !meshpath || !outputfile || gc < 1) return FALM_ERR_ARG;
+    const std::string dir(meshpath);
+    std::string kind;
+    {
+        FILE *f = fopen((dir + "/mesh.json").c_str(), "rb");
+        if (!f) return FALM_ERR_ARG;
+        std::string js;
+        char buf[4096];
+        size_t got;
+        while ((got = fread(buf, 1, sizeof(buf), f)) > 0) js.append(buf, got);
+        fclose(f);
+        size_t p = js.find("\"coordinatePoint\"");
+        if (p != std::string::npos) p = js.find(':', p);
+        if (p != std::string::npos) p = js.find('"', p);
+        const size_t q = p == std::string::npos ? p : js.find('"', p + 1);
+        if (q == std::string::npos) return FALM_ERR_ARG;
+        kind = js.substr(p + 1, q - p - 1);
+    }
+    const std::string mode(cvcenter);
+    if (kind != "node" || (mode != "cell" && mode != "innerNode")) return FALM_ERR_ARG;
+    auto read_nodes = [&](const char *name, std::vector<double> &v) -> bool {
+        std::ifstream in(dir + "/" + name);
+        std::string line;
+        if (!std::getline(in, line)) return false;
+        int n = 0;
+        try { n = std::stoi(line); } catch (...) { return false; }
+        if (n < 1) return false;
+        v.resize(n);
+        for (int q = 0; q < n; q++) {
+            if (!std::getline(in, line)) return false;
+            try { v[q] = std::stod(line); } catch (...) { return false; }
+        }
+        return true;
+    };
+    std::vector<double> nodes[3], c[3], h[3];
+    const char *names[3] = {"x.txt", "y.txt", "z.txt"};
+    for (int d = 0; d < 3; d++)
+        if (!read_nodes(names[d], nodes[d])) return FALM_ERR_ARG;
+    for (int d = 0; d < 3; d++) {
+        const std::vector<double> &t = nodes[d];
+        std::vector<double> &x = c[d], &w = h[d];
+        const int n = (int)t.size();
+        int m, g;
+        if (mode == "innerNode") {
+            g = gc - 1;
+            m = n + 2 * g;
+            if (m < 3) return FALM_ERR_ARG;
+            x.assign(m, 0.0); w.assign(m, 0.0);
+            for (int i = g; i < m - g; i++) x[i] = t[i - g];
+            for (int i = g + 1; i < m - g - 1; i++) w[i] = 0.5 * (x[i + 1] - x[i - 1]);
+            for (int i = g; i >= 0; i--) w[i] = 2 * w[i + 1] - w[i + 2];
+            for (int i = m - g - 1; i < m; i++) w[i] = d < 2 ? 2 * w[i - 1] - w[i - 2] : w[i - 1];
+        } else {
+            g = gc;
+            m = n - 1 + 2 * g;
+            if (n < 2) return FALM_ERR_ARG;
+            x.assign(m, 0.0); w.assign(m, 0.0);
+            for (int i = g; i < m - g; i++) w[i] = t[i - g + 1] - t[i - g];
+            for (int i = g - 1; i >= 0; i--) w[i] = n >= 3 ? 2 * w[i + 1] - w[i + 2] : w[i + 1];
+            for (int i = m - g; i < m; i++) w[i] = n >= 3 ? 2 * w[i - 1] - w[i - 2] : w[i - 1];
+            for (int i = g; i < m - g; i++) x[i] = t[i - g] + 0.5 * w[i];
+        }
+        for (int i = g - 1; i >= 0; i--) x[i] = x[i + 1] - 0.5 * (w[i] + w[i + 1]);
+        for (int i = m - g; i < m; i++) x[i] = x[i - 1] + 0.5 * (w[i] + w[i - 1]);
+    }
+    FILE *f = fopen(outputfile, "w");
+    if (!f) return FALM_ERR_ARG;
+    fprintf(f, "%d %d %d %d\n", (int)c[0].size(), (int)c[1].size(), (int)c[2].size(), gc);
+    for (int d = 0; d < 3; d++)
+        for (size_t q = 0; q < c[d].size(); q++) fprintf(f, "\t%.15e\t%.15e\n", c[d][q], h[d][q]);
+    return fclose(f) == 0 ? FALM_OK : FALM_ERR_ARG;
 }
 
 int falm_io_read_cv_file(const char *path, int dims[4], double *x, double *hx, double *y, double *hy, double *z, double *hz) {

@@ -240,6 +240,12 @@ int falm_io_write_index_file(const char *path, int nx, int ny, int nz, int gc, c
    (:99-116): dims = {sx, sy, sz, gc}; with all six arrays NULL only dims is read. */
 int falm_io_write_cv_file(falm_ctx *ctx, const char *path);
 int falm_io_read_cv_file(const char *path, int dims[4], double *x, double *hx, double *y, double *hy, double *z, double *hz);
+/* Mesher::build_mesh (src/mesher/mesher.hpp:12-260), host only: the control-volume file
+   `outputfile` (gc guide cells) from the node coordinates in meshpath/{x,y,z}.txt (a count,
+   then one value per line) with meshpath/mesh.json {"coordinatePoint": "node"}; cvcenter
+   "cell" (the nodes are cell faces) or "innerNode" (the nodes are cell centres, one guide
+   cell included on each side). */
+int falm_mesh_build(const char *cvcenter, const char *meshpath, const char *outputfile, int gc);
 
 /* ---------------- discrete adjoint of the step ---------------------------------------------- */
 /* No reference counterpart.  Adjoint of falm_step for FP64 contexts (Upwind3/UTOPIA/KK advection,

@@ -27,6 +27,7 @@
 #include "windtunnel/bcdevcall.h"
 #include "lid3d/bcdev.h"
 #include "FalmIO.h"
+#include "mesher/mesher.hpp"
 #include "falm_oracle.h"
 
 using namespace Falm;
@@ -406,6 +407,12 @@ int ref_write_cv(void *h, const char *path) {
     Int3 idmax{{R->c.sx, R->c.sy, R->c.sz}};
     FalmIO::writeControlVolumeFile(path, mesh, idmax, R->c.gc);
     mesh.release();
+    return 0;
+}
+
+/* Mesher::build_mesh (host only) */
+int ref_build_mesh(const char *cvcenter, const char *meshpath, const char *outputfile, int gc) {
+    Mesher::build_mesh(cvcenter, meshpath, outputfile, gc);
     return 0;
 }
 

@@ -109,3 +109,47 @@ def test_control_volume_reader_host_entry_point(lib_built, tmp_path):
     (tmp_path / "bad.cv").write_text("4 4\n")
     with pytest.raises(_lib.FalmError):
         api.read_cv_file(tmp_path / "bad.cv")
+
+
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libfalmref.so")
+
+
+def _node_files(d, xs, ys, zs):
+    os.makedirs(d, exist_ok=True)
+    with open(os.path.join(d, "mesh.json"), "w") as f:
+        f.write('{\n    "coordinatePoint":"node"\n}')
+    for name, v in (("x.txt", xs), ("y.txt", ys), ("z.txt", zs)):
+        with open(os.path.join(d, name), "w") as f:
+            f.write(f"{len(v)}\n" + "".join("%.15e\n" % a for a in v))
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SO), reason="oracle/_ref not built (needs the reference sources)")
+@pytest.mark.parametrize("mode", ["cell", "innerNode"])
+def test_mesher_matches_reference(lib_built, tmp_path, mode):
+    """falm_mesh_build against the reference's own Mesher::build_mesh (compiled
+    into oracle/_ref, host code only): byte-identical control-volume files for
+    stretched node coordinates, with a 2-node axis for the constant-width branch
+    of "cell"; the file reads back through falm_io_read_cv_file."""
+    from falm_b200 import api
+    xs = np.cumsum(np.concatenate([[-1.0], 0.05 * 1.07 ** np.arange(30)]))
+    ys = np.linspace(-0.5, 0.7, 13)
+    zs = np.array([0.0, 0.25]) if mode == "cell" else np.cumsum(np.concatenate([[0.0], 0.02 * 1.1 ** np.arange(9)]))
+    src = str(tmp_path / "mesh")
+    _node_files(src, xs, ys, zs)
+    ref = ctypes.CDLL(REF_SO)
+    ref.ref_build_mesh.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]
+    for gc in (2, 3):
+        a, b = str(tmp_path / f"ref{gc}.cv"), str(tmp_path / f"b200{gc}.cv")
+        assert ref.ref_build_mesh(mode.encode(), src.encode(), a.encode(), gc) == 0
+        api.build_mesh(mode, src, b, gc)
+        assert open(a, "rb").read() == open(b, "rb").read()
+        dims, x, hx, y, hy, z, hz = api.read_cv_file(b)
+        assert dims[3] == gc
+        if mode == "cell":
+            assert dims[:3] == (len(xs) - 1 + 2 * gc, len(ys) - 1 + 2 * gc, len(zs) - 1 + 2 * gc)
+            np.testing.assert_allclose(hx[gc:-gc], np.diff(xs), rtol=1e-14)
+        else:
+            assert dims[:3] == (len(xs) + 2 * (gc - 1), len(ys) + 2 * (gc - 1), len(zs) + 2 * (gc - 1))
+            np.testing.assert_allclose(x[gc - 1:len(x) - gc + 1], xs, rtol=0, atol=1e-15)
+    with pytest.raises(_lib.FalmError):
+        api.build_mesh("face", src, str(tmp_path / "x.cv"), 2)
