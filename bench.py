@@ -49,6 +49,10 @@ def parse():
                     help="instead of the benchmark: time-averaged rotor power and thrust over STEPS steps, "
                          "mixed against FP64, at --power-cfl")
     ap.add_argument("--power-cfl", type=float, default=0.05)
+    ap.add_argument("--configs", action="store_true",
+                    help="instead of the benchmark: the step on the reference's cavity 64^3, channel "
+                         "256x128x128 and 512x256x256 configurations, timed for the B200 step, the "
+                         "reference's CUDA step and the CPU oracle")
     return ap.parse_args()
 
 
@@ -342,6 +346,104 @@ def run_ours(args, rank, world, local):
     return case, out
 
 
+def run_configs(args):
+    """The step on the reference's configurations, each timed three ways on this
+    box: the B200 step (FP64 and mixed; fields in HBM, CUDA events on the
+    stream), the reference's own CUDA step (FP64, uniform inflow, wall clock
+    between synchronisations) and the CPU oracle (FP64, all host threads, a
+    bounded number of steps after one untimed step). Every timed run starts 3
+    steps in and returns to that state every RESTART steps."""
+    import tempfile
+    import numpy as np
+    import torch
+    from falm_b200 import cases
+    from falm_b200.driver import Simulation
+    from oracle.oracle import CaseStruct, Oracle, RefStep, build
+    # (name, case, timed steps, CPU oracle steps, the reference's input: the
+    # channels with uniform inflow, as the reference has no seeded inflow)
+    defs = [("C1 cavity 64^3 (Re 1000, dt 1e-3, tol 1e-8)", cases.cavity(64), 100, 100, None),
+            ("C2 channel 256x128x128 + rotor (5% inflow, CFL 0.3, tol 1e-8)", cases.channel(256, 128, 128).with_inflow(), 100, 3,
+             cases.channel(256, 128, 128, intensity=0.0)),
+            ("C3 channel 512x256x256 + rotor (5% inflow, CFL 0.3, tol 1e-6)", cases.channel_large().with_inflow(), 100, 0,
+             cases.channel(512, 256, 256, intensity=0.0, tol=1e-6, name="channel_large_uniform"))]
+    ref_ok = os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libfalmref.so"))
+    build()
+    lines = []
+    for name, case, K, kcpu, uniform in defs:
+        n = case.grid.n_interior
+        row = {"config": name, "cells": n, "steps": K, "unit": UNIT}
+        runs = [("fp64", case), ("mixed", case)]
+        if uniform is not None:
+            runs += [("fp64_uniform_inflow", uniform), ("mixed_uniform_inflow", uniform)]
+        for key, c in runs:
+            prec = "fp64" if key.startswith("fp64") else "mixed"
+            sim = Simulation(c, prec)
+            for _ in range(3):
+                sim.step()
+            sim.snapshot()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            its = []
+            e0.record()
+            for q in range(K):
+                if q and q % RESTART == 0:
+                    sim.restore()
+                its.append(sim.step()["it"])
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / K
+            row[key] = {"value": n / ms / 1e3, "ms_per_step": ms, "its_mean": sum(its) / K}
+            sim.close()
+            del sim
+            torch.cuda.empty_cache()
+        row["mixed_over_fp64"] = row["fp64"]["ms_per_step"] / row["mixed"]["ms_per_step"]
+        if ref_ok:
+            ref = RefStep(CaseStruct(uniform or case, use_inflow=False), tempfile.mkdtemp(prefix="falmref_"))
+            st = cases.initial_state(uniform or case)
+            ref.set("U", st["u"])
+            ref.op("UTOUU")
+            ref.op("SGS")
+            it = 0
+            for _ in range(3):
+                it += 1
+                ref.step(it * case.dt)
+            snap = {k: ref.get(k) for k in ("U", "UU", "P", "NUT")}
+            it0, el, its = it, 0.0, []
+            for q0 in range(0, K, RESTART):
+                if q0:
+                    for k, v in snap.items():
+                        ref.set(k, v)
+                    it = it0
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                for _ in range(min(RESTART, K - q0)):
+                    it += 1
+                    its.append(ref.step(it * case.dt)["it"])
+                torch.cuda.synchronize()
+                el += time.perf_counter() - t0
+            ref.close()
+            ms = 1e3 * el / K
+            row["reference_gpu"] = {"value": n / ms / 1e3, "ms_per_step": ms, "its_mean": sum(its) / K}
+            mine = row["mixed_uniform_inflow" if uniform is not None else "mixed"]
+            row["mixed_over_reference"] = ms / mine["ms_per_step"]
+        if kcpu:
+            O = Oracle()
+            cs = CaseStruct(case)
+            m = O.setup(cs)
+            st = cases.initial_state(case)
+            O.init_state(cs, m, st)
+            O.step(cs, st, m, case.dt)
+            t0 = time.perf_counter()
+            for q in range(kcpu):
+                O.step(cs, st, m, (q + 2) * case.dt)
+            el = time.perf_counter() - t0
+            row["cpu_oracle"] = {"value": n * kcpu / el / 1e6, "ms_per_step": 1e3 * el / kcpu, "cores": O.threads(),
+                                 "steps": kcpu}
+        lines.append(row)
+        print(json.dumps(row), flush=True)
+    return lines
+
+
 def power_run(args):
     """Time-averaged rotor power and thrust over a long run, mixed precision
     against FP64 (the FP64 step matches the CPU oracle step for step), on the
@@ -528,6 +630,9 @@ def main():
     args = parse()
     if args.power_run:
         print(json.dumps(power_run(args)), flush=True)
+        return
+    if args.configs:
+        run_configs(args)
         return
     rank, world, local = dist_setup(args)
     from falm_b200 import cases as _c
