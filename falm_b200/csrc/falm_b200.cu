@@ -735,6 +735,22 @@ int pseudo_u_t(falm_ctx *ctx, const T *un, const T *u, const T *uu, T *ua, const
     CUtensorMap mu, muu, mnut;
     if (!ctx->no_tma && make_map(ctx, &mu, u, 3, L::BX, L::BY) && make_map(ctx, &muu, uu, 3, L::BX, L::BY) &&
         make_map(ctx, &mnut, nut, 1, L::BX, L::BY)) {
+        // FP32 with a 4th-order scheme and an even interior width: the x-pair kernel
+        if constexpr (sizeof(T) == 4) {
+            if (!ctx->pu_v1 && (g.nx & 1) == 0 &&
+                (ctx->adv == FALM_ADV_UPWIND3 || ctx->adv == FALM_ADV_UTOPIA || ctx->adv == FALM_ADV_KK)) {
+                auto k2 = k_pseudo_u_tma2<NS, FALM_ADV_UPWIND3>;
+                if (ctx->adv == FALM_ADV_UTOPIA) k2 = k_pseudo_u_tma2<NS, FALM_ADV_UTOPIA>;
+                if (ctx->adv == FALM_ADV_KK) k2 = k_pseudo_u_tma2<NS, FALM_ADV_KK>;
+                const int bx = (g.nx + L::TX - 1) / L::TX, by = (g.ny + L::TY - 1) / L::TY;
+                const int kc = chunk_len(ctx, (long long)bx * by, g.nz, resident_per_sm(k2, 128, L::SMEM), 64, 4);
+                cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
+                dim3 grid(bx, by, (g.nz + kc - 1) / kc);
+                LAUNCH(FALM_K_PSEUDO_U, st, k2<<<grid, 128, L::SMEM, st>>>(g, kc, mview<T>(ctx), mu, muu, mnut, un, un == u ? 1 : 0, ua, ff, af,
+                                                                         (T)(1.0 / ctx->Re), (T)dt, ctx->kerr));
+                return FALM_OK;
+            }
+        }
         auto kern = k_pseudo_u_tma<T, NS, FALM_ADV_KK>;
         switch (ctx->adv) {
             case FALM_ADV_UPWIND1: kern = k_pseudo_u_tma<T, NS, FALM_ADV_UPWIND1>; break;
@@ -976,6 +992,8 @@ int falm_create(const falm_grid *grid, int precision, falm_ctx **out) {
         ctx->no_tma = (e && e[0] == '1') ? 1 : 0;
         const char *v = getenv("FALM_B200_SOR_V1");
         ctx->sor_v1 = (v && v[0] == '1') ? 1 : 0;
+        const char *pv = getenv("FALM_B200_PU_V1");
+        ctx->pu_v1 = (pv && pv[0] == '1') ? 1 : 0;
         const char *c = getenv("FALM_B200_CHECK");
         ctx->check_sync = (c && c[0] == '1') ? 1 : 0;
     }

@@ -162,6 +162,7 @@ struct falm_ctx {
     int *kerr;                              // device error word of bounded waits (FALM_ERR_TIMEOUT)
     int no_tma;                             // force the row kernels (tests, fallback)
     int sor_v1;                             // FP32 blocked SOR on the 32 x 8 tile kernel (tests)
+    int pu_v1;                              // FP32 pseudo-velocity on the one-cell-per-thread kernel (tests)
     int check_sync;                         // synchronise after every launch (fault location)
     std::string *last_error;
     fb::IoWriter *io;                       // snapshot writer (falm_io.cuh), created on first use

@@ -22,6 +22,7 @@ __device__ __forceinline__ double2 mul2(double2 a, double2 b) { return make_doub
 __device__ __forceinline__ double2 add2(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 // a - b, one rounding per lane
 template <typename V2> __device__ __forceinline__ V2 sub2(V2 a, V2 b) { return add2(a, mk2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 fabs2(float2 a) { return make_float2(fabsf(a.x), fabsf(a.y)); }
 
 // lane-wise conversion of a pair
 template <typename V, typename T> __device__ __forceinline__ P2<V> cvt2(P2<T> a) { return mk2((V)a.x, (V)a.y); }
