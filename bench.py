@@ -51,8 +51,8 @@ def parse():
     ap.add_argument("--power-cfl", type=float, default=0.05)
     ap.add_argument("--configs", action="store_true",
                     help="instead of the benchmark: the step on the reference's cavity 64^3, channel "
-                         "256x128x128 and 512x256x256 configurations, timed for the B200 step, the "
-                         "reference's CUDA step and the CPU oracle")
+                         "256x128x128 and 512x256x256 and floating-turbine 1024x256x256 configurations, "
+                         "timed for the B200 step, the reference's CUDA step and the CPU oracle")
     return ap.parse_args()
 
 
@@ -365,7 +365,9 @@ def run_configs(args):
             ("C2 channel 256x128x128 + rotor (5% inflow, CFL 0.3, tol 1e-8)", cases.channel(256, 128, 128).with_inflow(), 100, 3,
              cases.channel(256, 128, 128, intensity=0.0)),
             ("C3 channel 512x256x256 + rotor (5% inflow, CFL 0.3, tol 1e-6)", cases.channel_large().with_inflow(), 100, 0,
-             cases.channel(512, 256, 256, intensity=0.0, tol=1e-6, name="channel_large_uniform"))]
+             cases.channel(512, 256, 256, intensity=0.0, tol=1e-6, name="channel_large_uniform")),
+            ("C5 floating turbine 1024x256x256, forward step (8% inflow, platform pitch 3 deg, TSR 9, tol 1e-6)",
+             cases.floating().with_inflow(), 100, 0, cases.floating(intensity=0.0))]
     ref_ok = os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libfalmref.so"))
     build()
     lines = []

@@ -262,13 +262,13 @@ def adjoint_case():
     return channel(128, 64, 64, cells_per_radius=10, steps=200, name="adjoint")
 
 
-def floating():
+def floating(intensity=0.08):
     h = 1.0 / 24
     nx, ny, nz = 1024, 256, 256
     g = uniform_grid(nx, ny, nz, h)
     rotor = make_rotor((5.0, 0.5 * ny * h, 0.5 * nz * h), h, tsr=9.0, pitch=3.0, platform_pitch_deg=3.0,
                        platform_period=10.0, tower=3.0)
-    return Case("floating", g, 0, Re=1e4, dt=0.3 * h, tol=1e-6, alm=rotor, intensity=0.08, steps=3000)
+    return Case("floating", g, 0, Re=1e4, dt=0.3 * h, tol=1e-6, alm=rotor, intensity=intensity, steps=3000)
 
 
 def small_channel(nx=40, ny=24, nz=24, cells_per_radius=6, intensity=0.05, tol=1e-10, n_ap_per_blade=8):
