@@ -739,9 +739,12 @@ int pseudo_u_t(falm_ctx *ctx, const T *un, const T *u, const T *uu, T *ua, const
         if constexpr (sizeof(T) == 4) {
             if (!ctx->pu_v1 && (g.nx & 1) == 0 &&
                 (ctx->adv == FALM_ADV_UPWIND3 || ctx->adv == FALM_ADV_UTOPIA || ctx->adv == FALM_ADV_KK)) {
-                auto k2 = k_pseudo_u_tma2<NS, FALM_ADV_UPWIND3>;
-                if (ctx->adv == FALM_ADV_UTOPIA) k2 = k_pseudo_u_tma2<NS, FALM_ADV_UTOPIA>;
-                if (ctx->adv == FALM_ADV_KK) k2 = k_pseudo_u_tma2<NS, FALM_ADV_KK>;
+                // a ring of 4 planes (49 KB) and at most 128 registers: 4 CTAs per SM
+                constexpr int NS2 = 4;
+                using L = PUTile<T, NS2>;
+                auto k2 = k_pseudo_u_tma2<NS2, FALM_ADV_UPWIND3>;
+                if (ctx->adv == FALM_ADV_UTOPIA) k2 = k_pseudo_u_tma2<NS2, FALM_ADV_UTOPIA>;
+                if (ctx->adv == FALM_ADV_KK) k2 = k_pseudo_u_tma2<NS2, FALM_ADV_KK>;
                 const int bx = (g.nx + L::TX - 1) / L::TX, by = (g.ny + L::TY - 1) / L::TY;
                 const int kc = chunk_len(ctx, (long long)bx * by, g.nz, resident_per_sm(k2, 128, L::SMEM), 64, 4);
                 cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);

@@ -304,7 +304,7 @@ drain:
 // order.  For the 4th-order schemes (Upwind3, UTOPIA, KK) and an even interior
 // width, where every pair lies inside the interior or outside it.
 template <int NS, int ADV>
-__global__ void __launch_bounds__(128, 3) k_pseudo_u_tma2(Geom g, int kc, MetricView<float> mv,
+__global__ void __launch_bounds__(128, 4) k_pseudo_u_tma2(Geom g, int kc, MetricView<float> mv,
     const __grid_constant__ CUtensorMap mu, const __grid_constant__ CUtensorMap muu,
     const __grid_constant__ CUtensorMap mnut, const float *__restrict__ un, int un_is_u, float *__restrict__ ua,
     const float *__restrict__ ff, AlmFuse af, float ReI, float dt, int *err) {
