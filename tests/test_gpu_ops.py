@@ -54,10 +54,12 @@ def test_pseudo_u(oracle, lib_built, adv):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-@pytest.mark.parametrize("shape", [(20, 14, 12), (64, 24, 70), (36, 9, 5)])
+@pytest.mark.parametrize("shape", [(20, 14, 12), (64, 24, 70), (36, 9, 5), (21, 10, 7), (67, 13, 9)])
 def test_pseudo_u_tma_matches_row_kernel(lib_built, monkeypatch, precision, shape):
-    """The TMA-streamed 2.5D kernel and the plain row kernel agree (partial
-    tiles in x/y, z chunks, ALM force evaluated in-kernel)."""
+    """The TMA-streamed 2.5D kernels and the plain row kernel agree (partial
+    tiles in x/y, z chunks, ALM force evaluated in-kernel). An odd interior
+    width takes the one-cell kernel in FP32 too (the x-pair kernel needs every
+    pair inside the interior or outside it)."""
     case = cases.small_channel(*shape, intensity=0.0)
     st = random_state(case, seed=12)
     outs = []
