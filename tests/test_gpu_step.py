@@ -53,10 +53,13 @@ def small_cases():
     cav.tol = 1e-10
     # wide enough (nx >= 64) for every plane stream, including the 7-point one
     wide = cases.small_channel(72, 20, 16, intensity=0.05).with_inflow(nb=8)
-    return {"channel": ch, "cavity": cav, "wide": wide}
+    # an odd interior width: rows whose pitch is not a multiple of 16 bytes,
+    # so every plane stream gives way to the row kernels
+    odd = cases.small_channel(33, 19, 15, intensity=0.05).with_inflow(nb=8)
+    return {"channel": ch, "cavity": cav, "wide": wide, "odd": odd}
 
 
-@pytest.mark.parametrize("name", ["channel", "cavity", "wide"])
+@pytest.mark.parametrize("name", ["channel", "cavity", "wide", "odd"])
 def test_step_fp64_fixed_iterations(oracle, lib_built, name):
     case = small_cases()[name]
     ref, rs = run_oracle(oracle, case, 10, maxit=6, tol=0.0)
@@ -274,3 +277,16 @@ def test_driver_output_schedule(lib_built, tmp_path):
     hd, _ = api.read_vector_file(tmp_path / "o_000000_0000000006")
     assert hd["dsize"] == 8 and hd["step"] == 6
     sim.close()
+
+
+def test_step_mixed_odd_width(oracle, lib_built):
+    """Mixed precision on an odd interior width (row kernels throughout) against
+    the FP64 oracle."""
+    case = small_cases()["odd"]
+    case.tol = 1e-8
+    ref, rs = run_oracle(oracle, case, 10)
+    got, gs, _ = run_gpu(case, 10, precision="mixed")
+    err = compare(case, got, ref)
+    assert err["u"] < 2e-4 and err["uu"] < 2e-4, err
+    for a, b in zip(gs, rs):
+        assert a["torque"][0] == pytest.approx(b["torque"][0], rel=5e-3)
