@@ -290,3 +290,28 @@ def test_step_mixed_odd_width(oracle, lib_built):
     assert err["u"] < 2e-4 and err["uu"] < 2e-4, err
     for a, b in zip(gs, rs):
         assert a["torque"][0] == pytest.approx(b["torque"][0], rel=5e-3)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_step_reports_non_finite_input(lib_built, precision):
+    """A NaN in the velocity reaches the solver's FP64 reductions: falm_step
+    stops with FALM_ERR_NAN (3) instead of continuing, and the same context then
+    steps normally from a clean state."""
+    from falm_b200._lib import FalmError
+    case = small_cases()["channel"]
+    g = case.grid
+    ctx = make_ctx(case, precision)
+    st0 = cases.initial_state(case)
+    bad = st0["u"].copy()
+    bad[g.gc + 5 + g.sx * ((g.gc + 4) + g.sy * (g.gc + 3))] = np.nan
+    u, uu, p, nut = dev(ctx, bad), ctx.field(3), ctx.field(1), ctx.field(1)
+    ctx.utouu(u, uu)
+    ctx.sgs(u, nut)
+    with pytest.raises(FalmError) as e:
+        ctx.step(u, uu, p, nut, None, case.dt, case.dt)
+    assert e.value.code == 3
+    u, uu, p, nut = dev(ctx, st0["u"]), ctx.field(3), ctx.field(1), ctx.field(1)
+    ctx.utouu(u, uu)
+    ctx.sgs(u, nut)
+    s = ctx.step(u, uu, p, nut, None, case.dt, case.dt)
+    assert s["status"] == 0 and np.isfinite(host(u)).all()
