@@ -2,17 +2,22 @@
 """Throughput of the FALM LES step on B200: Mcell/s (and steps/s).
 
 Default workload: the 512x256x256 channel with one actuator-line rotor
-(33.5 M interior cells, h = 1/20, TSR 7, seeded 5% inflow, Poisson tol 1e-6)
-in mixed precision (FP32 storage, FP64 reductions), plus the FP64 step on the
-same case for the mixed/FP64 ratio.  One JSON line on rank 0.
+(33.5 M interior cells, h = 1/20, TSR 7, uniform inflow U = 1, CFL 0.3) with
+the Poisson tolerance at which ||div u|| stays below 1e-6 (1e-8; the case's
+own 1e-6 leaves it near 2e-6), in mixed precision (FP32 storage, FP64
+reductions).  Beside it: the FP64 step on the same workload (mixed/FP64),
+the same grid with seeded 5% inflow turbulence in both precisions, the case
+tolerance 1e-6, the field errors of mixed against FP64 after 10 steps, the
+CPU oracle on a slice, and the adjoint/forward cost ratio.  One JSON line on
+rank 0.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 --impl reference times the reference's own CUDA step (built from its sources
-into oracle/_ref) on the same grid in FP64 with uniform inflow (the reference
-has no seeded inflow); if that build is absent it times the CPU oracle.
-Multi-GPU (torchrun): every rank runs its own replica of the case (weak
-scaling); the time is the maximum over ranks.
+into oracle/_ref) on the same workload (same grid, rotor, uniform inflow and
+tolerance) in FP64, its only precision; if that build is absent it times the
+CPU oracle.  Multi-GPU (torchrun): every rank runs its own replica of the case
+(weak scaling); the time is the maximum over ranks.
 """
 import argparse
 import json
@@ -44,7 +49,12 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward cost ratio")
-    ap.add_argument("--no-div", action="store_true", help="skip the run at the tolerance that meets ||div u|| <= 1e-6")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the secondary runs (seeded inflow, the case tolerance 1e-6, field errors after 10 steps)")
+    ap.add_argument("--tol", type=float, default=DIV_TOL,
+                    help="Poisson tolerance (default 1e-8: the case's ||div u|| stays below 1e-6)")
+    ap.add_argument("--intensity", type=float, default=0.0,
+                    help="inflow turbulence intensity of the timed workload (default 0: uniform inflow, as the reference)")
     ap.add_argument("--power-run", type=int, default=0, metavar="STEPS",
                     help="instead of the benchmark: time-averaged rotor power and thrust over STEPS steps, "
                          "mixed against FP64, at --power-cfl")
@@ -96,22 +106,70 @@ def replica_rate(world, cells, steps, ms_max):
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 100 ms during the timed region"""
+    """SM clock, its maximum, power and the throttle reasons of this process's GPU,
+    sampled every 20 ms through NVML during the timed region (nvidia-smi every
+    100 ms where NVML is not available).  stop() keeps sampling, for at most one
+    second, until at least 3 samples were taken, so that even a short timed
+    region carries a clock record."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
 
     def __init__(self, gpu_index):
         self.idx = gpu_index
-        self.rows = []
+        self.rows = []          # (sm_mhz, sm_max_mhz, power_w, reason bits)
         self.proc = None
+        self.nvml = None
+        self.stop_flag = False
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        props = torch.cuda.get_device_properties(self.idx)
+        uuid = str(getattr(props, "uuid", "") or "")
+        if uuid:
+            try:
+                return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            except Exception:
+                pass
+        bus = getattr(props, "pci_bus_id", None)
+        if bus is not None:
+            dom = getattr(props, "pci_domain_id", 0)
+            dev = getattr(props, "pci_device_id", 0)
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(f"{dom:08x}:{bus:02x}:{dev:02x}.0")
+        return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.idx)
+
+    def _nvml_loop(self, nv, h):
+        while not self.stop_flag:
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((float(sm), float(mx), pw, int(rs)))
+            except Exception:
+                pass
+            time.sleep(0.02)
 
     def start(self):
+        try:
+            nv, h = self._nvml_handle()
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            self.source = "nvml, 20 ms"
+            self.thread.start()
+            return self
+        except Exception:
+            pass
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.Q,
                                           "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread = threading.Thread(target=self._smi_read, daemon=True)
+            self.source = "nvidia-smi, 100 ms"
             self.thread.start()
             # the first line comes at start-up: wait for it, then keep only the
             # samples taken from here on
@@ -123,39 +181,42 @@ class ClockSampler:
             self.proc = None
         return self
 
-    def _read(self):
+    def _smi_read(self):
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) >= 9:
-                self.rows.append(parts)
+                bits = 0
+                for k, (_, b) in enumerate(self.REASONS):
+                    if parts[5 + k].lower().startswith("active"):
+                        bits |= b
+                self.rows.append((num(parts[1]), num(parts[2]), num(parts[3]), bits))
 
     def stop(self):
+        t0 = time.perf_counter()
+        while self.source and len(self.rows) < 3 and time.perf_counter() - t0 < 1.0:
+            time.sleep(0.01)
+        self.stop_flag = True
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
-        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": len(self.rows)}
-        if not self.rows:
+        rows = list(self.rows)
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": len(rows), "source": self.source}
+        if not rows:
             return out
-        def num(v):
-            try:
-                return float(v)
-            except ValueError:
-                return None
-        sm = [num(r[1]) for r in self.rows if num(r[1])]
-        mx = [num(r[2]) for r in self.rows if num(r[2])]
+        sm = [r[0] for r in rows if r[0]]
+        mx = [r[1] for r in rows if r[1]]
+        pw = [r[2] for r in rows if r[2]]
         out["sm_mhz"] = statistics.median(sm) if sm else None
         out["sm_max_mhz"] = max(mx) if mx else None
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for r in self.rows:
-            for k, name in enumerate(names):
-                if r[5 + k].lower().startswith("active"):
-                    reasons.add(name)
-        out["reasons"] = sorted(reasons)
-        pw = [num(r[3]) for r in self.rows if num(r[3])]
+        out["reasons"] = sorted({name for r in rows for name, bit in self.REASONS if r[3] & bit})
         out["power_w_max"] = max(pw) if pw else None
         return out
 
@@ -210,21 +271,44 @@ def traffic_for(kernel):
         return None
 
 
+# ---------------------------------------------------------------- workload
+def bench_case(args, intensity=None, tol=None):
+    """The benchmark's case: the 512x256x256 channel with the rotor (the case of
+    --case) at Poisson tolerance `tol` (default --tol) and inflow turbulence
+    `intensity` (default: uniform inflow, which both arms run)."""
+    from falm_b200 import cases
+    c = getattr(cases, args.case)()
+    c.tol = args.tol if tol is None else tol
+    c.intensity = args.intensity if intensity is None else intensity
+    c.inflow = None
+    return c.with_inflow()
+
+
+def workload_config(args, case):
+    """the configuration dict both arms print (identical for the same arguments)"""
+    g = case.grid.interior
+    infl = "uniform inflow U = 1" if not case.intensity else f"seeded {case.intensity:.0%} inflow (Philox seed 20261203)"
+    return {"workload": f"{case.name} {g[0]}x{g[1]}x{g[2]} channel + 3-blade ALM rotor (R = 20 cells, TSR 7, 96 APs), "
+                        f"{infl}, Re 1e4, CFL 0.3, PBiCGStab + red-black SOR x{case.pc_maxit} (omega {case.pc_relax}), "
+                        f"tol {case.tol:g} (||div u|| <= 1e-6)",
+            "cells": case.grid.n_interior, "tol": case.tol, "inflow_intensity": case.intensity,
+            "l2": "inputs larger than L2 (one FP32 field is 140 MB, one FP64 field 280 MB; L2 126 MB)"}
+
+
 # ---------------------------------------------------------------- our arm
 def run_ours(args, rank, world, local):
     import torch
-    from falm_b200 import cases
     from falm_b200.driver import Simulation
-    case = getattr(cases, args.case)().with_inflow()
+    case = bench_case(args)
     n = case.grid.n_interior
     out = {}
 
     def timed(sim, K, e2e=False):
         # Every phase starts from the state kept after the warm-up, and the run
         # goes back to it every RESTART steps (device copies of the fields,
-        # inside the timed region): with 5% seeded inflow turbulence at CFL 0.3
-        # the explicit-Euler step with the Upwind3 scheme amplifies mid-wavenumber
-        # modes, and the flow leaves the stable range after about 240 steps.
+        # inside the timed region): at CFL 0.3 the explicit-Euler step with the
+        # Upwind3 scheme amplifies mid-wavenumber modes, and the flow leaves the
+        # stable range after about 240 (seeded inflow) or 450 (uniform) steps.
         ctx = sim.ctx
         sim.restore()
         planes = None
@@ -250,6 +334,25 @@ def run_ours(args, rank, world, local):
         barrier(world)
         return ms, stats, ctx.launches() - l0, wall
 
+    def arm(c, prec, K):
+        """W warm-up steps, then K timed steps; returns the summary and the stats"""
+        sim = Simulation(c, prec)
+        for _ in range(args.warmup):
+            sim.step()
+        sim.snapshot()
+        ms, st, _, _ = timed(sim, K)
+        ms = max_over_ranks(ms, world)
+        its = [x["it"] for x in st]
+        sb = step_bytes(4 if prec == "mixed" else 8, n, sum(its) / len(its))
+        res = {"value": replica_rate(world, n, K, ms), "ms_per_step": ms / K, "steps_per_s": 1e3 * K / ms,
+               "its": it_summary(its), "outer_max": max(x["outer"] for x in st),
+               "divnorm_max": max(x["divnorm"] for x in st), "step_roofline_frac": sb / (ms / K / 1e3) / 1e9 / peak}
+        sim.close()
+        del sim
+        torch.cuda.empty_cache()
+        return res
+
+    peak, peak_kind = peaks()
     sim = Simulation(case, args.precision)
     for _ in range(args.warmup):
         sim.step()
@@ -270,7 +373,6 @@ def run_ours(args, rank, world, local):
     its = [s["it"] for s in stats]
     mean_it = sum(its) / len(its)
     value = replica_rate(world, n, args.steps, ms_max)
-    peak, peak_kind = peaks()
     # dominant kernel class by device time
     cls = max((k for k in prof if k in KERNEL_VALUES), key=lambda k: prof[k][0])
     tms, tn = prof[cls]
@@ -278,11 +380,11 @@ def run_ours(args, rank, world, local):
     alg_bytes = KERNEL_VALUES[cls] * S * n
     achieved = alg_bytes / (avg_ms / 1e3) / 1e9
     step_b = step_bytes(S, n, mean_it)
+    divmax = max(s["divnorm"] for s in stats)
     out.update({
         "value": value, "ms_per_step": ms_max / args.steps, "steps_per_s": 1e3 * args.steps / ms_max,
-        "launches": launches, "its": it_summary(its), "divnorm_max": max(s["divnorm"] for s in stats),
+        "launches": launches, "its": it_summary(its), "divnorm_max": divmax, "div_ok": divmax <= 1e-6,
         "err_max": max(s["err"] for s in stats), "clocks": clk,
-        "power": [s["torque"][0] * case.alm.tip_rate[0] for s in stats] if case.alm is not None else None,
         "roofline": {"bound": "hbm", "kernel": cls, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic_for(cls), "peak_kind": peak_kind,
                      "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms},
@@ -299,51 +401,65 @@ def run_ours(args, rank, world, local):
                       "h2d_bytes_per_step": 3 * ny * nz * 8,
                       "d2h_bytes_per_step": 8 * 8 + 2 * 8 * 8,
                       "ms_per_step": ms_e / args.steps,
-                      "note": "per step: inlet plane H2D from pinned memory, falm_step through the C ABI, "
-                              "step statistics (it, err, div norm, torque, thrust) read back to the host"}
+                      "note": "per step: the inlet velocity plane (3 x nz x ny FP64) copied H2D from pinned host memory, "
+                              "falm_step through the C ABI, step statistics (it, err, div norm, torque, thrust) read "
+                              "back to the host"}
     sim.close()
     del sim
     torch.cuda.empty_cache()
-    if not args.no_fp64 and args.precision == "mixed":
-        sim64 = Simulation(case, "fp64")
-        for _ in range(args.warmup):
-            sim64.step()
-        sim64.snapshot()
-        ms64, st64, _, _ = timed(sim64, args.steps)
-        ms64 = max_over_ranks(ms64, world)
-        out["fp64"] = {"value": replica_rate(world, n, args.steps, ms64), "ms_per_step": ms64 / args.steps,
-                       "steps_per_s": 1e3 * args.steps / ms64, "its": it_summary([s["it"] for s in st64]),
-                       "divnorm_max": max(s["divnorm"] for s in st64)}
+    if args.precision == "mixed" and not args.no_fp64:
+        out["fp64"] = arm(case, "fp64", args.steps)
+        out["fp64"]["note"] = ("our FP64 step on the same workload; the reference arm (--impl reference) prints "
+                               "the reference's FP64 step on it")
         out["mixed_over_fp64"] = out["fp64"]["ms_per_step"] / out["ms_per_step"]
-        sim64.close()
-        del sim64
-        torch.cuda.empty_cache()
-    # the same case at the Poisson tolerance that brings ||div u|| under 1e-6
-    # (the case's own tolerance of 1e-6 leaves it at about 2e-6), both precisions
-    if not args.no_div and args.precision == "mixed":
+    if args.precision == "mixed" and not args.no_extra:
         K = min(args.steps, RESTART)
-        dv = {"tol": DIV_TOL, "steps": K}
-        for prec in ("mixed", "fp64"):
-            c = getattr(cases, args.case)().with_inflow()
-            c.tol = DIV_TOL
-            s2 = Simulation(c, prec)
-            for _ in range(args.warmup):
-                s2.step()
-            s2.snapshot()
-            ms2, st2, _, _ = timed(s2, K)
-            ms2 = max_over_ranks(ms2, world)
-            it2 = [s["it"] for s in st2]
-            sb = step_bytes(4 if prec == "mixed" else 8, n, sum(it2) / len(it2))
-            dv[prec] = {"value": replica_rate(world, n, K, ms2), "ms_per_step": ms2 / K,
-                        "its": it_summary(it2), "outer_max": max(s["outer"] for s in st2),
-                        "divnorm_max": max(s["divnorm"] for s in st2),
-                        "step_roofline_frac": sb / (ms2 / K / 1e3) / 1e9 / peak}
-            s2.close()
-            del s2
-            torch.cuda.empty_cache()
-        dv["mixed_over_fp64"] = dv["fp64"]["ms_per_step"] / dv["mixed"]["ms_per_step"]
-        out["div_target"] = dv
+        # the benchmark configuration's own physics: seeded 5% inflow turbulence
+        seeded = bench_case(args, intensity=0.05)
+        sd = {"config": workload_config(args, seeded)["workload"], "steps": K,
+              "mixed": arm(seeded, "mixed", K), "fp64": arm(seeded, "fp64", K)}
+        sd["mixed_over_fp64"] = sd["fp64"]["ms_per_step"] / sd["mixed"]["ms_per_step"]
+        out["seeded_inflow"] = sd
+        # the case's own Poisson tolerance, 1e-6, which leaves ||div u|| near 2e-6
+        loose = bench_case(args, tol=1e-6)
+        out["tol_1e-6"] = {"note": "secondary: the case's tolerance 1e-6 does not meet ||div u|| <= 1e-6",
+                           "mixed": arm(loose, "mixed", K)}
+        out["fields_10_steps"] = {"uniform_inflow": field_errors(case), "seeded_inflow": field_errors(seeded)}
     return case, out
+
+
+def field_errors(case, steps=10):
+    """mixed precision against the FP64 step after `steps` steps from the same
+    initial state: relative L2 of u, uu, p, nut over the interior, and the
+    relative differences of rotor power and thrust at the last step (the FP64
+    step matches the CPU oracle and the reference's step at 1e-10 on the
+    parity grids)"""
+    import torch
+    from falm_b200.driver import Simulation
+    res, keep = {}, {}
+    for prec in ("fp64", "mixed"):
+        sim = Simulation(case, prec)
+        for _ in range(steps):
+            st = sim.step()
+        g = case.grid
+        gc = g.gc
+        keep[prec] = ({k: getattr(sim, k).view(-1, g.sz, g.sy, g.sx)[:, gc:-gc, gc:-gc, gc:-gc].double().clone()
+                       for k in ("u", "p", "nut")}, st)
+        uu = sim.uu.view(3, g.sz, g.sy, g.sx)[:, gc - 1:-gc, gc - 1:-gc, gc - 1:-gc].double().clone()
+        keep[prec][0]["uu"] = uu
+        sim.close()
+        del sim
+        torch.cuda.empty_cache()
+    a, sa = keep["mixed"]
+    b, sb = keep["fp64"]
+    for k in ("u", "uu", "p", "nut"):
+        res[k] = float(torch.linalg.vector_norm(a[k] - b[k]) / torch.linalg.vector_norm(b[k]))
+    res["power"] = abs(sa["torque"][0] - sb["torque"][0]) / abs(sb["torque"][0])
+    res["thrust"] = abs(sa["thrust"][0] - sb["thrust"][0]) / abs(sb["thrust"][0])
+    res["steps"] = steps
+    del keep
+    torch.cuda.empty_cache()
+    return res
 
 
 def run_configs(args):
@@ -484,31 +600,37 @@ def power_run(args):
                           "fp64": b, "mixed": a, "rel_diff": rel}}
 
 
-def cpu_baseline(args):
-    """the CPU oracle (OpenMP, all host threads) on a bounded sample of the workload"""
+def cpu_baseline(args, steps=7, warm=2):
+    """the CPU oracle (OpenMP, all host threads) on a bounded sample of the
+    workload: the median time of `steps` steady-state steps after `warm` untimed
+    ones, on a 256x256x128 slice of the case (same h, rotor, tolerance and
+    inflow), about 10-20 s of CPU work"""
     from oracle.oracle import CaseStruct, Oracle, build
     from falm_b200 import cases
     build()
     O = Oracle()
-    big = getattr(cases, args.case)()
+    big = bench_case(args)
     nx, ny, nz = big.grid.interior
-    sx, sy, sz = max(nx // 4, 32), max(ny // 2, 32), max(nz // 2, 32)
+    sx, sy, sz = max(nx // 2, 32), max(ny, 32), max(nz // 2, 32)
     h = float(big.grid.hx[big.grid.gc])
-    sample = cases.channel(sx, sy, sz, cells_per_radius=round(1 / h), intensity=0.0, tol=big.tol,
-                           hub=(3.2, 0.5 * sy * h, 0.5 * sz * h), name="cpu_sample")
+    sample = cases.channel(sx, sy, sz, cells_per_radius=round(1 / h), intensity=big.intensity, tol=big.tol,
+                           hub=(3.2, 0.5 * sy * h, 0.5 * sz * h), name="cpu_sample").with_inflow()
     cs = CaseStruct(sample)
     m = O.setup(cs)
     st = cases.initial_state(sample)
     O.init_state(cs, m, st)
-    O.step(cs, st, m, sample.dt)
-    t0 = time.perf_counter()
-    steps = 2
+    for q in range(warm):
+        O.step(cs, st, m, (q + 1) * sample.dt)
+    times, its = [], []
     for q in range(steps):
-        O.step(cs, st, m, (q + 2) * sample.dt)
-    el = time.perf_counter() - t0
-    return {"value": sample.grid.n_interior * steps / el / 1e6, "unit": UNIT, "cores": O.threads(), "kind": "port",
-            "sample": f"{steps} FP64 steps of a {sx}x{sy}x{sz} slice of the case (same h, rotor, tolerance; "
-                      f"uniform inflow) after one warm-up step, CPU oracle on {O.threads()} threads"}
+        t0 = time.perf_counter()
+        its.append(O.step(cs, st, m, (warm + q + 1) * sample.dt)["it"])
+        times.append(time.perf_counter() - t0)
+    med = statistics.median(times)
+    return {"value": sample.grid.n_interior / med / 1e6, "unit": UNIT, "cores": O.threads(), "kind": "port",
+            "ms_per_step": 1e3 * med, "its": its,
+            "sample": f"median of {steps} FP64 steps (after {warm} untimed) of a {sx}x{sy}x{sz} slice of the workload "
+                      f"(same h, rotor, tolerance and inflow), CPU oracle on {O.threads()} threads"}
 
 
 # ---------------------------------------------------------------- adjoint cost
@@ -580,15 +702,21 @@ def adjoint_ratio(steps=200, checkpoint=20):
 
 # ---------------------------------------------------------------- reference arm
 def run_reference(args, rank, world, local):
-    from falm_b200 import cases
-    ref_so = os.path.join(ROOT, "oracle", "_ref", "libfalmref.so")
-    case = getattr(cases, args.case)()
+    """The reference's own CUDA step (oracle/_ref, compiled from its sources) on
+    the same workload: same grid, rotor, uniform inflow and Poisson tolerance,
+    in FP64 (its only precision).  Wall clock between device synchronisations
+    around each segment of steps."""
+    case = bench_case(args)
     n = case.grid.n_interior
-    if not os.path.exists(ref_so):
+    from oracle.oracle import REF_SO
+    if not os.path.exists(REF_SO) or case.intensity:
         cb = cpu_baseline(args)
-        return case, {"value": cb["value"], "kind": "port", "cpu_baseline": cb, "device": "cpu"}
+        return case, {"value": cb["value"], "ms_per_step": cb["ms_per_step"], "kind": "port", "cpu_baseline": cb,
+                      "device": "cpu", "note": "the reference's build is absent (or the workload has seeded inflow, "
+                                               "which the reference has no input for): the CPU oracle is timed"}
     import tempfile
     import torch
+    from falm_b200 import cases
     from oracle.oracle import CaseStruct, RefStep
     cs = CaseStruct(case, use_inflow=False)
     ref = RefStep(cs, tempfile.mkdtemp(prefix="falmref_"))
@@ -625,7 +753,8 @@ def run_reference(args, rank, world, local):
     clk = clocks.stop()
     ref.close()
     return case, {"value": n * args.steps / el / 1e6, "ms_per_step": 1e3 * el / args.steps, "device": "gpu",
-                  "its": it_summary([s["it"] for s in stats]), "clocks": clk, "kind": "reference"}
+                  "its": it_summary([s["it"] for s in stats]), "divnorm_max": max(s["divnorm"] for s in stats),
+                  "clocks": clk, "kind": "reference"}
 
 
 def main():
@@ -637,7 +766,6 @@ def main():
         run_configs(args)
         return
     rank, world, local = dist_setup(args)
-    from falm_b200 import cases as _c
     if args.impl == "reference":
         if rank != 0:
             return
@@ -645,16 +773,17 @@ def main():
         line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": r.get("ms_per_step"),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic", "device": r["device"],
-                "config": {"workload": f"{case.name} {case.grid.interior[0]}x{case.grid.interior[1]}x{case.grid.interior[2]}, "
-                                       "reference CUDA step (oracle/_ref), FP64, uniform inflow", "tol": case.tol},
+                "data": "synthetic", "device": r["device"], "config": workload_config(args, case),
                 "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-                "its": r.get("its"), "clocks": r.get("clocks")}
+                "its": r.get("its"), "divnorm_max": r.get("divnorm_max"), "clocks": r.get("clocks"),
+                "note": "the reference's own CUDA step (oracle/_ref, compiled from its sources for sm_100a; the "
+                        "reference has no CPU implementation of the step), FP64, one GPU; rank 0 only"}
         if "cpu_baseline" in r:
             line["cpu_baseline"] = r["cpu_baseline"]
+            line["note"] = r["note"]
         else:
             line["cpu_baseline"] = {"value": r["value"], "unit": UNIT, "cores": 0, "kind": "reference",
-                                    "sample": "the reference's own CUDA step (it has no CPU path), full case"}
+                                    "sample": "the reference's own CUDA step (it has no CPU path), full workload"}
         print(json.dumps(line), flush=True)
         return
     case, r = run_ours(args, rank, world, local)
@@ -666,31 +795,24 @@ def main():
             cb = cpu_baseline(args)
         except Exception as e:   # the baseline is reported, never required
             cb = {"value": None, "unit": UNIT, "cores": 0, "kind": "port", "sample": f"failed: {e}"}
-    g = case.grid.interior
     line = {
         "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "steps_per_s": r["steps_per_s"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 storage / f64 reductions" if args.precision == "mixed" else "f64",
-        "data": "synthetic (seeded Philox inflow, seed 20261203)",
-        "config": {"workload": f"{case.name} {g[0]}x{g[1]}x{g[2]} channel + 3-blade ALM rotor, {args.precision}",
-                   "cells": case.grid.n_interior, "tol": case.tol, "pc": f"{case.pc} x{case.pc_maxit}",
-                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                   "l2": f"inputs larger than L2 (one {'FP32' if args.precision == 'mixed' else 'FP64'} field is "
-                         f"{case.grid.n * (4 if args.precision == 'mixed' else 8) / 1e6:.0f} MB, L2 126 MB)",
-                   "dt": f"CFL 0.3 at the inflow speed; the state after the warm-up is restored every {RESTART} "
-                         f"steps inside the timed region (device copies, counted in the time)"},
+        "data": "synthetic" + (" (seeded Philox inflow, seed 20261203)" if case.intensity else " (uniform inflow)"),
+        "config": workload_config(args, case),
+        "precision": args.precision,
+        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+        "restart": f"the state after the warm-up is restored every {RESTART} steps inside the timed region "
+                   f"(device copies, counted in the time)",
         "clocks": r["clocks"], "gpu_launches": r["launches"], "roofline": r["roofline"],
-        "step_roofline": r["step_roofline"], "its": r["its"], "divnorm_max": r["divnorm_max"],
+        "step_roofline": r["step_roofline"], "its": r["its"], "divnorm_max": r["divnorm_max"], "div_ok": r["div_ok"],
         "err_max": r["err_max"], "profile": r["profile"],
     }
-    if "e2e" in r:
-        line["e2e"] = r["e2e"]
-    if "fp64" in r:
-        line["fp64"] = r["fp64"]
-        line["mixed_over_fp64"] = r["mixed_over_fp64"]
-    if "div_target" in r:
-        line["div_target"] = r["div_target"]
+    for k in ("e2e", "fp64", "mixed_over_fp64", "seeded_inflow", "tol_1e-6", "fields_10_steps"):
+        if k in r:
+            line[k] = r[k]
     if cb:
         line["cpu_baseline"] = cb
     if world == 1 and not args.no_adjoint:

@@ -11,6 +11,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libfalm_b200.so")
 
 FALM_OK = 0
+FALM_ERR_ARG = 1
+FALM_ERR_TIMEOUT = 6
 STATUS = {0: "ok", 1: "bad argument", 2: "cuda error", 3: "non-finite value", 4: "breakdown",
           5: "maxit", 6: "timeout", 7: "alloc", 8: "state", 9: "no alm", 10: "over capacity"}
 FP64, MIXED = 0, 1
@@ -99,6 +101,7 @@ SIGNATURES = {
     "falm_io_write_cv_file": [V, ctypes.c_char_p],
     "falm_io_read_cv_file": [ctypes.c_char_p, c_int_p, c_double_p, c_double_p, c_double_p, c_double_p, c_double_p, c_double_p],
     "falm_mesh_build": [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, I],
+    "falm_debug_arm_wait_probe": [V, LL],
     "falm_profile_enable": [V, I],
     "falm_profile_read": [V, c_double_p, ctypes.POINTER(ctypes.c_longlong), I, I],
 }

@@ -802,10 +802,30 @@ int ubc_t(falm_ctx *ctx, T *u, UPrev<T> up, double dt, double t, cudaStream_t st
     return FALM_OK;
 }
 
+// A wait on an mbarrier that nothing ever completes, through the same bounded
+// wait the plane-stream kernels use: it gives up after `cycles` clock64 cycles
+// and records FALM_ERR_TIMEOUT in the device error word.  No copy is issued,
+// so nothing is left in flight when the block returns.
+__global__ void k_wait_probe(int *err, long long cycles) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) mbar_wait_cycles(&bar, 0, err, cycles);
+    __syncthreads();
+}
+
 template <typename T>
 int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_t st, falm_step_stats *out) {
     int rc = ensure_work(ctx);
     if (rc) return rc;
+    if (ctx->wait_probe_cycles > 0) {   // armed by falm_debug_arm_wait_probe: one step only
+        const long long cycles = ctx->wait_probe_cycles;
+        ctx->wait_probe_cycles = 0;
+        LAUNCH(FALM_K_OTHER, st, k_wait_probe<<<1, 32, 0, st>>>(ctx->kerr, cycles));
+    }
     if (!ctx->op_ready) {
         if ((rc = build_poisson(ctx, ctx->bc_kind))) return rc;
     }
@@ -1733,6 +1753,12 @@ int falm_bc_set_inlet_plane(falm_ctx *ctx, const double *plane, void *stream) {
     return FALM_OK;
 }
 
+int falm_debug_arm_wait_probe(falm_ctx *ctx, long long cycles) {
+    if (!ctx || cycles <= 0 || cycles > kWaitCycles) return FALM_ERR_ARG;
+    ctx->wait_probe_cycles = cycles;
+    return FALM_OK;
+}
+
 int falm_profile_enable(falm_ctx *ctx, int enable) {
     if (!ctx) return FALM_ERR_ARG;
     ctx->profiling = enable ? 1 : 0;
@@ -1773,48 +1799,85 @@ int falm_profile_read(falm_ctx *ctx, double *ms, long long *launches, int nclass
 // Everything the reduction needs lives in one fixed device array, so the call
 // allocates nothing:
 //   [0, 8*kStaticDotBlocks)   per-block partial sums (written before use)
-//   counter at kCounterOff    arrival counter; MUST be zero when a call starts
-//                             (device storage starts zeroed, set-up writes
-//                             zero, the last block of every call resets it)
+//   counter at kCounterOff    arrival counter; cleared on the stream at the
+//                             start of every call (an earlier call that failed
+//                             part way may have left it non-zero)
 //   result at kResultOff      the total, copied back to the host
-// The array is shared by all calls on a device: two calls in flight at once
-// (two streams, two host threads) race.
+// The array is shared by all calls on a device and keeps the last call's
+// contents: two calls in flight at once (two streams, two host threads) race.
 namespace {
 constexpr int kStaticDotBlocks = 16384;                                   // 8 rows per block: 131072 rows
 constexpr size_t kCounterOff = (size_t)kStaticDotBlocks * sizeof(double);
 constexpr size_t kResultOff = kCounterOff + 64;
 constexpr size_t kStaticDotBytes = kResultOff + 64;                       // 131200 bytes
 constexpr int kMaxStaticDevices = 64;
+constexpr int kMaxStaticGc = 64;
+
+// the set-up of a device: the array's address in the device context it was
+// taken in (a context torn down by cudaDeviceReset is replaced by one with a
+// new id, whose module copy may sit at another address)
+struct StaticScratch {
+    unsigned long long ctx_id;
+    unsigned char *ptr;
+};
 std::mutex g_static_mu;
-unsigned char *g_static_ptr[kMaxStaticDevices];
+StaticScratch g_static[kMaxStaticDevices];
+
+typedef CUresult (*PfnCtxGetCurrent)(CUcontext *);
+typedef CUresult (*PfnCtxGetId)(CUcontext, unsigned long long *);
+
+// the unique id of the calling thread's current context (0 when none is current)
+unsigned long long current_ctx_id() {
+    static PfnCtxGetCurrent get_cur = nullptr;
+    static PfnCtxGetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void *f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+            get_cur = (PfnCtxGetCurrent)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+            get_id = (PfnCtxGetId)f;
+        cudaGetLastError();
+    });
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (!get_cur || !get_id || get_cur(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 }  // namespace
 
 static __device__ __align__(256) unsigned char g_dot_scratch[kStaticDotBytes];
 
 namespace {
-// once per device, with that device current: the array's address and a zeroed counter
+// once per device (and again if that device's context was replaced), with the
+// device current: the array's address, taken by cudaGetSymbolAddress
 int static_scratch(unsigned char **out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return FALM_ERR_CUDA; }
     if (dev < 0 || dev >= kMaxStaticDevices) return FALM_ERR_ARG;
+    unsigned long long id = current_ctx_id();
+    if (!id) {   // no context current yet on this thread: make the device's primary context current
+        if (cudaSetDevice(dev) != cudaSuccess) { cudaGetLastError(); return FALM_ERR_CUDA; }
+        id = current_ctx_id();
+    }
     std::lock_guard<std::mutex> lock(g_static_mu);
-    if (!g_static_ptr[dev]) {
+    StaticScratch &e = g_static[dev];
+    if (!e.ptr || e.ctx_id != id || !id) {
         void *p = nullptr;
         if (cudaGetSymbolAddress(&p, g_dot_scratch) != cudaSuccess || !p) { cudaGetLastError(); return FALM_ERR_CUDA; }
-        if (cudaMemset((unsigned char *)p + kCounterOff, 0, 64) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
-            cudaGetLastError();
-            return FALM_ERR_CUDA;
-        }
-        g_static_ptr[dev] = (unsigned char *)p;
+        e.ptr = (unsigned char *)p;
+        e.ctx_id = id;
     }
-    *out = g_static_ptr[dev];
+    *out = e.ptr;
     return FALM_OK;
 }
 }  // namespace
 
 extern "C" int falm_mv_dot_static(int sx, int sy, int sz, int gc, int precision, const void *a, const void *b, double *out,
                                   void *stream) {
-    if (!a || !b || !out || gc < 1 || sx < 2 * gc + 1 || sy < 2 * gc + 1 || sz < 2 * gc + 1 ||
+    if (!a || !b || !out || gc < 1 || gc > kMaxStaticGc || sx < 2 * gc + 1 || sy < 2 * gc + 1 || sz < 2 * gc + 1 ||
         (precision != FALM_FP64 && precision != FALM_MIXED))
         return FALM_ERR_ARG;
     const long long rows = (long long)(sy - 2 * gc) * (sz - 2 * gc);
@@ -1831,6 +1894,7 @@ extern "C" int falm_mv_dot_static(int sx, int sy, int sz, int gc, int precision,
     RedWork rw{(double *)p, (unsigned int *)(p + kCounterOff), kStaticDotBlocks};
     double *res = (double *)(p + kResultOff);
     cudaStream_t st = S(stream);
+    if (cudaMemsetAsync(p + kCounterOff, 0, sizeof(unsigned int), st) != cudaSuccess) { cudaGetLastError(); return FALM_ERR_CUDA; }
     if (precision == FALM_FP64)
         k_dot<double><<<(int)blocks, kRowThreads, 0, st>>>(g, R, (const double *)a, (const double *)b, 1, rw, res);
     else

@@ -164,6 +164,7 @@ struct falm_ctx {
     int sor_v1;                             // FP32 blocked SOR on the 32 x 8 tile kernel (tests)
     int pu_v1;                              // FP32 pseudo-velocity on the one-cell-per-thread kernel (tests)
     int check_sync;                         // synchronise after every launch (fault location)
+    long long wait_probe_cycles;            // >0: the next falm_step first runs a wait that nothing completes (tests)
     std::string *last_error;
     fb::IoWriter *io;                       // snapshot writer (falm_io.cuh), created on first use
 };

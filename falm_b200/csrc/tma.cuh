@@ -49,19 +49,25 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
+constexpr long long kWaitCycles = 2000000000LL;   // clock64 bound of one wait: about one second
+
 // bounded wait: try_wait suspends the thread in hardware until the phase
 // completes or the suspend-time hint passes; poll it, checking clock64 every
-// 4 polls, and give up after about one second (or kWaitLimit polls): false
-// (and *err set) then
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err) {
+// 4 polls, and give up after `cycles` clock64 cycles (or kWaitLimit polls):
+// false (and *err set to FALM_ERR_TIMEOUT) then
+__device__ __forceinline__ bool mbar_wait_cycles(uint64_t *bar, uint32_t parity, int *err, long long cycles) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     for (unsigned it = 1; it < kWaitLimit; it++) {
         if (mbar_try_wait(bar, parity)) return true;
-        if ((it & 3u) == 0 && clock64() - t0 > 2000000000LL) break;
+        if ((it & 3u) == 0 && clock64() - t0 > cycles) break;
     }
     if (err) atomicExch(err, FALM_ERR_TIMEOUT);
     return false;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err) {
+    return mbar_wait_cycles(bar, parity, err, kWaitCycles);
 }
 
 // origin of a box of width `box` (elements) inside an axis of `dim` elements:

@@ -269,20 +269,29 @@ int falm_step_adjoint(falm_ctx *ctx, const falm_fields *f0, const falm_fields *f
    device fields but may not allocate (a coupled solver or in-situ monitor beside a simulation
    that has claimed the device memory, where creating a context could fail): no context, and
    nothing is allocated -- the partial sums, arrival counter and result live in a fixed 128 KiB
-   device array inside the library.
+   device array inside the library, which every GPU that loads the library holds until exit.
    - One 256-thread block per 8 interior rows, (sy-2gc)*(sz-2gc) rows: grids with more than
-     131072 interior rows return FALM_ERR_SIZE without touching the device.
-   - The arrival counter must be zero when a call starts: device storage starts zeroed, the
-     set-up writes zero and every call's last block resets it.
-   - All calls on a device share the array: two calls in flight at once (two streams or two
-     host threads) race and give wrong results.
-   - The first call on a device performs the set-up (symbol address, counter reset, a device
-     synchronisation); make it before any stream capture.
+     131072 interior rows return FALM_ERR_SIZE without touching the device; gc must be 1..64.
+   - Every call clears the arrival counter on its stream before its kernel.
+   - All calls on a device share the array, which keeps the last call's contents: two calls in
+     flight at once (two streams or two host threads) race and give wrong results.
+   - The first call on a device (and the first after that device's context was replaced, e.g.
+     by cudaDeviceReset) performs the set-up: it takes the array's address with
+     cudaGetSymbolAddress, which may load the library's device code; make it before any
+     stream capture.
+   - The blocks sum in another order than falm_mv_dot's, so the two results agree to rounding
+     (relative 1e-12 in FP64), not bit for bit.
    precision FALM_FP64 (double fields) or FALM_MIXED (float fields); *out is a host double. */
 int falm_mv_dot_static(int sx, int sy, int sz, int gc, int precision, const void *a, const void *b,
                        double *out, void *stream);
 
 /* ---------------- instrumentation ----------------------------------------------------------- */
+/* Test hook for the bounded device waits (the reference only prints errors, src/error.h:20-26):
+   the next falm_step on this context first runs one wait on a barrier that no copy completes,
+   through the same bounded wait the plane-stream kernels use, limited to `cycles` clock64 cycles
+   (1 .. 2e9).  That step then returns FALM_ERR_TIMEOUT after the rest of it has run; the device
+   error word is cleared and the context stays usable.  One step only. */
+int falm_debug_arm_wait_probe(falm_ctx *ctx, long long cycles);
 /* Kernel classes timed with CUDA events when profiling is on (one event pair per launch). */
 enum { FALM_K_ALM = 0, FALM_K_PSEUDO_U, FALM_K_UTOUU_RHS, FALM_K_RES, FALM_K_BICG_P, FALM_K_SOR, FALM_K_MV_DOT1,
        FALM_K_BICG_S, FALM_K_MV_DOT2, FALM_K_BICG_XR, FALM_K_PBC, FALM_K_PROJECT, FALM_K_UBC, FALM_K_SGS_DIV,

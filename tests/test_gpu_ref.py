@@ -232,3 +232,137 @@ def test_output_files_match_reference(lib_built, tmp_path, precision):
     assert dims == (g.sx, g.sy, g.sz, g.gc)
     for a, b in ((x, g.x), (hx, g.hx), (y, g.y), (hy, g.hy), (z, g.z), (hz, g.hz)):
         np.testing.assert_allclose(a, b, rtol=1e-14, atol=0)
+
+
+# ---------------------------------------------------------------- the configurations' own sizes
+@needs_ref
+def test_b200_cavity_64_100_steps_matches_reference(oracle, lib_built):
+    """The lid-driven cavity configuration at its own size and length (64^3,
+    Re 1000, dt 1e-3, Upwind3, Smagorinsky Cs 0.1, PBiCGStab + RB-SOR x2): the
+    FP64 B200 step against the reference's own step over all 100 steps.
+      * fixed-iteration mode (tol 0, maxit 6): relative L2 <= 1e-10 on every field;
+      * convergence mode (tol 1e-8, err = ||r||/N): BiCGStab iteration counts
+        within +-1 at every step.  Each step's pressure is determined only to
+        the stopping tolerance, and over 100 steps the runs drift apart by the
+        accumulated solver truncation: the CPU oracle, a plain restatement,
+        drifts from the reference by the same order.  Bound: velocities 1e-7,
+        pressure 1e-5, and at most 10x the oracle's own distance (floor 1e-9)."""
+    case = cases.cavity(64)
+    ref, rs = ref_run(case, 100, maxit=6, tol=0.0)
+    got, gs, _ = run_gpu(case, 100, maxit=6, tol=0.0)
+    assert [a["it"] for a in gs] == [b["it"] for b in rs]
+    err = compare(case, got, ref)
+    for k, v in err.items():
+        assert v < 1e-10, (k, v, err)
+    ref, rs = ref_run(case, 100)
+    got, gs, _ = run_gpu(case, 100)
+    orc, os_ = run_oracle(oracle, case, 100)
+    for a, b in zip(gs, rs):
+        assert abs(a["it"] - b["it"]) <= 1, ([x["it"] for x in gs], [x["it"] for x in rs])
+        assert a["err"] <= case.tol
+    err = compare(case, got, ref)
+    spread = compare(case, orc, ref)
+    for k in ("u", "uu", "nut"):
+        assert err[k] < 1e-7 and err[k] < max(1e-9, 10 * spread[k]), (k, err, spread)
+    assert err["p"] < 1e-5 and err["p"] < max(1e-9, 10 * spread["p"]), (err, spread)
+
+
+@needs_ref
+def test_b200_channel_256_rotor_matches_reference(lib_built):
+    """The 256x128x128 channel with the full-size rotor (R = 20 cells, TSR 7,
+    3 x 32 actuator points, Gaussian width 2h; uniform inflow, which is the
+    reference's only inlet): 10 FP64 steps in fixed-iteration mode (tol 0,
+    maxit 6) against the reference's own step.  This size runs every multi-chunk
+    plane stream, the clamped boxes of a 260-wide row and the force-box ALM
+    projection at its real extent; the reference projects the AP forces densely
+    over the whole grid.  Relative L2 <= 1e-10 on u, uu, p, nut; torque and
+    thrust at every step within 1e-10."""
+    case = cases.channel(256, 128, 128, intensity=0.0)
+    ref, rs = ref_run(case, 10, maxit=6, tol=0.0)
+    got, gs, _ = run_gpu(case, 10, maxit=6, tol=0.0)
+    for a, b in zip(gs, rs):
+        assert a["it"] == b["it"]
+        for x, y in zip(a["torque"] + a["thrust"], b["torque"] + b["thrust"]):
+            assert x == pytest.approx(y, rel=1e-10)
+    err = compare(case, got, ref)
+    for k, v in err.items():
+        assert v < 1e-10, (k, v, err)
+
+
+def variant_cases():
+    """the reference's other advection schemes and the Jacobi preconditioner
+    (src/FalmCFDScheme.h:8-132, src/FalmEq.cpp:129-171), each on the channel and
+    the cavity, and the scheme-free step (no SGS model)"""
+    out = {}
+    for name, mk in (("channel", lambda: cases.small_channel(32, 20, 20, intensity=0.0)),
+                     ("cavity", lambda: cases.cavity(16))):
+        for adv in ("Upwind1", "QUICK", "UTOPIA", "KK"):
+            c = mk()
+            c.adv = adv
+            out[f"{name}-{adv}"] = c
+        c = mk()
+        c.pc, c.pc_maxit, c.pc_relax = "Jacobi", 2, 1.0
+        out[f"{name}-JacobiPC"] = c
+        c = mk()
+        c.adv, c.sgs = "KK", "Empty"
+        out[f"{name}-KK-noSGS"] = c
+    return out
+
+
+@needs_ref
+def test_csm_operator_matches_reference(oracle, lib_built):
+    """The CSM eddy viscosity (src/dev/FalmCFDDevCall.cu:478-555) of the
+    reference's own FalmCFD::SGS, of the oracle and of the B200 kernel on the
+    same random velocity field.  The reference takes sqrt(fcs^3) of the signed
+    coefficient fcs = Q/E (its |fcs| is computed and not used, :548-549), so
+    every cell with Q < 0 gets NaN there; all three give NaN at exactly the same
+    cells and agree to 1e-13 elsewhere.  (A time step with CSM meets such cells
+    at once in any sheared flow: the B200 step then stops with FALM_ERR_NAN,
+    where the reference carries the NaN on.)"""
+    import ctypes
+    from oracle.oracle import _p
+    from tests.helpers import dev, host, make_ctx
+    for name, case in (("channel", cases.small_channel(32, 20, 20, intensity=0.0)), ("cavity", cases.cavity(16))):
+        case.sgs = "CSM"
+        g = case.grid
+        ref, cs = ref_for(case)
+        m = oracle.setup(cs)
+        st = random_state(case, seed=11)
+        ref.set("U", st["u"])
+        ref.op("SGS")
+        want = interior(ref.get("NUT"), g)
+        ref.close()
+        nut_o = np.zeros(g.n)
+        oracle.L.oracle_sgs(ctypes.byref(cs.c), _p(st["u"]), _p(nut_o), _p(m["kx"]), _p(m["ja"]))
+        ctx = make_ctx(case)
+        nut_d = ctx.field(1)
+        ctx.sgs(dev(ctx, st["u"]), nut_d)
+        got = interior(host(nut_d), g)
+        orc = interior(nut_o, g)
+        ctx.close()
+        nan = np.isnan(want)
+        assert 0 < nan.sum() < nan.size, name
+        for other in (got, orc):
+            assert np.array_equal(np.isnan(other), nan), name
+            assert rel_l2(other[~nan], want[~nan]) < 1e-13, name
+
+
+@needs_ref
+@pytest.mark.parametrize("name", sorted(variant_cases()))
+def test_variants_match_reference(oracle, lib_built, name):
+    """Every variant through the reference's own FalmCFD / FalmEq (oracle/_ref):
+    the CPU oracle's restatement and the FP64 B200 step both within 1e-10
+    relative L2 of it after 10 steps in fixed-iteration mode (tol 0, maxit 6),
+    with equal BiCGStab iteration counts and equal rotor torque and thrust."""
+    case = variant_cases()[name]
+    ref, rs = ref_run(case, 10, maxit=6, tol=0.0)
+    orc, os_ = run_oracle(oracle, case, 10, maxit=6, tol=0.0)
+    got, gs, _ = run_gpu(case, 10, maxit=6, tol=0.0)
+    for other, st in ((orc, os_), (got, gs)):
+        err = compare(case, other, ref)
+        for k, v in err.items():
+            assert v < 1e-10, (k, v, err)
+        for a, b in zip(st, rs):
+            assert a["it"] == b["it"]
+            for x, y in zip(a["torque"] + a["thrust"], b["torque"] + b["thrust"]):
+                assert x == pytest.approx(y, rel=1e-10)

@@ -315,3 +315,54 @@ def test_step_reports_non_finite_input(lib_built, precision):
     ctx.sgs(u, nut)
     s = ctx.step(u, uu, p, nut, None, case.dt, case.dt)
     assert s["status"] == 0 and np.isfinite(host(u)).all()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_bounded_wait_gives_up_and_context_recovers(oracle, lib_built, precision):
+    """Failure detection of the bounded device waits.  falm_debug_arm_wait_probe
+    makes the next step start with a wait on an mbarrier that no copy ever
+    completes (the bounded wait of the plane streams, limited to 20000 clock64
+    cycles).  The wait gives up, the step finishes its other kernels, reads the
+    device error word and returns FALM_ERR_TIMEOUT instead of hanging; the
+    error word is then clear, and the same context runs the following steps
+    correctly (FP64: equal to the oracle at 1e-10 in fixed-iteration mode;
+    mixed: velocities within 2e-4 of the FP64 oracle in convergence mode)."""
+    import ctypes
+    import torch
+    from falm_b200 import _lib as L
+    case = small_cases()["wide"]
+    fixed = precision == "fp64"   # mixed: the drivers' convergence mode (outer FP64 refinement needs a tolerance)
+    if not fixed:
+        case.tol = 1e-8
+    ctx = make_ctx(case, precision)
+    if fixed:
+        ctx.eq_init(6, 0.0, case.pc, case.pc_maxit, case.pc_relax)
+    st0 = cases.initial_state(case)
+    u, uu, p, nut = dev(ctx, st0["u"]), ctx.field(3), ctx.field(1), ctx.field(1)
+    ctx.utouu(u, uu)
+    ctx.sgs(u, nut)
+    assert ctx.lib.falm_debug_arm_wait_probe(ctx.h, ctypes.c_longlong(0)) == L.FALM_ERR_ARG
+    assert ctx.lib.falm_debug_arm_wait_probe(ctx.h, ctypes.c_longlong(20000)) == L.FALM_OK
+    with pytest.raises(L.FalmError) as e:
+        ctx.step(u, uu, p, nut, None, case.dt, case.dt)
+    assert e.value.code == L.FALM_ERR_TIMEOUT
+    assert "bounded wait" in str(e.value)
+    # the context is usable: start again from the initial state
+    u.copy_(dev(ctx, st0["u"]))
+    p.zero_()
+    ctx.utouu(u, uu)
+    ctx.sgs(u, nut)
+    gs = [ctx.step(u, uu, p, nut, None, case.dt, (it + 1) * case.dt) for it in range(3)]
+    torch.cuda.synchronize()
+    ref, rs = run_oracle(oracle, case, 3, maxit=6 if fixed else None, tol=0.0 if fixed else None)
+    err = compare(case, {"u": host(u), "uu": host(uu), "p": host(p), "nut": host(nut)}, ref)
+    if fixed:
+        for k, v in err.items():
+            assert v < 1e-10, (k, v, err)
+        for a, b in zip(gs, rs):
+            assert a["it"] == b["it"]
+    else:
+        assert err["u"] < 2e-4 and err["uu"] < 2e-4, err
+        for a, b in zip(gs, rs):
+            assert a["torque"][0] == pytest.approx(b["torque"][0], rel=5e-3)
+    ctx.close()
