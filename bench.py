@@ -678,6 +678,15 @@ def adjoint_ratio(steps=200, checkpoint=20):
     A.mean_power_gradient(sim, steps, checkpoint)
     torch.cuda.synchronize()
     t_ck = time.perf_counter() - t0
+    # binomial checkpointing within a memory budget of 10 states (start, end and
+    # scratch included): 7 checkpoint slots
+    A._restore(sim, start[1])
+    sim.it = start[0]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    Jb, gpb, _, _ = A.mean_power_gradient_binomial(sim, steps, snaps=7)
+    torch.cuda.synchronize()
+    t_bin = time.perf_counter() - t0
     # device time per kernel class of one more gradient (the adjoint's own kernels are "other")
     A._restore(sim, start[1])
     sim.it = start[0]
@@ -693,11 +702,14 @@ def adjoint_ratio(steps=200, checkpoint=20):
             "states_kept": "all" if kept >= steps else f"checkpoint every {kept}",
             "forward_ms": 1e3 * t_fwd, "gradient_ms": 1e3 * t_adj, "ratio": t_adj / t_fwd,
             "ratio_checkpointed": t_ck / t_fwd, "checkpoint_every": checkpoint,
+            "ratio_binomial": t_bin / t_fwd, "binomial_states": 10,
+            "binomial_forward_steps": A.binomial_forward_steps(steps, 7), "dJ_dpitch_binomial": gpb,
             "J": J2, "dJ_dpitch": gp, "n_params": 1 + len(gc) + len(gt), "forward_its_mean": statistics.mean(fwd_its),
             "profile_ms_launches": prof,
-            "note": "gradient_ms = forward window keeping the states + reverse sweep (transposed Poisson solve to "
-                    "the case tolerance, relative); ratio_checkpointed adds the recomputation of all but the last "
-                    "segment; wall clock, each step synchronises"}
+            "note": "gradient_ms = forward window keeping the states + reverse sweep (transposed Poisson solves to "
+                    "relative residual 1e-5); ratio_checkpointed adds the recomputation of all but the last "
+                    "segment; ratio_binomial stores at most 10 states and recomputes along the binomial schedule; "
+                    "wall clock, each step synchronises"}
 
 
 # ---------------------------------------------------------------- reference arm

@@ -77,6 +77,7 @@ SIGNATURES = {
     "falm_mv_dot": [V, P, P, c_double_p, P],
     "falm_mv_dot_static": [I, I, I, I, I, P, P, c_double_p, P],
     "falm_step_adjoint": [V, ctypes.POINTER(Fields), ctypes.POINTER(Fields), D, D, D, P, P, P, P, P],
+    "falm_adjoint_set_tol": [V, D],
     "falm_mv_normsq": [V, P, I, c_double_p, P],
     "falm_mv_maxdiag": [V, c_double_p],
     "falm_mv_scale": [V, P, LL, D, P],

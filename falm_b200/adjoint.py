@@ -15,6 +15,11 @@ window is kept when that takes at most a quarter of the free device memory,
 and nothing is recomputed; otherwise segments of 20 steps.  States live in
 one preallocated device buffer that later calls reuse.
 
+`mean_power_gradient_binomial` reverses the window with binomial
+checkpointing instead: the states stored at any time are bounded by a number
+of slots (or a memory budget), and forward steps are recomputed along the
+optimal schedule of the binomial recursion (binomial_table).
+
 `MeanPower` wraps the same computation as a torch.autograd.Function; it is
 used only to check the gradients (torch.autograd.gradcheck-style comparisons),
 not as a training path.
@@ -52,17 +57,24 @@ class _StatePool:
             sim._adjoint_pool = buf
         self.buf, self.per, self.n = buf, per, 0
 
-    def save(self, sim):
-        """copy the simulation's state into the next free slot; returns a dict of views"""
-        base = self.n * self.per
-        self.n += 1
-        st, o = {}, base
+    def slot(self, i):
+        """views of the fields of slot i"""
+        st, o = {}, i * self.per
         for f, size in zip(FIELDS, self.sizes):
-            v = self.buf[o:o + size]
-            v.copy_(getattr(sim, f).reshape(-1))
-            st[f] = v
+            st[f] = self.buf[o:o + size]
             o += size
         return st
+
+    def put(self, i, sim):
+        """copy the simulation's state into slot i"""
+        for f, v in self.slot(i).items():
+            v.copy_(getattr(sim, f).reshape(-1))
+
+    def save(self, sim):
+        """copy the simulation's state into the next free slot; returns a dict of views"""
+        self.put(self.n, sim)
+        self.n += 1
+        return self.slot(self.n - 1)
 
 
 def state_bytes(sim):
@@ -146,6 +158,134 @@ def mean_power_gradient(sim, steps, checkpoint=None):
                              u_after=states[q + 1]["u"])
     _restore(sim, end_state)
     sim.it = end_it
+    g = grad.cpu().numpy()
+    return J, float(g[0]), g[1:1 + apc].copy(), g[1 + apc:].copy()
+
+
+# ---------------------------------------------------------------- binomial checkpointing
+_BINOMIAL = {}
+
+
+def binomial_table(steps, snaps):
+    """Optimal reversal schedule of `steps` steps with `snaps` free state slots
+    (besides the one holding the start of the window), by dynamic programming
+    over the recursion of binomial (revolve-type) checkpointing: to reverse
+    t >= 2 steps with s free slots, advance m steps from the start, store that
+    state, reverse the last t - m steps with s - 1 slots, then the first m with
+    s.  G[t][s] is the least number of forward steps those advances take (each
+    reversed step also recomputes its own forward step once); split[t][s] is an
+    m that attains it.  With s = 0 every reversal restarts from the start:
+    G[t][0] = t (t - 1) / 2."""
+    key = (steps, snaps)
+    if key in _BINOMIAL:
+        return _BINOMIAL[key]
+    T, S = steps, snaps
+    G = np.zeros((T + 1, S + 1), dtype=np.int64)
+    split = np.zeros((T + 1, S + 1), dtype=np.int64)
+    t = np.arange(T + 1, dtype=np.int64)
+    G[:, 0] = t * (t - 1) // 2
+    G[0, :] = 0
+    for s in range(1, S + 1):
+        for tt in range(2, T + 1):
+            m = np.arange(1, tt)
+            cost = m + G[tt - m, s - 1] + G[m, s]
+            k = int(np.argmin(cost))
+            G[tt, s] = cost[k]
+            split[tt, s] = m[k]
+    _BINOMIAL[key] = (G, split)
+    return G, split
+
+
+def binomial_forward_steps(steps, snaps):
+    """forward steps of a binomial reversal (the advances plus the one forward
+    step each reversed step recomputes), the initial pass included"""
+    G, _ = binomial_table(steps, snaps)
+    return int(G[steps, snaps]) + steps
+
+
+def snaps_for_budget(sim, budget_bytes):
+    """free state slots that `budget_bytes` of device memory holds (the slot of the
+    window's start not counted)"""
+    return max(0, int(budget_bytes // state_bytes(sim)) - 1)
+
+
+def mean_power_gradient_binomial(sim, steps, snaps=None, budget_bytes=None):
+    """J and its gradient (pitch, chord[apcount], twist[apcount]) like
+    mean_power_gradient, with binomial checkpointing: besides the window's
+    start, its end and one scratch state, at most `snaps` states (or as many as
+    `budget_bytes` of device memory holds, by default a quarter of the free
+    memory) are stored at any time, and the reversal recomputes forward steps
+    from them along the optimal schedule of binomial_table.  Each step's power
+    is taken from the first forward evaluation of that step (the step is
+    deterministic: every evaluation gives the same value).  sim ends after the
+    window."""
+    ctx = sim.ctx
+    torch = ctx.torch
+    if ctx.precision != "fp64":
+        raise ValueError("the discrete adjoint runs in FP64 contexts")
+    if snaps is None:
+        if budget_bytes is None:
+            budget_bytes = 0.25 * torch.cuda.mem_get_info(sim.u.device)[0]
+        snaps = snaps_for_budget(sim, budget_bytes) - 2
+    snaps = max(0, min(int(snaps), steps - 1))
+    _, split = binomial_table(steps, snaps)
+    apc = sim.case.alm.apcount
+    it0 = sim.it
+    n = sim.case.grid.n
+    dev, dt = ctx.device, sim.case.dt
+    pool = _StatePool(sim, snaps + 3)
+    START, SCRATCH, END = 0, snaps + 1, snaps + 2
+    free_slots = list(range(snaps, 0, -1))
+    au = torch.zeros(3 * n, dtype=torch.float64, device=dev)
+    auu = torch.zeros(3 * n, dtype=torch.float64, device=dev)
+    anut = torch.zeros(n, dtype=torch.float64, device=dev)
+    grad = torch.zeros(1 + 2 * apc, dtype=torch.float64, device=dev)
+    power = {}
+
+    def goto(a, slot):
+        _restore(sim, pool.slot(slot))
+        sim.it = it0 + a
+
+    def advance(a, m):
+        for q in range(m):
+            power.setdefault(a + q, _power(sim, sim.step()))
+
+    def reverse_one(a, slot):
+        # slot holds the state of step a, which sim is at: its forward step (the
+        # power, the velocity after it), then its adjoint
+        S = pool.slot(slot)
+        power.setdefault(a, _power(sim, sim.step()))
+        if a == steps - 1:
+            pool.put(END, sim)
+        ctx.step_adjoint(S["u"], S["uu"], S["p"], S["nut"], dt, (it0 + a + 1) * dt, 1.0 / steps, au, auu, anut, grad,
+                         u_after=sim.u)
+
+    def reverse(a, b, slot, free):
+        t = b - a
+        if t == 1:
+            goto(a, slot)
+            reverse_one(a, slot)
+        elif free == 0:
+            for i in reversed(range(t)):
+                goto(a, slot)
+                advance(a, i)
+                pool.put(SCRATCH, sim)
+                reverse_one(a + i, SCRATCH)
+        else:
+            m = int(split[t, free])
+            goto(a, slot)
+            advance(a, m)
+            s2 = free_slots.pop()
+            pool.put(s2, sim)
+            reverse(a + m, b, s2, free - 1)
+            free_slots.append(s2)
+            reverse(a, a + m, slot, free)
+
+    pool.put(START, sim)
+    reverse(0, steps, START, snaps)
+    J = sum(power[q] for q in range(steps)) / steps
+    _restore(sim, pool.slot(END))
+    sim.it = it0 + steps
     g = grad.cpu().numpy()
     return J, float(g[0]), g[1:1 + apc].copy(), g[1 + apc:].copy()
 

@@ -229,6 +229,10 @@ class Context:
                     "step_adjoint")
 
 
+    def adjoint_set_tol(self, rel_tol):
+        """relative residual of the adjoint's transposed Poisson solve (0: the default)"""
+        self._check(self.lib.falm_adjoint_set_tol(self.h, float(rel_tol)), "adjoint_set_tol")
+
     # ------------------------------------------------------------ output (FalmIO, TAvg)
     def tavg(self, avg, f, count):
         """FalmSolver::TAvg (src/falm.h:433-444): avg = (1 - 1/count) avg + f/count"""

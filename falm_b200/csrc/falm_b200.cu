@@ -1948,6 +1948,12 @@ int adj_work(falm_ctx *ctx, AdjWork *w) {
 
 }  // namespace
 
+extern "C" int falm_adjoint_set_tol(falm_ctx *ctx, double rel_tol) {
+    if (!ctx || !(rel_tol >= 0) || rel_tol >= 1) return FALM_ERR_ARG;
+    ctx->adj_rel_tol = rel_tol;
+    return FALM_OK;
+}
+
 extern "C" int falm_step_adjoint(falm_ctx *ctx, const falm_fields *f0, const falm_fields *f1, double dt, double t, double w_power,
                                  void *au, void *auu, void *anut, double *grad, void *stream) {
     if (!ctx || !f0 || !f0->u || !f0->uu || !f0->p || !f0->nut || !au || !auu || !anut || !grad || !(dt > 0)) return FALM_ERR_ARG;
@@ -2014,9 +2020,10 @@ extern "C" int falm_step_adjoint(falm_ctx *ctx, const falm_fields *f0, const fal
         ctx->ls_type = FALM_LS_PBICGSTAB;   // whatever solver the forward step uses
         if (!use_tables) ctx->A_explicit = w.AT;
         LAUNCH(FALM_K_OTHER, st, k_adj_extrapolate<<<grid, 256, 0, st>>>(w.arhs, w.arhs1, (long long)n));
-        // relative residual 1e-6 (1e-12 when the context's tolerance is below 1e-12):
-        // well below the gradient accuracy the forward solve's tolerance allows
-        ctx->tol = (tol_saved < 1e-12 ? 1e-12 : 1e-6) / ((double)g.nx * g.ny * g.nz);
+        // relative residual ctx->adj_rel_tol (falm_adjoint_set_tol); by default 1e-5
+        // (1e-12 when the context's tolerance is below 1e-12)
+        const double rel = ctx->adj_rel_tol > 0 ? ctx->adj_rel_tol : (tol_saved < 1e-12 ? 1e-12 : 1e-5);
+        ctx->tol = rel / ((double)g.nx * g.ny * g.nz);
         int it = 0, outer = 0;
         double err = 0;
         rc = solve_t<double>(ctx, w.arhs, w.ap, w.r, st, &it, &err, &outer);

@@ -134,6 +134,7 @@ struct falm_ctx {
     size_t esize;
     void *work_mem;
     void *adj_mem;                          // discrete-adjoint workspace (allocated on first use)
+    double adj_rel_tol;                     // relative residual of the adjoint's transposed Poisson solve (0: default)
     void *w_rr, *w_p, *w_q, *w_s, *w_pp, *w_ss, *w_t, *w_r, *w_rhs, *w_ua, *w_div, *w_xp;
     void *w_outlet;                         // 3 planes x 3 comps of the previous velocity at the outlet
     // reductions

@@ -251,7 +251,8 @@ int falm_mesh_build(const char *cvcenter, const char *meshpath, const char *outp
 /* No reference counterpart.  Adjoint of falm_step for FP64 contexts (Upwind3/UTOPIA/KK advection,
    Smagorinsky or no SGS, channel or cavity), with the Poisson solve treated as exact (its adjoint is
    one solve with the transposed operator, started from an extrapolation of the previous calls', to a
-   relative residual of 1e-6, or 1e-12 when the context's tolerance is below 1e-12).  f0: the DEVICE state
+   relative residual of 1e-5, or 1e-12 when the context's tolerance is below 1e-12; see
+   falm_adjoint_set_tol).  f0: the DEVICE state
    (u, uu, p, nut; ff unused) at the start of the step, left unchanged; t: that step's time (as given
    to falm_step); w_power: the weight of this step's rotor power (sum over turbines of torque x tip
    rate) in the objective.  au (3N), auu (3N), anut (N): DEVICE adjoint of the state after the step
@@ -263,6 +264,13 @@ int falm_mesh_build(const char *cvcenter, const char *meshpath, const char *outp
    pays one forward step less per adjoint step. */
 int falm_step_adjoint(falm_ctx *ctx, const falm_fields *f0, const falm_fields *f1, double dt, double t,
                       double w_power, void *au, void *auu, void *anut, double *grad, void *stream);
+/* No reference counterpart.  Relative residual (||r|| / ||b||) to which falm_step_adjoint solves
+   its transposed Poisson system; 0 restores the default (1e-5, or 1e-12 when the context's
+   tolerance is below 1e-12).  The gradient's error from an inexact transposed solve is of the
+   order of this tolerance times the sensitivity carried by the pressure: on the 128x64x64
+   rotor case over 200 steps, 1e-4 and 1e-5 leave the gradient within 1e-5 of central finite
+   differences, as an exact solve does. */
+int falm_adjoint_set_tol(falm_ctx *ctx, double rel_tol);
 
 /* ---------------- allocation-free inner product --------------------------------------------- */
 /* No reference counterpart.  The interior inner product of falm_mv_dot for callers that hold

@@ -115,3 +115,62 @@ def test_step_adjoint_with_and_without_the_next_state(run):
         out.append([x.cpu().numpy() for x in (au, auu, anut, grad)])
     for a, b in zip(*out):
         np.testing.assert_allclose(a, b, rtol=1e-9, atol=1e-9 * np.abs(b).max())
+
+
+@pytest.mark.parametrize("snaps", [0, 1, 3])
+def test_binomial_checkpointing_matches_keep_all(run, snaps):
+    """Binomial checkpointing (at most `snaps` stored states besides the start,
+    the end and one scratch state, steps recomputed along the optimal binomial
+    schedule) gives the objective and gradient of the keep-everything reversal
+    over a 9-step window: the forward steps are deterministic, so only the
+    transposed solves' warm starts differ (within their tolerance)."""
+    case, sim, start, J, gp, gc, gt = run
+    restart(sim, start)
+    Jk, gpk, gck, gtk = A.mean_power_gradient(sim, 9, checkpoint=9)
+    end_u = sim.u.clone()
+    restart(sim, start)
+    Jb, gpb, gcb, gtb = A.mean_power_gradient_binomial(sim, 9, snaps=snaps)
+    assert Jb == pytest.approx(Jk, rel=1e-14)
+    assert gpb == pytest.approx(gpk, rel=1e-9)
+    np.testing.assert_allclose(gcb, gck, rtol=1e-9, atol=1e-12 * np.abs(gck).max())
+    np.testing.assert_allclose(gtb, gtk, rtol=1e-9, atol=1e-12 * np.abs(gtk).max())
+    assert sim.it == start[0] + 9
+    assert np.array_equal(sim.u.cpu().numpy(), end_u.cpu().numpy())
+
+
+def test_adjoint_at_the_adjoint_configuration_size_matches_fd(lib_built):
+    """The adjoint configuration at its own size and length: 128x64x64 channel,
+    rotor of radius 10 cells with 3 x 32 actuator points, seeded 5% inflow,
+    J = mean rotor power over 200 steps from a spun-up state, a checkpoint every
+    20 steps with recomputation in between, the default transposed-solve
+    tolerance (relative 1e-5).  The forward Poisson solve runs at err 1e-13 here
+    so that J is a smooth function of the parameters (at 1e-8, iteration-count
+    changes make central differences of J noisy at the 1e-4 level).
+    Central differences (step 1e-4 for the collective pitch and the chord of
+    two actuator points; 1e-3 for their twist, whose derivatives are 100x
+    smaller, so that the difference of J stands above the solver's noise) agree
+    with the adjoint gradient to 1e-4 relative."""
+    case = cases.adjoint_case().with_inflow()
+    case.tol, case.maxit = 1e-13, 2000
+    sim = Simulation(case, "fp64")
+    for _ in range(10):
+        sim.step()
+    start = (sim.it, A._clone(sim))
+    steps, apc = 200, case.alm.apcount
+    J, gp, gc, gt = A.mean_power_gradient(sim, steps, checkpoint=20)
+    p0 = A.parameters(sim)
+
+    def J_at(params):
+        A._set_params(sim, params)
+        restart(sim, start)
+        return A.objective(sim, steps)
+
+    for idx, adj, h in ((0, gp, 1e-4), (1 + 20, gc[20], 1e-4), (1 + 57, gc[57], 1e-4),
+                        (1 + apc + 20, gt[20], 1e-3), (1 + apc + 57, gt[57], 1e-3)):
+        pp, pm = p0.copy(), p0.copy()
+        pp[idx] += h
+        pm[idx] -= h
+        fd = (J_at(pp) - J_at(pm)) / (2 * h)
+        assert adj == pytest.approx(fd, rel=1e-4), (idx, adj, fd)
+    A._set_params(sim, p0)
+    sim.close()
