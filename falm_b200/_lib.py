@@ -53,6 +53,11 @@ class StepStats(ctypes.Structure):
 
 V, D, I, LL, P = ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_longlong, ctypes.c_void_p
 
+
+class Transport(ctypes.Structure):
+    """falm_transport: halo exchange and reductions between the slabs of a grid"""
+    _fields_ = [("user", ctypes.c_void_p), ("exchange", ctypes.c_void_p), ("allreduce", ctypes.c_void_p)]
+
 # name -> argtypes (restype is int unless listed in _RESTYPE)
 SIGNATURES = {
     "falm_abi_version": [],
@@ -103,6 +108,14 @@ SIGNATURES = {
     "falm_io_read_cv_file": [ctypes.c_char_p, c_int_p, c_double_p, c_double_p, c_double_p, c_double_p, c_double_p, c_double_p],
     "falm_mesh_build": [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, I],
     "falm_debug_arm_wait_probe": [V, LL],
+    "falm_slab_init": [V, I, I, I, I, ctypes.POINTER(Transport)],
+    "falm_slab_halo": [V, P, I, I, P],
+    "falm_local_hub_create": [I, ctypes.POINTER(ctypes.c_void_p)],
+    "falm_local_hub_transport": [V, I, ctypes.POINTER(Transport)],
+    "falm_local_hub_destroy": [V],
+    "falm_nccl_unique_id": [ctypes.POINTER(ctypes.c_ubyte * 128)],
+    "falm_nccl_transport_create": [ctypes.POINTER(ctypes.c_ubyte * 128), I, I, ctypes.POINTER(Transport)],
+    "falm_nccl_transport_destroy": [ctypes.POINTER(Transport)],
     "falm_profile_enable": [V, I],
     "falm_profile_read": [V, c_double_p, ctypes.POINTER(ctypes.c_longlong), I, I],
 }

@@ -229,6 +229,17 @@ class Context:
                     "step_adjoint")
 
 
+    # ------------------------------------------------------------ z slabs
+    def slab_init(self, rank, nranks, z_offset, nz_global, transport):
+        """falm_slab_init: this context is slab `rank` of a grid split along z"""
+        self._transport = transport
+        self._check(self.lib.falm_slab_init(self.h, rank, nranks, z_offset, nz_global, ctypes.byref(transport)), "slab_init")
+
+    def slab_halo(self, field, depth=1):
+        """exchange `depth` guide planes of a field with the neighbouring slabs"""
+        ncol = field.numel() // self.grid.n
+        self._check(self.lib.falm_slab_halo(self.h, _ptr(field), ncol, depth, self.stream()), "slab_halo")
+
     def adjoint_set_tol(self, rel_tol):
         """relative residual of the adjoint's transposed Poisson solve (0: the default)"""
         self._check(self.lib.falm_adjoint_set_tol(self.h, float(rel_tol)), "adjoint_set_tol")

@@ -86,8 +86,10 @@ __global__ void __launch_bounds__(256) k_alm_force(Geom g, AlmDev a, const doubl
         for (int d = 0; d < 3; d++) a.ap_xyz[3 * ap + d] = c0[d];
         if (keep) for (int d = 0; d < 3; d++) s_xyz[3 * ap + d] = c0[d];
         int I = find_index(xc, c0[0], g.sx), J = find_index(yc, c0[1], g.sy), K = find_index(zc, c0[2], g.sz);
-        bool inside = I >= g.gc - 1 && I < g.sx - g.gc - 1 && J >= g.gc - 1 && J < g.sy - g.gc - 1 &&
-                      K >= g.gc - 1 && K < g.sz - g.gc - 1;
+        // a slab evaluates the points whose lower interpolation plane K it owns:
+        // its interior planes, and the guide plane below at a physical face
+        const int klo = (g.zphys & 1) ? g.gc - 1 : g.gc, khi = (g.zphys & 2) ? g.sz - g.gc - 1 : g.sz - g.gc;
+        bool inside = I >= g.gc - 1 && I < g.sx - g.gc - 1 && J >= g.gc - 1 && J < g.sy - g.gc - 1 && K >= klo && K < khi;
         if (!inside) {
             for (int d = 0; d < 3; d++) a.ap_force[3 * ap + d] = 0;
             a.ap_torque[ap] = 0; a.ap_thrust[ap] = 0;
@@ -158,6 +160,20 @@ __global__ void __launch_bounds__(256) k_alm_force(Geom g, AlmDev a, const doubl
             a.scal->torque[tid] = tq;
             a.scal->thrust[tid] = th;
         }
+    }
+}
+
+// per-turbine torque and thrust from the per-AP arrays (CalcTorqueAndThrust,
+// src/alm/almDevCall.cu:362-370), in the order k_alm_force sums them; run
+// after the per-AP arrays were summed over the slabs of a decomposed grid
+__global__ void k_alm_turbine_sums(AlmDev a) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int nappt = a.n_ap_per_blade * a.n_blade;
+    for (int tid = 0; tid < a.n_turbine && tid < kMaxTurbines; tid++) {
+        double tq = 0, th = 0;
+        for (int q = 0; q < nappt; q++) { tq += a.ap_torque[tid * nappt + q]; th += a.ap_thrust[tid * nappt + q]; }
+        a.scal->torque[tid] = tq;
+        a.scal->thrust[tid] = th;
     }
 }
 
@@ -298,7 +314,8 @@ __global__ void k_ubc(Geom g, int kind, T *u, UPrev<T> up, const double *xc, dou
                     long long s = (long long)fl % inf.nb;
                     if (s < 0) s += inf.nb;
                     int s0 = (int)s, s1 = (s0 + 1) % inf.nb;
-                    long long plane = (long long)(sy - 2 * gc) * (sz - 2 * gc), jk = (j - gc) + (long long)(k - gc) * (sy - 2 * gc);
+                    // the box covers the whole grid's inlet plane (a slab reads its own planes)
+                    long long plane = (long long)(sy - 2 * gc) * g.nzg, jk = (j - gc) + (long long)(k - gc + g.koff) * (sy - 2 * gc);
                     for (int d = 0; d < 3; d++) {
                         const double *bx = inf.box + (long long)d * inf.nb * plane;
                         ub[d] += (1.0 - fr) * bx[s0 * plane + jk] + fr * bx[s1 * plane + jk];
@@ -325,12 +342,14 @@ __global__ void k_ubc(Geom g, int kind, T *u, UPrev<T> up, const double *xc, dou
                 T v1[3] = {u[in], T(0), u[in + 2 * N]};
                 for (int d = 0; d < 3; d++) { u[g.id(i, sy - gc, k) + d * N] = v1[d]; u[g.id(i, sy - gc + 1, k) + d * N] = T(2) * v1[d] - u[in + d * N]; }
             } else {
-                int i = a, j = b;   // no-slip z- (:82-97), slip z+ (:100-115)
+                int i = a, j = b;   // no-slip z- (:82-97), slip z+ (:100-115); slab interfaces are left alone
                 long long in = g.id(i, j, gc);
-                for (int d = 0; d < 3; d++) { u[g.id(i, j, gc - 1) + d * N] = T(0); u[g.id(i, j, gc - 2) + d * N] = T(2) * T(0) - u[in + d * N]; }
+                if (g.zphys & 1)
+                    for (int d = 0; d < 3; d++) { u[g.id(i, j, gc - 1) + d * N] = T(0); u[g.id(i, j, gc - 2) + d * N] = T(2) * T(0) - u[in + d * N]; }
                 in = g.id(i, j, sz - gc - 1);
                 T w1[3] = {u[in], u[in + N], T(0)};
-                for (int d = 0; d < 3; d++) { u[g.id(i, j, sz - gc) + d * N] = w1[d]; u[g.id(i, j, sz - gc + 1) + d * N] = T(2) * w1[d] - u[in + d * N]; }
+                if (g.zphys & 2)
+                    for (int d = 0; d < 3; d++) { u[g.id(i, j, sz - gc) + d * N] = w1[d]; u[g.id(i, j, sz - gc + 1) + d * N] = T(2) * w1[d] - u[in + d * N]; }
             }
         } else {
             // cavity, app/lid3d/bcdev.cu:11-105: reflection about the wall value, lid on y+
@@ -351,10 +370,14 @@ __global__ void k_ubc(Geom g, int kind, T *u, UPrev<T> up, const double *xc, dou
                     ud[g.id(i, sy - gc + 1, k)] = T(2) * lid[d] - ud[g.id(i, sy - gc - 2, k)];
                 } else {
                     int i = a, j = b;
-                    ud[g.id(i, j, gc - 1)] = T(2) * T(0) - ud[g.id(i, j, gc)];
-                    ud[g.id(i, j, gc - 2)] = T(2) * T(0) - ud[g.id(i, j, gc + 1)];
-                    ud[g.id(i, j, sz - gc)] = T(2) * T(0) - ud[g.id(i, j, sz - gc - 1)];
-                    ud[g.id(i, j, sz - gc + 1)] = T(2) * T(0) - ud[g.id(i, j, sz - gc - 2)];
+                    if (g.zphys & 1) {
+                        ud[g.id(i, j, gc - 1)] = T(2) * T(0) - ud[g.id(i, j, gc)];
+                        ud[g.id(i, j, gc - 2)] = T(2) * T(0) - ud[g.id(i, j, gc + 1)];
+                    }
+                    if (g.zphys & 2) {
+                        ud[g.id(i, j, sz - gc)] = T(2) * T(0) - ud[g.id(i, j, sz - gc - 1)];
+                        ud[g.id(i, j, sz - gc + 1)] = T(2) * T(0) - ud[g.id(i, j, sz - gc - 2)];
+                    }
                 }
             }
         }
@@ -377,8 +400,8 @@ __global__ void k_pbc(Geom g, int kind, T *p) {
             p[g.id(a, gc - 1, b)] = p[g.id(a, gc, b)];
             p[g.id(a, sy - gc, b)] = p[g.id(a, sy - gc - 1, b)];
         } else {
-            p[g.id(a, b, gc - 1)] = p[g.id(a, b, gc)];
-            p[g.id(a, b, sz - gc)] = p[g.id(a, b, sz - gc - 1)];
+            if (g.zphys & 1) p[g.id(a, b, gc - 1)] = p[g.id(a, b, gc)];
+            if (g.zphys & 2) p[g.id(a, b, sz - gc)] = p[g.id(a, b, sz - gc - 1)];
         }
     }
 }
@@ -394,7 +417,10 @@ __global__ void k_uubc(Geom g, T *uu) {
         const int a = q % na + gc, b = q / na + gc;
         if (pair == 0) { uu[g.id(gc - 1, a, b)] = T(0); uu[g.id(sx - gc - 1, a, b)] = T(0); }
         else if (pair == 1) { uu[g.id(a, gc - 1, b) + g.n] = T(0); uu[g.id(a, sy - gc - 1, b) + g.n] = T(0); }
-        else { uu[g.id(a, b, gc - 1) + 2 * g.n] = T(0); uu[g.id(a, b, sz - gc - 1) + 2 * g.n] = T(0); }
+        else {
+            if (g.zphys & 1) uu[g.id(a, b, gc - 1) + 2 * g.n] = T(0);
+            if (g.zphys & 2) uu[g.id(a, b, sz - gc - 1) + 2 * g.n] = T(0);
+        }
     }
 }
 

@@ -206,7 +206,8 @@ __global__ void __launch_bounds__(kRowThreads) k_utouu(Geom g, Region3 R, Metric
             bool zero = false;
             if (d == 0) zero = (i == g.gc - 1 || i == g.sx - g.gc - 1) && j >= g.gc && j < g.sy - g.gc && k >= g.gc && k < g.sz - g.gc;
             if (d == 1) zero = (j == g.gc - 1 || j == g.sy - g.gc - 1) && i >= g.gc && i < g.sx - g.gc && k >= g.gc && k < g.sz - g.gc;
-            if (d == 2) zero = (k == g.gc - 1 || k == g.sz - g.gc - 1) && i >= g.gc && i < g.sx - g.gc && j >= g.gc && j < g.sy - g.gc;
+            if (d == 2) zero = ((k == g.gc - 1 && (g.zphys & 1)) || (k == g.sz - g.gc - 1 && (g.zphys & 2))) && i >= g.gc &&
+                               i < g.sx - g.gc && j >= g.gc && j < g.sy - g.gc;   // slab interfaces keep their faces
             if (zero) return T(0);
         }
         T a = ucv(d, i, j, k);

@@ -18,6 +18,10 @@
 #include <map>
 #include <climits>
 #include <tuple>
+#include <condition_variable>
+#include <chrono>
+#include <dlfcn.h>
+#include <nccl.h>
 #include "falm_internal.cuh"
 #include "common.cuh"
 #include "cfd.cuh"
@@ -408,10 +412,12 @@ int build_poisson(falm_ctx *ctx, int kind) {
             double coef_p = 0.5 * (gc0 + gmet(d, cp[0], cp[1], cp[2])) / jac;
             double coef_m = 0.5 * (gc0 + gmet(d, cm[0], cm[1], cm[2])) / jac;
             // app/nedo/main.cpp:55 keeps the x+ coefficient (p = 0 guide cell); every other
-            // physical face is Neumann (:60-83, app/lid3d/main.cpp:52-80)
+            // physical face is Neumann (:60-83, app/lid3d/main.cpp:52-80); a slab interface
+            // keeps its coefficients (the neighbour's plane lies beyond it)
             int plus_limit = (d == 0 && kind == FALM_BC_CHANNEL) ? s[d] - g.gc : s[d] - g.gc - 1;
+            if (d == 2 && !(g.zphys & 2)) plus_limit = s[d] - g.gc;
             if (q < plus_limit) up[d][q] = coef_p;
-            if (q > g.gc) um[d][q] = coef_m;
+            if (q > g.gc || (d == 2 && !(g.zphys & 1))) um[d][q] = coef_m;
         }
     }
     // maxdiag over the interior: |ac| is separable as well, but take the
@@ -422,6 +428,16 @@ int build_poisson(falm_ctx *ctx, int kind) {
                 double ac = ((((-up[0][i]) - um[0][i]) - up[1][j]) - um[1][j] - up[2][k]) - um[2][k];
                 maxdiag = std::max(maxdiag, std::fabs(ac));
             }
+    if (ctx->slab_on && ctx->slab_nranks > 1) {
+        // the maximum over the slabs (a collective: every rank builds its operator)
+        double *d = nullptr;
+        if (cudaMalloc(&d, sizeof(double)) != cudaSuccess) { cudaGetLastError(); return fail(ctx, FALM_ERR_ALLOC, "poisson: maxdiag"); }
+        int rc = cudaMemcpy(d, &maxdiag, sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess ? FALM_OK : FALM_ERR_CUDA;
+        if (!rc) rc = ctx->transport.allreduce(ctx->transport.user, d, 1, FALM_REDUCE_MAX, nullptr);
+        if (!rc && (cudaMemcpy(&maxdiag, d, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)) rc = FALM_ERR_CUDA;
+        cudaFree(d);
+        if (rc) { cudaGetLastError(); return fail(ctx, rc, "poisson: maxdiag over the slabs"); }
+    }
     double scale = 1.0 / maxdiag;
     // layout: for each d: cm, cp, um, up (s[d] each), then dx0 (sx)
     size_t tot = 0;
@@ -456,6 +472,7 @@ int build_poisson(falm_ctx *ctx, int kind) {
     }
     ctx->pt64.dx0 = d64 + o_dx0; ctx->pt32.dx0 = d32 + o_dx0;
     ctx->pt64.scale = scale; ctx->pt32.scale = (float)scale;
+    ctx->pt64.koff = ctx->pt32.koff = g.koff;
     ctx->maxdiag = maxdiag;
     ctx->op_ready = 1;
     ctx->bc_kind_op = kind;
@@ -474,7 +491,7 @@ int solver_init(falm_ctx *ctx, cudaStream_t st) {
     const Geom &g = ctx->geo;
     SolverScalars init;
     memset(&init, 0, sizeof(init));
-    init.gsize = (double)g.nx * g.ny * g.nz;
+    init.gsize = (double)g.nx * g.ny * g.nzg;   // interior cells of the whole grid (of all slabs)
     init.tol = ctx->tol;
     init.maxit = ctx->maxit;
     CK(cudaMemcpyAsync(ctx->scal, &init, sizeof(init), cudaMemcpyHostToDevice, st));
@@ -928,6 +945,8 @@ int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_
     return FALM_OK;
 }
 
+#include "slab.cuh"
+
 // run f with a value of the context's storage type (double or float)
 template <typename F>
 int dispatch(const falm_ctx *ctx, F &&f) {
@@ -959,6 +978,7 @@ int falm_create(const falm_grid *grid, int precision, falm_ctx **out) {
     g.sx = grid->sx; g.sy = grid->sy; g.sz = grid->sz; g.gc = grid->gc;
     g.n = (long long)g.sx * g.sy * g.sz;
     g.nx = g.sx - 2 * g.gc; g.ny = g.sy - 2 * g.gc; g.nz = g.sz - 2 * g.gc;
+    g.koff = 0; g.zphys = 3; g.nzg = g.nz;
     ctx->hx = new std::vector<double>(grid->hx, grid->hx + g.sx);
     ctx->hy = new std::vector<double>(grid->hy, grid->hy + g.sy);
     ctx->hz = new std::vector<double>(grid->hz, grid->hz + g.sz);
@@ -1174,6 +1194,7 @@ int falm_eq_solve(falm_ctx *ctx, void *x, const void *b, void *r, void *stream, 
     if (!ctx || !x || !b || !r) return FALM_ERR_ARG;
     int rc = dispatch(ctx, [&](auto z) {
         using T = decltype(z);
+        if (ctx->slab_on) return slab_solve_t<T>(ctx, (T *)x, (const T *)b, (T *)r, S(stream), it_out, err_out, nullptr);
         return solve_t<T>(ctx, (T *)x, (const T *)b, (T *)r, S(stream), it_out, err_out, nullptr);
     });
     if (rc) return rc;
@@ -1540,7 +1561,7 @@ int falm_bc_set_inflow(falm_ctx *ctx, const double *box, int nb, double dx) {
     if (ctx->inflow_box) { cudaFree(ctx->inflow_box); ctx->inflow_box = nullptr; }
     if (!box) return FALM_OK;
     if (nb < 2 || !(dx > 0)) return FALM_ERR_ARG;
-    size_t n = 3ull * nb * ctx->geo.ny * ctx->geo.nz;
+    size_t n = 3ull * nb * ctx->geo.ny * ctx->geo.nzg;   // the whole grid's inlet (a slab reads its own planes)
     CK(cudaMalloc(&ctx->inflow_box, n * sizeof(double)));
     CK(cudaMemcpy(ctx->inflow_box, box, n * sizeof(double), cudaMemcpyHostToDevice));
     ctx->inflow_nb = nb;
@@ -1736,6 +1757,7 @@ int falm_step(falm_ctx *ctx, const falm_fields *f, double dt, double t, void *st
     if (!ctx || !f || !f->u || !f->uu || !f->p || !f->nut || !(dt > 0)) return FALM_ERR_ARG;
     return dispatch(ctx, [&](auto z) {
         using T = decltype(z);
+        if (ctx->slab_on) return slab_step_t<T>(ctx, f, dt, t, S(stream), st);
         return step_t<T>(ctx, f, dt, t, S(stream), st);
     });
 }
@@ -1750,6 +1772,99 @@ int falm_bc_set_inlet_plane(falm_ctx *ctx, const double *plane, void *stream) {
     if (!ctx->inlet_plane) CK(cudaMalloc(&ctx->inlet_plane, n * sizeof(double)));
     CK(cudaMemcpyAsync(ctx->inlet_plane, plane, n * sizeof(double), cudaMemcpyHostToDevice, S(stream)));
     ctx->inlet_plane_valid = 1;
+    return FALM_OK;
+}
+
+int falm_slab_init(falm_ctx *ctx, int rank, int nranks, int z_offset, int nz_global, const falm_transport *t) {
+    if (!ctx || nranks < 1 || rank < 0 || rank >= nranks || !t || !t->exchange || !t->allreduce) return FALM_ERR_ARG;
+    Geom &g = ctx->geo;
+    if (z_offset < 0 || nz_global < g.nz || z_offset + g.nz > nz_global || g.nz < g.gc) return FALM_ERR_ARG;
+    if (ctx->op_ready || ctx->inflow_box || ctx->work_mem) return fail(ctx, FALM_ERR_STATE, "slab_init: call it right after falm_create");
+    if (rank == 0 && z_offset != 0) return FALM_ERR_ARG;
+    if (rank == nranks - 1 && z_offset + g.nz != nz_global) return FALM_ERR_ARG;
+    g.koff = z_offset;
+    g.nzg = nz_global;
+    g.zphys = (rank == 0 ? 1 : 0) | (rank == nranks - 1 ? 2 : 0);
+    ctx->slab_on = 1;
+    ctx->slab_rank = rank;
+    ctx->slab_nranks = nranks;
+    ctx->transport = *t;
+    return FALM_OK;
+}
+
+int falm_slab_halo(falm_ctx *ctx, void *field, int ncomp, int depth, void *stream) {
+    if (!ctx || !field || ncomp < 1 || depth < 1) return FALM_ERR_ARG;
+    if (!ctx->slab_on) return FALM_OK;
+    return dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        return slab_halo<T>(ctx, (T *)field, ncomp, depth, S(stream));
+    });
+}
+
+int falm_local_hub_create(int nranks, void **hub) {
+    if (nranks < 1 || !hub) return FALM_ERR_ARG;
+    LocalHub *h = new LocalHub();
+    h->n = nranks;
+    h->r.resize(nranks);
+    for (int q = 0; q < nranks; q++) h->users.push_back(new HubUser{h, q});
+    *hub = h;
+    return FALM_OK;
+}
+
+int falm_local_hub_transport(void *hub, int rank, falm_transport *out) {
+    LocalHub *h = (LocalHub *)hub;
+    if (!h || !out || rank < 0 || rank >= h->n) return FALM_ERR_ARG;
+    out->user = h->users[rank];
+    out->exchange = hub_exchange;
+    out->allreduce = hub_allreduce;
+    return FALM_OK;
+}
+
+int falm_local_hub_destroy(void *hub) {
+    LocalHub *h = (LocalHub *)hub;
+    if (!h) return FALM_ERR_ARG;
+    for (auto &r : h->r) {
+        if (r.ready) cudaEventDestroy(r.ready);
+        if (r.done) cudaEventDestroy(r.done);
+        if (r.scratch) cudaFree(r.scratch);
+    }
+    for (void *u : h->users) delete (HubUser *)u;
+    delete h;
+    return FALM_OK;
+}
+
+int falm_nccl_unique_id(unsigned char id[128]) {
+    const NcclApi *a = nccl_api();
+    if (!id) return FALM_ERR_ARG;
+    if (!a) return FALM_ERR_STATE;
+    static_assert(sizeof(ncclUniqueId) == 128, "ncclUniqueId is 128 bytes");
+    ncclUniqueId u;
+    if (a->get_unique_id(&u) != ncclSuccess) return FALM_ERR_CUDA;
+    memcpy(id, &u, 128);
+    return FALM_OK;
+}
+
+int falm_nccl_transport_create(const unsigned char id[128], int rank, int nranks, falm_transport *out) {
+    const NcclApi *a = nccl_api();
+    if (!id || !out || nranks < 1 || rank < 0 || rank >= nranks) return FALM_ERR_ARG;
+    if (!a) return FALM_ERR_STATE;
+    ncclUniqueId u;
+    memcpy(&u, id, 128);
+    NcclUser *nu = new NcclUser{nullptr, rank, nranks};
+    if (a->comm_init_rank(&nu->comm, nranks, u, rank) != ncclSuccess) { delete nu; return FALM_ERR_CUDA; }
+    out->user = nu;
+    out->exchange = nccl_exchange;
+    out->allreduce = nccl_allreduce;
+    return FALM_OK;
+}
+
+int falm_nccl_transport_destroy(falm_transport *t) {
+    const NcclApi *a = nccl_api();
+    if (!t || !t->user || t->exchange != nccl_exchange) return FALM_ERR_ARG;
+    NcclUser *nu = (NcclUser *)t->user;
+    if (a && nu->comm) a->comm_destroy(nu->comm);
+    delete nu;
+    t->user = nullptr;
     return FALM_OK;
 }
 
@@ -1890,6 +2005,7 @@ extern "C" int falm_mv_dot_static(int sx, int sy, int sz, int gc, int precision,
     g.sx = sx; g.sy = sy; g.sz = sz; g.gc = gc;
     g.n = (long long)sx * sy * sz;
     g.nx = sx - 2 * gc; g.ny = sy - 2 * gc; g.nz = sz - 2 * gc;
+    g.koff = 0; g.zphys = 3; g.nzg = g.nz;
     const Region3 R = interior(g);
     RedWork rw{(double *)p, (unsigned int *)(p + kCounterOff), kStaticDotBlocks};
     double *res = (double *)(p + kResultOff);
@@ -1958,6 +2074,7 @@ extern "C" int falm_step_adjoint(falm_ctx *ctx, const falm_fields *f0, const fal
                                  void *au, void *auu, void *anut, double *grad, void *stream) {
     if (!ctx || !f0 || !f0->u || !f0->uu || !f0->p || !f0->nut || !au || !auu || !anut || !grad || !(dt > 0)) return FALM_ERR_ARG;
     if (ctx->precision != FALM_FP64) return fail(ctx, FALM_ERR_ARG, "step_adjoint: FP64 contexts only");
+    if (ctx->slab_on && ctx->slab_nranks > 1) return fail(ctx, FALM_ERR_ARG, "step_adjoint: a grid of one slab only");
     if (ctx->adv != FALM_ADV_UPWIND3 && ctx->adv != FALM_ADV_UTOPIA && ctx->adv != FALM_ADV_KK)
         return fail(ctx, FALM_ERR_ARG, "step_adjoint: the 4th-order advection schemes (Upwind3, UTOPIA, KK) only");
     if (ctx->sgs != FALM_SGS_EMPTY && ctx->sgs != FALM_SGS_SMAGORINSKY) return fail(ctx, FALM_ERR_ARG, "step_adjoint: Smagorinsky or no SGS model only");

@@ -36,12 +36,17 @@ struct PoissonTables {
     const T *up[3];   // unscaled plus coefficients
     const T *dx0;     // (-e) - w, unscaled, per i: first two terms of the diagonal
     T scale;          // 1/maxdiag
+    int koff;         // the grid's Geom::koff: red-black colour (i + j + k + koff) & 1
 };
 
 struct Geom {
     int sx, sy, sz, gc;
     long long n;      // sx*sy*sz
     int nx, ny, nz;   // interior sizes
+    // z slab of a decomposed grid (falm_slab_init); one slab covers the grid otherwise
+    int koff;         // global index of local plane 0 minus 0: the red-black colour is (i + j + k + koff) & 1
+    int zphys;        // physical z faces: bit 0 the lower (k = gc - 1), bit 1 the upper; the others are slab interfaces
+    int nzg;          // interior planes of the whole grid
     __host__ __device__ inline long long id(int i, int j, int k) const {
         return (long long)i + (long long)j * sx + (long long)k * sx * sy;
     }
@@ -56,7 +61,8 @@ struct SolverScalars {
     int first;          // 1 before the first BiCGStab iteration of a solve
     int kerr;           // bounded device-side wait gave up (FALM_ERR_TIMEOUT)
     int checked;        // the queued outer check of the true residual ran (mixed precision)
-    int pad;
+    int defer;          // slab mode: reduction kernels leave their local totals in red[] for a reduction
+                        // over the slabs, and k_slab_derive derives the scalars from the reduced totals
 };
 
 struct AlmScalars {
@@ -166,6 +172,9 @@ struct falm_ctx {
     int pu_v1;                              // FP32 pseudo-velocity on the one-cell-per-thread kernel (tests)
     int check_sync;                         // synchronise after every launch (fault location)
     long long wait_probe_cycles;            // >0: the next falm_step first runs a wait that nothing completes (tests)
+    // z slab of a decomposed grid (falm_slab_init)
+    int slab_on, slab_rank, slab_nranks;
+    falm_transport transport;               // halo exchange and reductions between the slabs
     std::string *last_error;
     fb::IoWriter *io;                       // snapshot writer (falm_io.cuh), created on first use
 };

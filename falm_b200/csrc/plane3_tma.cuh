@@ -255,7 +255,7 @@ struct UtoUUBody {
         const bool jin = j >= g.gc && j < g.sy - g.gc, kin = k >= g.gc && k < g.sz - g.gc, iin = i >= g.gc && i < g.sx - g.gc;
         if (d == 0) return (i == g.gc - 1 || i == g.sx - g.gc - 1) && jin && kin;
         if (d == 1) return (j == g.gc - 1 || j == g.sy - g.gc - 1) && iin && kin;
-        return (k == g.gc - 1 || k == g.sz - g.gc - 1) && iin && jin;
+        return ((k == g.gc - 1 && (g.zphys & 1)) || (k == g.sz - g.gc - 1 && (g.zphys & 2))) && iin && jin;   // not at slab interfaces
     }
     // face d of cell (i+dx, j+dy, k+dz) (the face towards +d)
     __device__ __forceinline__ T face(const P3View<T, 1> &v, const ColMet<T> &cm, int d, int i, int j, int k, int dx, int dy,
@@ -381,7 +381,7 @@ struct UtoUUResBody {
             const double rv = (double)bv - ax;
             const T rt = (T)rv;
             rr[c] = rt;
-            pp[c] = pc_first<T>(pc_type, i, j, k, rt, ac, pc_omega);
+            pp[c] = pc_first<T>(pc_type, i, j, k + op.t.koff, rt, ac, pc_omega);
             acc[0] += rv * rv;
             acc[1] += (double)rt * (double)rt;
         }

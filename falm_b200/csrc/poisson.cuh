@@ -164,6 +164,66 @@ __global__ void k_axby(T a, const T *x, T b, const T *y, T *r, long long n) {
         r[q] = a * x[q] + b * y[q];
 }
 
+// ---------------------------------------------------------------- BiCGStab scalars
+// From the reduced totals of a kernel's products (one thread).
+// start of a pass (src/FalmEq.cpp:329-336, 348-351): tot = {r.r (FP64), rr.r}
+__device__ __forceinline__ void derive_res(SolverScalars *sc, const double (&tot)[2], int check_tol) {
+    double err = sqrt(tot[0]) / sc->gsize;
+    sc->err = err;
+    sc->rho = tot[1];
+    sc->rrho = 1.0; sc->alpha = 0.0; sc->omega = 1.0; sc->beta = 0.0;
+    sc->first = 1;
+    sc->done = 0;
+    if (!isfinite(err)) { sc->done = 1; sc->status = FALM_ERR_NAN; }
+    else if (check_tol && err <= sc->tol) { sc->done = 1; sc->status = FALM_OK; }
+    else if (fabs(tot[1]) < FLT_MIN) {
+        sc->err = tot[1];
+        sc->done = 1;
+        sc->status = (err <= sc->tol) ? FALM_OK : FALM_ERR_BREAKDOWN;
+    }
+}
+// alpha = rho / (rr.q) (src/FalmEq.cpp:371)
+__device__ __forceinline__ void derive_alpha(SolverScalars *sc, const double (&tot)[1]) {
+    double alpha = sc->rho / tot[0];
+    sc->alpha = alpha;
+    if (!isfinite(alpha)) { sc->done = 1; sc->status = FALM_ERR_NAN; }
+}
+__device__ __forceinline__ void derive_alpha(SolverScalars *sc, const double (&tot)[2]) {
+    const double t1[1] = {tot[0]};
+    derive_alpha(sc, t1);
+}
+// omega = (t.s) / (t.t) (src/FalmEq.cpp:389)
+__device__ __forceinline__ void derive_omega(SolverScalars *sc, const double (&tot)[2]) {
+    double omega = tot[0] / tot[1];
+    sc->omega = omega;
+    if (!isfinite(omega)) { sc->done = 1; sc->status = FALM_ERR_NAN; }
+}
+// after x, r: tot = {r.r, r.rr}; the stop test (src/FalmEq.cpp:400-407) and,
+// for the next iteration, rho and beta (:345-356)
+__device__ __forceinline__ void derive_xr(SolverScalars *sc, const double (&tot)[2]) {
+    double rho = sc->rho;
+    sc->rrho = rho;
+    double err = sqrt(tot[0]) / sc->gsize;
+    sc->err = err;
+    sc->it += 1;
+    sc->first = 0;
+    if (!isfinite(err)) { sc->done = 1; sc->status = FALM_ERR_NAN; return; }
+    if (!(sc->it < sc->maxit && err > sc->tol)) {
+        sc->done = 1;
+        sc->status = err > sc->tol ? FALM_ERR_MAXIT : FALM_OK;
+        return;
+    }
+    double rho_n = tot[1];
+    if (fabs(rho_n) < FLT_MIN) {
+        sc->err = rho_n;
+        sc->done = 1;
+        sc->status = err <= sc->tol ? FALM_OK : FALM_ERR_BREAKDOWN;
+        return;
+    }
+    sc->beta = (rho_n * sc->alpha) / (rho * sc->omega);
+    sc->rho = rho_n;
+}
+
 // ---------------------------------------------------------------- residual (+ solver start)
 // src/dev/FalmEqDevCall.cu:54-85; evaluated in FP64 whatever the storage type
 // (the true-residual recomputation of the mixed-precision mode).  With sc !=
@@ -185,19 +245,8 @@ __global__ void __launch_bounds__(kRowThreads) k_res(Geom g, Region3 R, Op7<T> o
     if (!sc) return;
     double tot[2];
     if (grid_sum<2>(acc, rw, tot) && threadIdx.x == 0) {
-        double err = sqrt(tot[0]) / sc->gsize;
-        sc->err = err;
-        sc->rho = tot[1];
-        sc->rrho = 1.0; sc->alpha = 0.0; sc->omega = 1.0; sc->beta = 0.0;
-        sc->first = 1;
-        sc->done = 0;
-        if (!isfinite(err)) { sc->done = 1; sc->status = FALM_ERR_NAN; }
-        else if (check_tol && err <= sc->tol) { sc->done = 1; sc->status = FALM_OK; }
-        else if (fabs(tot[1]) < FLT_MIN) {       // src/FalmEq.cpp:348-351
-            sc->err = tot[1];
-            sc->done = 1;
-            sc->status = (err <= sc->tol) ? FALM_OK : FALM_ERR_BREAKDOWN;
-        }
+        if (sc->defer) { sc->red[0] = tot[0]; sc->red[1] = tot[1]; }
+        else derive_res(sc, tot, check_tol);
     }
 }
 
@@ -234,7 +283,7 @@ __global__ void __launch_bounds__(kRowThreads) k_sor(Geom g, Region3 R, Op7<T> o
                                                    T omega, int color, const SolverScalars *sc) {
     if (sc && sc->done) return;
     FB_FOR_ROWS(R, j, k) FB_FOR_I(R, i) {
-        if (((i + j + k) & 1) != color) continue;
+        if (((i + j + k + g.koff) & 1) != color) continue;
         long long c = g.id(i, j, k);
         T ac, aw, ae, as, an, ab, at;
         op.get(i, j, k, c, ac, aw, ae, as, an, ab, at);
@@ -262,7 +311,8 @@ __global__ void __launch_bounds__(kRowThreads) k_jacobi(Geom g, Region3 R, Op7<T
     }
 }
 
-// first sweep of the preconditioner from z = 0, pointwise:
+// first sweep of the preconditioner from z = 0, pointwise (k: the plane's global
+// index, local k + Geom::koff, which only sets the colour):
 //   SOR:    black cells z = omega*(v/ac), red cells z = 0
 //   Jacobi: z = v/ac
 template <typename T>
@@ -308,7 +358,7 @@ __global__ void __launch_bounds__(kRowThreads) k_bicg_p(Geom g, Region3 R, Op7<T
                     const long long c = c0 + i;
                     const T v = first ? rv[u] : rv[u] + beta * (pv[u] - omega * qv[u]);   // src/dev/FalmEqDevCall.cu:261
                     if (p_out) p_out[c] = v;
-                    pp[c] = pc_first<T>(pc_type, i, j, k, v, op.diag_row(rd, i, c), pc_omega);
+                    pp[c] = pc_first<T>(pc_type, i, j, k + g.koff, v, op.diag_row(rd, i, c), pc_omega);
                 }
             }
         }
@@ -328,9 +378,8 @@ __global__ void __launch_bounds__(kRowThreads) k_mv_dot1(Geom g, Region3 R, Op7<
     }
     double tot[1];
     if (grid_sum<1>(acc, rw, tot) && threadIdx.x == 0) {
-        double alpha = sc->rho / tot[0];          // src/FalmEq.cpp:371
-        sc->alpha = alpha;
-        if (!isfinite(alpha)) { sc->done = 1; sc->status = FALM_ERR_NAN; }
+        if (sc->defer) sc->red[0] = tot[0];
+        else derive_alpha(sc, tot);
     }
 }
 
@@ -357,7 +406,7 @@ __global__ void __launch_bounds__(kRowThreads) k_bicg_s(Geom g, Region3 R, Op7<T
                     const long long c = c0 + i;
                     const T sv = rv[u] - alpha * qv[u];                   // src/dev/FalmEqDevCall.cu:284
                     s[c] = sv;
-                    ss[c] = pc_first<T>(pc_type, i, j, k, sv, op.diag_row(rd, i, c), pc_omega);
+                    ss[c] = pc_first<T>(pc_type, i, j, k + g.koff, sv, op.diag_row(rd, i, c), pc_omega);
                 }
             }
         }
@@ -379,9 +428,8 @@ __global__ void __launch_bounds__(kRowThreads) k_mv_dot2(Geom g, Region3 R, Op7<
     }
     double tot[2];
     if (grid_sum<2>(acc, rw, tot) && threadIdx.x == 0) {
-        double omega = tot[0] / tot[1];           // src/FalmEq.cpp:389
-        sc->omega = omega;
-        if (!isfinite(omega)) { sc->done = 1; sc->status = FALM_ERR_NAN; }
+        if (sc->defer) { sc->red[0] = tot[0]; sc->red[1] = tot[1]; }
+        else derive_omega(sc, tot);
     }
 }
 
@@ -422,29 +470,23 @@ __global__ void __launch_bounds__(kRowThreads) k_bicg_xr(Geom g, Region3 R, T *_
     }
     double tot[2];
     if (grid_sum<2>(acc, rw, tot) && threadIdx.x == 0) {
-        // src/FalmEq.cpp:400-407 and, for the next iteration, :345-356
-        double rho = sc->rho;
-        sc->rrho = rho;
-        double err = sqrt(tot[0]) / sc->gsize;
-        sc->err = err;
-        sc->it += 1;
-        sc->first = 0;
-        if (!isfinite(err)) { sc->done = 1; sc->status = FALM_ERR_NAN; return; }
-        if (!(sc->it < sc->maxit && err > sc->tol)) {
-            sc->done = 1;
-            sc->status = err > sc->tol ? FALM_ERR_MAXIT : FALM_OK;
-            return;
-        }
-        double rho_n = tot[1];
-        if (fabs(rho_n) < FLT_MIN) {
-            sc->err = rho_n;
-            sc->done = 1;
-            sc->status = err <= sc->tol ? FALM_OK : FALM_ERR_BREAKDOWN;
-            return;
-        }
-        sc->beta = (rho_n * sc->alpha) / (rho * sc->omega);
-        sc->rho = rho_n;
+        if (sc->defer) { sc->red[0] = tot[0]; sc->red[1] = tot[1]; }
+        else derive_xr(sc, tot);
     }
+}
+
+// The scalars of a slab-decomposed solve (SolverScalars::defer): the kernels
+// above left their local totals in red[], the totals were summed over the
+// slabs in place, and one thread derives the scalars from them.
+// stage 0: pass start (k_res, check_tol 0), 1: check (k_res, check_tol 1),
+// 2: alpha, 3: omega, 4: x/r update
+__global__ void k_slab_derive(SolverScalars *sc, int stage) {
+    if (stage >= 2 && sc->done) return;
+    double tot[2] = {sc->red[0], sc->red[1]};
+    if (stage <= 1) derive_res(sc, tot, stage);
+    else if (stage == 2) derive_alpha(sc, tot);
+    else if (stage == 3) derive_omega(sc, tot);
+    else derive_xr(sc, tot);
 }
 
 }  // namespace fb

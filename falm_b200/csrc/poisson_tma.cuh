@@ -223,7 +223,7 @@ struct SorBody {
     __device__ const Op7<T> &op_() const { return op; }
     __device__ void cell2(int i, int j, int k, long long c, const Coef7<P2<T>> &a, P2<T> xc, P2<T> xe, P2<T> xw, P2<T> xn, P2<T> xs,
                           P2<T> xt, P2<T> xb, P2<T> bv, double (&)[1]) const {
-        const int e = (color ^ (i + j + k)) & 1;
+        const int e = (color ^ (i + j + k + op.t.koff)) & 1;
         auto L = [e](P2<T> v) { return e ? v.y : v.x; };
         const T ac = L(a.ac), xcc = L(xc);
         const T r7 = ac * xcc + L(a.ae) * L(xe) + L(a.aw) * L(xw) + L(a.an) * L(xn) + L(a.as) * L(xs) + L(a.at) * L(xt) + L(a.ab) * L(xb);
@@ -269,9 +269,8 @@ struct MvDot1Body {
         acc[0] += to_d(rrv.y) * to_d(qv.y);
     }
     __device__ void finish(const double (&tot)[1]) const {
-        double alpha = sc->rho / tot[0];
-        sc->alpha = alpha;
-        if (!isfinite(alpha)) { sc->done = 1; sc->status = FALM_ERR_NAN; }
+        if (sc->defer) sc->red[0] = tot[0];
+        else derive_alpha(sc, tot);
     }
 };
 
@@ -298,9 +297,8 @@ struct MvDot2Body {
         acc[1] += t1 * t1;
     }
     __device__ void finish(const double (&tot)[2]) const {
-        double omega = tot[0] / tot[1];
-        sc->omega = omega;
-        if (!isfinite(omega)) { sc->done = 1; sc->status = FALM_ERR_NAN; }
+        if (sc->defer) { sc->red[0] = tot[0]; sc->red[1] = tot[1]; }
+        else derive_omega(sc, tot);
     }
 };
 
@@ -334,8 +332,8 @@ struct ResBody {
         const P2<T> rt = mk2((T)r0, (T)r1);
         if (!CHECK && r) st2(r + c, rt);
         if (!CHECK && rr) st2(rr + c, rt);
-        if (!CHECK && pp) st2(pp + c, mk2(pc_first<T>(pc_type, i, j, k, rt.x, (T)a.ac.x, pc_omega),
-                                pc_first<T>(pc_type, i + 1, j, k, rt.y, (T)a.ac.y, pc_omega)));
+        if (!CHECK && pp) st2(pp + c, mk2(pc_first<T>(pc_type, i, j, k + op.t.koff, rt.x, (T)a.ac.x, pc_omega),
+                                pc_first<T>(pc_type, i + 1, j, k + op.t.koff, rt.y, (T)a.ac.y, pc_omega)));
         acc[0] += r0 * r0;
         acc[0] += r1 * r1;
         if constexpr (!CHECK) {

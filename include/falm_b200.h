@@ -293,6 +293,62 @@ int falm_adjoint_set_tol(falm_ctx *ctx, double rel_tol);
 int falm_mv_dot_static(int sx, int sy, int sz, int gc, int precision, const void *a, const void *b,
                        double *out, void *stream);
 
+/* ---------------- z-slab decomposition over several GPUs ------------------------------------ */
+/* The reference decomposes the grid into per-rank boxes with a 6-face MPI halo exchange (CPM:
+   partition src/CPMBase.h:36-112, exchange src/CPMComm.h:182-364, pack/unpack
+   src/dev/CPMDevCall.cu:7-60; its drivers split x, app/nedo/main.cpp:105).  Here the grid is
+   split into slabs of whole z planes, one per GPU, so every halo is a run of contiguous planes
+   of each component (no packing), exchanged through a transport:
+     exchange: send `bytes` from send_lo to the rank below (it receives them into its recv_hi)
+               and from send_hi to the rank above (into its recv_lo), ordered on `stream`; NULL
+               pointers where there is no neighbour.  On return, work queued on `stream` may
+               read the received planes and overwrite the sent ones.
+     allreduce: reduce n doubles in device memory in place over all ranks (op FALM_REDUCE_SUM or
+               FALM_REDUCE_MAX), ordered on `stream`; every rank gets the same values.
+   Both return a falm_status.  Two transports are built in (below); a caller may supply its own. */
+typedef struct falm_transport {
+    void *user;
+    int (*exchange)(void *user, const void *send_lo, void *recv_lo, const void *send_hi, void *recv_hi,
+                    size_t bytes, void *stream);
+    int (*allreduce)(void *user, double *buf, int n, int op, void *stream);
+} falm_transport;
+enum { FALM_REDUCE_SUM = 0, FALM_REDUCE_MAX = 1 };
+
+/* Make ctx one slab of a grid decomposed along z: the context was created with the slab's grid
+   (its nz_local interior planes plus the guide planes, with the global grid's z and hz values
+   there: across a slab interface the guide planes are the neighbour's interior planes).
+   z_offset: global interior index of the slab's first plane; nz_global: interior planes of the
+   whole grid; rank 0 holds the lowest slab.  Call right after falm_create, before
+   falm_bc_set_inflow (whose box then covers the whole grid's inlet) and falm_eq_poisson_operator
+   (a collective: every rank calls it; the operator keeps its coefficients across interfaces and
+   maxdiag is the maximum over the slabs).  falm_step and falm_eq_solve then exchange the halos
+   they need and reduce every inner product, norm and AP force over the slabs (BiCGStab solver;
+   preconditioner half sweeps one at a time, each after an exchange of the iterate's halo);
+   boundary conditions apply on physical faces only.  Every rank makes the same calls in the same
+   order.  The other entry points act on the slab alone: exchange halos before them with
+   falm_slab_halo.  The discrete adjoint and the plain Jacobi/SOR solvers are single-slab only. */
+int falm_slab_init(falm_ctx *ctx, int rank, int nranks, int z_offset, int nz_global, const falm_transport *t);
+/* exchange `depth` (1 or 2) guide planes of a field of ncomp components with the neighbours (CPM
+   IExchange6Face + PostExchange6Face, src/CPMComm.h:182-325, for the z faces) */
+int falm_slab_halo(falm_ctx *ctx, void *field, int ncomp, int depth, void *stream);
+
+/* In-process transport: the ranks are contexts of one process, each driven by its own host
+   thread (on one GPU or several).  Every exchange and reduction is a host rendezvous of the
+   threads (limited to 120 s, then FALM_ERR_TIMEOUT on every rank) followed by device copies
+   ordered by CUDA events; no kernel waits on another.  Reductions sum in rank order, so every
+   rank gets bitwise the same values; at most 64 doubles per reduction. */
+int falm_local_hub_create(int nranks, void **hub);
+int falm_local_hub_transport(void *hub, int rank, falm_transport *out);
+int falm_local_hub_destroy(void *hub);
+
+/* NCCL transport (one process per GPU): libnccl.so.2 is loaded at run time (the copy already in
+   the process, else the system's).  Rank 0 calls falm_nccl_unique_id and hands the 128 bytes to
+   every rank (e.g. through torch.distributed); each rank then creates its communicator on its
+   current device.  exchange = grouped ncclSend/ncclRecv, allreduce = ncclAllReduce (FP64). */
+int falm_nccl_unique_id(unsigned char id[128]);
+int falm_nccl_transport_create(const unsigned char id[128], int rank, int nranks, falm_transport *out);
+int falm_nccl_transport_destroy(falm_transport *t);
+
 /* ---------------- instrumentation ----------------------------------------------------------- */
 /* Test hook for the bounded device waits (the reference only prints errors, src/error.h:20-26):
    the next falm_step on this context first runs one wait on a barrier that no copy completes,
