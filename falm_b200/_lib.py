@@ -54,6 +54,15 @@ class StepStats(ctypes.Structure):
 V, D, I, LL, P = ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_longlong, ctypes.c_void_p
 
 
+class RmcpDesc(ctypes.Structure):
+    _fields_ = [("n_turbine", ctypes.c_int), ("n_blade", ctypes.c_int), ("radius", ctypes.c_double),
+                ("hub_radius", ctypes.c_double), ("blade_width", ctypes.c_double), ("blade_thick", ctypes.c_double),
+                ("base", c_double_p), ("hub", c_double_p), ("angle", c_double_p), ("angle_type", c_int_p),
+                ("tip_rate", c_double_p), ("n_station", ctypes.c_int), ("n_attack", ctypes.c_int),
+                ("st_r", c_double_p), ("st_chord", c_double_p), ("st_twist", c_double_p), ("attack", c_double_p),
+                ("cl", c_double_p), ("cd", c_double_p)]
+
+
 class Transport(ctypes.Structure):
     """falm_transport: halo exchange and reductions between the slabs of a grid"""
     _fields_ = [("user", ctypes.c_void_p), ("exchange", ctypes.c_void_p), ("allreduce", ctypes.c_void_p)]
@@ -108,6 +117,8 @@ SIGNATURES = {
     "falm_io_read_cv_file": [ctypes.c_char_p, c_int_p, c_double_p, c_double_p, c_double_p, c_double_p, c_double_p, c_double_p],
     "falm_mesh_build": [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, I],
     "falm_debug_arm_wait_probe": [V, LL],
+    "falm_rmcp_init": [V, ctypes.POINTER(RmcpDesc)],
+    "falm_rmcp_run": [V, P, P, D, P, P, c_double_p, c_double_p],
     "falm_slab_init": [V, I, I, I, I, ctypes.POINTER(Transport)],
     "falm_slab_halo": [V, P, I, I, P],
     "falm_local_hub_create": [I, ctypes.POINTER(ctypes.c_void_p)],

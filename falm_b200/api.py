@@ -229,6 +229,28 @@ class Context:
                     "step_adjoint")
 
 
+    # ------------------------------------------------------------ RMCP rotor model
+    def rmcp_init(self, r):
+        """Rmcp::RmcpAlm::init from a cases.RmcpSetup: the step's forcing becomes the RMCP model"""
+        k = r.arrays()
+        self._rmcp_keep = k
+        d = L.RmcpDesc(r.n_turbine, r.n_blade, r.radius, r.hub_radius, r.width, r.thick, _dp(k["base"]), _dp(k["hub"]),
+                       _dp(k["angle"]), k["angle_type"].ctypes.data_as(L.c_int_p), _dp(k["tip_rate"]), len(k["st_r"]),
+                       len(k["attack"]), _dp(k["st_r"]), _dp(k["st_chord"]), _dp(k["st_twist"]), _dp(k["attack"]),
+                       _dp(k["cl"]), _dp(k["cd"]))
+        self._check(self.lib.falm_rmcp_init(self.h, ctypes.byref(d)), "rmcp_init")
+        self.n_turbine = r.n_turbine
+        self.alm_on = False
+
+    def rmcp_run(self, u, ff, t, flag=None):
+        """SetALMFlag + ALM of the RMCP model at time t into ff (and the paint into the int32
+        device tensor flag); returns per-turbine torque and thrust"""
+        n = self.n_turbine
+        tq, th = np.zeros(n), np.zeros(n)
+        self._check(self.lib.falm_rmcp_run(self.h, _ptr(u), _ptr(ff), t, self.stream(), _ptr(flag), _dp(tq), _dp(th)),
+                    "rmcp_run")
+        return tq, th
+
     # ------------------------------------------------------------ z slabs
     def slab_init(self, rank, nranks, z_offset, nz_global, transport):
         """falm_slab_init: this context is slab `rank` of a grid split along z"""

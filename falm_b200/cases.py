@@ -191,6 +191,54 @@ def make_rotor(hub_xyz, h, tsr=7.0, n_ap_per_blade=32, eps_cells=2.0, pitch=0.0,
                     st, aps, pitch)
 
 
+@dataclass
+class RmcpSetup:
+    """The reference's RMCP rotor model (src/rmcp/turbineHandler.h, bladeHandler.h):
+    turbines of a fixed orientation whose rotating blades paint the cells they
+    cover.  angle_deg: one Euler angle per turbine in degrees (the reference's
+    JSON unit), angle_type 0 none / 1 roll / 2 pitch / 3 yaw."""
+    n_turbine: int
+    n_blade: int
+    radius: float
+    hub_radius: float
+    width: float
+    thick: float
+    base: np.ndarray          # (n_turbine, 3)
+    hub: np.ndarray           # (n_turbine, 3): (-overhang, 0, tower)
+    angle_deg: np.ndarray     # (n_turbine, 3)
+    angle_type: np.ndarray
+    tip_rate: np.ndarray
+    stations: dict
+
+    def arrays(self):
+        st = self.stations
+        return {
+            "base": np.ascontiguousarray(self.base, dtype=np.float64).ravel(),
+            "hub": np.ascontiguousarray(self.hub, dtype=np.float64).ravel(),
+            # deg2rad as the reference converts its JSON angles (src/falmath.h:51-53)
+            "angle": np.ascontiguousarray([a * math.pi / 180.0 for a in np.asarray(self.angle_deg, dtype=np.float64).ravel()]),
+            "angle_type": np.ascontiguousarray(self.angle_type, dtype=np.int32),
+            "tip_rate": np.ascontiguousarray(self.tip_rate, dtype=np.float64),
+            "st_r": np.ascontiguousarray(st["r"], dtype=np.float64),
+            "st_chord": np.ascontiguousarray(st["chord"], dtype=np.float64),
+            "st_twist": np.ascontiguousarray(st["twist"], dtype=np.float64),
+            "attack": np.ascontiguousarray(st["attack"], dtype=np.float64),
+            "cl": np.ascontiguousarray(st["cl"], dtype=np.float64).ravel(),
+            "cd": np.ascontiguousarray(st["cd"], dtype=np.float64).ravel(),
+        }
+
+
+def make_rmcp(hub_xyz, tsr=7.0, width=0.1, thick=0.1, yaw_deg=0.0, tower=0.0):
+    """One 3-blade RMCP rotor of radius 1 centred at hub_xyz, with the reference's
+    blade strip width and thickness (BLADE_WIDTH, BLADE_THICK: 0.1), the blade
+    stations of blade_stations() and an optional yaw of the whole turbine"""
+    base = np.array([[hub_xyz[0], hub_xyz[1], hub_xyz[2] - tower]])
+    hub = np.array([[0.0, 0.0, tower]])
+    ang = np.array([[0.0, 0.0, yaw_deg]])
+    atype = np.array([3 if yaw_deg else 0], dtype=np.int32)
+    return RmcpSetup(1, 3, 1.0, 0.0, width, thick, base, hub, ang, atype, np.array([tsr]), blade_stations())
+
+
 # ---------------------------------------------------------------- inflow
 def inflow_box(ny, nz, intensity, nb=128, corr=8, seed=INFLOW_SEED):
     """Periodic 3 x nb x ny x nz perturbation box: i.i.d. N(0,1) from Philox(seed),
@@ -224,6 +272,7 @@ class Case:
     pc_relax: float = 1.2
     u_inlet: float = 1.0
     alm: AlmSetup = None
+    rmcp: RmcpSetup = None
     intensity: float = 0.0
     steps: int = 1
     inflow: np.ndarray = field(default=None, repr=False)

@@ -33,6 +33,7 @@
 #include "falm_io.cuh"
 #include "sor_rb_tma.cuh"
 #include "adjoint.cuh"
+#include "rmcp.cuh"
 #include <cudaTypedefs.h>
 
 using namespace fb;
@@ -819,6 +820,19 @@ int ubc_t(falm_ctx *ctx, T *u, UPrev<T> up, double dt, double t, cudaStream_t st
     return FALM_OK;
 }
 
+// the RMCP forcing into ff over the turbines' boxes; torque and thrust sums
+// into ctx->rmcp_sums (device)
+template <typename T>
+int rmcp_run_t(falm_ctx *ctx, const T *u, T *ff, int *flag, double t, cudaStream_t st) {
+    const RmcpDev &a = *ctx->rmcp;
+    const long long blocks = std::max(1LL, std::min<long long>((a.bs.total + 255) / 256, (long long)ctx->sm_count * 8));
+    // 2 x kMaxTurbines values per block: a quarter of the workspace's blocks
+    const RedWork rw{ctx->red.partials, ctx->red.counter, ctx->red.maxBlocks / 4};
+    LAUNCH(FALM_K_ALM, st, k_rmcp<T><<<(int)blocks, 256, 0, st>>>(ctx->geo, a, ctx->m64.x[0], ctx->m64.x[1], ctx->m64.x[2], u, ff, flag, t, rw,
+                                                                 ctx->rmcp_sums));
+    return FALM_OK;
+}
+
 // A wait on an mbarrier that nothing ever completes, through the same bounded
 // wait the plane-stream kernels use: it gives up after `cycles` clock64 cycles
 // and records FALM_ERR_TIMEOUT in the device error word.  No copy is issued,
@@ -851,9 +865,12 @@ int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_
     T *ua = (T *)ctx->w_ua, *rhs = (T *)ctx->w_rhs, *r = (T *)ctx->w_r;
     const bool chan = ctx->bc_kind == FALM_BC_CHANNEL;
     bool fused_res = false;
-    // 1. ALM (src/alm/alm.h:66-77) at the previous velocity
+    // 1. ALM (src/alm/alm.h:66-77) at the previous velocity, or the RMCP model
     if (ctx->alm_on) {
         if ((rc = alm_run_t<T>(ctx, u, ff, t, st))) return rc;
+    } else if (ctx->rmcp_on) {
+        ff = (T *)ctx->w_ff;
+        if ((rc = rmcp_run_t<T>(ctx, u, ff, nullptr, t, st))) return rc;
     }
     // 2. pseudo-velocity into ua (ALM force projected in-kernel when ff == NULL)
     if ((rc = pseudo_u_t<T>(ctx, u, u, uu, ua, nut, ff, dt, ctx->alm_on != 0, st))) return rc;
@@ -919,6 +936,7 @@ int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_
     }
     CK(cudaMemcpyAsync(ctx->scal_host, ctx->scal, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
     if (ctx->alm_on) CK(cudaMemcpyAsync(ctx->alm_scal_host, ctx->alm.scal, sizeof(AlmScalars), cudaMemcpyDeviceToHost, st));
+    if (ctx->rmcp_on) CK(cudaMemcpyAsync(ctx->rmcp_sums_host, ctx->rmcp_sums, 2 * kMaxTurbines * sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(&ctx->scal_host->kerr, ctx->kerr, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     if (ctx->scal_host->kerr) {
@@ -940,6 +958,11 @@ int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_
             for (int q = 0; q < ctx->alm.n_turbine && q < kMaxTurbines; q++) {
                 out->torque[q] = ctx->alm_scal_host->torque[q];
                 out->thrust[q] = ctx->alm_scal_host->thrust[q];
+            }
+        if (ctx->rmcp_on)
+            for (int q = 0; q < ctx->rmcp->n_turbine && q < kMaxTurbines; q++) {
+                out->torque[q] = ctx->rmcp_sums_host[q];
+                out->thrust[q] = ctx->rmcp_sums_host[kMaxTurbines + q];
             }
     }
     return FALM_OK;
@@ -1054,6 +1077,10 @@ int falm_destroy(falm_ctx *ctx) {
     cudaFree(ctx->op_mem);
     cudaFree(ctx->work_mem);
     cudaFree(ctx->adj_mem);
+    cudaFree(ctx->rmcp_mem);
+    cudaFree(ctx->w_ff);
+    if (ctx->rmcp_sums_host) cudaFreeHost(ctx->rmcp_sums_host);
+    delete ctx->rmcp;
     cudaFree(ctx->red.partials);
     cudaFree(ctx->red.counter);
     cudaFree(ctx->scal);
@@ -1657,6 +1684,7 @@ int falm_alm_init(falm_ctx *ctx, const falm_alm_desc *d) {
         if (src) cudaMemcpy(dst, src, n * sizeof(double), cudaMemcpyHostToDevice);
         return dst;
     };
+    ctx->rmcp_on = 0;
     AlmDev &a = ctx->alm;
     a.n_turbine = nt; a.n_blade = d->n_blade; a.n_ap_per_blade = d->n_ap_per_blade; a.n_attack = na; a.apcount = apc;
     a.radius = d->radius; a.hub_radius = d->hub_radius; a.euler_eps = d->euler_eps; a.pitch = d->pitch;
@@ -1753,6 +1781,95 @@ int falm_alm_get_aps(falm_ctx *ctx, double *xyz, double *force, double *torque, 
 }
 
 // ---------------------------------------------------------------- step
+int falm_rmcp_init(falm_ctx *ctx, const falm_rmcp_desc *d) {
+    if (!ctx || !d || d->n_turbine < 1 || d->n_turbine > kMaxTurbines || d->n_blade < 1 || d->n_station < 1 || d->n_attack < 1 ||
+        !(d->radius > 0) || !(d->blade_width > 0) || !(d->blade_thick > 0) || !d->base || !d->hub || !d->angle || !d->angle_type ||
+        !d->tip_rate || !d->st_r || !d->st_chord || !d->st_twist || !d->attack || !d->cl || !d->cd)
+        return FALM_ERR_ARG;
+    const int nt = d->n_turbine, ns = d->n_station, na = d->n_attack;
+    for (int q = 0; q < nt; q++)
+        if (d->angle_type[q] < 0 || d->angle_type[q] > 3) return FALM_ERR_ARG;
+    const size_t nd = 3 * nt + 3 * nt + 3 * nt + nt + 3 * (size_t)ns + na + 2 * (size_t)ns * na;
+    const size_t bytes = nd * sizeof(double) + nt * sizeof(int) + 2 * kMaxTurbines * sizeof(double) + 512;
+    if (ctx->rmcp_mem) { cudaFree(ctx->rmcp_mem); ctx->rmcp_mem = nullptr; }
+    CK(cudaMalloc(&ctx->rmcp_mem, bytes));
+    CK(cudaMemset(ctx->rmcp_mem, 0, bytes));
+    if (!ctx->rmcp) ctx->rmcp = new RmcpDev();
+    if (!ctx->rmcp_sums_host) CK(cudaMallocHost(&ctx->rmcp_sums_host, 2 * kMaxTurbines * sizeof(double)));
+    double *p = (double *)ctx->rmcp_mem;
+    auto put = [&](const double *src, size_t n) -> const double * {
+        double *dst = p;
+        p += n;
+        cudaMemcpy(dst, src, n * sizeof(double), cudaMemcpyHostToDevice);
+        return dst;
+    };
+    RmcpDev &a = *ctx->rmcp;
+    a.n_turbine = nt; a.n_blade = d->n_blade; a.n_station = ns; a.n_attack = na;
+    a.radius = d->radius; a.hub_radius = d->hub_radius; a.width = d->blade_width; a.thick = d->blade_thick;
+    a.base = put(d->base, 3 * nt); a.hub = put(d->hub, 3 * nt); a.angle = put(d->angle, 3 * nt); a.tip_rate = put(d->tip_rate, nt);
+    a.st_r = put(d->st_r, ns); a.st_chord = put(d->st_chord, ns); a.st_twist = put(d->st_twist, ns); a.attack = put(d->attack, na);
+    a.cl = put(d->cl, (size_t)ns * na); a.cd = put(d->cd, (size_t)ns * na);
+    ctx->rmcp_sums = p;
+    p += 2 * kMaxTurbines;
+    int *ip = (int *)p;
+    CK(cudaMemcpy(ip, d->angle_type, nt * sizeof(int), cudaMemcpyHostToDevice));
+    a.angle_type = ip;
+    if (cudaGetLastError() != cudaSuccess) return fail(ctx, FALM_ERR_CUDA, "rmcp_init: table copy");
+    // boxes: every painted point lies within |hub| + radius + thickness of its turbine's base
+    {
+        BoxSet &bs = a.bs;
+        memset(&bs, 0, sizeof(bs));
+        const Geom &g = ctx->geo;
+        const std::vector<double> *cs[3] = {ctx->xc, ctx->yc, ctx->zc};
+        const int s3[3] = {g.sx, g.sy, g.sz};
+        long long off = 0;
+        for (int t = 0; t < nt; t++) {
+            const double *hb = d->hub + 3 * t;
+            const double reach = std::sqrt(hb[0] * hb[0] + hb[1] * hb[1] + hb[2] * hb[2]) + d->radius + d->blade_thick;
+            long long cells = 1;
+            for (int ax = 0; ax < 3; ax++) {
+                int lo = s3[ax], hi = -1;
+                for (int q = g.gc; q < s3[ax] - g.gc; q++) {
+                    const double c = (*cs[ax])[q], b = d->base[3 * t + ax];
+                    if (c >= b - reach && c <= b + reach) { lo = std::min(lo, q); hi = std::max(hi, q); }
+                }
+                if (hi >= lo) { lo = std::max(g.gc, lo - 1); hi = std::min(s3[ax] - g.gc - 1, hi + 1); }
+                bs.lo[t][ax] = hi >= lo ? lo : g.gc;
+                bs.ext[t][ax] = hi >= lo ? hi - lo + 1 : 0;
+                cells *= bs.ext[t][ax];
+            }
+            bs.off[t] = off;
+            off += cells;
+        }
+        bs.n = nt;
+        bs.total = off;
+    }
+    if (!ctx->w_ff) CK(cudaMalloc(&ctx->w_ff, 3 * (size_t)ctx->geo.n * ctx->esize));
+    CK(cudaMemset(ctx->w_ff, 0, 3 * (size_t)ctx->geo.n * ctx->esize));
+    ctx->rmcp_on = 1;
+    ctx->alm_on = 0;
+    return FALM_OK;
+}
+
+int falm_rmcp_run(falm_ctx *ctx, const void *u, void *ff, double t, void *stream, int *flag, double *torque, double *thrust) {
+    if (!ctx || !u || !ff) return FALM_ERR_ARG;
+    if (!ctx->rmcp_on) return fail(ctx, FALM_ERR_STATE, "rmcp_run: no RMCP model (falm_rmcp_init)");
+    cudaStream_t st = S(stream);
+    int rc = dispatch(ctx, [&](auto z) {
+        using T = decltype(z);
+        return rmcp_run_t<T>(ctx, (const T *)u, (T *)ff, flag, t, st);
+    });
+    if (rc) return rc;
+    if ((rc = slab_reduce(ctx, ctx->rmcp_sums, 2 * kMaxTurbines, FALM_REDUCE_SUM, st))) return rc;
+    CK(cudaMemcpyAsync(ctx->rmcp_sums_host, ctx->rmcp_sums, 2 * kMaxTurbines * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int q = 0; q < ctx->rmcp->n_turbine; q++) {
+        if (torque) torque[q] = ctx->rmcp_sums_host[q];
+        if (thrust) thrust[q] = ctx->rmcp_sums_host[kMaxTurbines + q];
+    }
+    return FALM_OK;
+}
+
 int falm_step(falm_ctx *ctx, const falm_fields *f, double dt, double t, void *stream, falm_step_stats *st) {
     if (!ctx || !f || !f->u || !f->uu || !f->p || !f->nut || !(dt > 0)) return FALM_ERR_ARG;
     return dispatch(ctx, [&](auto z) {
@@ -2075,6 +2192,7 @@ extern "C" int falm_step_adjoint(falm_ctx *ctx, const falm_fields *f0, const fal
     if (!ctx || !f0 || !f0->u || !f0->uu || !f0->p || !f0->nut || !au || !auu || !anut || !grad || !(dt > 0)) return FALM_ERR_ARG;
     if (ctx->precision != FALM_FP64) return fail(ctx, FALM_ERR_ARG, "step_adjoint: FP64 contexts only");
     if (ctx->slab_on && ctx->slab_nranks > 1) return fail(ctx, FALM_ERR_ARG, "step_adjoint: a grid of one slab only");
+    if (ctx->rmcp_on) return fail(ctx, FALM_ERR_ARG, "step_adjoint: the ALM forcing only (not the RMCP model)");
     if (ctx->adv != FALM_ADV_UPWIND3 && ctx->adv != FALM_ADV_UTOPIA && ctx->adv != FALM_ADV_KK)
         return fail(ctx, FALM_ERR_ARG, "step_adjoint: the 4th-order advection schemes (Upwind3, UTOPIA, KK) only");
     if (ctx->sgs != FALM_SGS_EMPTY && ctx->sgs != FALM_SGS_SMAGORINSKY) return fail(ctx, FALM_ERR_ARG, "step_adjoint: Smagorinsky or no SGS model only");

@@ -102,6 +102,7 @@ struct AlmDev {
 };
 
 struct IoWriter;
+struct RmcpDev;
 }  // namespace fb
 
 // host-side context
@@ -172,6 +173,13 @@ struct falm_ctx {
     int pu_v1;                              // FP32 pseudo-velocity on the one-cell-per-thread kernel (tests)
     int check_sync;                         // synchronise after every launch (fault location)
     long long wait_probe_cycles;            // >0: the next falm_step first runs a wait that nothing completes (tests)
+    // RMCP rotor model (falm_rmcp_init): the step's forcing instead of the ALM
+    int rmcp_on;
+    void *rmcp_mem;
+    fb::RmcpDev *rmcp;                      // host copy of the device tables' descriptor
+    void *w_ff;                             // 3N force field of the RMCP step (zero outside the boxes)
+    double *rmcp_sums;                      // device: torque, thrust per turbine (2 x kMaxTurbines)
+    double *rmcp_sums_host;                 // pinned
     // z slab of a decomposed grid (falm_slab_init)
     int slab_on, slab_rank, slab_nranks;
     falm_transport transport;               // halo exchange and reductions between the slabs

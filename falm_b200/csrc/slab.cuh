@@ -428,13 +428,17 @@ int slab_step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaSt
     const bool chan = ctx->bc_kind == FALM_BC_CHANNEL;
     // 0. halos of the state
     if ((rc = slab_halo<T>(ctx, u, 3, 2, st)) || (rc = slab_halo<T>(ctx, nut, 1, 1, st))) return rc;
-    // 1. ALM at the previous velocity
+    // 1. ALM at the previous velocity, or the RMCP model (cells of the slab; sums over the slabs)
     if (ctx->alm_on) {
         if ((rc = slab_alm_t<T>(ctx, u, t, st))) return rc;
         if (ff) {
             const Region3 R = interior(g);
             LAUNCH(FALM_K_ALM, st, k_alm_project<T><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), ctx->alm, ff));
         }
+    } else if (ctx->rmcp_on) {
+        ff = (T *)ctx->w_ff;
+        if ((rc = rmcp_run_t<T>(ctx, u, ff, nullptr, t, st))) return rc;
+        if ((rc = slab_reduce(ctx, ctx->rmcp_sums, 2 * kMaxTurbines, FALM_REDUCE_SUM, st))) return rc;
     }
     // 2. pseudo-velocity; its guide layer takes the previous velocity, across
     //    the slab interfaces the neighbours' pseudo-velocity
@@ -482,6 +486,7 @@ int slab_step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaSt
     if ((rc = slab_reduce(ctx, &ctx->scal->red[3], 1, FALM_REDUCE_SUM, st))) return rc;
     CK(cudaMemcpyAsync(ctx->scal_host, ctx->scal, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
     if (ctx->alm_on) CK(cudaMemcpyAsync(ctx->alm_scal_host, ctx->alm.scal, sizeof(AlmScalars), cudaMemcpyDeviceToHost, st));
+    if (ctx->rmcp_on) CK(cudaMemcpyAsync(ctx->rmcp_sums_host, ctx->rmcp_sums, 2 * kMaxTurbines * sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(&ctx->scal_host->kerr, ctx->kerr, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     if (ctx->scal_host->kerr) {
@@ -500,6 +505,11 @@ int slab_step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaSt
             for (int q = 0; q < ctx->alm.n_turbine && q < kMaxTurbines; q++) {
                 out->torque[q] = ctx->alm_scal_host->torque[q];
                 out->thrust[q] = ctx->alm_scal_host->thrust[q];
+            }
+        if (ctx->rmcp_on)
+            for (int q = 0; q < ctx->rmcp->n_turbine && q < kMaxTurbines; q++) {
+                out->torque[q] = ctx->rmcp_sums_host[q];
+                out->thrust[q] = ctx->rmcp_sums_host[kMaxTurbines + q];
             }
     }
     return FALM_OK;

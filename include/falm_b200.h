@@ -293,6 +293,38 @@ int falm_adjoint_set_tol(falm_ctx *ctx, double rel_tol);
 int falm_mv_dot_static(int sx, int sy, int sz, int gc, int precision, const void *a, const void *b,
                        double *out, void *stream);
 
+/* ---------------- RMCP rotor model (the reference's alternate forcing) ---------------------- */
+/* Rmcp::RmcpAlm (src/rmcp/alm.h:13-96; TurbineHandler src/rmcp/turbineHandler.h:119-185,
+   BladeHandler src/rmcp/bladeHandler.h:134-185): turbines with a fixed orientation whose rotating
+   blades paint the cells they cover (kernel_SetALMFlag, src/rmcp/almDevCall.cu:13-65); every
+   painted cell gets the blade-element force of its own velocity (kernel_ALM, :144-209).
+   angle_type 0 none, 1 roll, 2 pitch, 3 yaw (one Euler angle, in radians); hub = (-overhang, 0,
+   tower); blade_width / blade_thick: the blade strip's width about the blade axis and its
+   thickness downstream of the rotor plane (the reference's BLADE_WIDTH and BLADE_THICK, 0.1,
+   src/rmcp/almDevCall.cu:6-7); stations: r/R, chord/R, twist [deg] and the Cl/Cd rows
+   (station-major, n_attack per station) over attack [deg].  Lengths in rotor radii, as the
+   reference's tables require. */
+typedef struct falm_rmcp_desc {
+    int n_turbine, n_blade;
+    double radius, hub_radius;
+    double blade_width, blade_thick;
+    const double *base, *hub, *angle;   /* 3 per turbine */
+    const int *angle_type;
+    const double *tip_rate;
+    int n_station, n_attack;
+    const double *st_r, *st_chord, *st_twist, *attack, *cl, *cd;
+} falm_rmcp_desc;
+/* RmcpAlm::init: the RMCP model becomes the step's forcing (replacing the ALM; falm_alm_init
+   replaces it in turn).  falm_step then paints and forces the cells of each turbine's box into a
+   force field of the context and reports per turbine the torque sum(r |f_t|) over its painted
+   cells (the reference's CalcTorque formula, almDevCall.cu:368-411) and the thrust sum(|f_x|). */
+int falm_rmcp_init(falm_ctx *ctx, const falm_rmcp_desc *d);
+/* RmcpAlm::SetALMFlag + RmcpAlm::ALM at time t: the force of every cell of the turbines' boxes
+   into ff (3 components, zero where not painted; cells outside the boxes are not written, keep
+   them zero), the paint (0 or turbine + 1) of the box cells into the optional DEVICE int field
+   flag, and per turbine torque and thrust (host arrays of n_turbine, optional). */
+int falm_rmcp_run(falm_ctx *ctx, const void *u, void *ff, double t, void *stream, int *flag, double *torque, double *thrust);
+
 /* ---------------- z-slab decomposition over several GPUs ------------------------------------ */
 /* The reference decomposes the grid into per-rank boxes with a 6-face MPI halo exchange (CPM:
    partition src/CPMBase.h:36-112, exchange src/CPMComm.h:182-364, pack/unpack

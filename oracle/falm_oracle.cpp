@@ -913,6 +913,112 @@ void oracle_alm(const or_case *c, const double *u, double *ff, double t,
 /* app/nedo/main.cpp:150-204 (channel) and app/lid3d/main.cpp:121-168
  * (cavity, uubc after UtoUU), with the race-free pseudo-velocity call
  * FSPseudoU(un=u_prev, u=u_prev, uu, ua=u). */
+/* src/rmcp/bladeHandler.h:83-96 (find_position) and :98-107 (interpolate) */
+static int rmcp_find(const double *m, double x, int n) {
+    if (x < m[0]) return -1;
+    if (x >= m[n - 1]) return n - 1;
+    for (int i = 0; i < n - 1; i++)
+        if (m[i] <= x && m[i + 1] > x) return i;
+    return -2;
+}
+static double rmcp_interp(const double *m, const double *d, double x, int i, int n) {
+    if (i < 0) return d[0];
+    if (i >= n - 1) return d[n - 1];
+    double p = (x - m[i]) / (m[i + 1] - m[i]);
+    return (1. - p) * d[i] + p * d[i + 1];
+}
+/* src/rmcp/bladeHandler.h:109-131 (get_airfoil_params) */
+static void rmcp_airfoil(const or_rmcp *r, double rr, double phi, double *chord, double *twist, double *cl, double *cd) {
+    const int nr = r->n_station, na = r->n_attack;
+    int rid = rmcp_find(r->st_r, rr, nr);
+    *chord = rmcp_interp(r->st_r, r->st_chord, rr, rid, nr);
+    *twist = rmcp_interp(r->st_r, r->st_twist, rr, rid, nr);
+    double attack = phi - *twist;
+    int aid = rmcp_find(r->attack, attack, na);
+    if (rid < 0) {
+        *cl = rmcp_interp(r->attack, r->cl, attack, aid, na);
+        *cd = rmcp_interp(r->attack, r->cd, attack, aid, na);
+    } else if (rid >= nr - 1) {
+        *cl = rmcp_interp(r->attack, r->cl + (long)(nr - 1) * na, attack, aid, na);
+        *cd = rmcp_interp(r->attack, r->cd + (long)(nr - 1) * na, attack, aid, na);
+    } else {
+        double p = (rr - r->st_r[rid]) / (r->st_r[rid + 1] - r->st_r[rid]);
+        double cl0 = rmcp_interp(r->attack, r->cl + (long)rid * na, attack, aid, na);
+        double cl1 = rmcp_interp(r->attack, r->cl + (long)(rid + 1) * na, attack, aid, na);
+        double cd0 = rmcp_interp(r->attack, r->cd + (long)rid * na, attack, aid, na);
+        double cd1 = rmcp_interp(r->attack, r->cd + (long)(rid + 1) * na, attack, aid, na);
+        *cl = (1. - p) * cl0 + p * cl1;
+        *cd = (1. - p) * cd0 + p * cd1;
+    }
+}
+
+void oracle_rmcp(const or_case *c, const or_rmcp *r, const double *u, double *ff, int *flag, double t,
+                 double *torque, double *thrust) {
+    Box b(c);
+    const long N = b.n;
+    const double Pi = 3.14159265358979323846;
+    const int Nb = r->n_blade;
+    for (int q = 0; q < r->n_turbine; q++) { torque[q] = 0; thrust[q] = 0; }
+    for (int k = b.gc; k < b.sz - b.gc; k++)
+    for (int j = b.gc; j < b.sy - b.gc; j++)
+    for (int i = b.gc; i < b.sx - b.gc; i++) {
+        const long id = b.id(i, j, k);
+        const double point[3] = {c->x[i], c->y[j], c->z[k]};
+        /* the flag: src/rmcp/almDevCall.cu:13-65 */
+        int f = 0;
+        for (int tid = 0; tid < r->n_turbine; tid++) {
+            double d0[3] = {point[0] - r->base[3 * tid], point[1] - r->base[3 * tid + 1], point[2] - r->base[3 * tid + 2]}, d[3];
+            frame_rotation(d0, &r->angle[3 * tid], r->angle_type[tid], d);
+            for (int a = 0; a < 3; a++) d[a] -= r->hub[3 * tid + a];
+            double dx = d[0], dy = d[1], dz = d[2];
+            double rr = sqrt(dy * dy + dz * dz);
+            double th = atan2(dz, dy);
+            if (th < 0) th += 2 * Pi;
+            double rt = r->tip_rate[tid] * t;
+            for (int bid = 0; bid < Nb; bid++) {
+                double rtblade = rt + (bid * 2. / Nb) * Pi;
+                double x_ = th - rtblade, thblade = x_ - floor(x_ / (2. * Pi)) * (2. * Pi);
+                bool isblade = (rr <= r->radius && rr > r->hub_radius);
+                isblade = isblade && (thblade >= (Nb - 1) * Pi / (Nb * 2)) && (thblade <= (Nb + 1) * Pi / (Nb * 2));
+                isblade = isblade && (rr <= r->width / (2 * cos(thblade)) || rr <= r->width / (2 * cos(thblade + Pi)));
+                isblade = isblade && dx >= 0 && dx < r->thick;
+                if (isblade) f = tid + 1;
+            }
+        }
+        if (flag) flag[id] = f;
+        /* the force: src/rmcp/almDevCall.cu:144-209 */
+        if (f > 0) {
+            const int tid = f - 1;
+            double xyz0[3] = {point[0] - r->base[3 * tid], point[1] - r->base[3 * tid + 1], point[2] - r->base[3 * tid + 2]}, xyz[3];
+            double uvw0[3] = {u[id], u[id + N], u[id + 2 * N]}, uvw[3];
+            const double omega0[3] = {0, 0, 0};
+            frame_rotation(xyz0, &r->angle[3 * tid], r->angle_type[tid], xyz);
+            frame_rotation_dt(xyz, uvw0, &r->angle[3 * tid], omega0, r->angle_type[tid], uvw);
+            double dy = xyz[1] - r->hub[3 * tid + 1], dz = xyz[2] - r->hub[3 * tid + 2];
+            double th = atan2(dz, dy);
+            double rr = sqrt(dy * dy + dz * dz);
+            double ux = uvw[0];
+            double ut = r->tip_rate[tid] * rr + uvw[1] * sin(th) - uvw[2] * cos(th);
+            double urel2 = ux * ux + ut * ut;
+            double phi = atan(ux / ut);
+            double chord, twist, cl, cd;
+            rmcp_airfoil(r, rr, phi * 180. / Pi, &chord, &twist, &cl, &cd);
+            double ps = (rr > r->width) ? asin(0.5 * r->width / rr) : 0.5 * Pi / Nb;
+            double Cf = 0.5 * chord / (2 * rr * ps * r->thick);
+            double ffx = fabs((cl * cos(phi) + cd * sin(phi)) * Cf * urel2);
+            double fft = fabs((cl * sin(phi) - cd * cos(phi)) * Cf * urel2);
+            double loc[3] = {-ffx, fft * sin(th), -fft * cos(th)}, nang[3], out[3];
+            for (int a = 0; a < 3; a++) nang[a] = -r->angle[3 * tid + a];
+            frame_rotation(loc, nang, r->angle_type[tid], out);
+            ff[id] = out[0]; ff[id + N] = out[1]; ff[id + 2 * N] = out[2];
+            torque[tid] += rr * fft;
+            thrust[tid] += ffx;
+        } else {
+            ff[id] = 0; ff[id + N] = 0; ff[id + 2 * N] = 0;
+        }
+    }
+}
+
 void oracle_step(const or_case *c, double *u, double *uu, double *p, double *nut, double *ff,
                  const double *kx, const double *g, const double *ja, const double *A, double maxdiag,
                  double t, or_stats *st) {

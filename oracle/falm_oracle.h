@@ -60,6 +60,23 @@ typedef struct {
     or_alm alm;
 } or_case;
 
+/* RMCP rotor model (src/rmcp/turbineHandler.h:13-185, bladeHandler.h:11-134): turbines with
+   a fixed orientation whose rotating blades paint the cells they cover */
+typedef struct {
+    int n_turbine, n_blade;
+    double radius, hub_radius;
+    double width, thick;      /* blade strip width and axial thickness (almDevCall.cu:6-7: 0.1) */
+    const double *base;       /* 3*n_turbine                                                 */
+    const double *hub;        /* 3*n_turbine: (-overhang, 0, tower)                          */
+    const double *angle;      /* 3*n_turbine [rad], one non-zero entry at most               */
+    const int    *angle_type; /* n_turbine: 0 none, 1 roll, 2 pitch, 3 yaw                   */
+    const double *tip_rate;   /* n_turbine                                                   */
+    int n_station, n_attack;
+    const double *st_r, *st_chord, *st_twist;   /* n_station                                 */
+    const double *attack;                        /* n_attack [deg]                            */
+    const double *cl, *cd;    /* n_station*n_attack, element (station, atk) at station*n_attack + atk */
+} or_rmcp;
+
 typedef struct {
     int it; double err; double divnorm;   /* BiCGStab iterations, residual, sqrt(sum div^2)/N */
     double torque[8], thrust[8];          /* per turbine                                        */
@@ -103,6 +120,12 @@ void oracle_alm(const or_case *c, const double *u, double *ff, double t,
                 double *ap_xyz, double *ap_force, double *ap_torque, double *ap_thrust,
                 double *turb_torque, double *turb_thrust);
 /* ---- one full step (app/nedo/main.cpp:150-204 order, race-free pseudo-velocity) ----- */
+/* RMCP forcing at time t: flag (0, or turbine + 1) and force ff of every interior cell from
+   the cell-centre velocity u; torque[t] = sum of r x |tangential force| over the turbine's
+   cells (the formula of the reference's CalcTorque for its other turbine description,
+   almDevCall.cu:368-411), thrust[t] = sum of the axial force magnitudes (no counterpart) */
+void oracle_rmcp(const or_case *c, const or_rmcp *r, const double *u, double *ff, int *flag, double t,
+                 double *torque, double *thrust);
 void oracle_step(const or_case *c, double *u, double *uu, double *p, double *nut, double *ff,
                  const double *kx, const double *g, const double *ja, const double *A, double maxdiag,
                  double t, or_stats *st);

@@ -30,6 +30,23 @@ class OrAlm(ctypes.Structure):
                 ("cl", dp), ("cd", dp), ("pitch", ctypes.c_double)]
 
 
+class OrRmcp(ctypes.Structure):
+    _fields_ = [("n_turbine", ctypes.c_int), ("n_blade", ctypes.c_int), ("radius", ctypes.c_double),
+                ("hub_radius", ctypes.c_double), ("width", ctypes.c_double), ("thick", ctypes.c_double),
+                ("base", dp), ("hub", dp), ("angle", dp), ("angle_type", ip), ("tip_rate", dp),
+                ("n_station", ctypes.c_int), ("n_attack", ctypes.c_int), ("st_r", dp), ("st_chord", dp),
+                ("st_twist", dp), ("attack", dp), ("cl", dp), ("cd", dp)]
+
+
+def rmcp_struct(r):
+    """an or_rmcp for a cases.RmcpSetup (and the arrays it points into)"""
+    k = r.arrays()
+    s = OrRmcp(r.n_turbine, r.n_blade, r.radius, r.hub_radius, r.width, r.thick, _p(k["base"]), _p(k["hub"]),
+               _p(k["angle"]), k["angle_type"].ctypes.data_as(ip), _p(k["tip_rate"]), len(k["st_r"]), len(k["attack"]),
+               _p(k["st_r"]), _p(k["st_chord"]), _p(k["st_twist"]), _p(k["attack"]), _p(k["cl"]), _p(k["cd"]))
+    return s, k
+
+
 class OrCase(ctypes.Structure):
     _fields_ = [("sx", ctypes.c_int), ("sy", ctypes.c_int), ("sz", ctypes.c_int), ("gc", ctypes.c_int),
                 ("x", dp), ("hx", dp), ("y", dp), ("hy", dp), ("z", dp), ("hz", dp),
@@ -116,6 +133,7 @@ class Oracle:
             "oracle_num_threads": [],
             "oracle_transpose_matrix": [C, dp, dp],
             "oracle_step_adjoint": [C, dp, dp, dp, dp, dp, dp, dp, dp, dp, D, D, D, dp, dp, dp, dp, dp, dp],
+            "oracle_rmcp": [C, ctypes.POINTER(OrRmcp), dp, dp, ip, D, dp, dp],
         }
         for k, v in sig.items():
             getattr(L, k).argtypes = v
@@ -125,7 +143,7 @@ class Oracle:
         for k in ("oracle_metrics", "oracle_pseudo_u", "oracle_utouu", "oracle_divergence", "oracle_poisson_rhs",
                   "oracle_project_p", "oracle_sgs", "oracle_mv", "oracle_res", "oracle_sor_sweep",
                   "oracle_pbicgstab", "oracle_plain_solve", "oracle_ubc", "oracle_pbc", "oracle_uubc", "oracle_build_aps",
-                  "oracle_alm", "oracle_step", "oracle_transpose_matrix"):
+                  "oracle_alm", "oracle_step", "oracle_transpose_matrix", "oracle_rmcp"):
             getattr(L, k).restype = None
 
     def threads(self):
@@ -203,6 +221,15 @@ class Oracle:
                 raise ValueError("oracle_step_adjoint: unsupported scheme or SGS model")
         return J, float(gp[0]), gch, gtw
 
+    def rmcp(self, cs, r, u, t):
+        """oracle_rmcp: force field, paint, per-turbine torque and thrust of the RMCP model"""
+        rs, keep = rmcp_struct(r)
+        n = cs.case.grid.n
+        ff, flag = np.zeros(3 * n), np.zeros(n, dtype=np.int32)
+        tq, th = np.zeros(r.n_turbine), np.zeros(r.n_turbine)
+        self.L.oracle_rmcp(ctypes.byref(cs.c), ctypes.byref(rs), _p(u), _p(ff), flag.ctypes.data_as(ip), t, _p(tq), _p(th))
+        return ff, flag, tq, th
+
     def alm(self, cs, u, ff, t):
         a = cs.c.alm
         apc = a.n_turbine * a.n_blade * a.n_ap_per_blade
@@ -238,6 +265,8 @@ class RefStep:
         L.ref_write_index.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_ulonglong), dp,
                                       ctypes.POINTER(ctypes.c_int), ctypes.c_int]
         L.ref_write_cv.argtypes = [P, ctypes.c_char_p]
+        L.ref_rmcp_init.argtypes = [P, ctypes.POINTER(OrRmcp)]
+        L.ref_rmcp_run.argtypes = [P, ctypes.c_double, dp, ip]
         self.cs = cs
         self.n = cs.case.grid.n
         st = cs.case.alm.stations if cs.case.alm is not None else None
@@ -315,6 +344,21 @@ class RefStep:
         times = np.ascontiguousarray([float(q[1]) for q in snapshots] or [0.0])
         tav = (ctypes.c_int * max(n, 1))(*[1 if q[2] else 0 for q in snapshots])
         self.L.ref_write_index(self.h, str(path).encode(), steps, _p(times), tav, n)
+
+    def rmcp_init(self, r):
+        """the reference's RmcpAlm::init for a cases.RmcpSetup"""
+        self._rmcp = rmcp_struct(r)
+        rc = self.L.ref_rmcp_init(self.h, ctypes.byref(self._rmcp[0]))
+        if rc:
+            raise RuntimeError(f"ref_rmcp_init: {rc}")
+
+    def rmcp_run(self, t):
+        """RmcpAlm::SetALMFlag + ALM on the harness's U: (ff, flag)"""
+        ff, flag = np.zeros(3 * self.n), np.zeros(self.n, dtype=np.int32)
+        rc = self.L.ref_rmcp_run(self.h, t, _p(ff), flag.ctypes.data_as(ip))
+        if rc:
+            raise RuntimeError(f"ref_rmcp_run: {rc}")
+        return ff, flag
 
     def write_cv(self, path):
         """FalmIO::writeControlVolumeFile of the case grid"""

@@ -24,6 +24,7 @@
 #include "FalmEq.h"
 #include "MV.h"
 #include "alm/alm.h"
+#include "rmcp/alm.h"
 #include "windtunnel/bcdevcall.h"
 #include "lid3d/bcdev.h"
 #include "FalmIO.h"
@@ -45,6 +46,8 @@ struct RefCase {
     FalmEq eq;
     Alm::AlmHandler alm;
     bool alm_on = false;
+    Rmcp::RmcpAlm rmcp;
+    bool rmcp_on = false;
     Real maxdiag = 1.0;
     dim3 block{8, 8, 8};
     Stream streams[CPM::NFACE];
@@ -281,6 +284,7 @@ void ref_destroy(void *h) {
     RefCase *R = (RefCase *)h;
     if (!R) return;
     if (R->alm_on) R->alm.finalize();
+    if (R->rmcp_on) R->rmcp.finalize();
     R->cfd.release();
     R->eq.release();
     for (auto &s : R->streams) cudaStreamDestroy(s);
@@ -435,6 +439,61 @@ int ref_step(void *h, double t, or_stats *st) {
     ref_op(h, RO_SGS, t, nullptr);
     ref_op(h, RO_DIV, t, &local);
     if (st) *st = local;
+    return (int)cudaDeviceSynchronize();
+}
+
+/* The reference's RMCP model (src/rmcp/alm.h: RmcpAlm::init from the turbine parameters and
+ * the blade property file it names, as its drivers do), on the harness's grid */
+int ref_rmcp_init(void *h, const or_rmcp *r) {
+    RefCase *R = (RefCase *)h;
+    Json blade;
+    blade["attacks"] = std::vector<double>(r->attack, r->attack + r->n_attack);
+    Json afs = Json::array();
+    for (int s = 0; s < r->n_station; s++) {
+        Json af;
+        af["r/R"] = r->st_r[s];
+        af["chord/R"] = r->st_chord[s];
+        af["twist[deg]"] = r->st_twist[s];
+        af["Cl"] = std::vector<double>(r->cl + (long)s * r->n_attack, r->cl + (long)(s + 1) * r->n_attack);
+        af["Cd"] = std::vector<double>(r->cd + (long)s * r->n_attack, r->cd + (long)(s + 1) * r->n_attack);
+        afs.push_back(af);
+    }
+    blade["airfoils"] = afs;
+    std::ofstream bf(R->workdir + "/rmcp_blade.json");
+    bf << blade.dump(2);
+    bf.close();
+    Json params;
+    params["radius"] = r->radius;
+    params["hubRadius"] = r->hub_radius;
+    params["bladeNumber"] = r->n_blade;
+    params["overhang"] = -r->hub[0];
+    params["tower"] = r->hub[2];
+    params["bladeProperties"] = "rmcp_blade.json";
+    Json arr = Json::array();
+    for (int t = 0; t < r->n_turbine; t++) {
+        Json tj;
+        tj["tipRate"] = r->tip_rate[t];
+        tj["baseLocation"] = {r->base[3 * t], r->base[3 * t + 1], r->base[3 * t + 2]};
+        /* degrees, as the reference reads them (TurbineHandler::alloc converts with deg2rad) */
+        tj["angle"] = {r->angle[3 * t] * 180.0 / M_PI, r->angle[3 * t + 1] * 180.0 / M_PI, r->angle[3 * t + 2] * 180.0 / M_PI};
+        arr.push_back(tj);
+    }
+    params["turbineArray"] = arr;
+    R->rmcp.init(R->cpm, params, R->workdir);
+    R->rmcp_on = true;
+    return (int)cudaDeviceSynchronize();
+}
+
+/* RmcpAlm::SetALMFlag + RmcpAlm::ALM at time t on the harness's u: ff (3N) and flag (N) out */
+int ref_rmcp_run(void *h, double t, double *ff, int *flag) {
+    RefCase *R = (RefCase *)h;
+    if (!R->rmcp_on) return 2;
+    R->rmcp.SetALMFlag(R->xyz, t, R->cpm);
+    R->rmcp.ALM(R->u, R->xyz, R->ff, t, R->cpm);
+    int rc = (int)cudaDeviceSynchronize();
+    if (rc) return rc;
+    copy_out(R->ff, ff);
+    if (flag) cudaMemcpy(flag, R->rmcp.alm_flag.dev.ptr, sizeof(int) * R->rmcp.alm_flag.size, cudaMemcpyDeviceToHost);
     return (int)cudaDeviceSynchronize();
 }
 
