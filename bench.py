@@ -44,6 +44,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--case", default="channel_large")
+    ap.add_argument("--slabs", action="store_true",
+                    help="with N ranks: one grid of N z-stacked copies of the case's planes, one slab per GPU, halos and "
+                         "reductions over NCCL (weak scaling), instead of N independent replicas")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
@@ -769,6 +772,52 @@ def run_reference(args, rank, world, local):
                   "clocks": clk, "kind": "reference"}
 
 
+def run_slabs_bench(args, rank, world, local):
+    """The case's grid stacked `world` times along z (each rank one slab of the
+    case's size: weak scaling), every rank a SlabSimulation over the NCCL
+    transport; W warm-up steps, then K timed steps between barriers (CUDA
+    events on each rank's stream, maximum over the ranks).  The state after the
+    warm-up is restored every RESTART steps inside the timed region."""
+    import ctypes
+    import torch
+    from falm_b200 import _lib as L
+    from falm_b200 import cases
+    from falm_b200 import slab as SL
+    base = bench_case(args)
+    nx, ny, nz = base.grid.interior
+    h = float(base.grid.hx[base.grid.gc])
+    case = cases.channel(nx, ny, nz * world, cells_per_radius=round(1 / h), intensity=args.intensity, tol=args.tol,
+                         hub=(3.2, 0.5 * ny * h, 0.5 * nz * h), name=f"{base.name}_stacked{world}").with_inflow()
+    transport = SL.nccl_transport(rank, world)
+    sim = SL.SlabSimulation(case, rank, world, transport, args.precision, f"cuda:{local}")
+    for _ in range(args.warmup):
+        sim.step()
+    snap = ({k: getattr(sim, k).clone() for k in ("u", "uu", "p", "nut")}, sim.it)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = ClockSampler(local).start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    ev0.record()
+    for q in range(args.steps):
+        if q and q % RESTART == 0:
+            for k, v in snap[0].items():
+                getattr(sim, k).copy_(v)
+            sim.it = snap[1]
+        stats.append(sim.step())
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world)
+    barrier(world)
+    clk = clocks.stop()
+    n = case.grid.n_interior
+    sim.close()
+    L.load().falm_nccl_transport_destroy(ctypes.byref(transport))
+    return case, {"value": n * args.steps / (ms / 1e3) / 1e6, "ms_per_step": ms / args.steps,
+                  "steps_per_s": 1e3 * args.steps / ms, "its": it_summary([x["it"] for x in stats]),
+                  "divnorm_max": max(x["divnorm"] for x in stats), "clocks": clk}
+
+
 def main():
     args = parse()
     if args.power_run:
@@ -797,6 +846,21 @@ def main():
             line["cpu_baseline"] = {"value": r["value"], "unit": UNIT, "cores": 0, "kind": "reference",
                                     "sample": "the reference's own CUDA step (it has no CPU path), full workload"}
         print(json.dumps(line), flush=True)
+        return
+    if args.slabs:
+        case, r = run_slabs_bench(args, rank, world, local)
+        if rank == 0:
+            g = case.grid.interior
+            print(json.dumps({
+                "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "steps_per_s": r["steps_per_s"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 storage / f64 reductions" if args.precision == "mixed" else "f64",
+                "data": "synthetic" + (" (seeded Philox inflow, seed 20261203)" if case.intensity else " (uniform inflow)"),
+                "config": workload_config(args, bench_case(args)), "precision": args.precision,
+                "parallelism": f"z slabs x{world} (NCCL halos and reductions)",
+                "slab_grid": f"{g[0]}x{g[1]}x{g[2]}", "its": r["its"], "divnorm_max": r["divnorm_max"],
+                "clocks": r["clocks"]}), flush=True)
         return
     case, r = run_ours(args, rank, world, local)
     if rank != 0:

@@ -329,6 +329,9 @@ int sor_rb2_launch(falm_ctx *ctx, cudaStream_t st, const T *xin, const T *b, T *
 
 template <typename T>
 int sor_rb_launch(falm_ctx *ctx, cudaStream_t st, int H, const T *xin, const T *b, T *xout, T omega, int c1, const SolverScalars *sc) {
+    // the blocked kernels take the colour parity of local plane indices: a grid
+    // whose planes are offset by koff flips the first colour instead
+    c1 ^= ctx->geo.koff & 1;
     if constexpr (sizeof(T) == 4) {
         if (H == 3 && !ctx->sor_v1) {
             const int r = sor_rb2_launch<T>(ctx, st, xin, b, xout, omega, c1, sc);

@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(256) k_sor_rb_tma(Geom g, int kc, const __grid
             const int p = q - h, kp = P0 + p, ring = H - h;
             if (p >= 1 && kp >= max(klo, k0 - ring) && kp < min(khi, k1 + ring)) {
                 const int color = (c1 + h - 1) & 1;
-                const int e = (color ^ (x0 + y + kp + tb.koff)) & 1;   // the pair's cell of this colour
+                const int e = (color ^ (x0 + y + kp)) & 1;          // the pair's cell of this colour
                 if ((((e ? live1 : live0) >> (h - 1)) & 1u) != 0u) {
                     T *X0 = (T *)sl[h];
                     const T *Xm = (const T *)sl[h + 1], *Xp = (const T *)sl[h - 1];
@@ -436,7 +436,7 @@ __global__ void __launch_bounds__(RB2Tile<T>::NT, 4) k_sor_rb2_tma(Geom g, int k
                 const int p = q - (2 * h - 1), kp = P0 + p, ring = H - h;
                 if (p >= 1 && p + 1 < nplanes && kp >= max(klo, k0 - ring) && kp < min(khi, k1 + ring)) {
                     const int color = (c1 + h - 1) & 1;
-                    const int e = (color ^ par0 ^ (kp + tb.koff)) & 1;   // the pairs' cell of this colour (both row sets)
+                    const int e = (color ^ par0 ^ kp) & 1;   // the pairs' cell of this colour (both row sets)
                     const unsigned l0 = (live >> (3 * e + h - 1)) & 1u, l1 = (live >> (3 * (2 + e) + h - 1)) & 1u;
                     if (l0 | l1) {
                         float *X0 = (float *)sl(2 * h - 1);

@@ -98,15 +98,16 @@ def broadcast_id(id_bytes, src=0):
 def nccl_transport(rank, nranks):
     """falm_nccl_transport_create on every rank of an initialised torch.distributed
     group (one process per GPU, the current device set): rank 0's NCCL unique id
-    is broadcast through the group"""
+    is broadcast through the group (one rank needs no group)"""
     lib = L.load()
     raw = (ctypes.c_ubyte * 128)()
     if rank == 0:
         rc = lib.falm_nccl_unique_id(ctypes.byref(raw))
         if rc:
             raise L.FalmError(rc, "falm_nccl_unique_id")
-    uid = broadcast_id(bytes(raw), 0)
-    raw = (ctypes.c_ubyte * 128)(*uid)
+    if nranks > 1:
+        uid = broadcast_id(bytes(raw), 0)
+        raw = (ctypes.c_ubyte * 128)(*uid)
     t = L.Transport()
     rc = lib.falm_nccl_transport_create(ctypes.byref(raw), rank, nranks, ctypes.byref(t))
     if rc:
