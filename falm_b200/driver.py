@@ -18,12 +18,15 @@ class Simulation:
             ctx.set_inflow(case.inflow, float(case.grid.hx[case.grid.gc]))
         if case.alm is not None:
             ctx.alm_init(case.alm)
+        if getattr(case, "rmcp", None) is not None:
+            ctx.rmcp_init(case.rmcp)        # the RMCP model replaces the ALM as the step's forcing
         self.ctx = ctx
         torch = ctx.torch
         st = C.initial_state(case)
         self.u = torch.as_tensor(st["u"], dtype=ctx.dtype, device=ctx.device).contiguous()
         self.uu, self.p, self.nut = ctx.field(3), ctx.field(1), ctx.field(1)
-        self.ff = None if (fuse_alm and case.alm is not None) else ctx.field(3)
+        rmcp = getattr(case, "rmcp", None) is not None
+        self.ff = None if rmcp or (fuse_alm and case.alm is not None) else ctx.field(3)
         ctx.utouu(self.u, self.uu)         # app/nedo/main.cpp:132-133
         ctx.sgs(self.u, self.nut)
         self.it = 0

@@ -136,6 +136,8 @@ class SlabSimulation:
             ctx.set_inflow(case.inflow, float(case.grid.hx[case.grid.gc]))
         if case.alm is not None:
             ctx.alm_init(case.alm)
+        if getattr(case, "rmcp", None) is not None:
+            ctx.rmcp_init(case.rmcp)
         self.ctx = ctx
         torch = ctx.torch
         st = C.initial_state(self.local)

@@ -1,7 +1,8 @@
 /*
  * falm_b200.hpp -- C++ host shim with the reference's solver-class surface
- * (FalmCFD, FalmEq, FalmMV, Alm::AlmHandler; src/FalmCFD.h, src/FalmEq.h,
- * src/MV.h, src/alm/alm.h) over the C ABI of include/falm_b200.h.
+ * (FalmCFD, FalmEq, FalmMV, Alm::AlmHandler, Rmcp::RmcpAlm, CPMComm;
+ * src/FalmCFD.h, src/FalmEq.h, src/MV.h, src/alm/alm.h, src/rmcp/alm.h,
+ * src/CPMComm.h) over the C ABI of include/falm_b200.h.
  *
  * Method names, argument order and meaning follow the reference, so a driver
  * such as app/nedo/main.cpp:150-204 keeps its shape.  Differences:
@@ -10,8 +11,12 @@
  *  - kx, g, ja are accepted for signature compatibility and ignored: the
  *    metrics are evaluated from the control-volume tables bound to the
  *    Context (what the reference builds those planes from).
- *  - CPM is one rank with no neighbours (no MPI); block / stream-array
+ *  - CPM is one rank with no neighbours unless Context::slab makes the context
+ *    one z-slab of a decomposed grid; CPMComm<T> then exchanges a field's z
+ *    halo through the slab's transport (no MPI).  Block / stream-array
  *    arguments are accepted and ignored (the library sizes its own launches).
+ *  - Rmcp::RmcpAlm (src/rmcp/alm.h) is the RMCP rotor model over
+ *    falm_rmcp_init / falm_rmcp_run.
  *  - The reference prints error codes and continues (src/error.h:20-26); here
  *    every call returns the falm_status and a failing call throws Falm::Error.
  *  - FalmIO takes the Context where the reference takes CPM, writes vector
@@ -52,13 +57,18 @@ struct Region {
 };
 
 struct CPM {
+    static const Int XMINUS = 0, XPLUS = 1, YMINUS = 2, YPLUS = 3, ZMINUS = 4, ZPLUS = 5, NFACE = 6;
     int rank = 0, size = 1;
     Int gc = 2;
     Region global;
     std::vector<Region> pdm_list;
     CPM() {}
     CPM(Int3 shape, Int gc_) : gc(gc_), global(shape, Int3{{0, 0, 0}}), pdm_list(1, Region(shape, Int3{{0, 0, 0}})) {}
-    bool validNeighbour(Int) const { return false; }
+    /* a z-slab decomposition (the reference splits x, src/CPMBase.h:36-112): the only
+       neighbours are the slabs below (ZMINUS) and above (ZPLUS) */
+    bool validNeighbour(Int fid) const {
+        return (fid == ZMINUS && rank > 0) || (fid == ZPLUS && rank < size - 1);
+    }
 };
 
 /* device-first field in the reference layout (src/matrix.h:129-188) */
@@ -107,6 +117,31 @@ public:
     ~Context() { if (h) falm_destroy(h); }
     Context(const Context &) = delete;
     Context &operator=(const Context &) = delete;
+    /* make this context slab `rank` of `nranks` (falm_slab_init): the grid given to the
+       constructor is the slab's, z_offset its first interior plane in the whole grid of
+       nz_global interior planes; call before any other set-up */
+    void slab(int rank, int nranks, int z_offset, int nz_global, const falm_transport &t) {
+        check(falm_slab_init(h, rank, nranks, z_offset, nz_global, &t), h, "Context::slab");
+        cpm.rank = rank;
+        cpm.size = nranks;
+    }
+};
+
+/* CPMComm<T> (src/CPMComm.h:95-364) over the slab halo exchange: the exchange is ordered on the
+   stream and complete for the stream's later work when IExchange6Face returns, so Wait6Face and
+   PostExchange6Face have nothing left to do.  margin is the reference's inner offset of the sent
+   planes, which is the guide-cell depth here; only the z faces of a slab have neighbours. */
+template <typename T>
+class CPMComm {
+public:
+    Context *c;
+    explicit CPMComm(Context &ctx) : c(&ctx) {}
+    void IExchange6Face(T *data, Int thick, Int /*margin*/, int /*grp_tag*/, void *stream = nullptr) {
+        if (c->cpm.size > 1)
+            check(falm_slab_halo(c->h, data, 1, thick, stream), c->h, "CPMComm::IExchange6Face");
+    }
+    void Wait6Face() {}
+    void PostExchange6Face(void * = nullptr) {}
 };
 
 struct AdvectionSchemeType { static const Flag Upwind1 = 0, Upwind3 = 1, QUICK = 2, UTOPIA = 3, KK = 4; };
@@ -317,6 +352,34 @@ public:
     double power(int tid) const { return torque[tid] * tip_rate[tid]; }
 };
 }  // namespace Alm
+
+namespace Rmcp {
+/* RmcpAlm (src/rmcp/alm.h:11-96); init takes the turbine and blade tables instead of a JSON
+   file.  The cell centres come from the bound context, so the x argument is dropped.  init also
+   makes RMCP the forcing of falm_step. */
+template <typename Real>
+class RmcpAlm {
+public:
+    Context *c;
+    int n_turbine = 0;
+    std::vector<double> torque, thrust;
+    explicit RmcpAlm(Context &ctx) : c(&ctx) {}
+    void init(const falm_rmcp_desc &d) {
+        check(falm_rmcp_init(c->h, &d), c->h, "RmcpAlm::init");
+        n_turbine = d.n_turbine;
+        torque.assign(n_turbine, 0.0);
+        thrust.assign(n_turbine, 0.0);
+    }
+    /* SetALMFlag (alm.h:53-63): the paint of the turbines' box cells at time t into flag */
+    void SetALMFlag(Matrix<int> &flag, Matrix<Real> &u, Matrix<Real> &ff, Real t) {
+        check(falm_rmcp_run(c->h, u.dev.ptr, ff.dev.ptr, t, nullptr, flag.dev.ptr, nullptr, nullptr), c->h, "RmcpAlm::SetALMFlag");
+    }
+    /* ALM (alm.h:35-52) + CalcTorque (alm.h:26-33): ff at the painted cells, and the turbine sums */
+    void ALM(Matrix<Real> &u, Matrix<Real> &ff, Real t) {
+        check(falm_rmcp_run(c->h, u.dev.ptr, ff.dev.ptr, t, nullptr, nullptr, torque.data(), thrust.data()), c->h, "RmcpAlm::ALM");
+    }
+};
+}  // namespace Rmcp
 
 }  // namespace Falm
 

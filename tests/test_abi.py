@@ -153,3 +153,45 @@ def test_mesher_matches_reference(lib_built, tmp_path, mode):
             np.testing.assert_allclose(x[gc - 1:len(x) - gc + 1], xs, rtol=0, atol=1e-15)
     with pytest.raises(_lib.FalmError):
         api.build_mesh("face", src, str(tmp_path / "x.cv"), 2)
+
+
+def test_class_shim_compiles(tmp_path):
+    """Every class of the C++ shim (include/falm_b200.hpp) instantiated in both
+    precisions, including the slab (Context::slab, CPMComm) and RMCP
+    (Rmcp::RmcpAlm) surfaces: a syntax-only compile against the CUDA headers."""
+    import shutil
+    import subprocess
+    nvcc = shutil.which("nvcc")
+    if nvcc is None:
+        pytest.skip("no CUDA toolkit")
+    cuda_inc = os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(nvcc))), "include")
+    src = tmp_path / "shim.cpp"
+    src.write_text(r'''
+#include "falm_b200.hpp"
+using namespace Falm;
+template <typename Real> void use(Context &ctx, const falm_transport &t, const falm_rmcp_desc &rd) {
+    ctx.slab(0, 2, 0, 64, t);
+    FalmCFD<Real> cfd(ctx);
+    FalmEq<Real> eq(ctx);
+    Alm::AlmHandler<Real> alm(ctx);
+    Rmcp::RmcpAlm<Real> rmcp(ctx);
+    CPMComm<Real> comm(ctx);
+    Int3 dom{{8, 8, 8}};
+    Matrix<Real> u(dom, 3), ff(dom, 3), p(dom, 1);
+    Matrix<int> flag(dom, 1);
+    rmcp.init(rd);
+    rmcp.SetALMFlag(flag, u, ff, Real(0));
+    rmcp.ALM(u, ff, Real(0));
+    comm.IExchange6Face(p.dev.ptr, 1, 2, 0);
+    comm.Wait6Face();
+    comm.PostExchange6Face();
+    (void)FalmMV<Real>::DotProduct(ctx, p, p);
+    (void)ctx.cpm.validNeighbour(CPM::ZPLUS);
+    (void)cfd; (void)eq; (void)alm;
+}
+template void use<double>(Context &, const falm_transport &, const falm_rmcp_desc &);
+template void use<float>(Context &, const falm_transport &, const falm_rmcp_desc &);
+''')
+    r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-Wall", "-I", os.path.join(ROOT, "include"), "-I", cuda_inc,
+                        str(src)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr

@@ -83,6 +83,40 @@ def test_slabs_converged_and_mixed(lib_built):
     assert compare(case, two_m, one)["u"] < 2e-4
 
 
+def test_slabs_with_rmcp_match_one_slab_and_the_driver(lib_built):
+    """The RMCP rotor (48^3 channel, rotor in the middle, so its blades cross the
+    slab interfaces): each slab paints and forces its own cells and the turbine
+    sums are reduced over the slabs.  2 slabs against 1 slab after 5 FP64 steps
+    in fixed-iteration mode within 1e-12 (velocities) and 1e-10 (pressure),
+    torque and thrust within 1e-12; the one-slab path against the Python
+    driver's fused one-GPU step (driver.Simulation) within 1e-10."""
+    from falm_b200.driver import Simulation
+    from tests.test_gpu_rmcp import rmcp_case
+    case = rmcp_case(10.0)
+    one, s1 = SL.run_slabs(case, 1, 5, maxit=6, tol=0.0)
+    two, s2 = SL.run_slabs(case, 2, 5, maxit=6, tol=0.0)
+    err = compare(case, two, one)
+    for k in ("u", "uu", "nut"):
+        assert err[k] < 1e-12, (k, err)
+    assert err["p"] < 1e-10, err
+    for r in range(2):
+        for a, b in zip(s2[r], s1[0]):
+            assert a["it"] == b["it"]
+            assert b["torque"][0] > 0
+            for x, y in zip(a["torque"] + a["thrust"], b["torque"] + b["thrust"]):
+                assert x == pytest.approx(y, rel=1e-12)
+    case.maxit, case.tol = 6, 0.0
+    sim = Simulation(case)
+    st = [sim.step() for _ in range(5)]
+    got = {k: getattr(sim, k).double().cpu().numpy() for k in ("u", "uu", "p", "nut")}
+    sim.ctx.close()
+    err = compare(case, got, one)
+    for k, v in err.items():
+        assert v < 1e-10, (k, v, err)
+    for a, b in zip(st, s1[0]):
+        assert a["torque"][0] == pytest.approx(b["torque"][0], rel=1e-10)
+
+
 def test_nccl_transport_one_rank(lib_built):
     """libnccl through the library (a one-rank communicator: no exchange, the
     reductions an identity): the slab step is the local transport's, and the
