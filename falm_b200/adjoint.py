@@ -20,6 +20,11 @@ checkpointing instead: the states stored at any time are bounded by a number
 of slots (or a memory budget), and forward steps are recomputed along the
 optimal schedule of the binomial recursion (binomial_table).
 
+Precision: the adjoint fields and gradients are FP64 in every context.  In a
+mixed-precision context the forward steps run in mixed precision, the stored
+states and checkpoints are FP32 (half the memory of an FP64 context), and the
+adjoint of each step is evaluated at those FP32 states.
+
 `MeanPower` wraps the same computation as a torch.autograd.Function; it is
 used only to check the gradients (torch.autograd.gradcheck-style comparisons),
 not as a training path.
@@ -105,8 +110,6 @@ def mean_power_gradient(sim, steps, checkpoint=None):
     recomputes nothing; None chooses, see auto_checkpoint)."""
     ctx = sim.ctx
     torch = ctx.torch
-    if ctx.precision != "fp64":
-        raise ValueError("the discrete adjoint runs in FP64 contexts")
     if checkpoint is None:
         checkpoint = auto_checkpoint(sim, steps)
     checkpoint = max(1, min(checkpoint, steps))
@@ -221,8 +224,6 @@ def mean_power_gradient_binomial(sim, steps, snaps=None, budget_bytes=None):
     window."""
     ctx = sim.ctx
     torch = ctx.torch
-    if ctx.precision != "fp64":
-        raise ValueError("the discrete adjoint runs in FP64 contexts")
     if snaps is None:
         if budget_bytes is None:
             budget_bytes = 0.25 * torch.cuda.mem_get_info(sim.u.device)[0]

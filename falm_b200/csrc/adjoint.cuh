@@ -1,4 +1,4 @@
-// Discrete adjoint of one time step (FP64).  No reference counterpart: this is
+// Discrete adjoint of one time step.  No reference counterpart: this is
 // the adjoint of this library's own discretisation of the step, with the
 // Poisson solve treated as exact (p = A^-1 rhs), so that its adjoint is one
 // solve with the transposed operator.  Each kernel below is the transpose of
@@ -6,7 +6,9 @@
 // stencil neighbours use double-precision atomics.
 //
 // Arrays: au/auu/anut hold the adjoint of the state after the step (they are
-// consumed), au0/auu0/anut0 collect the adjoint of the state before it.
+// consumed), au0/auu0/anut0 collect the adjoint of the state before it.  The
+// adjoint is FP64 throughout; the forward state it is evaluated at (u, uu, nut
+// of type T) is FP64 or, for a mixed-precision context, FP32.
 #pragma once
 #include "common.cuh"
 #include "alm_bc.cuh"
@@ -31,7 +33,8 @@ __device__ __forceinline__ bool adj_facemap(const Geom &g, int i, int j, int k) 
 __device__ __forceinline__ double adj_sgn(double v) { return (v > 0) - (v < 0); }
 
 // (9) Smagorinsky eddy viscosity of the new velocity (SgsDivBody / k_sgs_div)
-__global__ void k_adj_sgs(Geom g, MetricView<double> mv, const double *__restrict__ un, const double *__restrict__ anut,
+template <typename T>
+__global__ void k_adj_sgs(Geom g, MetricView<double> mv, const T *__restrict__ un, const double *__restrict__ anut,
                           double *au, double Cs) {
     const long long N = g.n;
     ADJ_FOR_BOX(g.gc, g.sx - g.gc, g.gc, g.sy - g.gc, g.gc, g.sz - g.gc, i, j, k) {
@@ -45,7 +48,7 @@ __global__ void k_adj_sgs(Geom g, MetricView<double> mv, const double *__restric
 #pragma unroll
         for (int m = 0; m < 3; m++)
 #pragma unroll
-            for (int a = 0; a < 3; a++) d[m][a] = 0.5 * kk[a] * (un[nbp[a] + m * N] - un[nbm[a] + m * N]);
+            for (int a = 0; a < 3; a++) d[m][a] = 0.5 * kk[a] * (to_d(un[nbp[a] + m * N]) - to_d(un[nbm[a] + m * N]));
         const double S = 2 * (d[0][0] * d[0][0]) + 2 * (d[1][1] * d[1][1]) + 2 * (d[2][2] * d[2][2]) + (d[0][1] + d[1][0]) * (d[0][1] + d[1][0]) +
                          (d[1][2] + d[2][1]) * (d[1][2] + d[2][1]) + (d[0][2] + d[2][0]) * (d[0][2] + d[2][0]);
         const double Du = sqrt(S);
@@ -283,7 +286,8 @@ __global__ void k_adj_carry_ghosts(Geom g, const double *aua, double *au0) {
 }
 
 // (2) pseudo-velocity with a 4th-order scheme: ua = u0 + dt (-adv + vis + ff)
-__global__ void k_adj_pseudo_u(Geom g, MetricView<double> mv, const double *u0, const double *uu0, const double *nut0,
+template <typename T>
+__global__ void k_adj_pseudo_u(Geom g, MetricView<double> mv, const T *u0, const T *uu0, const T *nut0,
                                const double *aua, double *au0, double *auu0, double *anut0, double *aff,
                                double ReI, double dt, double alpha) {
     const long long N = g.n;
@@ -298,28 +302,28 @@ __global__ void k_adj_pseudo_u(Geom g, MetricView<double> mv, const double *u0, 
         const double jac = mv.ja(i, j, k);
         double Uc[3], Ua[3], Gp[3], Gm[3], Np[3], Nm[3];
         for (int q = 0; q < 3; q++) {
-            Uc[q] = u0[cc + q * N] * mv.kx(q, idx[q]);
+            Uc[q] = to_d(u0[cc + q * N]) * mv.kx(q, idx[q]);
             Ua[q] = fabs(Uc[q]);
             const int ip[3] = {i + (q == 0), j + (q == 1), k + (q == 2)}, im[3] = {i - (q == 0), j - (q == 1), k - (q == 2)};
             Gp[q] = mv.g(q, i, j, k) + mv.g(q, ip[0], ip[1], ip[2]);
             Gm[q] = mv.g(q, i, j, k) + mv.g(q, im[0], im[1], im[2]);
-            Np[q] = ReI + 0.5 * (nut0[cc] + nut0[nbp[q][0]]);
-            Nm[q] = ReI + 0.5 * (nut0[cc] + nut0[nbm[q][0]]);
+            Np[q] = ReI + 0.5 * (to_d(nut0[cc]) + to_d(nut0[nbp[q][0]]));
+            Nm[q] = ReI + 0.5 * (to_d(nut0[cc]) + to_d(nut0[nbm[q][0]]));
         }
         double aUa[3] = {0, 0, 0};
         const double f = 0.5 / (24. * jac);
         for (int d = 0; d < 3; d++) {
             const double a = aua[cc + d * N];
             if (a == 0.0) continue;
-            const double *ud = u0 + d * N;
+            const T *ud = u0 + d * N;
             double *aud = au0 + d * N;
             atomicAdd(aud + cc, a);
             aff[cc + d * N] += dt * a;
             const double aadv = -dt * a, avis = dt * a / (2 * jac);
-            const double ucc = ud[cc];
+            const double ucc = to_d(ud[cc]);
             for (int ax = 0; ax < 3; ax++) {
-                const double up1 = ud[nbp[ax][0]], up2 = ud[nbp[ax][1]], um1 = ud[nbm[ax][0]], um2 = ud[nbm[ax][1]];
-                const double JP = uu0[facep[ax]], JM = uu0[facem[ax]];
+                const double up1 = to_d(ud[nbp[ax][0]]), up2 = to_d(ud[nbp[ax][1]]), um1 = to_d(ud[nbm[ax][0]]), um2 = to_d(ud[nbm[ax][1]]);
+                const double JP = to_d(uu0[facep[ax]]), JM = to_d(uu0[facem[ax]]);
                 const double L = -up2 + 27 * up1 - 27 * ucc + um1, R = -up1 + 27 * ucc - 27 * um1 + um2;
                 const double D = up2 - 4 * up1 + 6 * ucc - 4 * um1 + um2;
                 atomicAdd(auu0 + facep[ax], aadv * f * L);
@@ -382,8 +386,9 @@ __global__ void __launch_bounds__(256) k_adj_alm_project(Geom g, AlmDev a, const
 // (1b) per AP: recompute k_alm_force's chain and apply its transpose, plus the
 // objective term wP * tip * |ft| * r; gradients: grad[0] pitch, grad[1 + ap]
 // chord, grad[1 + apcount + ap] twist
+template <typename T>
 __global__ void __launch_bounds__(128) k_adj_alm_ap(Geom g, AlmDev a, const double *xc, const double *yc, const double *zc,
-                                                    const double *u0, double t, const double *aF, double wP, double *au0,
+                                                    const T *u0, double t, const double *aF, double wP, double *au0,
                                                     double *grad) {
     const long long N = g.n;
     const int nappt = a.n_ap_per_blade * a.n_blade;
@@ -419,9 +424,9 @@ __global__ void __launch_bounds__(128) k_adj_alm_ap(Geom g, AlmDev a, const doub
                            (1 - xd) * (1 - yd) * zd, xd * (1 - yd) * zd, (1 - xd) * yd * zd, xd * yd * zd};
     double uvw[3];
     for (int d = 0; d < 3; d++) {
-        const double *ud = u0 + d * N;
-        const double c01 = ud[id[0]] * (1. - xd) + ud[id[1]] * xd, c23 = ud[id[2]] * (1. - xd) + ud[id[3]] * xd;
-        const double c45 = ud[id[4]] * (1. - xd) + ud[id[5]] * xd, c67 = ud[id[6]] * (1. - xd) + ud[id[7]] * xd;
+        const T *ud = u0 + d * N;
+        const double c01 = to_d(ud[id[0]]) * (1. - xd) + to_d(ud[id[1]]) * xd, c23 = to_d(ud[id[2]]) * (1. - xd) + to_d(ud[id[3]]) * xd;
+        const double c45 = to_d(ud[id[4]]) * (1. - xd) + to_d(ud[id[5]]) * xd, c67 = to_d(ud[id[6]]) * (1. - xd) + to_d(ud[id[7]]) * xd;
         uvw[d] = (c01 * (1. - yd) + c23 * yd) * (1. - zd) + (c45 * (1. - yd) + c67 * yd) * zd;
     }
     const double rel[3] = {c0[0] - a.base[3 * tid], c0[1] - a.base[3 * tid + 1], c0[2] - a.base[3 * tid + 2]};

@@ -243,9 +243,10 @@ bool tma_encode_available() {
 // 4D map (x, y, z, component) of a field in the reference layout with a
 // (bx, by, 1, ncomp) box.  TMA needs a 16 B aligned base and row pitch; the
 // caller falls back to the row kernels otherwise.
-bool make_map(const falm_ctx *ctx, CUtensorMap *m, const void *base, int ncomp, int bx, int by) {
+template <typename T>
+bool make_map(const falm_ctx *ctx, CUtensorMap *m, const T *base, int ncomp, int bx, int by) {
     const Geom &g = ctx->geo;
-    const size_t e = ctx->esize;
+    const size_t e = sizeof(T);   // the field's own type (a mixed context also runs FP64 vectors)
     // every box lies inside the tensor: x and y at least one box long (the
     // kernels clamp the box origins), x rows a whole number of 16-byte units
     // (the kernels' box x origins are 16-byte aligned for gc = 2)
@@ -254,7 +255,7 @@ bool make_map(const falm_ctx *ctx, CUtensorMap *m, const void *base, int ncomp, 
     cuuint64_t strides[3] = {(cuuint64_t)(g.sx * e), (cuuint64_t)(g.sx * (size_t)g.sy * e), (cuuint64_t)(g.n * e)};
     cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, 1, (cuuint32_t)ncomp};
     cuuint32_t es[4] = {1, 1, 1, 1};
-    CUresult r = g_encode(m, e == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void *>(base),
+    CUresult r = g_encode(m, e == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, (void *)base,
                           dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
@@ -358,7 +359,7 @@ int p3_launch(falm_ctx *ctx, int cls, cudaStream_t st, const Region3 &R, int org
     MapSet<NF> maps;
     int slot = 0;
     for (int f = 0; f < NF; f++) {
-        if (!make_map(ctx, &maps.m[f], ptr[f], ncomp[f], L::BX, L::BY)) return 0;
+        if (!make_map(ctx, &maps.m[f], (const T *)ptr[f], ncomp[f], L::BX, L::BY)) return 0;
         maps.ncomp[f] = ncomp[f];
         slot += ncomp[f] * L::FB;
     }
@@ -2149,6 +2150,7 @@ namespace {
 
 struct AdjWork {
     double *uc, *uuc, *pc, *nutc, *au0, *auu0, *anut0, *aua, *auu1, *aff, *ap, *arhs, *r, *AT, *aF, *arhs1;
+    double *v64;  // mixed contexts: the eight FP64 vectors of the transposed BiCGStab solve
 };
 
 // initial guess of the transposed solve: linear extrapolation from the two
@@ -2168,9 +2170,10 @@ __global__ void k_adj_zero_interior(Geom g, double *a) {
 int adj_work(falm_ctx *ctx, AdjWork *w) {
     const size_t n = (size_t)ctx->geo.n;
     const size_t apc = ctx->alm_on ? (size_t)ctx->alm.apcount : 0;
-    const size_t counts[16] = {3 * n, 3 * n, n, n, 3 * n, 3 * n, n, 3 * n, 3 * n, 3 * n, n, n, n, 7 * n, 3 * apc + 1, n};
+    const size_t v64n = ctx->precision == FALM_FP64 ? 1 : 8 * ((n + 31) / 32 * 32);
+    const size_t counts[17] = {3 * n, 3 * n, n, n, 3 * n, 3 * n, n, 3 * n, 3 * n, 3 * n, n, n, n, 7 * n, 3 * apc + 1, n, v64n};
     size_t bytes = 0;
-    for (int q = 0; q < 16; q++) bytes += (counts[q] * sizeof(double) + 255) / 256 * 256;
+    for (int q = 0; q < 17; q++) bytes += (counts[q] * sizeof(double) + 255) / 256 * 256;
     if (!ctx->adj_mem) {
         if (cudaMalloc(&ctx->adj_mem, bytes) != cudaSuccess) { cudaGetLastError(); ctx->adj_mem = nullptr; return fail(ctx, FALM_ERR_ALLOC, "step_adjoint: workspace"); }
         if (cudaMemset(ctx->adj_mem, 0, bytes) != cudaSuccess) { cudaGetLastError(); return fail(ctx, FALM_ERR_CUDA, "step_adjoint: workspace"); }
@@ -2179,7 +2182,40 @@ int adj_work(falm_ctx *ctx, AdjWork *w) {
     double **dst[16] = {&w->uc, &w->uuc, &w->pc, &w->nutc, &w->au0, &w->auu0, &w->anut0, &w->aua, &w->auu1, &w->aff, &w->ap,
                         &w->arhs, &w->r, &w->AT, &w->aF, &w->arhs1};
     for (int q = 0; q < 16; q++) { *dst[q] = (double *)p; p += (counts[q] * sizeof(double) + 255) / 256 * 256; }
+    w->v64 = (double *)p;
     return FALM_OK;
+}
+
+// The transposed Poisson solve of the adjoint, A^T y = b with |b| = 1 (b = w.ap),
+// y in w.arhs (FP64; on entry the extrapolated guess), to |b - A^T y| <= rel,
+// by the context's PBiCGStab in FP64.  A mixed-precision context runs it on
+// FP64 copies of its solver vectors (swapped in for the call) and its FP64
+// operator tables: FP32 BiCGStab cannot be used here, since on the nearly
+// singular operator of a long channel (one Dirichlet face) the transposed
+// solves take hundreds of iterations, over which the FP32 recursion breaks
+// down (non-finite scalars at 512x128x128 where FP64 converges in ~300
+// iterations), and FP32 storage of y would bound its residual near
+// 2 eps_32 / lambda_min, a few 1e-2 for smooth solutions 1024 cells long.
+template <typename T>
+int adj_transposed_solve(falm_ctx *ctx, AdjWork &w, double rel, cudaStream_t st) {
+    const Geom &g = ctx->geo;
+    int it = 0, outer = 0;
+    double err = 0;
+    ctx->tol = rel / ((double)g.nx * g.ny * g.nz);
+    if constexpr (sizeof(T) == 8) {
+        return solve_t<double>(ctx, w.arhs, w.ap, w.r, st, &it, &err, &outer);
+    } else {
+        void **vec[8] = {&ctx->w_rr, &ctx->w_p, &ctx->w_q, &ctx->w_s, &ctx->w_pp, &ctx->w_ss, &ctx->w_t, &ctx->w_xp};
+        void *saved[8];
+        const size_t stride = (size_t)(g.n + 31) / 32 * 32;
+        for (int q = 0; q < 8; q++) { saved[q] = *vec[q]; *vec[q] = w.v64 + q * stride; }
+        const int outer_saved = ctx->max_outer;
+        ctx->max_outer = 1;   // y is FP64: no outer checks of an FP32 iterate
+        const int rc = solve_t<double>(ctx, w.arhs, w.ap, w.r, st, &it, &err, &outer);
+        ctx->max_outer = outer_saved;
+        for (int q = 0; q < 8; q++) *vec[q] = saved[q];
+        return rc;
+    }
 }
 
 }  // namespace
@@ -2190,37 +2226,34 @@ extern "C" int falm_adjoint_set_tol(falm_ctx *ctx, double rel_tol) {
     return FALM_OK;
 }
 
-extern "C" int falm_step_adjoint(falm_ctx *ctx, const falm_fields *f0, const falm_fields *f1, double dt, double t, double w_power,
-                                 void *au, void *auu, void *anut, double *grad, void *stream) {
-    if (!ctx || !f0 || !f0->u || !f0->uu || !f0->p || !f0->nut || !au || !auu || !anut || !grad || !(dt > 0)) return FALM_ERR_ARG;
-    if (ctx->precision != FALM_FP64) return fail(ctx, FALM_ERR_ARG, "step_adjoint: FP64 contexts only");
-    if (ctx->slab_on && ctx->slab_nranks > 1) return fail(ctx, FALM_ERR_ARG, "step_adjoint: a grid of one slab only");
-    if (ctx->rmcp_on) return fail(ctx, FALM_ERR_ARG, "step_adjoint: the ALM forcing only (not the RMCP model)");
-    if (ctx->adv != FALM_ADV_UPWIND3 && ctx->adv != FALM_ADV_UTOPIA && ctx->adv != FALM_ADV_KK)
-        return fail(ctx, FALM_ERR_ARG, "step_adjoint: the 4th-order advection schemes (Upwind3, UTOPIA, KK) only");
-    if (ctx->sgs != FALM_SGS_EMPTY && ctx->sgs != FALM_SGS_SMAGORINSKY) return fail(ctx, FALM_ERR_ARG, "step_adjoint: Smagorinsky or no SGS model only");
+namespace {
+
+// falm_step_adjoint for a context of storage type T (the forward state f0, f1)
+template <typename T>
+int step_adjoint_t(falm_ctx *ctx, const falm_fields *f0, const falm_fields *f1, double dt, double t, double w_power,
+                   void *au, void *auu, void *anut, double *grad, cudaStream_t st) {
     int rc = ensure_work(ctx);
     if (rc) return rc;
     AdjWork w;
     if ((rc = adj_work(ctx, &w))) return rc;
     const Geom &g = ctx->geo;
-    const size_t n = (size_t)g.n, nb = n * sizeof(double);
-    cudaStream_t st = S(stream);
-    const double *un;
+    const size_t n = (size_t)g.n, nb = n * sizeof(double), nt = n * sizeof(T);
+    const T *un;
     if (f1 && f1->u) {
         // the state after the step is given: only the ALM state of the step is needed again
-        un = (const double *)f1->u;
-        if (ctx->alm_on && (rc = alm_run_t<double>(ctx, (const double *)f0->u, nullptr, t, st))) return rc;
+        un = (const T *)f1->u;
+        if (ctx->alm_on && (rc = alm_run_t<T>(ctx, (const T *)f0->u, nullptr, t, st))) return rc;
     } else {
         // forward recomputation of the step on copies of the state
-        CK(cudaMemcpyAsync(w.uc, f0->u, 3 * nb, cudaMemcpyDeviceToDevice, st));
-        CK(cudaMemcpyAsync(w.uuc, f0->uu, 3 * nb, cudaMemcpyDeviceToDevice, st));
-        CK(cudaMemcpyAsync(w.pc, f0->p, nb, cudaMemcpyDeviceToDevice, st));
-        CK(cudaMemcpyAsync(w.nutc, f0->nut, nb, cudaMemcpyDeviceToDevice, st));
-        falm_fields fc{w.uc, w.uuc, w.pc, w.nutc, nullptr};
+        T *uc = (T *)w.uc, *uuc = (T *)w.uuc, *pc = (T *)w.pc, *nutc = (T *)w.nutc;
+        CK(cudaMemcpyAsync(uc, f0->u, 3 * nt, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(uuc, f0->uu, 3 * nt, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(pc, f0->p, nt, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(nutc, f0->nut, nt, cudaMemcpyDeviceToDevice, st));
+        falm_fields fc{uc, uuc, pc, nutc, nullptr};
         falm_step_stats sst;
-        if ((rc = step_t<double>(ctx, &fc, dt, t, st, &sst))) return rc;
-        un = w.uc;
+        if ((rc = step_t<T>(ctx, &fc, dt, t, st, &sst))) return rc;
+        un = uc;
     }
     // reverse sweep
     for (double *z : {w.au0, w.auu0, w.aua, w.auu1, w.aff}) CK(cudaMemsetAsync(z, 0, 3 * nb, st));
@@ -2233,16 +2266,16 @@ extern "C" int falm_step_adjoint(falm_ctx *ctx, const falm_fields *f0, const fal
     double *pu = (double *)au, *puu = (double *)auu, *pnut = (double *)anut;
     if (ctx->sgs == FALM_SGS_SMAGORINSKY) {
         LAUNCH(FALM_K_OTHER, st, k_adj_zero_interior<<<grid, 256, 0, st>>>(g, w.anut0));
-        LAUNCH(FALM_K_OTHER, st, k_adj_sgs<<<grid, 256, 0, st>>>(g, mv, un, pnut, pu, ctx->Cs));
+        LAUNCH(FALM_K_OTHER, st, k_adj_sgs<T><<<grid, 256, 0, st>>>(g, mv, un, pnut, pu, ctx->Cs));
     }
     LAUNCH(FALM_K_OTHER, st, k_adj_ubc<<<dim3(64, 3), 256, 0, st>>>(g, ctx->bc_kind, pu, w.au0, ctx->m64.x[0], dt));
     LAUNCH(FALM_K_OTHER, st, k_adj_carry_edges<<<grid, 256, 0, st>>>(g, pu, w.au0, 3));
     LAUNCH(FALM_K_OTHER, st, k_adj_project<<<grid, 256, 0, st>>>(g, mv, pu, puu, w.aua, w.auu1, w.auu0, w.ap, dt));
     LAUNCH(FALM_K_OTHER, st, k_adj_pbc<<<dim3(64, 3), 256, 0, st>>>(g, ctx->bc_kind, w.ap));
     LAUNCH(FALM_K_OTHER, st, k_adj_zero_ghosts<<<grid, 256, 0, st>>>(g, w.ap));
-    // transposed Poisson solve, warm-started; a
-    // symmetric table operator is its own transpose, otherwise the transpose is
-    // built as an explicit 7-column matrix
+    // transposed Poisson solve, warm-started; a symmetric table operator is its
+    // own transpose, otherwise the transpose is built as an explicit FP64
+    // 7-column matrix
     const bool use_tables = !ctx->A_explicit && ctx->op_symmetric;
     if (!use_tables) LAUNCH(FALM_K_OTHER, st, k_adj_transpose_op<<<grid, 256, 0, st>>>(g, op7<double>(ctx), w.AT));
     // the right-hand side is normalised to unit norm (the solver's breakdown test
@@ -2261,10 +2294,7 @@ extern "C" int falm_step_adjoint(falm_ctx *ctx, const falm_fields *f0, const fal
         // relative residual ctx->adj_rel_tol (falm_adjoint_set_tol); by default 1e-5
         // (1e-12 when the context's tolerance is below 1e-12)
         const double rel = ctx->adj_rel_tol > 0 ? ctx->adj_rel_tol : (tol_saved < 1e-12 ? 1e-12 : 1e-5);
-        ctx->tol = rel / ((double)g.nx * g.ny * g.nz);
-        int it = 0, outer = 0;
-        double err = 0;
-        rc = solve_t<double>(ctx, w.arhs, w.ap, w.r, st, &it, &err, &outer);
+        rc = adj_transposed_solve<T>(ctx, w, rel, st);
         ctx->A_explicit = a_saved;
         ctx->tol = tol_saved;
         ctx->ls_type = ls_saved;
@@ -2276,17 +2306,33 @@ extern "C" int falm_step_adjoint(falm_ctx *ctx, const falm_fields *f0, const fal
     LAUNCH(FALM_K_OTHER, st, k_adj_utouu<<<grid, 256, 0, st>>>(g, mv, w.auu1, w.aua));
     LAUNCH(FALM_K_OTHER, st, k_adj_carry_ghosts<<<grid, 256, 0, st>>>(g, w.aua, w.au0));
     const double alpha = ctx->adv == FALM_ADV_UTOPIA ? 1. / 12. : (ctx->adv == FALM_ADV_KK ? 1. / 4. : 1. / 24.);
-    LAUNCH(FALM_K_OTHER, st, k_adj_pseudo_u<<<grid, 256, 0, st>>>(g, mv, (const double *)f0->u, (const double *)f0->uu,
-                                                                  (const double *)f0->nut, w.aua, w.au0, w.auu0, w.anut0, w.aff,
-                                                                  1.0 / ctx->Re, dt, alpha));
+    LAUNCH(FALM_K_OTHER, st, k_adj_pseudo_u<T><<<grid, 256, 0, st>>>(g, mv, (const T *)f0->u, (const T *)f0->uu, (const T *)f0->nut,
+                                                                     w.aua, w.au0, w.auu0, w.anut0, w.aff, 1.0 / ctx->Re, dt, alpha));
     if (ctx->alm_on) {
         const int apc = ctx->alm.apcount;
         LAUNCH(FALM_K_ALM, st, k_adj_alm_project<<<apc, 256, 0, st>>>(g, ctx->alm, ctx->m64.x[0], ctx->m64.x[1], ctx->m64.x[2], w.aff, w.aF));
-        LAUNCH(FALM_K_ALM, st, k_adj_alm_ap<<<(apc + 127) / 128, 128, 0, st>>>(g, ctx->alm, ctx->m64.x[0], ctx->m64.x[1], ctx->m64.x[2],
-                                                                              (const double *)f0->u, t, w.aF, w_power, w.au0, grad));
+        LAUNCH(FALM_K_ALM, st, k_adj_alm_ap<T><<<(apc + 127) / 128, 128, 0, st>>>(g, ctx->alm, ctx->m64.x[0], ctx->m64.x[1], ctx->m64.x[2],
+                                                                                 (const T *)f0->u, t, w.aF, w_power, w.au0, grad));
     }
     CK(cudaMemcpyAsync(pu, w.au0, 3 * nb, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(puu, w.auu0, 3 * nb, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(pnut, w.anut0, nb, cudaMemcpyDeviceToDevice, st));
     return FALM_OK;
+}
+
+}  // namespace
+
+extern "C" int falm_step_adjoint(falm_ctx *ctx, const falm_fields *f0, const falm_fields *f1, double dt, double t, double w_power,
+                                 void *au, void *auu, void *anut, double *grad, void *stream) {
+    if (!ctx || !f0 || !f0->u || !f0->uu || !f0->p || !f0->nut || !au || !auu || !anut || !grad || !(dt > 0)) return FALM_ERR_ARG;
+    if (ctx->slab_on && ctx->slab_nranks > 1) return fail(ctx, FALM_ERR_ARG, "step_adjoint: a grid of one slab only");
+    if (ctx->rmcp_on) return fail(ctx, FALM_ERR_ARG, "step_adjoint: the ALM forcing only (not the RMCP model)");
+    if (ctx->adv != FALM_ADV_UPWIND3 && ctx->adv != FALM_ADV_UTOPIA && ctx->adv != FALM_ADV_KK)
+        return fail(ctx, FALM_ERR_ARG, "step_adjoint: the 4th-order advection schemes (Upwind3, UTOPIA, KK) only");
+    if (ctx->sgs != FALM_SGS_EMPTY && ctx->sgs != FALM_SGS_SMAGORINSKY) return fail(ctx, FALM_ERR_ARG, "step_adjoint: Smagorinsky or no SGS model only");
+    cudaStream_t st = S(stream);
+    if (ctx->precision == FALM_FP64) return step_adjoint_t<double>(ctx, f0, f1, dt, t, w_power, au, auu, anut, grad, st);
+    if (ctx->A_explicit)
+        return fail(ctx, FALM_ERR_ARG, "step_adjoint: mixed precision needs the operator of falm_eq_poisson_operator (not a caller's matrix)");
+    return step_adjoint_t<float>(ctx, f0, f1, dt, t, w_power, au, auu, anut, grad, st);
 }

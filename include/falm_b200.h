@@ -248,14 +248,18 @@ int falm_io_read_cv_file(const char *path, int dims[4], double *x, double *hx, d
 int falm_mesh_build(const char *cvcenter, const char *meshpath, const char *outputfile, int gc);
 
 /* ---------------- discrete adjoint of the step ---------------------------------------------- */
-/* No reference counterpart.  Adjoint of falm_step for FP64 contexts (Upwind3/UTOPIA/KK advection,
-   Smagorinsky or no SGS, channel or cavity), with the Poisson solve treated as exact (its adjoint is
-   one solve with the transposed operator, started from an extrapolation of the previous calls', to a
-   relative residual of 1e-5, or 1e-12 when the context's tolerance is below 1e-12; see
-   falm_adjoint_set_tol).  f0: the DEVICE state
+/* No reference counterpart.  Adjoint of falm_step (Upwind3/UTOPIA/KK advection, Smagorinsky or no
+   SGS, channel or cavity, the ALM forcing, one slab), with the Poisson solve treated as exact (its
+   adjoint is one solve with the transposed operator, started from an extrapolation of the previous
+   calls', to a relative residual of 1e-5, or 1e-12 when the context's tolerance is below 1e-12; see
+   falm_adjoint_set_tol).  The adjoint fields and the gradient are FP64 in every context.  In a
+   FALM_MIXED context the states f0, f1 are the context's FP32 fields and the recomputed step is the
+   mixed-precision step, while the transposed solve runs in FP64 (on FP64 solver vectors of the
+   adjoint workspace); the operator must be falm_eq_poisson_operator's (FALM_ERR_ARG after
+   falm_eq_set_matrix).  f0: the DEVICE state
    (u, uu, p, nut; ff unused) at the start of the step, left unchanged; t: that step's time (as given
    to falm_step); w_power: the weight of this step's rotor power (sum over turbines of torque x tip
-   rate) in the objective.  au (3N), auu (3N), anut (N): DEVICE adjoint of the state after the step
+   rate) in the objective.  au (3N), auu (3N), anut (N): DEVICE FP64 adjoint of the state after the step
    on entry, of the state before it on return.  grad: DEVICE array of 1 + 2*apcount doubles
    (collective pitch [deg], per-AP chord, per-AP twist [deg]) to which the step's gradient
    contributions are added.  f1: the DEVICE state after the step (only its u is read), or NULL:

@@ -174,3 +174,79 @@ def test_adjoint_at_the_adjoint_configuration_size_matches_fd(lib_built):
         assert adj == pytest.approx(fd, rel=1e-4), (idx, adj, fd)
     A._set_params(sim, p0)
     sim.close()
+
+
+def test_mixed_precision_adjoint(lib_built):
+    """The adjoint in a mixed-precision context -- FP32 forward steps, states
+    and checkpoints; FP64 adjoint fields, gradient and transposed Poisson
+    solve -- on the adjoint configuration (128x64x64, rotor of radius 10
+    cells, seeded inflow), 20 steps from a spun-up state at the configuration's
+    Poisson tolerance 1e-8.
+      * The mixed adjoint along the mixed trajectory equals the FP64 context's
+        adjoint evaluated at the same (FP32) states, step by step, to 1e-6
+        relative (both transposed solves to relative residual 1e-9).
+      * Against the FP64 run from the same start (a trajectory that differs by
+        the mixed step's rounding and solver truncation): J within 1e-4, the
+        gradient within 1e-2 relative.
+      * Binomial checkpointing in the mixed context (3 stored states) gives the
+        periodic checkpointing's objective to 1e-12 and its gradient to 1e-9."""
+    import torch
+    case = cases.adjoint_case().with_inflow()
+    s64 = Simulation(case, "fp64")
+    for _ in range(10):
+        s64.step()
+    start, it0 = A._clone(s64), s64.it
+    s32 = Simulation(case, "mixed")
+
+    def to_start(sim):
+        for k in A.FIELDS:
+            getattr(sim, k).copy_(start[k].to(sim.u.dtype))
+        sim.it = it0
+
+    steps, apc, n, dt = 20, case.alm.apcount, case.grid.n, case.dt
+    # the mixed trajectory, every state kept
+    to_start(s32)
+    states = []
+    for _ in range(steps):
+        states.append(A._clone(s32))
+        s32.step()
+    states.append({"u": s32.u.clone()})
+
+    def reverse(ctx, dtype):
+        z = lambda m: torch.zeros(m, dtype=torch.float64, device=ctx.device)
+        au, auu, anut, grad = z(3 * n), z(3 * n), z(n), z(1 + 2 * apc)
+        for q in reversed(range(steps)):
+            S = {k: v.to(dtype) for k, v in states[q].items()}
+            ctx.step_adjoint(S["u"], S["uu"], S["p"], S["nut"], dt, (it0 + q + 1) * dt, 1.0 / steps, au, auu, anut, grad,
+                             u_after=states[q + 1]["u"].to(dtype))
+        return grad.cpu().numpy()
+
+    s32.ctx.adjoint_set_tol(1e-9)
+    s64.ctx.adjoint_set_tol(1e-9)
+    g32 = reverse(s32.ctx, torch.float32)
+    g64 = reverse(s64.ctx, torch.float64)
+    assert g32[0] == pytest.approx(g64[0], rel=1e-6)
+    for sl in (slice(1, 1 + apc), slice(1 + apc, None)):
+        assert np.linalg.norm(g32[sl] - g64[sl]) <= 1e-6 * np.linalg.norm(g64[sl]), \
+            np.linalg.norm(g32[sl] - g64[sl]) / np.linalg.norm(g64[sl])
+    # the drivers: FP64 and mixed from the same start; binomial in mixed (the
+    # transposed solves stay at 1e-9, so that their warm starts, which differ
+    # between the runs, do not show)
+    to_start(s64)
+    J64, gp64, gc64, gt64 = A.mean_power_gradient(s64, steps, checkpoint=steps)
+    to_start(s32)
+    J32, gp32, gc32, gt32 = A.mean_power_gradient(s32, steps, checkpoint=5)
+    assert J32 == pytest.approx(J64, rel=1e-4)
+    assert gp32 == pytest.approx(gp64, rel=1e-2)
+    for a, b in ((gc32, gc64), (gt32, gt64)):
+        assert np.linalg.norm(a - b) <= 1e-2 * np.linalg.norm(b), np.linalg.norm(a - b) / np.linalg.norm(b)
+    to_start(s32)
+    Jb, gpb, gcb, gtb = A.mean_power_gradient_binomial(s32, steps, snaps=3)
+    assert Jb == pytest.approx(J32, rel=1e-12)
+    assert gpb == pytest.approx(gp32, rel=1e-9)
+    np.testing.assert_allclose(gcb, gc32, rtol=1e-9, atol=1e-12 * np.abs(gc32).max())
+    np.testing.assert_allclose(gtb, gt32, rtol=1e-9, atol=1e-12 * np.abs(gt32).max())
+    print("mixed vs fp64 trajectory: J", J32 / J64 - 1, "pitch", gp32 / gp64 - 1,
+          "chord", np.linalg.norm(gc32 - gc64) / np.linalg.norm(gc64))
+    s64.close()
+    s32.close()
