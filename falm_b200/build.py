@@ -2,6 +2,7 @@
 
 Run as ``python -m falm_b200.build``; __graft_entry__.build() calls build().
 """
+import glob
 import os
 import subprocess
 import sys
@@ -9,8 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SOURCES = [os.path.join(HERE, "csrc", "falm_b200.cu")]
-HEADERS = [os.path.join(HERE, "csrc", f) for f in ("falm_internal.cuh", "common.cuh", "cfd.cuh", "poisson.cuh", "alm_bc.cuh",
-                                                 "tma.cuh", "stencil_tma.cuh", "poisson_tma.cuh", "plane3_tma.cuh", "sor_rb_tma.cuh", "adjoint.cuh", "pair.cuh")]
+HEADERS = sorted(glob.glob(os.path.join(HERE, "csrc", "*.cuh")))
 OUT = os.path.join(HERE, "libfalm_b200.so")
 NVCC_FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-shared"]
