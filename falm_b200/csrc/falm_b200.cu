@@ -18,6 +18,7 @@
 #include <map>
 #include <climits>
 #include <tuple>
+#include <functional>
 #include <condition_variable>
 #include <chrono>
 #include <dlfcn.h>
@@ -344,6 +345,47 @@ int sor_rb_launch(falm_ctx *ctx, cudaStream_t st, int H, const T *xin, const T *
     return sor_rb_launch_h<T, 3>(ctx, st, xin, b, xout, omega, c1, sc);
 }
 
+// the conditions of make_map for a context vector (256-byte aligned) of element size e
+bool map_ok(const falm_ctx *ctx, size_t e, int bx, int by) {
+    const Geom &g = ctx->geo;
+    return tma_encode_available() && ((g.sx * e) & 15) == 0 && g.sx >= bx && g.sy >= by && g.gc == 2;
+}
+
+// whether sor_rb_launch runs an H-half-sweep blocked pass on the context's vectors
+// (1) or declines (0), decided without a launch
+template <typename T>
+bool sor_pass_ok(const falm_ctx *ctx, int H) {
+    if (ctx->no_tma || ctx->A_explicit) return false;
+    const size_t e = sizeof(T);
+    if constexpr (sizeof(T) == 4) {
+        using L2 = RB2Tile<T>;
+        if (H == 3 && !ctx->sor_v1 && map_ok(ctx, e, L2::BX, L2::BY) && map_ok(ctx, e, L2::BXB, L2::BYB)) return true;
+    }
+    if (H == 1) return map_ok(ctx, e, RBTile<T, 1>::BX, RBTile<T, 1>::BY);
+    if (H == 2) return map_ok(ctx, e, RBTile<T, 2>::BX, RBTile<T, 2>::BY);
+    return map_ok(ctx, e, RBTile<T, 3>::BX, RBTile<T, 3>::BY);
+}
+
+// Whether the preconditioner's pointwise first sweep writes the work vector xp
+// rather than its target z: the sweeps after it that run out of place (Jacobi
+// sweeps 2..m; blocked SOR passes) alternate between xp and z, so an odd
+// number of them starts from xp and the last one lands in z.  The buffers of
+// an application are then the same at every iteration.
+template <typename T>
+bool pc_first_in_xp(const falm_ctx *ctx) {
+    const int m = ctx->pc_maxit;
+    if (ctx->pc_type == FALM_LS_JACOBI) return ((m - 1) & 1) != 0;
+    if (ctx->pc_type != FALM_LS_SOR) return false;
+    int passes = 0;
+    for (int hs = 1; hs < 2 * m;) {
+        const int H = std::min(3, 2 * m - hs);
+        if (!sor_pass_ok<T>(ctx, H)) break;
+        passes++;
+        hs += H;
+    }
+    return (passes & 1) != 0;
+}
+
 // ring depth of the multi-field plane stream: keep >= 2 planes in flight and
 // at least two CTAs per SM
 template <typename T, int NF> struct P3Conf { static constexpr int NS = NF > 1 ? 4 : 6; };
@@ -554,6 +596,110 @@ int plain_solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *i
     return ctx->scal_host->status == FALM_ERR_NAN ? fail(ctx, FALM_ERR_NAN, "solve: non-finite residual") : FALM_OK;
 }
 
+// ---------------------------------------------------------------- device-side BiCGStab loop
+// A pass's iterations as one CUDA graph: iterations 0 and 1 of the pass, then
+// a conditional while node whose body is one later iteration; the last kernel
+// of the prefix and of the body sets the loop condition from the solver's done
+// flag (convergence, maxit, breakdown or a non-finite scalar), so the loop ends
+// on the device within maxit iterations.  Graphs are kept per solve signature
+// (vectors, element type, whether the first preconditioner sweep is ready) and
+// dropped when the solver settings or the operator change.  Used where launch
+// and host-synchronisation latency dominate: grids of at most kGraphCells
+// interior cells (FALM_B200_GRAPH=1 / 0 forces it on / off), never while
+// profiling or checking launches one by one.
+constexpr long long kGraphCells = 1ll << 22;
+
+bool use_graph(const falm_ctx *ctx) {
+    if (ctx->profiling || ctx->check_sync || ctx->graph_mode == 0) return false;
+    return ctx->graph_mode == 1 || (long long)ctx->geo.nx * ctx->geo.ny * ctx->geo.nz <= kGraphCells;
+}
+
+__global__ void k_graph_continue(const SolverScalars *sc, cudaGraphConditionalHandle h) {
+    cudaGraphSetConditional(h, sc->done ? 0u : 1u);
+}
+
+void graphs_clear(falm_ctx *ctx) {
+    if (!ctx->graphs) return;
+    for (auto &e : *ctx->graphs) {
+        cudaGraphExecDestroy(e.exec);
+        cudaGraphDestroy(e.graph);
+    }
+    ctx->graphs->clear();
+}
+
+// the graph of a pass (built on first use: emit(itp) launches iteration itp's
+// kernels on `ist`, which points at the capture stream meanwhile); prefix and
+// per_iter: kernel launches of iterations 0-1 and of one later iteration
+int solve_graph(falm_ctx *ctx, const void *x, const void *b, const void *r, int esize, int pp_ready,
+                const std::function<int(int)> &emit, cudaStream_t &ist, cudaGraphExec_t *out, int *prefix, int *per_iter) {
+    for (auto &e : *ctx->graphs)
+        if (e.x == x && e.b == b && e.r == r && e.w0 == ctx->w_rr && e.A == ctx->A_explicit && e.esize == esize && e.pp_ready == pp_ready) {
+            *out = e.exec; *prefix = e.prefix; *per_iter = e.per_iter;
+            return FALM_OK;
+        }
+    if (!ctx->cap_stream) CK(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
+    cudaGraph_t gr = nullptr;
+    CK(cudaGraphCreate(&gr, 0));
+    cudaGraphConditionalHandle h;
+    cudaGraphExec_t ex = nullptr;
+    const cudaStream_t saved = ist;
+    ist = ctx->cap_stream;
+    // capture iterations first..last and the condition kernel into `into`
+    auto capture = [&](cudaGraph_t into, int first, int last, int *count) -> int {
+        if (cudaStreamBeginCaptureToGraph(ist, into, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+            return fail(ctx, FALM_ERR_CUDA, "solve graph: capture");
+        const long long l0 = ctx->launches;
+        int crc = FALM_OK;
+        for (int itp = first; itp <= last && !crc; itp++) crc = emit(itp);
+        if (!crc) {
+            k_graph_continue<<<1, 1, 0, ist>>>(ctx->scal, h);
+            if (cudaGetLastError() != cudaSuccess) crc = fail(ctx, FALM_ERR_CUDA, "solve graph: condition kernel");
+        }
+        *count = (int)(ctx->launches - l0);
+        ctx->launches = l0;
+        cudaGraph_t got = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(ist, &got);
+        if (!crc && (e != cudaSuccess || got != into)) crc = fail(ctx, FALM_ERR_CUDA, "solve graph: end of capture");
+        cudaGetLastError();
+        return crc;
+    };
+    int rc = FALM_OK, np = 0, nb = 0;
+    if (cudaGraphConditionalHandleCreate(&h, gr, 1, cudaGraphCondAssignDefault) != cudaSuccess) rc = fail(ctx, FALM_ERR_CUDA, "solve graph: handle");
+    if (!rc) rc = capture(gr, 0, 1, &np);
+    if (!rc) {
+        // the loop follows the prefix's last node(s)
+        size_t nn = 0, ne = 0;
+        cudaGraphGetNodes(gr, nullptr, &nn);
+        std::vector<cudaGraphNode_t> nodes(nn);
+        if (nn) cudaGraphGetNodes(gr, nodes.data(), &nn);
+        cudaGraphGetEdges(gr, nullptr, nullptr, &ne);
+        std::vector<cudaGraphNode_t> from(ne), to(ne);
+        if (ne) cudaGraphGetEdges(gr, from.data(), to.data(), &ne);
+        std::vector<cudaGraphNode_t> leaves;
+        for (auto nd : nodes)
+            if (std::find(from.begin(), from.end(), nd) == from.end()) leaves.push_back(nd);
+        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};   // every other byte zero
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cn;
+        if (cudaGraphAddNode(&cn, gr, leaves.data(), leaves.size(), &cp) != cudaSuccess) rc = fail(ctx, FALM_ERR_CUDA, "solve graph: loop node");
+        else rc = capture(cp.conditional.phGraph_out[0], 2, 2, &nb);
+    }
+    if (!rc && cudaGraphInstantiate(&ex, gr, 0) != cudaSuccess) rc = fail(ctx, FALM_ERR_CUDA, "solve graph: instantiate");
+    ist = saved;
+    cudaGetLastError();
+    if (rc) {
+        if (ex) cudaGraphExecDestroy(ex);
+        cudaGraphDestroy(gr);
+        return rc;
+    }
+    ctx->graphs->push_back(falm_ctx::SolveGraph{x, b, r, ctx->w_rr, ctx->A_explicit, esize, pp_ready, np, nb, gr, ex});
+    *out = ex; *prefix = np; *per_iter = nb;
+    return FALM_OK;
+}
+
 template <typename T>
 int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out, double *err_out, int *outer_out,
             bool first_res_done = false) {
@@ -583,23 +729,33 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
     int total_it = 0, outer = 0;
     const bool mixed = ctx->precision == FALM_MIXED;
     const int max_outer = mixed ? ctx->max_outer : 1;
-    // launch the remaining sweeps of one preconditioner application z ~ A^-1 v;
-    // the temporally blocked sweeps run out of place and swap z with xp
-    auto precondition_rest = [&](T *&z, const T *v) -> int {
+    // the stream of the iteration kernels: st, or the capture stream while a
+    // device-side loop (CUDA graph) is recorded
+    cudaStream_t ist = st;
+    const bool first_xp = pc_first_in_xp<T>(ctx);
+    auto first_target = [&](T *z) -> T * { return first_xp ? xp : z; };
+    // launch the remaining sweeps of one preconditioner application z ~ A^-1 v
+    // (the first, pointwise sweep wrote first_target(z)); the temporally blocked
+    // sweeps run out of place, alternating between xp and z
+    auto precondition_rest = [&](T *z, const T *v) -> int {
         if (pct == FALM_LS_SOR) {
             int hs = 1;
+            T *src = first_target(z);
             while (hs < 2 * m) {                       // up to 3 half sweeps per pass over HBM
                 const int H = std::min(3, 2 * m - hs);
-                const int r = sor_rb_launch<T>(ctx, st, H, z, v, xp, pcw, hs & 1, sc);
-                if (r < 0) return -r;
-                if (r == 0) break;
-                std::swap(z, xp);
+                T *dst = src == z ? xp : z;
+                const int lr = sor_rb_launch<T>(ctx, ist, H, src, v, dst, pcw, hs & 1, sc);
+                if (lr < 0) return -lr;
+                if (lr == 0) break;
+                src = dst;
                 hs += H;
             }
+            // a pass declined after all (pc_first_in_xp checks the same conditions)
+            if (src != z) CK(cudaMemcpyAsync(z, src, (size_t)g.n * sizeof(T), cudaMemcpyDeviceToDevice, ist));
             for (; hs < 2 * m; hs++) {                // red, then (black, red) x (m-1)
                 const int color = hs & 1;
-                S7_OR(FALM_K_SOR, st, T, 0, z, (SorBody<T>{op, z, v, pcw, color, sc}),
-                      (k_sor<T><<<grid, kRowThreads, 0, st>>>(g, R, op, z, v, pcw, color, sc)));
+                S7_OR(FALM_K_SOR, ist, T, 0, z, (SorBody<T>{op, z, v, pcw, color, sc}),
+                      (k_sor<T><<<grid, kRowThreads, 0, ist>>>(g, R, op, z, v, pcw, color, sc)));
             }
         } else if (pct == FALM_LS_JACOBI) {
             // sweeps 2..m ping-pong between xp and z; the first sweep wrote to
@@ -607,12 +763,11 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
             T *bufs[2] = {z, xp};
             for (int it = 2; it <= m; it++) {
                 T *dst = bufs[(m - it) & 1], *src = bufs[(m - it + 1) & 1];
-                LAUNCH(FALM_K_SOR, st, k_jacobi<T><<<grid, kRowThreads, 0, st>>>(g, R, op, dst, src, v, sc));
+                LAUNCH(FALM_K_SOR, ist, k_jacobi<T><<<grid, kRowThreads, 0, ist>>>(g, R, op, dst, src, v, sc));
             }
         }
         return FALM_OK;
     };
-    auto first_target = [&](T *z) -> T * { return (pct == FALM_LS_JACOBI && ((m - 1) & 1)) ? xp : z; };
     // a pass's residual also gives the first iteration's first preconditioner
     // sweep (pp_ready: the stream kernel stored it, so k_bicg_p is skipped)
     bool pp_ready = first_res_done;
@@ -642,7 +797,12 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
     // the stream kernel is not available it runs at the start of the next pass.
     // A pass stores its residual in rr only: r equals rr until the pass's first
     // k_bicg_xr, which writes r, and the iteration reads rr before.
-    bool explicit_check = false, pass_queued = first_res_done;
+    // a device-side loop (CUDA graph) runs a pass's iterations without host
+    // checks in between; the FP64 check of a mixed-precision pass then follows
+    // it as a kernel of its own
+    const bool graph = use_graph(ctx);
+    bool explicit_check = graph, pass_queued = first_res_done;
+    int passes = 0;   // passes run (a pass whose success an explicit check finds ends the loop at the next outer step)
     for (outer = 0; outer < max_outer; outer++) {
         if (outer > 0 && explicit_check) {
             if ((rc = res_pass(1))) return rc;
@@ -657,26 +817,42 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
         pass_queued = false;
         const bool want_check = mixed && outer + 1 < max_outer && !explicit_check;
         bool checked = false;
-        // iteration itp of the pass: r equals rr until the first k_bicg_xr, and
-        // the first iteration's p equals r, so it reads rr in their place.
-        // Iterations are queued in batches of 1, 2, 4, 8, 8, ... between host
-        // checks of the convergence flag; every kernel of an iteration queued
-        // after convergence returns at once.
-        int batch = 1, queued = 0;
-        for (int itp = 0;; itp++) {
+        // the kernels of iteration itp of the pass (2 stands for every later
+        // one): r equals rr until the first k_bicg_xr, and the first
+        // iteration's p equals r, so it reads rr in their place
+        auto emit_iter = [&](int itp) -> int {
             const T *rin = itp == 0 ? rr : r;
             T *pout = itp == 0 ? nullptr : p;
             const T *pin = itp == 1 ? rr : p, *pv = itp == 0 ? rr : p;
+            int erc;
             if (!(itp == 0 && pp_ready))
-                LAUNCH(FALM_K_BICG_P, st, k_bicg_p<T><<<grid_p, kRowThreads, 0, st>>>(g, R, op, pout, pin, q, rin, first_target(pp), pct, pcw, sc));
-            if ((rc = precondition_rest(pp, pv))) return rc;
-            S7_OR(FALM_K_MV_DOT1, st, T, 1, pp, (MvDot1Body<T>{op, q, rr, sc}),
-                  (k_mv_dot1<T><<<grid, kRowThreads, 0, st>>>(g, R, op, pp, q, rr, ctx->red, sc)));
-            LAUNCH(FALM_K_BICG_S, st, k_bicg_s<T><<<grid_s, kRowThreads, 0, st>>>(g, R, op, s, q, rin, first_target(ss), pct, pcw, sc));
-            if ((rc = precondition_rest(ss, s))) return rc;
-            S7_OR(FALM_K_MV_DOT2, st, T, 2, ss, (MvDot2Body<T>{op, t, s, sc}),
-                  (k_mv_dot2<T><<<grid, kRowThreads, 0, st>>>(g, R, op, ss, t, s, ctx->red, sc)));
-            LAUNCH(FALM_K_BICG_XR, st, k_bicg_xr<T><<<grid_xr, kRowThreads, 0, st>>>(g, R, x, pp, ss, r, s, t, rr, ctx->red, sc));
+                LAUNCH(FALM_K_BICG_P, ist, k_bicg_p<T><<<grid_p, kRowThreads, 0, ist>>>(g, R, op, pout, pin, q, rin, first_target(pp), pct, pcw, sc));
+            if ((erc = precondition_rest(pp, pv))) return erc;
+            S7_OR(FALM_K_MV_DOT1, ist, T, 1, pp, (MvDot1Body<T>{op, q, rr, sc}),
+                  (k_mv_dot1<T><<<grid, kRowThreads, 0, ist>>>(g, R, op, pp, q, rr, ctx->red, sc)));
+            LAUNCH(FALM_K_BICG_S, ist, k_bicg_s<T><<<grid_s, kRowThreads, 0, ist>>>(g, R, op, s, q, rin, first_target(ss), pct, pcw, sc));
+            if ((erc = precondition_rest(ss, s))) return erc;
+            S7_OR(FALM_K_MV_DOT2, ist, T, 2, ss, (MvDot2Body<T>{op, t, s, sc}),
+                  (k_mv_dot2<T><<<grid, kRowThreads, 0, ist>>>(g, R, op, ss, t, s, ctx->red, sc)));
+            LAUNCH(FALM_K_BICG_XR, ist, k_bicg_xr<T><<<grid_xr, kRowThreads, 0, ist>>>(g, R, x, pp, ss, r, s, t, rr, ctx->red, sc));
+            return FALM_OK;
+        };
+        if (graph) {
+            // the whole pass on the device: one graph launch, one host read
+            cudaGraphExec_t ge = nullptr;
+            int prefix = 0, per_iter = 0;
+            if ((rc = solve_graph(ctx, x, b, r, (int)sizeof(T), pp_ready ? 1 : 0, emit_iter, ist, &ge, &prefix, &per_iter))) return rc;
+            CK(cudaGraphLaunch(ge, st));
+            CK(cudaMemcpyAsync(ctx->scal_host, sc, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            ctx->launches += prefix + (long long)per_iter * std::max(0, ctx->scal_host->it - 2);
+        }
+        // otherwise iterations are queued in batches of 1, 2, 4, 8, 8, ... between
+        // host checks of the convergence flag; every kernel of an iteration
+        // queued after convergence returns at once
+        int batch = 1, queued = 0;
+        for (int itp = 0; !graph; itp++) {
+            if ((rc = emit_iter(itp))) return rc;
             if (++queued < batch) continue;
             if (want_check && !explicit_check) {
                 ResBody<T, true> cb{op, b, nullptr, nullptr, sc, 1};
@@ -693,6 +869,7 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
             batch = std::min(2 * batch, 8);
         }
         total_it += ctx->scal_host->it;
+        passes++;
         if (ctx->scal_host->status == FALM_ERR_NAN) break;
         if (checked) {
             if (ctx->scal_host->done) break;   // the true residual meets the tolerance
@@ -710,7 +887,7 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
     }
     if (it_out) *it_out = total_it;
     if (err_out) *err_out = ctx->scal_host->err;
-    if (outer_out) *outer_out = std::min(outer + 1, max_outer);
+    if (outer_out) *outer_out = std::max(1, passes);
     return ctx->scal_host->status == FALM_ERR_NAN ? fail(ctx, FALM_ERR_NAN, "solve: non-finite scalar") : FALM_OK;
 }
 
@@ -889,7 +1066,7 @@ int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_
         fused_res = false;
         if (!ctx->A_explicit && ctx->ls_type == FALM_LS_PBICGSTAB && (ctx->pc_type == FALM_LS_SOR || ctx->pc_type == FALM_LS_JACOBI)) {
             if ((rc = ensure_work(ctx)) || (rc = solver_init(ctx, st))) return rc;
-            T *ppt = (ctx->pc_type == FALM_LS_JACOBI && ((ctx->pc_maxit - 1) & 1)) ? (T *)ctx->w_xp : (T *)ctx->w_pp;
+            T *ppt = pc_first_in_xp<T>(ctx) ? (T *)ctx->w_xp : (T *)ctx->w_pp;
             const void *const fp[2] = {ua, p};
             const int nc[2] = {3, 1};
             int s3;
@@ -999,6 +1176,11 @@ int falm_create(const falm_grid *grid, int precision, falm_ctx **out) {
     falm_ctx *ctx = new falm_ctx();
     memset((void *)ctx, 0, sizeof(*ctx));
     ctx->last_error = new std::string();
+    ctx->graphs = new std::vector<falm_ctx::SolveGraph>();
+    {
+        const char *gm = getenv("FALM_B200_GRAPH");
+        ctx->graph_mode = (gm && gm[0] == '0') ? 0 : ((gm && gm[0] == '1') ? 1 : -1);
+    }
     ctx->precision = precision;
     ctx->esize = precision == FALM_FP64 ? sizeof(double) : sizeof(float);
     Geom &g = ctx->geo;
@@ -1077,6 +1259,9 @@ int falm_create(const falm_grid *grid, int precision, falm_ctx **out) {
 int falm_destroy(falm_ctx *ctx) {
     if (!ctx) return FALM_ERR_ARG;
     delete ctx->io;   // writes the queued snapshots, then stops its thread
+    graphs_clear(ctx);
+    delete ctx->graphs;
+    if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
     cudaFree(ctx->metric_mem);
     cudaFree(ctx->op_mem);
     cudaFree(ctx->work_mem);
@@ -1204,11 +1389,13 @@ int falm_eq_init(falm_ctx *ctx, int type, int maxit, double tol, double relax, i
     if (pc_maxit < 1) return FALM_ERR_ARG;
     ctx->ls_type = type; ctx->maxit = maxit; ctx->tol = tol; ctx->relax = relax;
     ctx->pc_type = pc_type; ctx->pc_maxit = pc_maxit; ctx->pc_relax = pc_relax;
+    graphs_clear(ctx);   // the preconditioner settings are kernel arguments of the recorded loops
     return FALM_OK;
 }
 
 int falm_eq_poisson_operator(falm_ctx *ctx, int bc_kind, double *maxdiag_out) {
     if (!ctx || (bc_kind != FALM_BC_CHANNEL && bc_kind != FALM_BC_CAVITY)) return FALM_ERR_ARG;
+    graphs_clear(ctx);
     int rc = build_poisson(ctx, bc_kind);
     if (rc) return rc;
     if (maxdiag_out) *maxdiag_out = ctx->maxdiag;
@@ -1217,6 +1404,7 @@ int falm_eq_poisson_operator(falm_ctx *ctx, int bc_kind, double *maxdiag_out) {
 
 int falm_eq_set_matrix(falm_ctx *ctx, const void *A) {
     if (!ctx) return FALM_ERR_ARG;
+    graphs_clear(ctx);
     ctx->A_explicit = A;
     return FALM_OK;
 }

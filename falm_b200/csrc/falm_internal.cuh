@@ -185,4 +185,14 @@ struct falm_ctx {
     falm_transport transport;               // halo exchange and reductions between the slabs
     std::string *last_error;
     fb::IoWriter *io;                       // snapshot writer (falm_io.cuh), created on first use
+    // device-side BiCGStab loops (CUDA graphs), one per solve signature
+    struct SolveGraph {
+        const void *x, *b, *r, *w0, *A;
+        int esize, pp_ready, prefix, per_iter;
+        cudaGraph_t graph;
+        cudaGraphExec_t exec;
+    };
+    std::vector<SolveGraph> *graphs;
+    int graph_mode;                         // -1 small grids, 0 never, 1 always (FALM_B200_GRAPH)
+    cudaStream_t cap_stream;                // stream the graphs are captured on
 };

@@ -205,6 +205,28 @@ def test_step_launch_count_and_statuses(lib_built):
         assert np.isfinite(s["divnorm"])
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("name", ["channel", "cavity"])
+def test_device_loop_equals_host_loop(lib_built, monkeypatch, precision, name):
+    """The BiCGStab iterations of a pass as one CUDA graph with a conditional
+    while node (FALM_B200_GRAPH=1; the default on grids of up to 2^22 cells)
+    run the same kernels in the same order as the host loop that queues them
+    in batches between reads of the convergence flag (FALM_B200_GRAPH=0): the
+    same iteration counts and bitwise the same fields, in convergence mode
+    (where the loop's exit matters) and in fixed-iteration mode."""
+    case = small_cases()[name]
+    for maxit, tol in ((None, None), (6, 0.0)):
+        outs = []
+        for mode in ("0", "1"):
+            monkeypatch.setenv("FALM_B200_GRAPH", mode)
+            got, st, ctx = run_gpu(case, 4, precision=precision, maxit=maxit, tol=tol)
+            ctx.close()
+            outs.append((got, [x["it"] for x in st], [x["outer"] for x in st]))
+        assert outs[0][1] == outs[1][1] and outs[0][2] == outs[1][2], (outs[0][1:], outs[1][1:])
+        for k in outs[0][0]:
+            assert np.array_equal(outs[0][0][k], outs[1][0][k]), k
+
+
 @pytest.mark.parametrize("shape", [(40, 20, 72), (72, 20, 40)])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_step_tma_matches_row_kernels_multichunk(lib_built, monkeypatch, precision, shape):
