@@ -299,7 +299,8 @@ int slab_derive(falm_ctx *ctx, int n, int stage, cudaStream_t st) {
     return FALM_OK;
 }
 
-// The BiCGStab solve of a slab (src/FalmEq.cpp:305-410) on the row kernels:
+// The BiCGStab solve of a slab (src/FalmEq.cpp:305-410) on the 7-point plane
+// streams (row kernels where a grid is not streamable):
 // every reduction kernel leaves its slab's totals in red[] (SolverScalars::
 // defer), the totals are summed over the slabs and k_slab_derive derives the
 // scalars; each preconditioner half sweep after the first (pointwise, from
@@ -333,7 +334,8 @@ int slab_solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it
             for (int hs = 1; hs < 2 * m; hs++) {            // red, then (black, red) x (m - 1)
                 int rc2 = slab_halo<T>(ctx, z, 1, 1, st);
                 if (rc2) return rc2;
-                LAUNCH(FALM_K_SOR, st, k_sor<T><<<grid, kRowThreads, 0, st>>>(g, R, op, z, v, pcw, hs & 1, sc));
+                S7_OR(FALM_K_SOR, st, T, 0, z, (SorBody<T>{op, z, v, pcw, hs & 1, sc}),
+                      (k_sor<T><<<grid, kRowThreads, 0, st>>>(g, R, op, z, v, pcw, hs & 1, sc)));
             }
         } else if (pct == FALM_LS_JACOBI) {
             // the first sweep wrote to the buffer that makes the last one land in z
@@ -364,12 +366,14 @@ int slab_solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it
             LAUNCH(FALM_K_BICG_P, st, k_bicg_p<T><<<grid, kRowThreads, 0, st>>>(g, R, op, p, p, q, r, first_target(pp), pct, pcw, sc));
             if ((rc = precondition_rest(pp, p))) return rc;
             if ((rc = slab_halo<T>(ctx, pp, 1, 1, st))) return rc;
-            LAUNCH(FALM_K_MV_DOT1, st, k_mv_dot1<T><<<grid, kRowThreads, 0, st>>>(g, R, op, pp, q, rr, ctx->red, sc));
+            S7_OR(FALM_K_MV_DOT1, st, T, 1, pp, (MvDot1Body<T>{op, q, rr, sc}),
+                  (k_mv_dot1<T><<<grid, kRowThreads, 0, st>>>(g, R, op, pp, q, rr, ctx->red, sc)));
             if ((rc = slab_derive(ctx, 1, 2, st))) return rc;
             LAUNCH(FALM_K_BICG_S, st, k_bicg_s<T><<<grid, kRowThreads, 0, st>>>(g, R, op, s, q, r, first_target(ss), pct, pcw, sc));
             if ((rc = precondition_rest(ss, s))) return rc;
             if ((rc = slab_halo<T>(ctx, ss, 1, 1, st))) return rc;
-            LAUNCH(FALM_K_MV_DOT2, st, k_mv_dot2<T><<<grid, kRowThreads, 0, st>>>(g, R, op, ss, t, s, ctx->red, sc));
+            S7_OR(FALM_K_MV_DOT2, st, T, 2, ss, (MvDot2Body<T>{op, t, s, sc}),
+                  (k_mv_dot2<T><<<grid, kRowThreads, 0, st>>>(g, R, op, ss, t, s, ctx->red, sc)));
             if ((rc = slab_derive(ctx, 2, 3, st))) return rc;
             LAUNCH(FALM_K_BICG_XR, st, k_bicg_xr<T><<<grid, kRowThreads, 0, st>>>(g, R, x, pp, ss, r, s, t, rr, ctx->red, sc));
             if ((rc = slab_derive(ctx, 2, 4, st))) return rc;
