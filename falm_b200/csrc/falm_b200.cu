@@ -9,6 +9,7 @@
 #include <fstream>
 #include <string>
 #include <cstring>
+#include <cstddef>
 #include <cstdio>
 #include <cmath>
 #include <algorithm>
@@ -608,6 +609,7 @@ int plain_solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *i
 // interior cells (FALM_B200_GRAPH=1 / 0 forces it on / off), never while
 // profiling or checking launches one by one.
 constexpr long long kGraphCells = 1ll << 22;
+constexpr int kMixedPassIts = 50;   // FP32 BiCGStab iterations between FP64 true-residual checks
 
 bool use_graph(const falm_ctx *ctx) {
     if (ctx->profiling || ctx->check_sync || ctx->graph_mode == 0) return false;
@@ -728,7 +730,13 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
     SolverScalars *sc = ctx->scal;
     int total_it = 0, outer = 0;
     const bool mixed = ctx->precision == FALM_MIXED;
-    const int max_outer = mixed ? ctx->max_outer : 1;
+    // Mixed precision: a pass runs at most kMixedPassIts FP32 iterations before
+    // the FP64 true residual replaces the recursive one (a check, then a new
+    // pass from it), and as many passes as maxit needs: over longer FP32
+    // recursions BiCGStab diverged on the nearly singular operator of a long
+    // channel (unit-norm right-hand sides at 512x128x128).
+    const int pass_its = mixed ? std::min(ctx->maxit, kMixedPassIts) : ctx->maxit;
+    const int max_outer = mixed ? std::max(ctx->max_outer, (ctx->maxit + kMixedPassIts - 1) / kMixedPassIts) : 1;
     // the stream of the iteration kernels: st, or the capture stream while a
     // device-side loop (CUDA graph) is recorded
     cudaStream_t ist = st;
@@ -785,11 +793,15 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
         pp_ready = !check && s7 == 1;
         return FALM_OK;
     };
+    // a new pass: iteration count zero, the pass's iteration limit
+    static_assert(offsetof(SolverScalars, maxit) == offsetof(SolverScalars, it) + sizeof(int), "it, maxit adjacent");
     auto zero_it = [&]() -> int {
-        static const int zero = 0;
-        CK(cudaMemcpyAsync(&sc->it, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
+        const int itmax[2] = {0, pass_its};   // SolverScalars::it, ::maxit
+        CK(cudaMemcpyAsync(&sc->it, itmax, sizeof(itmax), cudaMemcpyHostToDevice, st));
         return FALM_OK;
     };
+    if (mixed && pass_its != ctx->maxit)
+        CK(cudaMemcpyAsync(&sc->maxit, &pass_its, sizeof(int), cudaMemcpyHostToDevice, st));
     // In mixed precision each pass but the last is followed by a check of the
     // true residual in FP64 (stop when it meets the tolerance; the check stores
     // nothing). The check is queued behind the pass's iterations and runs only
@@ -803,8 +815,10 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
     const bool graph = use_graph(ctx);
     bool explicit_check = graph, pass_queued = first_res_done;
     int passes = 0;   // passes run (a pass whose success an explicit check finds ends the loop at the next outer step)
+    bool restart_check = false;   // the previous pass broke down: check the true residual before restarting
     for (outer = 0; outer < max_outer; outer++) {
-        if (outer > 0 && explicit_check) {
+        if (outer > 0 && (explicit_check || restart_check)) {
+            restart_check = false;
             if ((rc = res_pass(1))) return rc;
             CK(cudaMemcpyAsync(ctx->scal_host, sc, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
@@ -870,7 +884,17 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
         }
         total_it += ctx->scal_host->it;
         passes++;
-        if (ctx->scal_host->status == FALM_ERR_NAN) break;
+        if (ctx->scal_host->status == FALM_ERR_NAN) {
+            // In mixed precision a non-finite alpha or omega of the FP32
+            // recursion (a breakdown: the kernels after it skipped, so x is the
+            // last iterate) restarts a pass from the FP64 true residual while
+            // passes remain; non-finite data ends the solve.
+            if (!mixed || outer + 1 >= max_outer) break;
+            static const int ok = FALM_OK;
+            CK(cudaMemcpyAsync(&sc->status, &ok, sizeof(int), cudaMemcpyHostToDevice, st));
+            restart_check = true;
+            continue;
+        }
         if (checked) {
             if (ctx->scal_host->done) break;   // the true residual meets the tolerance
             if ((rc = res_pass(0))) return rc;
