@@ -456,3 +456,38 @@ def test_alm_pitch_motion(oracle, lib_built):
     tq, th = ctx.alm_run(dev(ctx, st["u"]), None, 2.5)
     np.testing.assert_allclose(tq, out["torque"], rtol=1e-12)
     np.testing.assert_allclose(th, out["thrust"], rtol=1e-12)
+
+
+def test_mixed_solve_long_channel_stays_finite(lib_built):
+    """The mixed-precision PBiCGStab on the nearly singular operator of a long
+    channel (512x128x128, one Dirichlet face) with a smooth unit-norm
+    right-hand side, which FP64 solves in about 240 iterations to a relative
+    residual of 1e-2: FP32 recursions of that length diverge, so the solve
+    replaces the recursive residual by the FP64 true one every 50 iterations.
+    It must end with finite iterates and meet the relative residual 1e-2 within
+    maxit 1000, and a relative residual of 1e-5, below what an FP32 iterate
+    of this smooth solution can hold, must end at maxit (status 5) with finite
+    iterates instead of non-finite scalars."""
+    from falm_b200.api import _ptr
+    case = cases.channel(512, 128, 128, cells_per_radius=20, tol=1e-6)
+    g = case.grid
+    ctx = make_ctx(case, "mixed")
+    N = g.interior[0] * g.interior[1] * g.interior[2]
+    z, y, x = np.meshgrid(np.arange(g.sz), np.arange(g.sy), np.arange(g.sx), indexing="ij")
+    b = np.exp(-(((x - 64) / 6.0) ** 2 + ((y - g.sy / 2) / 6.0) ** 2 + ((z - g.sz / 2) / 6.0) ** 2))
+    gc = g.gc
+    b[:gc] = b[-gc:] = 0
+    b[:, :gc] = b[:, -gc:] = 0
+    b[:, :, :gc] = b[:, :, -gc:] = 0
+    b /= np.linalg.norm(b)
+    bt = dev(ctx, b.reshape(-1))
+    for rel, want in ((1e-2, (0,)), (1e-5, (5,))):
+        ctx.eq_init(1000, rel / N, case.pc, case.pc_maxit, case.pc_relax)
+        xt, r = ctx.field(1), ctx.field(1)
+        it, err = ctypes.c_int(), ctypes.c_double()
+        rc = ctx.lib.falm_eq_solve(ctx.h, _ptr(xt), _ptr(bt), _ptr(r), ctx.stream(), ctypes.byref(it), ctypes.byref(err))
+        assert rc in want, (rel, rc, it.value, err.value * N)
+        assert np.isfinite(host(xt)).all() and np.isfinite(err.value)
+        if rc == 0:
+            assert err.value * N <= rel
+    ctx.close()
