@@ -111,6 +111,8 @@ SIGNATURES = {
     "falm_bc_set_inlet_plane": [V, c_double_p, P],
     "falm_tavg": [V, P, P, I, LL, P],
     "falm_io_write_vector_file": [V, ctypes.c_char_p, ctypes.POINTER(P), c_int_p, I, ctypes.c_ulonglong, D, I, P],
+    "falm_io_read_vector_file": [V, ctypes.c_char_p, ctypes.POINTER(P), c_int_p, I, ctypes.POINTER(ctypes.c_ulonglong),
+                                 ctypes.POINTER(D), P],
     "falm_io_wait": [V],
     "falm_io_write_index_file": [ctypes.c_char_p, I, I, I, I, ctypes.POINTER(ctypes.c_ulonglong), c_double_p, c_int_p, I, I],
     "falm_io_write_cv_file": [V, ctypes.c_char_p],

@@ -281,6 +281,16 @@ class Context:
                                                        float(time), 1 if as_fp64 else 0, self.stream()),
                     "write_vector_file")
 
+    def read_vector_file(self, path, fields):
+        """the inverse of write_vector_file: the file's columns into `fields` (device
+        tensors, in order); returns (step, time) of its header"""
+        ptrs = (L.P * len(fields))(*[f.data_ptr() for f in fields])
+        ncols = (ctypes.c_int * len(fields))(*[f.numel() // self.grid.n for f in fields])
+        step, time = ctypes.c_ulonglong(), ctypes.c_double()
+        self._check(self.lib.falm_io_read_vector_file(self.h, str(path).encode(), ptrs, ncols, len(fields), ctypes.byref(step),
+                                                      ctypes.byref(time), self.stream()), "read_vector_file")
+        return step.value, time.value
+
     def io_wait(self):
         """wait for every queued snapshot file"""
         self._check(self.lib.falm_io_wait(self.h), "io_wait")

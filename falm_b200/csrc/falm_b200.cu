@@ -1626,6 +1626,59 @@ int falm_io_write_vector_file(falm_ctx *ctx, const char *path, const void *const
     return FALM_OK;
 }
 
+int falm_io_read_vector_file(falm_ctx *ctx, const char *path, void *const *fields, const int *ncols, int nfields,
+                             unsigned long long *step_out, double *time_out, void *stream) {
+    if (!ctx || !path || !fields || !ncols || nfields < 1) return FALM_ERR_ARG;
+    long long cols = 0;
+    for (int q = 0; q < nfields; q++) {
+        if (!fields[q] || ncols[q] < 1) return FALM_ERR_ARG;
+        cols += ncols[q];
+    }
+    const Geom &g = ctx->geo;
+    const size_t n = (size_t)g.n, es = ctx->esize;
+    FILE *f = fopen(path, "rb");
+    if (!f) return fail(ctx, FALM_ERR_ARG, (std::string("io: cannot open ") + path).c_str());
+    uint64_t head[6] = {0, 0, 0, 0, 0, 0}, dsize = 0;
+    double time = 0;
+    bool ok = fread(head, sizeof(uint64_t), 6, f) == 6 && fread(&time, sizeof(double), 1, f) == 1 &&
+              fread(&dsize, sizeof(uint64_t), 1, f) == 1;
+    if (!ok) { fclose(f); return fail(ctx, FALM_ERR_ARG, "io: truncated header"); }
+    if (head[0] != (uint64_t)g.sx || head[1] != (uint64_t)g.sy || head[2] != (uint64_t)g.sz || head[3] != (uint64_t)cols ||
+        head[4] != (uint64_t)g.gc || (dsize != 4 && dsize != 8)) {
+        fclose(f);
+        return fail(ctx, FALM_ERR_ARG, "io: the file's grid, column count or value size does not match");
+    }
+    const size_t count = (size_t)cols * n;
+    std::vector<unsigned char> raw(count * dsize);
+    ok = fread(raw.data(), 1, raw.size(), f) == raw.size();
+    const bool extra = ok && fgetc(f) != EOF;
+    fclose(f);
+    if (!ok) return fail(ctx, FALM_ERR_ARG, "io: truncated data");
+    if (extra) return fail(ctx, FALM_ERR_ARG, "io: data beyond the columns the header announces");
+    // to the context's precision on the host (FP64 -> FP32 rounds to nearest)
+    std::vector<unsigned char> conv;
+    const unsigned char *src = raw.data();
+    if (dsize != es) {
+        conv.resize(count * es);
+        if (es == sizeof(float))
+            for (size_t q = 0; q < count; q++) ((float *)conv.data())[q] = (float)((const double *)raw.data())[q];
+        else
+            for (size_t q = 0; q < count; q++) ((double *)conv.data())[q] = (double)((const float *)raw.data())[q];
+        src = conv.data();
+    }
+    cudaStream_t st = S(stream);
+    size_t off = 0;
+    for (int q = 0; q < nfields; q++) {
+        const size_t len = (size_t)ncols[q] * n;
+        CK(cudaMemcpyAsync(fields[q], src + off * es, len * es, cudaMemcpyHostToDevice, st));
+        off += len;
+    }
+    CK(cudaStreamSynchronize(st));   // the host buffers go out of scope
+    if (step_out) *step_out = head[5];
+    if (time_out) *time_out = time;
+    return FALM_OK;
+}
+
 int falm_io_wait(falm_ctx *ctx) {
     if (!ctx) return FALM_ERR_ARG;
     if (!ctx->io) return FALM_OK;

@@ -34,6 +34,19 @@ class Simulation:
     def t(self):
         return self.it * self.case.dt
 
+    def save_state(self, path):
+        """a restart file of the step state (u, uu, p, nut: the snapshot format of
+        FalmIO::writeVectorFile with the step index and time in its header),
+        written before this returns"""
+        self.ctx.write_vector_file(path, [self.u, self.uu, self.p, self.nut], self.it, self.t())
+        self.ctx.io_wait()
+
+    def load_state(self, path):
+        """resume from a restart file of save_state (the same case and grid): the
+        following steps continue the saved run exactly"""
+        step, _ = self.ctx.read_vector_file(path, [self.u, self.uu, self.p, self.nut])
+        self.it = int(step)
+
     def step(self):
         """one main_loop iteration (then TAvg and outputUVWP, app/nedo/main.cpp:199-200,
         when output is enabled); returns the step statistics"""

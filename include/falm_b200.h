@@ -228,6 +228,15 @@ int falm_tavg(falm_ctx *ctx, void *avg, const void *f, int ncol, long long count
    file and returns the first write error since its last call. */
 int falm_io_write_vector_file(falm_ctx *ctx, const char *path, const void *const *fields, const int *ncols, int nfields,
                               unsigned long long step, double time, int as_fp64, void *stream);
+/* No reference counterpart (the reference writes these files and never reads them back): the
+   inverse of falm_io_write_vector_file, for restarting a run from a snapshot.  Reads `path` into
+   the DEVICE fields (ncols[q] columns each, in the file's column order), converting FP64 <-> FP32
+   to the context's precision; the file's grid (sx, sy, sz, gc) and column count must be the
+   context's.  step_out / time_out (optional) receive the header's step and time.  A truncated
+   file, a mismatched header or data beyond the announced columns return FALM_ERR_ARG and leave
+   the fields unchanged.  Synchronous. */
+int falm_io_read_vector_file(falm_ctx *ctx, const char *path, void *const *fields, const int *ncols, int nfields,
+                             unsigned long long *step_out, double *time_out, void *stream);
 int falm_io_wait(falm_ctx *ctx);
 /* FalmIO::writeIndexFile (src/FalmIO.h:25-67) for one rank: nlohmann::json's dump(2) of
    {dataType, global, guidePoint, outputSteps[{step, time, timeAvg}], ranks, variables}, byte for

@@ -388,3 +388,75 @@ def test_bounded_wait_gives_up_and_context_recovers(oracle, lib_built, precision
         for a, b in zip(gs, rs):
             assert a["torque"][0] == pytest.approx(b["torque"][0], rel=5e-3)
     ctx.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_restart_from_saved_state(lib_built, tmp_path, precision):
+    """Checkpoint/resume: the step state saved after 3 steps (the snapshot
+    format, falm_io_write_vector_file) and read back into a new simulation
+    (falm_io_read_vector_file) continues the run exactly -- 3 + 2 steps equal 5
+    uninterrupted steps bit for bit; a truncated or mismatched file is refused
+    with FALM_ERR_ARG and leaves the fields unchanged."""
+    from falm_b200 import _lib as L
+    from falm_b200.driver import Simulation
+    case = small_cases()["channel"]
+    ref = Simulation(case, precision)
+    for _ in range(5):
+        ref.step()
+    a = Simulation(case, precision)
+    for _ in range(3):
+        a.step()
+    a.save_state(tmp_path / "s3")
+    b = Simulation(case, precision)
+    b.load_state(tmp_path / "s3")
+    assert b.it == 3
+    for _ in range(2):
+        b.step()
+    for k in ("u", "uu", "p", "nut"):
+        assert np.array_equal(getattr(b, k).cpu().numpy(), getattr(ref, k).cpu().numpy()), k
+    raw = (tmp_path / "s3").read_bytes()
+    (tmp_path / "cut").write_bytes(raw[:len(raw) - 8])
+    (tmp_path / "long").write_bytes(raw + b"\0" * 8)
+    (tmp_path / "head").write_bytes(raw[:40])
+    before = b.u.cpu().numpy().copy()
+    for name in ("cut", "long", "head"):
+        with pytest.raises(L.FalmError) as e:
+            b.load_state(tmp_path / name)
+        assert e.value.code == L.FALM_ERR_ARG
+    assert np.array_equal(b.u.cpu().numpy(), before)
+    b.step()
+    for s in (ref, a, b):
+        s.ctx.close()
+
+
+def test_inconsistent_rhs_ends_in_a_status(lib_built):
+    """A right-hand side outside the range of the singular all-Neumann cavity
+    operator (a constant: the system has no solution) makes BiCGStab stall or
+    break down: the solve ends in a status (FALM_ERR_MAXIT, FALM_ERR_BREAKDOWN,
+    or FALM_ERR_NAN for a non-finite alpha/omega, after which no kernel updates
+    the iterate) with a finite iterate, never a trap or a hang, and the
+    context then solves a consistent system normally."""
+    from falm_b200.api import _ptr
+    import ctypes
+    case = cases.cavity(16)
+    g = case.grid
+    ctx = make_ctx(case)
+    ctx.eq_init(200, 1e-12, case.pc, case.pc_maxit, case.pc_relax)
+    b = np.zeros((g.sz, g.sy, g.sx))
+    gc = g.gc
+    b[gc:-gc, gc:-gc, gc:-gc] = 1.0
+    x, r = ctx.field(1), ctx.field(1)
+    it, err = ctypes.c_int(), ctypes.c_double()
+    rc = ctx.lib.falm_eq_solve(ctx.h, _ptr(x), _ptr(dev(ctx, b.reshape(-1))), _ptr(r), ctx.stream(), ctypes.byref(it),
+                               ctypes.byref(err))
+    assert rc in (3, 4, 5), rc
+    assert np.isfinite(host(x)).all()
+    # a consistent right-hand side (zero mean) on the same context
+    bc = b.copy()
+    bc[gc:-gc, gc:-gc, gc:-gc] = np.random.default_rng(2).standard_normal((g.sz - 2 * gc, g.sy - 2 * gc, g.sx - 2 * gc))
+    bc[gc:-gc, gc:-gc, gc:-gc] -= bc[gc:-gc, gc:-gc, gc:-gc].mean()
+    ctx.eq_init(200, 1e-10, case.pc, case.pc_maxit, case.pc_relax)
+    x2 = ctx.field(1)
+    its, errv, rc2 = ctx.solve(x2, dev(ctx, bc.reshape(-1)), r)
+    assert rc2 == 0 and errv <= 1e-10 and np.isfinite(host(x2)).all()
+    ctx.close()
