@@ -24,6 +24,7 @@
 #include <chrono>
 #include <dlfcn.h>
 #include <nccl.h>
+#include <nvtx3/nvToolsExt.h>
 #include "falm_internal.cuh"
 #include "common.cuh"
 #include "cfd.cuh"
@@ -116,6 +117,24 @@ int launch_k(falm_ctx *ctx, int cls, cudaStream_t st, F &&f) {
         int _lrc = launch_k(ctx, (CLS), (ST), [&] { __VA_ARGS__; });                         \
         if (_lrc) return _lrc;                                                               \
     } while (0)
+
+// NVTX ranges (a profiler or tracer attached through NVTX shows them; without
+// one they cost a few ns): one range per call and one per phase of the step
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
+struct NvtxPhases {   // consecutive ranges: next() closes the open one
+    bool open = false;
+    void next(const char *name) {
+        if (open) nvtxRangePop();
+        nvtxRangePushA(name);
+        open = true;
+    }
+    ~NvtxPhases() { if (open) nvtxRangePop(); }
+};
 
 // resident CTAs per SM of a kernel at a launch shape, looked up once per
 // kernel and shape
@@ -705,6 +724,7 @@ int solve_graph(falm_ctx *ctx, const void *x, const void *b, const void *r, int 
 template <typename T>
 int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out, double *err_out, int *outer_out,
             bool first_res_done = false) {
+    NvtxRange range("falm_solve");
     int rc = ensure_work(ctx);
     if (rc) return rc;
     if (!ctx->op_ready && !ctx->A_explicit) return fail(ctx, FALM_ERR_STATE, "solve: no operator (call falm_eq_poisson_operator or falm_eq_set_matrix)");
@@ -1055,6 +1075,8 @@ __global__ void k_wait_probe(int *err, long long cycles) {
 
 template <typename T>
 int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_t st, falm_step_stats *out) {
+    NvtxRange whole("falm_step");
+    NvtxPhases phase;
     int rc = ensure_work(ctx);
     if (rc) return rc;
     if (ctx->wait_probe_cycles > 0) {   // armed by falm_debug_arm_wait_probe: one step only
@@ -1071,6 +1093,7 @@ int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_
     const bool chan = ctx->bc_kind == FALM_BC_CHANNEL;
     bool fused_res = false;
     // 1. ALM (src/alm/alm.h:66-77) at the previous velocity, or the RMCP model
+    phase.next("forcing");
     if (ctx->alm_on) {
         if ((rc = alm_run_t<T>(ctx, u, ff, t, st))) return rc;
     } else if (ctx->rmcp_on) {
@@ -1078,8 +1101,10 @@ int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_
         if ((rc = rmcp_run_t<T>(ctx, u, ff, nullptr, t, st))) return rc;
     }
     // 2. pseudo-velocity into ua (ALM force projected in-kernel when ff == NULL)
+    phase.next("pseudo_velocity");
     if ((rc = pseudo_u_t<T>(ctx, u, u, uu, ua, nut, ff, dt, ctx->alm_on != 0, st))) return rc;
     // 3. face velocity + [uubc] + RHS in one pass
+    phase.next("face_velocity_rhs");
     {
         const Region3 R = facemap(g);
         T scale = (T)(1.0 / (dt * ctx->maxdiag));
@@ -1115,12 +1140,14 @@ int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_
         }
     }
     // 4. Poisson
+    phase.next("poisson");
     int it = 0, outer = 1;
     double err = 0;
     rc = solve_t<T>(ctx, p, rhs, r, st, &it, &err, &outer, fused_res);
     int solve_status = ctx->scal_host->status;
     if (rc) return rc;
     // 5. pbc
+    phase.next("projection_bcs");
     LAUNCH(FALM_K_PBC, st, k_pbc<T><<<dim3(face_blocks(ctx), 3), 256, 0, st>>>(g, ctx->bc_kind, p));
     // 6. keep the previous velocity at the outlet planes, then project
     if (chan) { LAUNCH(FALM_K_OTHER, st, k_save_outlet<T><<<std::min(ctx->sm_count * 4, (3 * g.sy * g.sz + 255) / 256), 256, 0, st>>>(g, u, (T *)ctx->w_outlet)); }
@@ -1132,6 +1159,7 @@ int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_
     // 7. ubc
     if ((rc = ubc_t<T>(ctx, u, UPrev<T>{(const T *)ctx->w_outlet, 1}, dt, t, st))) return rc;
     // 8. SGS + divergence norm
+    phase.next("sgs_divergence");
     {
         const Region3 R = interior(g);
         P3_OR(FALM_K_SGS_DIV, st, T, 2, 1, R, 2, FB_ARR(u, uu), FB_ARR(3, 3),
@@ -2497,6 +2525,7 @@ namespace {
 template <typename T>
 int step_adjoint_t(falm_ctx *ctx, const falm_fields *f0, const falm_fields *f1, double dt, double t, double w_power,
                    void *au, void *auu, void *anut, double *grad, cudaStream_t st) {
+    NvtxRange range("falm_step_adjoint");
     int rc = ensure_work(ctx);
     if (rc) return rc;
     AdjWork w;

@@ -423,6 +423,7 @@ int slab_alm_t(falm_ctx *ctx, const T *u, double t, cudaStream_t st) {
 // velocity, right-hand side and first residual run as separate passes here.
 template <typename T>
 int slab_step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_t st, falm_step_stats *out) {
+    NvtxRange range("falm_step_slab");
     int rc = ensure_work(ctx);
     if (rc) return rc;
     if (!ctx->op_ready) return fail(ctx, FALM_ERR_STATE, "slab step: build the operator first (falm_eq_poisson_operator, a collective)");
