@@ -50,7 +50,8 @@ __device__ inline int find_index(const double *seq, double v, int n) {
 // end are kept in shared memory too (up to kMaxFusedAp points).
 template <typename T>
 __global__ void __launch_bounds__(256) k_alm_force(Geom g, AlmDev a, const double *xc_g, const double *yc_g, const double *zc_g,
-                                                 const T *__restrict__ u, double t, int stage) {
+                                                 const T *__restrict__ u, double t_arg, int stage, const double *t_dev) {
+    const double t = t_dev ? *t_dev : t_arg;   // a recorded step (CUDA graph) reads its time from device memory
     extern __shared__ double s_coord[];
     __shared__ double s_xyz[3 * kMaxFusedAp], s_tq[kMaxFusedAp], s_th[kMaxFusedAp];
     const bool keep = a.apcount <= kMaxFusedAp;
@@ -294,7 +295,9 @@ struct Inflow {
 // own guide cells and reads interior cells, so the three pairs are independent
 // (the reference launches them on six concurrent streams).
 template <typename T>
-__global__ void k_ubc(Geom g, int kind, T *u, UPrev<T> up, const double *xc, double dt, double t, double u_inlet, Inflow inf) {
+__global__ void k_ubc(Geom g, int kind, T *u, UPrev<T> up, const double *xc, double dt, double t_arg, double u_inlet, Inflow inf,
+                      const double *t_dev) {
+    const double t = t_dev ? *t_dev : t_arg;   // a recorded step (CUDA graph) reads its time from device memory
     const long long N = g.n;
     const int gc = g.gc, sx = g.sx, sy = g.sy, sz = g.sz;
     const int pair = blockIdx.y;

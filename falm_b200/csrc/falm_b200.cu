@@ -639,14 +639,99 @@ __global__ void k_graph_continue(const SolverScalars *sc, cudaGraphConditionalHa
     cudaGraphSetConditional(h, sc->done ? 0u : 1u);
 }
 
+// drop every recorded loop and step (the settings they were recorded with changed)
 void graphs_clear(falm_ctx *ctx) {
-    if (!ctx->graphs) return;
-    for (auto &e : *ctx->graphs) {
-        cudaGraphExecDestroy(e.exec);
-        cudaGraphDestroy(e.graph);
+    if (ctx->graphs) {
+        for (auto &e : *ctx->graphs) {
+            cudaGraphExecDestroy(e.exec);
+            cudaGraphDestroy(e.graph);
+        }
+        ctx->graphs->clear();
     }
-    ctx->graphs->clear();
+    if (ctx->step_graphs) {
+        for (auto &e : *ctx->step_graphs) {
+            cudaGraphExecDestroy(e.exec);
+            cudaGraphDestroy(e.graph);
+        }
+        ctx->step_graphs->clear();
+    }
 }
+
+// ---- recording on the device: the solver control the host loop does otherwise
+// the scalars of a solve's start (solver_init on the device)
+__global__ void k_solver_init(SolverScalars *sc, double gsize, double tol, int maxit) {
+    SolverScalars z;
+    memset(&z, 0, sizeof(z));
+    z.gsize = gsize;
+    z.tol = tol;
+    z.maxit = maxit;
+    *sc = z;
+}
+// a pass has ended: its iterations into the totals
+__global__ void k_pass_end(SolverScalars *sc) {
+    sc->it_total += sc->it;
+    sc->passes += 1;
+}
+// a new pass: iteration count zero, the pass's limit
+__global__ void k_pass_reset(SolverScalars *sc, int maxit) {
+    sc->it = 0;
+    sc->maxit = maxit;
+}
+// after the FP64 check of a mixed pass: another pass while the true residual
+// misses the tolerance and passes remain (a breakdown's status is cleared: the
+// pass restarts from the true residual); non-finite data ends the solve (done)
+__global__ void k_outer_cond(SolverScalars *sc, cudaGraphConditionalHandle h, int max_passes) {
+    const bool more = !sc->done && sc->passes < max_passes;
+    if (more) sc->status = FALM_OK;
+    cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+
+// the recording stream's current leaf nodes after fn's launches on it, which go
+// into `graph` after `deps` (deps becomes the new leaves)
+int capture_into(falm_ctx *ctx, cudaGraph_t graph, std::vector<cudaGraphNode_t> &deps, const std::function<int()> &fn) {
+    const cudaStream_t cs = ctx->cap_stream;
+    if (cudaStreamBeginCaptureToGraph(cs, graph, deps.empty() ? nullptr : deps.data(), nullptr, deps.size(),
+                                      cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, FALM_ERR_CUDA, "graph: begin capture");
+    }
+    int rc = fn();
+    cudaStreamCaptureStatus stt;
+    const cudaGraphNode_t *d = nullptr;
+    size_t nd = 0;
+    std::vector<cudaGraphNode_t> leaves;
+    if (cudaStreamGetCaptureInfo(cs, &stt, nullptr, nullptr, &d, &nd) == cudaSuccess && d) leaves.assign(d, d + nd);
+    cudaGraph_t got = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(cs, &got);
+    cudaGetLastError();
+    if (!rc && (e != cudaSuccess || got != graph)) rc = fail(ctx, FALM_ERR_CUDA, "graph: end capture");
+    if (!rc && !leaves.empty()) deps = leaves;
+    return rc;
+}
+
+// a conditional while node after deps (deps becomes the node); its body graph in *body
+int add_while(falm_ctx *ctx, cudaGraph_t graph, std::vector<cudaGraphNode_t> &deps, cudaGraphConditionalHandle h, cudaGraph_t *body) {
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};   // every other byte zero
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (cudaGraphAddNode(&node, graph, deps.empty() ? nullptr : deps.data(), deps.size(), &cp) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, FALM_ERR_CUDA, "graph: while node");
+    }
+    deps.assign(1, node);
+    *body = cp.conditional.phGraph_out[0];
+    return FALM_OK;
+}
+
+// a solve recorded into a graph after deps (see solve_t); counts the kernels
+// recorded outside and inside the iteration loops
+struct SolveRec {
+    cudaGraph_t graph;
+    std::vector<cudaGraphNode_t> deps;
+    long long fixed = 0, per_iter = 0;
+};
 
 // the graph of a pass (built on first use: emit(itp) launches iteration itp's
 // kernels on `ist`, which points at the capture stream meanwhile); prefix and
@@ -723,13 +808,13 @@ int solve_graph(falm_ctx *ctx, const void *x, const void *b, const void *r, int 
 
 template <typename T>
 int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out, double *err_out, int *outer_out,
-            bool first_res_done = false) {
+            bool first_res_done = false, SolveRec *rec = nullptr) {
     NvtxRange range("falm_solve");
     int rc = ensure_work(ctx);
     if (rc) return rc;
     if (!ctx->op_ready && !ctx->A_explicit) return fail(ctx, FALM_ERR_STATE, "solve: no operator (call falm_eq_poisson_operator or falm_eq_set_matrix)");
     if (ctx->ls_type == FALM_LS_JACOBI || ctx->ls_type == FALM_LS_SOR) {
-        if (first_res_done) return fail(ctx, FALM_ERR_STATE, "solve: a BiCGStab start was prepared for a plain solver");
+        if (first_res_done || rec) return fail(ctx, FALM_ERR_STATE, "solve: a BiCGStab start was prepared for a plain solver");
         return plain_solve_t<T>(ctx, x, b, r, st, it_out, err_out, outer_out);
     }
     if (ctx->ls_type != FALM_LS_PBICGSTAB) return fail(ctx, FALM_ERR_ARG, "solve: unknown linear solver type");
@@ -744,7 +829,7 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
     // first_res_done: the caller initialised the scalars (solver_init) and a
     // kernel of its own already computed the first pass's residual into rr with
     // the first preconditioner sweep into pp (the step's face-velocity kernel)
-    if (!first_res_done && (rc = solver_init(ctx, st))) return rc;
+    if (!first_res_done && !rec && (rc = solver_init(ctx, st))) return rc;
     const T pcw = (T)ctx->pc_relax;
     const int pct = ctx->pc_type, m = ctx->pc_maxit;
     SolverScalars *sc = ctx->scal;
@@ -802,14 +887,14 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
     auto res_pass = [&](int check) -> int {
         int s7;
         if (check) {
-            s7 = s7_launch<T, 1>(ctx, FALM_K_RES, st, x, ResBody<T, true>{op, b, nullptr, nullptr, sc, 1});
+            s7 = s7_launch<T, 1>(ctx, FALM_K_RES, ist, x, ResBody<T, true>{op, b, nullptr, nullptr, sc, 1});
         } else {
             ResBody<T> body{op, b, nullptr, rr, sc, 0};
             body.pp = first_target(pp); body.pc_type = pct; body.pc_omega = pcw;
-            s7 = s7_launch<T, 2>(ctx, FALM_K_RES, st, x, body);
+            s7 = s7_launch<T, 2>(ctx, FALM_K_RES, ist, x, body);
         }
         if (s7 < 0) return -s7;
-        if (s7 == 0) LAUNCH(FALM_K_RES, st, (k_res<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, r, rr, ctx->red, sc, check)));
+        if (s7 == 0) LAUNCH(FALM_K_RES, ist, (k_res<T><<<grid, kRowThreads, 0, ist>>>(g, R, op, x, b, r, rr, ctx->red, sc, check)));
         pp_ready = !check && s7 == 1;
         return FALM_OK;
     };
@@ -820,6 +905,105 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
         CK(cudaMemcpyAsync(&sc->it, itmax, sizeof(itmax), cudaMemcpyHostToDevice, st));
         return FALM_OK;
     };
+    // the kernels of iteration itp of the pass (2 stands for every later
+    // one): r equals rr until the first k_bicg_xr, and the first
+    // iteration's p equals r, so it reads rr in their place
+    auto emit_iter = [&](int itp) -> int {
+        const T *rin = itp == 0 ? rr : r;
+        T *pout = itp == 0 ? nullptr : p;
+        const T *pin = itp == 1 ? rr : p, *pv = itp == 0 ? rr : p;
+        int erc;
+        if (!(itp == 0 && pp_ready))
+            LAUNCH(FALM_K_BICG_P, ist, k_bicg_p<T><<<grid_p, kRowThreads, 0, ist>>>(g, R, op, pout, pin, q, rin, first_target(pp), pct, pcw, sc));
+        if ((erc = precondition_rest(pp, pv))) return erc;
+        S7_OR(FALM_K_MV_DOT1, ist, T, 1, pp, (MvDot1Body<T>{op, q, rr, sc}),
+              (k_mv_dot1<T><<<grid, kRowThreads, 0, ist>>>(g, R, op, pp, q, rr, ctx->red, sc)));
+        LAUNCH(FALM_K_BICG_S, ist, k_bicg_s<T><<<grid_s, kRowThreads, 0, ist>>>(g, R, op, s, q, rin, first_target(ss), pct, pcw, sc));
+        if ((erc = precondition_rest(ss, s))) return erc;
+        S7_OR(FALM_K_MV_DOT2, ist, T, 2, ss, (MvDot2Body<T>{op, t, s, sc}),
+              (k_mv_dot2<T><<<grid, kRowThreads, 0, ist>>>(g, R, op, ss, t, s, ctx->red, sc)));
+        LAUNCH(FALM_K_BICG_XR, ist, k_bicg_xr<T><<<grid_xr, kRowThreads, 0, ist>>>(g, R, x, pp, ss, r, s, t, rr, ctx->red, sc));
+        return FALM_OK;
+    };
+    if (rec) {
+        // The whole solve recorded into rec->graph after rec->deps, with no
+        // host decision: pass 0 (solver start and first residual unless the
+        // caller recorded them), and in mixed precision a while node of FP64
+        // checks and further passes; a pass is iterations 0 and 1 and a while
+        // node of later iterations, its condition the done flag.
+        ist = ctx->cap_stream;
+        const long long l_start = ctx->launches;
+        long long fixed = 0, per_iter = 0;
+        auto cap = [&](cudaGraph_t gr, std::vector<cudaGraphNode_t> &deps, long long *cnt, const std::function<int()> &fn) -> int {
+            const long long l0 = ctx->launches;
+            const int crc = capture_into(ctx, gr, deps, fn);
+            *cnt += ctx->launches - l0;
+            ctx->launches = l0;
+            return crc;
+        };
+        auto cond = [&](cudaGraphConditionalHandle h) -> int {
+            k_graph_continue<<<1, 1, 0, ist>>>(sc, h);
+            return cudaGetLastError() == cudaSuccess ? FALM_OK : fail(ctx, FALM_ERR_CUDA, "graph: condition kernel");
+        };
+        auto rec_pass = [&](cudaGraph_t gr, std::vector<cudaGraphNode_t> &deps) -> int {
+            cudaGraphConditionalHandle h;
+            if (cudaGraphConditionalHandleCreate(&h, gr, 1, cudaGraphCondAssignDefault) != cudaSuccess)
+                return fail(ctx, FALM_ERR_CUDA, "graph: handle");
+            int e = cap(gr, deps, &fixed, [&]() -> int {
+                int q2 = emit_iter(0);
+                if (!q2) q2 = emit_iter(1);
+                if (!q2) q2 = cond(h);
+                return q2;
+            });
+            cudaGraph_t body = nullptr;
+            if (!e) e = add_while(ctx, gr, deps, h, &body);
+            std::vector<cudaGraphNode_t> bd;
+            long long pi = 0;
+            if (!e) e = cap(body, bd, &pi, [&]() -> int {
+                int q2 = emit_iter(2);
+                if (!q2) q2 = cond(h);
+                return q2;
+            });
+            per_iter = pi;
+            if (!e) e = cap(gr, deps, &fixed, [&]() -> int {
+                LAUNCH(FALM_K_OTHER, ist, k_pass_end<<<1, 1, 0, ist>>>(sc));
+                return FALM_OK;
+            });
+            return e;
+        };
+        int e = FALM_OK;
+        if (!first_res_done)
+            e = cap(rec->graph, rec->deps, &fixed, [&]() -> int {
+                LAUNCH(FALM_K_OTHER, ist, k_solver_init<<<1, 1, 0, ist>>>(sc, (double)g.nx * g.ny * g.nzg, ctx->tol, pass_its));
+                return res_pass(0);
+            });
+        if (!e) e = rec_pass(rec->graph, rec->deps);
+        if (!e && mixed && max_outer > 1) {
+            cudaGraphConditionalHandle ho;
+            if (cudaGraphConditionalHandleCreate(&ho, rec->graph, 0, cudaGraphCondAssignDefault) != cudaSuccess)
+                e = fail(ctx, FALM_ERR_CUDA, "graph: handle");
+            auto check = [&]() -> int {
+                int q2 = res_pass(1);
+                if (!q2) LAUNCH(FALM_K_OTHER, ist, k_outer_cond<<<1, 1, 0, ist>>>(sc, ho, max_outer));
+                return q2;
+            };
+            if (!e) e = cap(rec->graph, rec->deps, &fixed, check);
+            cudaGraph_t ob = nullptr;
+            if (!e) e = add_while(ctx, rec->graph, rec->deps, ho, &ob);
+            std::vector<cudaGraphNode_t> od;
+            if (!e) e = cap(ob, od, &fixed, [&]() -> int {
+                LAUNCH(FALM_K_OTHER, ist, k_pass_reset<<<1, 1, 0, ist>>>(sc, pass_its));
+                return res_pass(0);
+            });
+            if (!e) e = rec_pass(ob, od);
+            if (!e) e = cap(ob, od, &fixed, check);
+        }
+        ist = st;
+        ctx->launches = l_start;
+        rec->fixed += fixed;
+        rec->per_iter = per_iter;
+        return e;
+    }
     if (mixed && pass_its != ctx->maxit)
         CK(cudaMemcpyAsync(&sc->maxit, &pass_its, sizeof(int), cudaMemcpyHostToDevice, st));
     // In mixed precision each pass but the last is followed by a check of the
@@ -851,26 +1035,6 @@ int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out,
         pass_queued = false;
         const bool want_check = mixed && outer + 1 < max_outer && !explicit_check;
         bool checked = false;
-        // the kernels of iteration itp of the pass (2 stands for every later
-        // one): r equals rr until the first k_bicg_xr, and the first
-        // iteration's p equals r, so it reads rr in their place
-        auto emit_iter = [&](int itp) -> int {
-            const T *rin = itp == 0 ? rr : r;
-            T *pout = itp == 0 ? nullptr : p;
-            const T *pin = itp == 1 ? rr : p, *pv = itp == 0 ? rr : p;
-            int erc;
-            if (!(itp == 0 && pp_ready))
-                LAUNCH(FALM_K_BICG_P, ist, k_bicg_p<T><<<grid_p, kRowThreads, 0, ist>>>(g, R, op, pout, pin, q, rin, first_target(pp), pct, pcw, sc));
-            if ((erc = precondition_rest(pp, pv))) return erc;
-            S7_OR(FALM_K_MV_DOT1, ist, T, 1, pp, (MvDot1Body<T>{op, q, rr, sc}),
-                  (k_mv_dot1<T><<<grid, kRowThreads, 0, ist>>>(g, R, op, pp, q, rr, ctx->red, sc)));
-            LAUNCH(FALM_K_BICG_S, ist, k_bicg_s<T><<<grid_s, kRowThreads, 0, ist>>>(g, R, op, s, q, rin, first_target(ss), pct, pcw, sc));
-            if ((erc = precondition_rest(ss, s))) return erc;
-            S7_OR(FALM_K_MV_DOT2, ist, T, 2, ss, (MvDot2Body<T>{op, t, s, sc}),
-                  (k_mv_dot2<T><<<grid, kRowThreads, 0, ist>>>(g, R, op, ss, t, s, ctx->red, sc)));
-            LAUNCH(FALM_K_BICG_XR, ist, k_bicg_xr<T><<<grid_xr, kRowThreads, 0, ist>>>(g, R, x, pp, ss, r, s, t, rr, ctx->red, sc));
-            return FALM_OK;
-        };
         if (graph) {
             // the whole pass on the device: one graph launch, one host read
             cudaGraphExec_t ge = nullptr;
@@ -1019,12 +1183,13 @@ int pseudo_u_t(falm_ctx *ctx, const T *un, const T *u, const T *uu, T *ua, const
 }
 
 template <typename T>
-int alm_run_t(falm_ctx *ctx, const T *u, T *ff, double t, cudaStream_t st) {
+int alm_run_t(falm_ctx *ctx, const T *u, T *ff, double t, cudaStream_t st, const double *t_dev = nullptr) {
     // stage the coordinate tables in shared memory when they fit in 96 KB
     const int csm = (ctx->geo.sx + ctx->geo.sy + ctx->geo.sz) * (int)sizeof(double);
     const int stage = csm <= 96 * 1024 ? 1 : 0;
     if (stage && csm > 32 * 1024) cudaFuncSetAttribute(k_alm_force<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
-    LAUNCH(FALM_K_ALM, st, k_alm_force<T><<<1, 256, stage ? csm : 0, st>>>(ctx->geo, ctx->alm, ctx->m64.x[0], ctx->m64.x[1], ctx->m64.x[2], u, t, stage));
+    LAUNCH(FALM_K_ALM, st, k_alm_force<T><<<1, 256, stage ? csm : 0, st>>>(ctx->geo, ctx->alm, ctx->m64.x[0], ctx->m64.x[1], ctx->m64.x[2], u, t, stage,
+                                                                            t_dev));
     if (ff) {
         const Region3 R = interior(ctx->geo);
         LAUNCH(FALM_K_ALM, st, k_alm_project<T><<<row_grid(ctx, R), kRowThreads, 0, st>>>(ctx->geo, R, mview<T>(ctx), ctx->alm, ff));
@@ -1037,11 +1202,11 @@ int alm_run_t(falm_ctx *ctx, const T *u, T *ff, double t, cudaStream_t st) {
 }
 
 template <typename T>
-int ubc_t(falm_ctx *ctx, T *u, UPrev<T> up, double dt, double t, cudaStream_t st) {
+int ubc_t(falm_ctx *ctx, T *u, UPrev<T> up, double dt, double t, cudaStream_t st, const double *t_dev = nullptr) {
     Inflow inf{ctx->inflow_box, ctx->inflow_nb, ctx->inflow_dx, ctx->inlet_plane_valid ? ctx->inlet_plane : nullptr};
     ctx->inlet_plane_valid = 0;
     dim3 grid(face_blocks(ctx), 3);
-    LAUNCH(FALM_K_UBC, st, k_ubc<T><<<grid, 256, 0, st>>>(ctx->geo, ctx->bc_kind, u, up, ctx->m64.x[0], dt, t, ctx->u_inlet, inf));
+    LAUNCH(FALM_K_UBC, st, k_ubc<T><<<grid, 256, 0, st>>>(ctx->geo, ctx->bc_kind, u, up, ctx->m64.x[0], dt, t, ctx->u_inlet, inf, t_dev));
     return FALM_OK;
 }
 
@@ -1073,38 +1238,31 @@ __global__ void k_wait_probe(int *err, long long cycles) {
     __syncthreads();
 }
 
+// The phases of the step before and after the Poisson solve, shared by the
+// host-driven step and the recorded one: t_dev is the recorded step's time in
+// device memory (NULL: the host passes t), phase the NVTX phases (or NULL).
 template <typename T>
-int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_t st, falm_step_stats *out) {
-    NvtxRange whole("falm_step");
-    NvtxPhases phase;
-    int rc = ensure_work(ctx);
-    if (rc) return rc;
-    if (ctx->wait_probe_cycles > 0) {   // armed by falm_debug_arm_wait_probe: one step only
-        const long long cycles = ctx->wait_probe_cycles;
-        ctx->wait_probe_cycles = 0;
-        LAUNCH(FALM_K_OTHER, st, k_wait_probe<<<1, 32, 0, st>>>(ctx->kerr, cycles));
-    }
-    if (!ctx->op_ready) {
-        if ((rc = build_poisson(ctx, ctx->bc_kind))) return rc;
-    }
+int step_pre_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_t st, const double *t_dev, bool *fused_res_out,
+               NvtxPhases *phase) {
+    int rc;
     const Geom &g = ctx->geo;
     T *u = (T *)f->u, *uu = (T *)f->uu, *p = (T *)f->p, *nut = (T *)f->nut, *ff = (T *)f->ff;
-    T *ua = (T *)ctx->w_ua, *rhs = (T *)ctx->w_rhs, *r = (T *)ctx->w_r;
+    T *ua = (T *)ctx->w_ua, *rhs = (T *)ctx->w_rhs;
     const bool chan = ctx->bc_kind == FALM_BC_CHANNEL;
     bool fused_res = false;
     // 1. ALM (src/alm/alm.h:66-77) at the previous velocity, or the RMCP model
-    phase.next("forcing");
+    if (phase) phase->next("forcing");
     if (ctx->alm_on) {
-        if ((rc = alm_run_t<T>(ctx, u, ff, t, st))) return rc;
+        if ((rc = alm_run_t<T>(ctx, u, ff, t, st, t_dev))) return rc;
     } else if (ctx->rmcp_on) {
         ff = (T *)ctx->w_ff;
         if ((rc = rmcp_run_t<T>(ctx, u, ff, nullptr, t, st))) return rc;
     }
     // 2. pseudo-velocity into ua (ALM force projected in-kernel when ff == NULL)
-    phase.next("pseudo_velocity");
+    if (phase) phase->next("pseudo_velocity");
     if ((rc = pseudo_u_t<T>(ctx, u, u, uu, ua, nut, ff, dt, ctx->alm_on != 0, st))) return rc;
     // 3. face velocity + [uubc] + RHS in one pass
-    phase.next("face_velocity_rhs");
+    if (phase) phase->next("face_velocity_rhs");
     {
         const Region3 R = facemap(g);
         T scale = (T)(1.0 / (dt * ctx->maxdiag));
@@ -1114,7 +1272,13 @@ int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_
         // first preconditioner sweep (pp) from the pressure p, the initial guess
         fused_res = false;
         if (!ctx->A_explicit && ctx->ls_type == FALM_LS_PBICGSTAB && (ctx->pc_type == FALM_LS_SOR || ctx->pc_type == FALM_LS_JACOBI)) {
-            if ((rc = ensure_work(ctx)) || (rc = solver_init(ctx, st))) return rc;
+            if ((rc = ensure_work(ctx))) return rc;
+            if (t_dev) {   // recording: the solver start as a kernel (the mixed pass limit included)
+                const int pass_its = ctx->precision == FALM_MIXED ? std::min(ctx->maxit, kMixedPassIts) : ctx->maxit;
+                LAUNCH(FALM_K_OTHER, st, k_solver_init<<<1, 1, 0, st>>>(ctx->scal, (double)g.nx * g.ny * g.nzg, ctx->tol, pass_its));
+            } else if ((rc = solver_init(ctx, st))) {
+                return rc;
+            }
             T *ppt = pc_first_in_xp<T>(ctx) ? (T *)ctx->w_xp : (T *)ctx->w_pp;
             const void *const fp[2] = {ua, p};
             const int nc[2] = {3, 1};
@@ -1139,15 +1303,19 @@ int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_
                       (k_utouu<T, true, true><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), ua, u, uu, rhs, scale)));
         }
     }
-    // 4. Poisson
-    phase.next("poisson");
-    int it = 0, outer = 1;
-    double err = 0;
-    rc = solve_t<T>(ctx, p, rhs, r, st, &it, &err, &outer, fused_res);
-    int solve_status = ctx->scal_host->status;
-    if (rc) return rc;
+    *fused_res_out = fused_res;
+    return FALM_OK;
+}
+
+template <typename T>
+int step_post_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_t st, const double *t_dev, NvtxPhases *phase) {
+    int rc;
+    const Geom &g = ctx->geo;
+    T *u = (T *)f->u, *uu = (T *)f->uu, *p = (T *)f->p, *nut = (T *)f->nut;
+    T *ua = (T *)ctx->w_ua;
+    const bool chan = ctx->bc_kind == FALM_BC_CHANNEL;
     // 5. pbc
-    phase.next("projection_bcs");
+    if (phase) phase->next("projection_bcs");
     LAUNCH(FALM_K_PBC, st, k_pbc<T><<<dim3(face_blocks(ctx), 3), 256, 0, st>>>(g, ctx->bc_kind, p));
     // 6. keep the previous velocity at the outlet planes, then project
     if (chan) { LAUNCH(FALM_K_OTHER, st, k_save_outlet<T><<<std::min(ctx->sm_count * 4, (3 * g.sy * g.sz + 255) / 256), 256, 0, st>>>(g, u, (T *)ctx->w_outlet)); }
@@ -1157,9 +1325,9 @@ int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_
               (k_project<T><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), u, ua, uu, uu, p, (T)dt)));
     }
     // 7. ubc
-    if ((rc = ubc_t<T>(ctx, u, UPrev<T>{(const T *)ctx->w_outlet, 1}, dt, t, st))) return rc;
+    if ((rc = ubc_t<T>(ctx, u, UPrev<T>{(const T *)ctx->w_outlet, 1}, dt, t, st, t_dev))) return rc;
     // 8. SGS + divergence norm
-    phase.next("sgs_divergence");
+    if (phase) phase->next("sgs_divergence");
     {
         const Region3 R = interior(g);
         P3_OR(FALM_K_SGS_DIV, st, T, 2, 1, R, 2, FB_ARR(u, uu), FB_ARR(3, 3),
@@ -1167,11 +1335,21 @@ int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_
               (k_sgs_div<T, true><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), ctx->m64, u, nut, (T)ctx->Cs, ctx->sgs, uu,
                                                                             nullptr, ctx->red, &ctx->scal->red[3])));
     }
+    return FALM_OK;
+}
+
+// the step's results into the pinned host copies
+int step_stats_copy(falm_ctx *ctx, cudaStream_t st) {
     CK(cudaMemcpyAsync(ctx->scal_host, ctx->scal, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
     if (ctx->alm_on) CK(cudaMemcpyAsync(ctx->alm_scal_host, ctx->alm.scal, sizeof(AlmScalars), cudaMemcpyDeviceToHost, st));
     if (ctx->rmcp_on) CK(cudaMemcpyAsync(ctx->rmcp_sums_host, ctx->rmcp_sums, 2 * kMaxTurbines * sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(&ctx->scal_host->kerr, ctx->kerr, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    return FALM_OK;
+}
+
+// after the step's synchronisation: the device error word, then the statistics
+int step_finish(falm_ctx *ctx, cudaStream_t st, falm_step_stats *out, int it, double err, int outer, int solve_status) {
+    const Geom &g = ctx->geo;
     if (ctx->scal_host->kerr) {
         cudaMemsetAsync(ctx->kerr, 0, sizeof(int), st);
         std::string m = "step: device error word " + std::to_string(ctx->scal_host->kerr) +
@@ -1199,6 +1377,102 @@ int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_
             }
     }
     return FALM_OK;
+}
+
+// Whole steps as CUDA graphs (grids where launch and synchronisation latency
+// dominate, see use_graph): the phases before the solve, the solve with its
+// loops on the device (solve_t's recording), the phases after it and the
+// copies of the results, recorded once per set of fields and dt; the time goes
+// in through device memory, written by the graph's first node from a pinned
+// host value.  Not for streamed inlet planes (a new buffer each step), the
+// RMCP forcing, z slabs, the plain solvers or an explicit matrix.
+template <typename T>
+bool step_graph_ok(const falm_ctx *ctx) {
+    return use_graph(ctx) && !ctx->slab_on && !ctx->rmcp_on && !ctx->inlet_plane_valid && ctx->wait_probe_cycles == 0 && ctx->op_ready &&
+           !ctx->A_explicit && ctx->ls_type == FALM_LS_PBICGSTAB && (ctx->pc_type == FALM_LS_SOR || ctx->pc_type == FALM_LS_JACOBI);
+}
+
+template <typename T>
+int step_graph_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_t st, falm_step_stats *out) {
+    falm_ctx::StepGraph *sg = nullptr;
+    for (auto &e : *ctx->step_graphs)
+        if (e.u == f->u && e.uu == f->uu && e.p == f->p && e.nut == f->nut && e.ff == f->ff && e.dt == dt) sg = &e;
+    if (!sg) {
+        if (!ctx->cap_stream) CK(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
+        if (!ctx->t_dev) {
+            CK(cudaMalloc(&ctx->t_dev, sizeof(double)));
+            CK(cudaHostAlloc(&ctx->t_host, sizeof(double), cudaHostAllocDefault));
+        }
+        const cudaStream_t cs = ctx->cap_stream;
+        cudaGraph_t gr = nullptr;
+        CK(cudaGraphCreate(&gr, 0));
+        SolveRec rec;
+        rec.graph = gr;
+        bool fused = false;
+        const long long l0 = ctx->launches;
+        int rc = capture_into(ctx, gr, rec.deps, [&]() -> int {
+            CK(cudaMemcpyAsync(ctx->t_dev, ctx->t_host, sizeof(double), cudaMemcpyHostToDevice, cs));
+            return step_pre_t<T>(ctx, f, dt, t, cs, ctx->t_dev, &fused, nullptr);
+        });
+        const long long n_pre = ctx->launches - l0;
+        ctx->launches = l0;
+        int it = 0, outer = 0;
+        double err = 0;
+        if (!rc) rc = solve_t<T>(ctx, (T *)f->p, (const T *)ctx->w_rhs, (T *)ctx->w_r, st, &it, &err, &outer, fused, &rec);
+        if (!rc) rc = capture_into(ctx, gr, rec.deps, [&]() -> int {
+            int q = step_post_t<T>(ctx, f, dt, t, cs, ctx->t_dev, nullptr);
+            if (!q) q = step_stats_copy(ctx, cs);
+            return q;
+        });
+        const long long n_post = ctx->launches - l0;
+        ctx->launches = l0;
+        cudaGraphExec_t ex = nullptr;
+        if (!rc && cudaGraphInstantiate(&ex, gr, 0) != cudaSuccess) rc = fail(ctx, FALM_ERR_CUDA, "step graph: instantiate");
+        cudaGetLastError();
+        if (rc) {
+            cudaGraphDestroy(gr);
+            return rc;
+        }
+        ctx->step_graphs->push_back(falm_ctx::StepGraph{f->u, f->uu, f->p, f->nut, f->ff, dt, n_pre + rec.fixed + n_post, rec.per_iter, gr, ex});
+        sg = &ctx->step_graphs->back();
+    }
+    *ctx->t_host = t;
+    CK(cudaGraphLaunch(sg->exec, st));
+    CK(cudaStreamSynchronize(st));
+    const SolverScalars &sh = *ctx->scal_host;
+    ctx->launches += sg->fixed + sg->per_iter * std::max(0, sh.it_total);
+    if (sh.status == FALM_ERR_NAN) return fail(ctx, FALM_ERR_NAN, "solve: non-finite scalar");
+    return step_finish(ctx, st, out, sh.it_total, sh.err, std::max(1, sh.passes), sh.status);
+}
+
+template <typename T>
+int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_t st, falm_step_stats *out) {
+    NvtxRange whole("falm_step");
+    NvtxPhases phase;
+    int rc = ensure_work(ctx);
+    if (rc) return rc;
+    if (ctx->wait_probe_cycles > 0) {   // armed by falm_debug_arm_wait_probe: one step only
+        const long long cycles = ctx->wait_probe_cycles;
+        ctx->wait_probe_cycles = 0;
+        LAUNCH(FALM_K_OTHER, st, k_wait_probe<<<1, 32, 0, st>>>(ctx->kerr, cycles));
+    }
+    if (!ctx->op_ready) {
+        if ((rc = build_poisson(ctx, ctx->bc_kind))) return rc;
+    }
+    if (step_graph_ok<T>(ctx)) return step_graph_t<T>(ctx, f, dt, t, st, out);
+    bool fused_res = false;
+    if ((rc = step_pre_t<T>(ctx, f, dt, t, st, nullptr, &fused_res, &phase))) return rc;
+    // 4. Poisson
+    phase.next("poisson");
+    int it = 0, outer = 1;
+    double err = 0;
+    rc = solve_t<T>(ctx, (T *)f->p, (const T *)ctx->w_rhs, (T *)ctx->w_r, st, &it, &err, &outer, fused_res);
+    const int solve_status = ctx->scal_host->status;
+    if (rc) return rc;
+    if ((rc = step_post_t<T>(ctx, f, dt, t, st, nullptr, &phase))) return rc;
+    if ((rc = step_stats_copy(ctx, st))) return rc;
+    CK(cudaStreamSynchronize(st));
+    return step_finish(ctx, st, out, it, err, outer, solve_status);
 }
 
 #include "slab.cuh"
@@ -1229,6 +1503,7 @@ int falm_create(const falm_grid *grid, int precision, falm_ctx **out) {
     memset((void *)ctx, 0, sizeof(*ctx));
     ctx->last_error = new std::string();
     ctx->graphs = new std::vector<falm_ctx::SolveGraph>();
+    ctx->step_graphs = new std::vector<falm_ctx::StepGraph>();
     {
         const char *gm = getenv("FALM_B200_GRAPH");
         ctx->graph_mode = (gm && gm[0] == '0') ? 0 : ((gm && gm[0] == '1') ? 1 : -1);
@@ -1313,7 +1588,10 @@ int falm_destroy(falm_ctx *ctx) {
     delete ctx->io;   // writes the queued snapshots, then stops its thread
     graphs_clear(ctx);
     delete ctx->graphs;
+    delete ctx->step_graphs;
     if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
+    cudaFree(ctx->t_dev);
+    if (ctx->t_host) cudaFreeHost(ctx->t_host);
     cudaFree(ctx->metric_mem);
     cudaFree(ctx->op_mem);
     cudaFree(ctx->work_mem);
@@ -1348,6 +1626,7 @@ int falm_destroy(falm_ctx *ctx) {
 
 // ---------------------------------------------------------------- FalmCFD
 int falm_cfd_init(falm_ctx *ctx, double Re, int adv, int sgs, double Cs) {
+    if (ctx) graphs_clear(ctx);   // recorded steps take these settings as kernel arguments
     if (!ctx || !(Re > 0) || adv < 0 || adv > 4 || sgs < 0 || sgs > 2) return FALM_ERR_ARG;
     ctx->Re = Re; ctx->adv = adv; ctx->sgs = sgs; ctx->Cs = Cs;
     return FALM_OK;
@@ -1874,6 +2153,7 @@ int falm_io_read_cv_file(const char *path, int dims[4], double *x, double *hx, d
 
 // ---------------------------------------------------------------- boundary conditions
 int falm_bc_init(falm_ctx *ctx, int kind, double u_inlet) {
+    if (ctx) graphs_clear(ctx);   // recorded steps take these settings as kernel arguments
     if (!ctx || (kind != FALM_BC_CHANNEL && kind != FALM_BC_CAVITY)) return FALM_ERR_ARG;
     ctx->bc_kind = kind;
     ctx->u_inlet = u_inlet;
@@ -1881,6 +2161,7 @@ int falm_bc_init(falm_ctx *ctx, int kind, double u_inlet) {
 }
 
 int falm_bc_set_inflow(falm_ctx *ctx, const double *box, int nb, double dx) {
+    if (ctx) graphs_clear(ctx);   // recorded steps take these settings as kernel arguments
     if (!ctx) return FALM_ERR_ARG;
     if (ctx->inflow_box) { cudaFree(ctx->inflow_box); ctx->inflow_box = nullptr; }
     if (!box) return FALM_OK;
@@ -1961,6 +2242,7 @@ int falm_alm_build_aps(int n_station, const double *st_r, const double *st_chord
 }
 
 int falm_alm_init(falm_ctx *ctx, const falm_alm_desc *d) {
+    if (ctx) graphs_clear(ctx);   // recorded steps take these settings as kernel arguments
     if (!ctx || !d || d->n_turbine < 1 || d->n_turbine > kMaxTurbines || d->n_blade < 1 || d->n_ap_per_blade < 1 ||
         d->n_attack < 2 || !(d->euler_eps > 0) || !d->base || !d->hub || !d->tip_rate || !d->motion || !d->angle_type ||
         !d->ap_r || !d->ap_chord || !d->ap_twist || !d->attack || !d->cl || !d->cd)
@@ -2040,6 +2322,7 @@ int falm_alm_init(falm_ctx *ctx, const falm_alm_desc *d) {
 }
 
 int falm_alm_set_pitch(falm_ctx *ctx, double pitch_deg) {
+    if (ctx) graphs_clear(ctx);   // recorded steps take these settings as kernel arguments
     if (!ctx) return FALM_ERR_ARG;
     if (!ctx->alm_on) return FALM_ERR_NOALM;
     ctx->alm.pitch = pitch_deg;
@@ -2079,6 +2362,7 @@ int falm_alm_get_aps(falm_ctx *ctx, double *xyz, double *force, double *torque, 
 
 // ---------------------------------------------------------------- step
 int falm_rmcp_init(falm_ctx *ctx, const falm_rmcp_desc *d) {
+    if (ctx) graphs_clear(ctx);   // recorded steps take these settings as kernel arguments
     if (!ctx || !d || d->n_turbine < 1 || d->n_turbine > kMaxTurbines || d->n_blade < 1 || d->n_station < 1 || d->n_attack < 1 ||
         !(d->radius > 0) || !(d->blade_width > 0) || !(d->blade_thick > 0) || !d->base || !d->hub || !d->angle || !d->angle_type ||
         !d->tip_rate || !d->st_r || !d->st_chord || !d->st_twist || !d->attack || !d->cl || !d->cd)

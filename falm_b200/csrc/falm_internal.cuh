@@ -63,6 +63,8 @@ struct SolverScalars {
     int checked;        // the queued outer check of the true residual ran (mixed precision)
     int defer;          // slab mode: reduction kernels leave their local totals in red[] for a reduction
                         // over the slabs, and k_slab_derive derives the scalars from the reduced totals
+    int it_total;       // a recorded step (CUDA graph): iterations of all passes
+    int passes;         // a recorded step: passes run
 };
 
 struct AlmScalars {
@@ -193,6 +195,17 @@ struct falm_ctx {
         cudaGraphExec_t exec;
     };
     std::vector<SolveGraph> *graphs;
+    // whole steps recorded as CUDA graphs (small grids), one per set of fields and dt
+    struct StepGraph {
+        const void *u, *uu, *p, *nut, *ff;
+        double dt;
+        long long fixed, per_iter;      // kernels outside the loops, kernels per iteration
+        cudaGraph_t graph;
+        cudaGraphExec_t exec;
+    };
+    std::vector<StepGraph> *step_graphs;
+    double *t_dev;                          // the recorded step's time (device), from t_host
+    double *t_host;                         // pinned
     int graph_mode;                         // -1 small grids, 0 never, 1 always (FALM_B200_GRAPH)
     cudaStream_t cap_stream;                // stream the graphs are captured on
 };

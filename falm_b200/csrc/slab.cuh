@@ -402,7 +402,8 @@ int slab_alm_t(falm_ctx *ctx, const T *u, double t, cudaStream_t st) {
     const int csm = (ctx->geo.sx + ctx->geo.sy + ctx->geo.sz) * (int)sizeof(double);
     const int stage = csm <= 96 * 1024 ? 1 : 0;
     if (stage && csm > 32 * 1024) cudaFuncSetAttribute(k_alm_force<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
-    LAUNCH(FALM_K_ALM, st, k_alm_force<T><<<1, 256, stage ? csm : 0, st>>>(ctx->geo, ctx->alm, ctx->m64.x[0], ctx->m64.x[1], ctx->m64.x[2], u, t, stage));
+    LAUNCH(FALM_K_ALM, st, k_alm_force<T><<<1, 256, stage ? csm : 0, st>>>(ctx->geo, ctx->alm, ctx->m64.x[0], ctx->m64.x[1], ctx->m64.x[2], u, t, stage,
+                                                                            nullptr));
     const int apc = ctx->alm.apcount;
     int rc;
     for (int q = 0; q < 3 * apc; q += LocalHub::kMaxVals)
