@@ -1213,13 +1213,13 @@ int ubc_t(falm_ctx *ctx, T *u, UPrev<T> up, double dt, double t, cudaStream_t st
 // the RMCP forcing into ff over the turbines' boxes; torque and thrust sums
 // into ctx->rmcp_sums (device)
 template <typename T>
-int rmcp_run_t(falm_ctx *ctx, const T *u, T *ff, int *flag, double t, cudaStream_t st) {
+int rmcp_run_t(falm_ctx *ctx, const T *u, T *ff, int *flag, double t, cudaStream_t st, const double *t_dev = nullptr) {
     const RmcpDev &a = *ctx->rmcp;
     const long long blocks = std::max(1LL, std::min<long long>((a.bs.total + 255) / 256, (long long)ctx->sm_count * 8));
     // 2 x kMaxTurbines values per block: a quarter of the workspace's blocks
     const RedWork rw{ctx->red.partials, ctx->red.counter, ctx->red.maxBlocks / 4};
     LAUNCH(FALM_K_ALM, st, k_rmcp<T><<<(int)blocks, 256, 0, st>>>(ctx->geo, a, ctx->m64.x[0], ctx->m64.x[1], ctx->m64.x[2], u, ff, flag, t, rw,
-                                                                 ctx->rmcp_sums));
+                                                                 ctx->rmcp_sums, t_dev));
     return FALM_OK;
 }
 
@@ -1256,7 +1256,7 @@ int step_pre_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStr
         if ((rc = alm_run_t<T>(ctx, u, ff, t, st, t_dev))) return rc;
     } else if (ctx->rmcp_on) {
         ff = (T *)ctx->w_ff;
-        if ((rc = rmcp_run_t<T>(ctx, u, ff, nullptr, t, st))) return rc;
+        if ((rc = rmcp_run_t<T>(ctx, u, ff, nullptr, t, st, t_dev))) return rc;
     }
     // 2. pseudo-velocity into ua (ALM force projected in-kernel when ff == NULL)
     if (phase) phase->next("pseudo_velocity");
@@ -1384,19 +1384,21 @@ int step_finish(falm_ctx *ctx, cudaStream_t st, falm_step_stats *out, int it, do
 // loops on the device (solve_t's recording), the phases after it and the
 // copies of the results, recorded once per set of fields and dt; the time goes
 // in through device memory, written by the graph's first node from a pinned
-// host value.  Not for streamed inlet planes (a new buffer each step), the
-// RMCP forcing, z slabs, the plain solvers or an explicit matrix.
+// host value; a streamed inlet plane (falm_bc_set_inlet_plane, copied into
+// the context's fixed plane buffer before the step) makes a recording of its
+// own.  Not for z slabs, the plain solvers or an explicit matrix.
 template <typename T>
 bool step_graph_ok(const falm_ctx *ctx) {
-    return use_graph(ctx) && !ctx->slab_on && !ctx->rmcp_on && !ctx->inlet_plane_valid && ctx->wait_probe_cycles == 0 && ctx->op_ready &&
+    return use_graph(ctx) && !ctx->slab_on && ctx->wait_probe_cycles == 0 && ctx->op_ready &&
            !ctx->A_explicit && ctx->ls_type == FALM_LS_PBICGSTAB && (ctx->pc_type == FALM_LS_SOR || ctx->pc_type == FALM_LS_JACOBI);
 }
 
 template <typename T>
 int step_graph_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_t st, falm_step_stats *out) {
     falm_ctx::StepGraph *sg = nullptr;
+    const int inlet = ctx->inlet_plane_valid ? 1 : 0;
     for (auto &e : *ctx->step_graphs)
-        if (e.u == f->u && e.uu == f->uu && e.p == f->p && e.nut == f->nut && e.ff == f->ff && e.dt == dt) sg = &e;
+        if (e.u == f->u && e.uu == f->uu && e.p == f->p && e.nut == f->nut && e.ff == f->ff && e.dt == dt && e.inlet == inlet) sg = &e;
     if (!sg) {
         if (!ctx->cap_stream) CK(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
         if (!ctx->t_dev) {
@@ -1433,10 +1435,12 @@ int step_graph_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaS
             cudaGraphDestroy(gr);
             return rc;
         }
-        ctx->step_graphs->push_back(falm_ctx::StepGraph{f->u, f->uu, f->p, f->nut, f->ff, dt, n_pre + rec.fixed + n_post, rec.per_iter, gr, ex});
+        ctx->step_graphs->push_back(falm_ctx::StepGraph{f->u, f->uu, f->p, f->nut, f->ff, dt, inlet, n_pre + rec.fixed + n_post, rec.per_iter,
+                                                        gr, ex});
         sg = &ctx->step_graphs->back();
     }
     *ctx->t_host = t;
+    ctx->inlet_plane_valid = 0;   // the streamed plane serves one step
     CK(cudaGraphLaunch(sg->exec, st));
     CK(cudaStreamSynchronize(st));
     const SolverScalars &sh = *ctx->scal_host;

@@ -199,6 +199,7 @@ struct falm_ctx {
     struct StepGraph {
         const void *u, *uu, *p, *nut, *ff;
         double dt;
+        int inlet;                      // recorded with a streamed inlet plane
         long long fixed, per_iter;      // kernels outside the loops, kernels per iteration
         cudaGraph_t graph;
         cudaGraphExec_t exec;

@@ -137,8 +137,9 @@ __device__ inline void rmcp_force(const RmcpDev &a, int tid, const double (&poin
 // sums[0..kMaxTurbines) and sums[kMaxTurbines..2 kMaxTurbines).
 template <typename T>
 __global__ void __launch_bounds__(256) k_rmcp(Geom g, RmcpDev a, const double *xc, const double *yc, const double *zc,
-                                              const T *__restrict__ u, T *__restrict__ ff, int *flag, double t, RedWork rw,
-                                              double *sums) {
+                                              const T *__restrict__ u, T *__restrict__ ff, int *flag, double t_arg, RedWork rw,
+                                              double *sums, const double *t_dev) {
+    const double t = t_dev ? *t_dev : t_arg;   // a recorded step (CUDA graph) reads its time from device memory
     double acc[2 * kMaxTurbines];
 #pragma unroll
     for (int q = 0; q < 2 * kMaxTurbines; q++) acc[q] = 0.0;
