@@ -45,1439 +45,13 @@ namespace {
 
 inline cudaStream_t S(void *s) { return (cudaStream_t)s; }
 
-int fail(falm_ctx *c, int code, const char *msg) {
-    if (c && c->last_error) *c->last_error = msg;
-    return code;
-}
+#include "launch.cuh"
 
-#define CK(call)                                                                           \
-    do {                                                                                   \
-        cudaError_t _e = (call);                                                           \
-        if (_e != cudaSuccess) {                                                           \
-            if (ctx && ctx->last_error) *ctx->last_error = std::string(#call ": ") + cudaGetErrorString(_e); \
-            return (int)FALM_ERR_CUDA;                                                     \
-        }                                                                                  \
-    } while (0)
+#include "operator.cuh"
 
-#define LAUNCHED()                                                                         \
-    do {                                                                                   \
-        ctx->launches++;                                                                   \
-        cudaError_t _e = cudaGetLastError();                                               \
-        if (_e != cudaSuccess) {                                                           \
-            *ctx->last_error = std::string("launch: ") + cudaGetErrorString(_e);           \
-            return (int)FALM_ERR_CUDA;                                                     \
-        }                                                                                  \
-    } while (0)
+#include "solve.cuh"
 
-cudaEvent_t ev_get(falm_ctx *ctx) {
-    if (!ctx->ev_pool->empty()) {
-        cudaEvent_t e = ctx->ev_pool->back();
-        ctx->ev_pool->pop_back();
-        return e;
-    }
-    cudaEvent_t e = nullptr;
-    cudaEventCreate(&e);
-    return e;
-}
-
-// launch one kernel of class `cls`; with profiling on, bracket it with an event pair
-template <typename F>
-int launch_k(falm_ctx *ctx, int cls, cudaStream_t st, F &&f) {
-    cudaEvent_t a = nullptr;
-    if (ctx->profiling) {
-        a = ev_get(ctx);
-        cudaEventRecord(a, st);
-    }
-    f();
-    ctx->launches++;
-    cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess && ctx->check_sync) e = cudaStreamSynchronize(st);   // FALM_B200_CHECK=1: locate faults
-    if (e != cudaSuccess) {
-        *ctx->last_error = std::string("launch of kernel class ") + std::to_string(cls) + ": " + cudaGetErrorString(e);
-        return FALM_ERR_CUDA;
-    }
-    if (ctx->check_sync) {   // and the device error word of the kernels' self-checks
-        int w = 0;
-        if (cudaMemcpy(&w, ctx->kerr, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess && w) {
-            cudaMemset(ctx->kerr, 0, sizeof(int));
-            *ctx->last_error = std::string("kernel class ") + std::to_string(cls) + ": device error word " + std::to_string(w);
-            return w >= 200 ? FALM_ERR_ARG : FALM_ERR_TIMEOUT;
-        }
-    }
-    if (ctx->profiling) {
-        cudaEvent_t b = ev_get(ctx);
-        cudaEventRecord(b, st);
-        ctx->ev_pending->push_back(falm_ctx::EvRec{cls, a, b});
-    }
-    return FALM_OK;
-}
-
-#define LAUNCH(CLS, ST, ...)                                                                 \
-    do {                                                                                     \
-        int _lrc = launch_k(ctx, (CLS), (ST), [&] { __VA_ARGS__; });                         \
-        if (_lrc) return _lrc;                                                               \
-    } while (0)
-
-// NVTX ranges (a profiler or tracer attached through NVTX shows them; without
-// one they cost a few ns): one range per call and one per phase of the step
-struct NvtxRange {
-    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
-    ~NvtxRange() { nvtxRangePop(); }
-    NvtxRange(const NvtxRange &) = delete;
-    NvtxRange &operator=(const NvtxRange &) = delete;
-};
-struct NvtxPhases {   // consecutive ranges: next() closes the open one
-    bool open = false;
-    void next(const char *name) {
-        if (open) nvtxRangePop();
-        nvtxRangePushA(name);
-        open = true;
-    }
-    ~NvtxPhases() { if (open) nvtxRangePop(); }
-};
-
-// resident CTAs per SM of a kernel at a launch shape, looked up once per
-// kernel and shape
-template <typename K>
-int resident_per_sm(K kernel, int threads, int smem) {
-    static std::mutex mu;
-    static std::map<std::tuple<const void *, int, int>, int> known;
-    const auto key = std::make_tuple((const void *)kernel, threads, smem);
-    {
-        std::lock_guard<std::mutex> lk(mu);
-        auto it = known.find(key);
-        if (it != known.end()) return it->second;
-    }
-    if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess || n <= 0) {
-        cudaGetLastError();
-        n = 1;
-    }
-    std::lock_guard<std::mutex> lk(mu);
-    known[key] = n;
-    return n;
-}
-
-// z planes per CTA of a plane-streaming kernel: the chunk length kc in
-// [8, cap] that minimises the modelled time ceil(CTAs / resident slots) *
-// (kc + halo + 2): the CTAs run in waves of SMs x per_sm, and a CTA's time
-// grows with its planes (the halo planes included) plus a start-up of about
-// two planes.  Ties keep the longer chunk.
-int chunk_len(const falm_ctx *ctx, long long blocks_xy, int nz, int per_sm, int cap, int halo) {
-    const long long slots = (long long)ctx->sm_count * std::max(1, per_sm);
-    const int lo = std::min(8, nz), hi = std::max(lo, std::min(cap, nz));
-    int best = hi;
-    long long best_t = -1;
-    for (int kc = hi; kc >= lo; kc--) {
-        const long long ctas = blocks_xy * ((nz + kc - 1) / kc);
-        const long long t = ((ctas + slots - 1) / slots) * (kc + halo + 2);
-        if (best_t < 0 || t < best_t) { best_t = t; best = kc; }
-    }
-    return std::max(1, best);
-}
-
-// blocks along x of a face-pair kernel (blockIdx.y = pair): the largest face's
-// cells at one per thread, at most four blocks per SM
-int face_blocks(const falm_ctx *ctx) {
-    const Geom &g = ctx->geo;
-    const long long mx = std::max({(long long)g.ny * g.nz, (long long)g.nx * g.nz, (long long)g.nx * g.ny});
-    return (int)std::max(1LL, std::min((mx + 255) / 256, (long long)ctx->sm_count * 4));
-}
-
-int row_grid(const falm_ctx *ctx, const Region3 &R) {
-    long long rows = R.nrows();
-    long long need = (rows + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    long long cap = (long long)ctx->sm_count * 8;
-    return (int)std::max(1LL, std::min(need, cap));
-}
-
-// one wave of a row kernel: as many blocks as are resident at once on all SMs
-// (the kernel's occupancy, looked up once per kernel), at most one warp per row
-template <typename K>
-int row_grid_wave(const falm_ctx *ctx, const Region3 &R, K kernel) {
-    static std::mutex mu;
-    static std::unordered_map<const void *, int> per_sm_of;
-    int per_sm = 0;
-    {
-        std::lock_guard<std::mutex> lk(mu);
-        auto it = per_sm_of.find((const void *)kernel);
-        if (it != per_sm_of.end()) per_sm = it->second;
-    }
-    if (per_sm <= 0) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kRowThreads, 0) != cudaSuccess || per_sm <= 0) {
-            cudaGetLastError();
-            return row_grid(ctx, R);
-        }
-        std::lock_guard<std::mutex> lk(mu);
-        per_sm_of[(const void *)kernel] = per_sm;
-    }
-    const long long need = ((long long)R.nrows() + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    return (int)std::max(1LL, std::min(need, (long long)ctx->sm_count * per_sm));
-}
-
-template <typename T> MetricView<T> mview(const falm_ctx *ctx);
-template <> MetricView<double> mview<double>(const falm_ctx *ctx) { return MetricView<double>{ctx->m64}; }
-template <> MetricView<float> mview<float>(const falm_ctx *ctx) { return MetricView<float>{ctx->m32}; }
-
-template <typename T> Op7<T> op7(const falm_ctx *ctx);
-template <> Op7<double> op7<double>(const falm_ctx *ctx) { return Op7<double>{ctx->pt64, (const double *)ctx->A_explicit, ctx->geo.n}; }
-template <> Op7<float> op7<float>(const falm_ctx *ctx) { return Op7<float>{ctx->pt32, (const float *)ctx->A_explicit, ctx->geo.n}; }
-
-int ensure_work(falm_ctx *ctx) {
-    if (ctx->work_mem) return FALM_OK;
-    const size_t n = (size_t)ctx->geo.n, e = ctx->esize;
-    const int nvec = 12;   // rr p q s pp ss t r rhs div xp + ua(3)
-    size_t outlet = 9ull * ctx->geo.sy * ctx->geo.sz;
-    size_t bytes = ((size_t)(nvec + 2) * n + outlet) * e + 256 * 16;
-    void *mem = nullptr;
-    if (cudaMalloc(&mem, bytes) != cudaSuccess) { cudaGetLastError(); return fail(ctx, FALM_ERR_ALLOC, "work vectors: cudaMalloc failed"); }
-    if (cudaMemset(mem, 0, bytes) != cudaSuccess) return fail(ctx, FALM_ERR_CUDA, "work vectors: cudaMemset failed");
-    char *p = (char *)mem;
-    auto take = [&](size_t count) { void *r = p; p += ((count * e + 255) / 256) * 256; return r; };
-    ctx->w_rr = take(n); ctx->w_p = take(n); ctx->w_q = take(n); ctx->w_s = take(n);
-    ctx->w_pp = take(n); ctx->w_ss = take(n); ctx->w_t = take(n); ctx->w_r = take(n);
-    ctx->w_rhs = take(n); ctx->w_div = take(n); ctx->w_xp = take(n);
-    ctx->w_ua = take(3 * n);
-    ctx->w_outlet = take(outlet);
-    ctx->work_mem = mem;
-    return FALM_OK;
-}
-
-// ---------------------------------------------------------------- TMA tensor maps
-PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
-
-bool tma_encode_available() {
-    static int state = -1;
-    if (state < 0) {
-        cudaDriverEntryPointQueryResult q;
-        void *fn = nullptr;
-        state = (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
-                 q == cudaDriverEntryPointSuccess && fn)
-                    ? 1 : 0;
-        cudaGetLastError();
-        g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
-    }
-    return state == 1;
-}
-
-// 4D map (x, y, z, component) of a field in the reference layout with a
-// (bx, by, 1, ncomp) box.  TMA needs a 16 B aligned base and row pitch; the
-// caller falls back to the row kernels otherwise.
-template <typename T>
-bool make_map(const falm_ctx *ctx, CUtensorMap *m, const T *base, int ncomp, int bx, int by) {
-    const Geom &g = ctx->geo;
-    const size_t e = sizeof(T);   // the field's own type (a mixed context also runs FP64 vectors)
-    // every box lies inside the tensor: x and y at least one box long (the
-    // kernels clamp the box origins), x rows a whole number of 16-byte units
-    // (the kernels' box x origins are 16-byte aligned for gc = 2)
-    if (!tma_encode_available() || ((uintptr_t)base & 15) || ((g.sx * e) & 15) || g.sx < bx || g.sy < by || g.gc != 2) return false;
-    cuuint64_t dims[4] = {(cuuint64_t)g.sx, (cuuint64_t)g.sy, (cuuint64_t)g.sz, (cuuint64_t)ncomp};
-    cuuint64_t strides[3] = {(cuuint64_t)(g.sx * e), (cuuint64_t)(g.sx * (size_t)g.sy * e), (cuuint64_t)(g.n * e)};
-    cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, 1, (cuuint32_t)ncomp};
-    cuuint32_t es[4] = {1, 1, 1, 1};
-    CUresult r = g_encode(m, e == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, (void *)base,
-                          dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    return r == CUDA_SUCCESS;
-}
-
-// 7-point scalar stencil over the interior through the TMA plane stream;
-// returns 1 when launched, 0 when the operand is not TMA-eligible (the caller
-// then uses its row kernel), <0 on a launch error.
-template <typename T, int NV, class Body>
-int s7_launch(falm_ctx *ctx, int cls, cudaStream_t st, const T *x, const Body &body) {
-    CUtensorMap m;
-    if (ctx->no_tma || !make_map(ctx, &m, x, 1, S7Tile<T>::BX, S7Tile<T>::BY)) return 0;
-    const Geom &g = ctx->geo;
-    const int bx = (g.nx + S7Tile<T>::TX - 1) / S7Tile<T>::TX, by = (g.ny + S7Tile<T>::TY - 1) / S7Tile<T>::TY;
-    const int kc = chunk_len(ctx, (long long)bx * by, g.nz, resident_per_sm(k_s7_tma<T, NV, Body>, 256, s7_smem<T>()), 64, 2);
-    dim3 grid(bx, by, (g.nz + kc - 1) / kc);
-    if ((long long)grid.x * grid.y * grid.z > ctx->red.maxBlocks) return 0;
-    if (s7_smem<T>() > 48 * 1024) cudaFuncSetAttribute(k_s7_tma<T, NV, Body>, cudaFuncAttributeMaxDynamicSharedMemorySize, s7_smem<T>());
-    int rc = launch_k(ctx, cls, st, [&] {
-        k_s7_tma<T, NV, Body><<<grid, 256, s7_smem<T>(), st>>>(g, kc, m, body, ctx->red, ctx->kerr);
-    });
-    return rc ? -rc : 1;
-}
-
-#define S7_OR(CLS, ST, T_, NV_, X_, BODY_, ROWLAUNCH)                                     \
-    do {                                                                                   \
-        int _s7 = s7_launch<T_, NV_>(ctx, (CLS), (ST), (X_), BODY_);                       \
-        if (_s7 < 0) return -_s7;                                                          \
-        if (_s7 == 0) LAUNCH((CLS), (ST), ROWLAUNCH);                                      \
-    } while (0)
-
-// H consecutive red-black half sweeps (first colour c1) in one pass, x_in -> x_out;
-// 1 launched, 0 not eligible, <0 launch error
-template <typename T, int H>
-int sor_rb_launch_h(falm_ctx *ctx, cudaStream_t st, const T *xin, const T *b, T *xout, T omega, int c1, const SolverScalars *sc) {
-    using L = RBTile<T, H>;
-    if (ctx->no_tma || ctx->A_explicit) return 0;
-    CUtensorMap mx, mb;
-    if (!make_map(ctx, &mx, xin, 1, L::BX, L::BY) || !make_map(ctx, &mb, b, 1, L::BX, L::BY)) return 0;
-    const Geom &g = ctx->geo;
-    const int bx = (g.nx + L::TX - 1) / L::TX, by = (g.ny + L::TY - 1) / L::TY;
-    const int kc = chunk_len(ctx, (long long)bx * by, g.nz, resident_per_sm(k_sor_rb_tma<T, H>, 256, L::SMEM), 64, 2 * H);
-    dim3 grid(bx, by, (g.nz + kc - 1) / kc);
-    cudaFuncSetAttribute(k_sor_rb_tma<T, H>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
-    const PoissonTables<T> tb = op7<T>(ctx).t;
-    int rc = launch_k(ctx, FALM_K_SOR, st, [&] {
-        k_sor_rb_tma<T, H><<<grid, 256, L::SMEM, st>>>(g, kc, mx, mb, tb, xout, omega, c1, sc, ctx->kerr);
-    });
-    return rc ? -rc : 1;
-}
-
-// three FP32 half sweeps on the 28 x 16 tile; 1 launched, 0 not eligible, <0 launch error
-template <typename T>
-int sor_rb2_launch(falm_ctx *ctx, cudaStream_t st, const T *xin, const T *b, T *xout, T omega, int c1, const SolverScalars *sc) {
-    using L = RB2Tile<T>;
-    if (ctx->no_tma || ctx->A_explicit) return 0;
-    CUtensorMap mx, mb;
-    if (!make_map(ctx, &mx, xin, 1, L::BX, L::BY) || !make_map(ctx, &mb, b, 1, L::BXB, L::BYB)) return 0;
-    const Geom &g = ctx->geo;
-    const int bx = (g.nx + L::TX - 1) / L::TX, by = (g.ny + L::TY - 1) / L::TY;
-    // a CTA runs kc + 3H iterations and stages at most ZMAX planes of z coefficients
-    const int kc = chunk_len(ctx, (long long)bx * by, g.nz, resident_per_sm(k_sor_rb2_tma<T>, L::NT, L::SMEM),
-                             std::min(64, L::ZMAX - 2 * L::H), 3 * L::H);
-    dim3 grid(bx, by, (g.nz + kc - 1) / kc);
-    cudaFuncSetAttribute(k_sor_rb2_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
-    const PoissonTables<T> tb = op7<T>(ctx).t;
-    int rc = launch_k(ctx, FALM_K_SOR, st, [&] {
-        k_sor_rb2_tma<T><<<grid, L::NT, L::SMEM, st>>>(g, kc, mx, mb, tb, xout, omega, c1, sc, ctx->kerr);
-    });
-    return rc ? -rc : 1;
-}
-
-template <typename T>
-int sor_rb_launch(falm_ctx *ctx, cudaStream_t st, int H, const T *xin, const T *b, T *xout, T omega, int c1, const SolverScalars *sc) {
-    // the blocked kernels take the colour parity of local plane indices: a grid
-    // whose planes are offset by koff flips the first colour instead
-    c1 ^= ctx->geo.koff & 1;
-    if constexpr (sizeof(T) == 4) {
-        if (H == 3 && !ctx->sor_v1) {
-            const int r = sor_rb2_launch<T>(ctx, st, xin, b, xout, omega, c1, sc);
-            if (r != 0) return r;
-        }
-    }
-    if (H == 1) return sor_rb_launch_h<T, 1>(ctx, st, xin, b, xout, omega, c1, sc);
-    if (H == 2) return sor_rb_launch_h<T, 2>(ctx, st, xin, b, xout, omega, c1, sc);
-    return sor_rb_launch_h<T, 3>(ctx, st, xin, b, xout, omega, c1, sc);
-}
-
-// the conditions of make_map for a context vector (256-byte aligned) of element size e
-bool map_ok(const falm_ctx *ctx, size_t e, int bx, int by) {
-    const Geom &g = ctx->geo;
-    return tma_encode_available() && ((g.sx * e) & 15) == 0 && g.sx >= bx && g.sy >= by && g.gc == 2;
-}
-
-// whether sor_rb_launch runs an H-half-sweep blocked pass on the context's vectors
-// (1) or declines (0), decided without a launch
-template <typename T>
-bool sor_pass_ok(const falm_ctx *ctx, int H) {
-    if (ctx->no_tma || ctx->A_explicit) return false;
-    const size_t e = sizeof(T);
-    if constexpr (sizeof(T) == 4) {
-        using L2 = RB2Tile<T>;
-        if (H == 3 && !ctx->sor_v1 && map_ok(ctx, e, L2::BX, L2::BY) && map_ok(ctx, e, L2::BXB, L2::BYB)) return true;
-    }
-    if (H == 1) return map_ok(ctx, e, RBTile<T, 1>::BX, RBTile<T, 1>::BY);
-    if (H == 2) return map_ok(ctx, e, RBTile<T, 2>::BX, RBTile<T, 2>::BY);
-    return map_ok(ctx, e, RBTile<T, 3>::BX, RBTile<T, 3>::BY);
-}
-
-// Whether the preconditioner's pointwise first sweep writes the work vector xp
-// rather than its target z: the sweeps after it that run out of place (Jacobi
-// sweeps 2..m; blocked SOR passes) alternate between xp and z, so an odd
-// number of them starts from xp and the last one lands in z.  The buffers of
-// an application are then the same at every iteration.
-template <typename T>
-bool pc_first_in_xp(const falm_ctx *ctx) {
-    const int m = ctx->pc_maxit;
-    if (ctx->pc_type == FALM_LS_JACOBI) return ((m - 1) & 1) != 0;
-    if (ctx->pc_type != FALM_LS_SOR) return false;
-    int passes = 0;
-    for (int hs = 1; hs < 2 * m;) {
-        const int H = std::min(3, 2 * m - hs);
-        if (!sor_pass_ok<T>(ctx, H)) break;
-        passes++;
-        hs += H;
-    }
-    return (passes & 1) != 0;
-}
-
-// ring depth of the multi-field plane stream: keep >= 2 planes in flight and
-// at least two CTAs per SM
-template <typename T, int NF> struct P3Conf { static constexpr int NS = NF > 1 ? 4 : 6; };
-
-// multi-field radius-1 plane stream over region R (see plane3_tma.cuh);
-// 1 launched, 0 not eligible (row-kernel fallback), <0 launch error
-template <typename T, int NF, int NV, class Body>
-int p3_launch(falm_ctx *ctx, int cls, cudaStream_t st, const Region3 &R, int org, const void *const (&ptr)[NF],
-              const int (&ncomp)[NF], const Body &body) {
-    if (ctx->no_tma) return 0;
-    using L = P3Layout<T, NF>;
-    constexpr int NS = P3Conf<T, NF>::NS;
-    MapSet<NF> maps;
-    int slot = 0;
-    for (int f = 0; f < NF; f++) {
-        if (!make_map(ctx, &maps.m[f], (const T *)ptr[f], ncomp[f], L::BX, L::BY)) return 0;
-        maps.ncomp[f] = ncomp[f];
-        slot += ncomp[f] * L::FB;
-    }
-    // the kernel lays the slot out from the body's component counts
-    if (slot != (Body::NC0 + Body::NC1) * L::FB) return -fail(ctx, FALM_ERR_ARG, "plane stream: field components do not match the body");
-    const int smem = NS * slot + 256;
-    const int bx = (R.i1 - R.i0 + L::TX - 1) / L::TX, by = (R.j1 - R.j0 + L::TY - 1) / L::TY;
-    auto kern = k_plane3_tma<T, NF, NS, NV, Body>;
-    const int kc = chunk_len(ctx, (long long)bx * by, R.k1 - R.k0, resident_per_sm(kern, 256, smem), 64, 2);
-    dim3 grid(bx, by, (R.k1 - R.k0 + kc - 1) / kc);
-    if ((long long)grid.x * grid.y * grid.z > ctx->red.maxBlocks) return 0;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    int rc = launch_k(ctx, cls, st, [&] { kern<<<grid, 256, smem, st>>>(ctx->geo, R, org, kc, maps, body, ctx->red, ctx->kerr); });
-    return rc ? -rc : 1;
-}
-
-#define P3_OR(CLS, ST, T_, NF_, NV_, R_, ORG_, PTRS_, NCOMP_, BODY_, ROWLAUNCH)            \
-    do {                                                                                   \
-        const void *const _pp[NF_] = PTRS_;                                                \
-        const int _nc[NF_] = NCOMP_;                                                       \
-        int _p3 = p3_launch<T_, NF_, NV_>(ctx, (CLS), (ST), (R_), (ORG_), _pp, _nc, BODY_);\
-        if (_p3 < 0) return -_p3;                                                          \
-        if (_p3 == 0) LAUNCH((CLS), (ST), ROWLAUNCH);                                      \
-    } while (0)
-#define FB_ARR(...) {__VA_ARGS__}
-
-// Build the separable Poisson tables.  For a Cartesian control volume
-//   0.5*(g_d(c) + g_d(c+e_d))/ja(c)  with g_d = ja*kx_d^2
-// depends on the index along d only; the table entry is evaluated with the
-// reference's arithmetic (src/falm.h:394-400, app/nedo/main.cpp:43-83) at the
-// cell (i, gc, gc) (resp. (gc, j, gc), (gc, gc, k)).  A dropped (Neumann)
-// coefficient is stored as 0.
-int build_poisson(falm_ctx *ctx, int kind) {
-    const Geom &g = ctx->geo;
-    const std::vector<double> *h[3] = {ctx->hx, ctx->hy, ctx->hz};
-    const int s[3] = {g.sx, g.sy, g.sz};
-    std::vector<double> up[3], um[3];
-    double maxdiag = 0.0;
-    auto gmet = [&](int d, int i, int j, int k) {
-        double vol = (*h[0])[i] * (*h[1])[j] * (*h[2])[k];
-        int id = d == 0 ? i : (d == 1 ? j : k);
-        double kd = 1.0 / (*h[d])[id];
-        return vol * kd * kd;
-    };
-    for (int d = 0; d < 3; d++) {
-        up[d].assign(s[d], 0.0);
-        um[d].assign(s[d], 0.0);
-        for (int q = g.gc; q < s[d] - g.gc; q++) {
-            int c[3] = {g.gc, g.gc, g.gc};
-            c[d] = q;
-            int cp[3] = {c[0], c[1], c[2]}, cm[3] = {c[0], c[1], c[2]};
-            cp[d] += 1; cm[d] -= 1;
-            double jac = (*h[0])[c[0]] * (*h[1])[c[1]] * (*h[2])[c[2]];
-            double gc0 = gmet(d, c[0], c[1], c[2]);
-            double coef_p = 0.5 * (gc0 + gmet(d, cp[0], cp[1], cp[2])) / jac;
-            double coef_m = 0.5 * (gc0 + gmet(d, cm[0], cm[1], cm[2])) / jac;
-            // app/nedo/main.cpp:55 keeps the x+ coefficient (p = 0 guide cell); every other
-            // physical face is Neumann (:60-83, app/lid3d/main.cpp:52-80); a slab interface
-            // keeps its coefficients (the neighbour's plane lies beyond it)
-            int plus_limit = (d == 0 && kind == FALM_BC_CHANNEL) ? s[d] - g.gc : s[d] - g.gc - 1;
-            if (d == 2 && !(g.zphys & 2)) plus_limit = s[d] - g.gc;
-            if (q < plus_limit) up[d][q] = coef_p;
-            if (q > g.gc || (d == 2 && !(g.zphys & 1))) um[d][q] = coef_m;
-        }
-    }
-    // maxdiag over the interior: |ac| is separable as well, but take the
-    // exact maximum of the reference's accumulation order
-    for (int k = g.gc; k < g.sz - g.gc; k++)
-        for (int j = g.gc; j < g.sy - g.gc; j++)
-            for (int i = g.gc; i < g.sx - g.gc; i++) {
-                double ac = ((((-up[0][i]) - um[0][i]) - up[1][j]) - um[1][j] - up[2][k]) - um[2][k];
-                maxdiag = std::max(maxdiag, std::fabs(ac));
-            }
-    if (ctx->slab_on && ctx->slab_nranks > 1) {
-        // the maximum over the slabs (a collective: every rank builds its operator)
-        double *d = nullptr;
-        if (cudaMalloc(&d, sizeof(double)) != cudaSuccess) { cudaGetLastError(); return fail(ctx, FALM_ERR_ALLOC, "poisson: maxdiag"); }
-        int rc = cudaMemcpy(d, &maxdiag, sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess ? FALM_OK : FALM_ERR_CUDA;
-        if (!rc) rc = ctx->transport.allreduce(ctx->transport.user, d, 1, FALM_REDUCE_MAX, nullptr);
-        if (!rc && (cudaMemcpy(&maxdiag, d, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)) rc = FALM_ERR_CUDA;
-        cudaFree(d);
-        if (rc) { cudaGetLastError(); return fail(ctx, rc, "poisson: maxdiag over the slabs"); }
-    }
-    double scale = 1.0 / maxdiag;
-    // layout: for each d: cm, cp, um, up (s[d] each), then dx0 (sx)
-    size_t tot = 0;
-    for (int d = 0; d < 3; d++) tot += 4 * (size_t)s[d];
-    tot += g.sx;
-    std::vector<double> h64(tot);
-    std::vector<float> h32(tot);
-    size_t off = 0;
-    size_t o_cm[3], o_cp[3], o_um[3], o_up[3], o_dx0;
-    for (int d = 0; d < 3; d++) {
-        o_cm[d] = off; for (int q = 0; q < s[d]; q++) h64[off + q] = um[d][q] * scale; off += s[d];
-        o_cp[d] = off; for (int q = 0; q < s[d]; q++) h64[off + q] = up[d][q] * scale; off += s[d];
-        o_um[d] = off; for (int q = 0; q < s[d]; q++) h64[off + q] = um[d][q]; off += s[d];
-        o_up[d] = off; for (int q = 0; q < s[d]; q++) h64[off + q] = up[d][q]; off += s[d];
-    }
-    o_dx0 = off;
-    for (int q = 0; q < g.sx; q++) h64[off + q] = (-up[0][q]) - um[0][q];
-    off += g.sx;
-    for (size_t q = 0; q < tot; q++) h32[q] = (float)h64[q];
-    if (ctx->op_mem) { cudaFree(ctx->op_mem); ctx->op_mem = nullptr; }
-    void *mem = nullptr;
-    if (cudaMalloc(&mem, tot * (sizeof(double) + sizeof(float))) != cudaSuccess) { cudaGetLastError(); return fail(ctx, FALM_ERR_ALLOC, "poisson tables"); }
-    double *d64 = (double *)mem;
-    float *d32 = (float *)(d64 + tot);
-    if (cudaMemcpy(d64, h64.data(), tot * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(d32, h32.data(), tot * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
-        return fail(ctx, FALM_ERR_CUDA, "poisson tables copy");
-    ctx->op_mem = mem;
-    for (int d = 0; d < 3; d++) {
-        ctx->pt64.cm[d] = d64 + o_cm[d]; ctx->pt64.cp[d] = d64 + o_cp[d]; ctx->pt64.um[d] = d64 + o_um[d]; ctx->pt64.up[d] = d64 + o_up[d];
-        ctx->pt32.cm[d] = d32 + o_cm[d]; ctx->pt32.cp[d] = d32 + o_cp[d]; ctx->pt32.um[d] = d32 + o_um[d]; ctx->pt32.up[d] = d32 + o_up[d];
-    }
-    ctx->pt64.dx0 = d64 + o_dx0; ctx->pt32.dx0 = d32 + o_dx0;
-    ctx->pt64.scale = scale; ctx->pt32.scale = (float)scale;
-    ctx->pt64.koff = ctx->pt32.koff = g.koff;
-    ctx->maxdiag = maxdiag;
-    ctx->op_ready = 1;
-    ctx->bc_kind_op = kind;
-    // the coefficient of cell q towards q+1 equals that of q+1 towards q on every
-    // axis (uniform spacing): the operator is symmetric over the interior
-    ctx->op_symmetric = 1;
-    for (int d = 0; d < 3; d++)
-        for (int q = g.gc; q + 1 < s[d] - g.gc; q++)
-            if (std::fabs(up[d][q] - um[d][q + 1]) > 1e-13 * std::fabs(up[d][q])) ctx->op_symmetric = 0;
-    return FALM_OK;
-}
-
-// ---------------------------------------------------------------- solver driver
-// solver scalars at the start of a solve
-int solver_init(falm_ctx *ctx, cudaStream_t st) {
-    const Geom &g = ctx->geo;
-    SolverScalars init;
-    memset(&init, 0, sizeof(init));
-    init.gsize = (double)g.nx * g.ny * g.nzg;   // interior cells of the whole grid (of all slabs)
-    init.tol = ctx->tol;
-    init.maxit = ctx->maxit;
-    CK(cudaMemcpyAsync(ctx->scal, &init, sizeof(init), cudaMemcpyHostToDevice, st));
-    return FALM_OK;
-}
-
-// The plain solvers of FalmEq::Solve (src/FalmEq.h:56-64): Jacobi
-// (src/FalmEq.cpp:80-127) and red-black SOR (:173-240, the Black half sweep then
-// the Red one, with the solver's relaxation factor).  Each iteration ends with
-// the residual r = b - A x and the loop test (k_res_plain).  Iterations are
-// queued in batches of 1, 2, 4, 8, 8, ... between host checks of the stop
-// flag, and every kernel of an iteration queued after the stop returns at once.
-// Jacobi alternates between x and the work vector xp instead of copying x to
-// xp each iteration: after one copy of x (ghosts included) the ghost cells of
-// both agree, iteration n reads {x, xp}[n % 2] and writes the other, and an odd
-// final count copies the result back into x.
-template <typename T>
-int plain_solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out, double *err_out, int *outer_out) {
-    int rc = solver_init(ctx, st);
-    if (rc) return rc;
-    const Geom &g = ctx->geo;
-    const Region3 R = interior(g);
-    const int grid = row_grid(ctx, R);
-    const Op7<T> op = op7<T>(ctx);
-    SolverScalars *sc = ctx->scal;
-    T *xp = (T *)ctx->w_xp;
-    const bool jac = ctx->ls_type == FALM_LS_JACOBI;
-    const T w = (T)ctx->relax;
-    if (jac) CK(cudaMemcpyAsync(xp, x, (size_t)g.n * sizeof(T), cudaMemcpyDeviceToDevice, st));
-    int batch = 1, queued = 0;
-    for (int n = 0;; n++) {
-        T *dst = x;
-        if (jac) {
-            const T *src = (n & 1) ? xp : x;
-            dst = (n & 1) ? x : xp;
-            LAUNCH(FALM_K_SOR, st, k_jacobi<T><<<grid, kRowThreads, 0, st>>>(g, R, op, dst, src, b, sc));
-        } else {
-            for (int color = 0; color < 2; color++)
-                S7_OR(FALM_K_SOR, st, T, 0, x, (SorBody<T>{op, x, b, w, color, sc}),
-                      (k_sor<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, w, color, sc)));
-        }
-        LAUNCH(FALM_K_RES, st, k_res_plain<T><<<grid, kRowThreads, 0, st>>>(g, R, op, dst, b, r, ctx->red, sc));
-        if (++queued < batch) continue;
-        CK(cudaMemcpyAsync(ctx->scal_host, sc, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        if (ctx->scal_host->done) break;
-        queued = 0;
-        batch = std::min(2 * batch, 8);
-    }
-    const int it = ctx->scal_host->it;
-    if (jac && (it & 1)) CK(cudaMemcpyAsync(x, xp, (size_t)g.n * sizeof(T), cudaMemcpyDeviceToDevice, st));
-    if (it_out) *it_out = it;
-    if (err_out) *err_out = ctx->scal_host->err;
-    if (outer_out) *outer_out = 1;
-    return ctx->scal_host->status == FALM_ERR_NAN ? fail(ctx, FALM_ERR_NAN, "solve: non-finite residual") : FALM_OK;
-}
-
-// ---------------------------------------------------------------- device-side BiCGStab loop
-// A pass's iterations as one CUDA graph: iterations 0 and 1 of the pass, then
-// a conditional while node whose body is one later iteration; the last kernel
-// of the prefix and of the body sets the loop condition from the solver's done
-// flag (convergence, maxit, breakdown or a non-finite scalar), so the loop ends
-// on the device within maxit iterations.  Graphs are kept per solve signature
-// (vectors, element type, whether the first preconditioner sweep is ready) and
-// dropped when the solver settings or the operator change.  Used where launch
-// and host-synchronisation latency dominate: grids of at most kGraphCells
-// interior cells (FALM_B200_GRAPH=1 / 0 forces it on / off), never while
-// profiling or checking launches one by one.
-constexpr long long kGraphCells = 1ll << 22;
-constexpr int kMixedPassIts = 50;   // FP32 BiCGStab iterations between FP64 true-residual checks
-
-bool use_graph(const falm_ctx *ctx) {
-    if (ctx->profiling || ctx->check_sync || ctx->graph_mode == 0) return false;
-    return ctx->graph_mode == 1 || (long long)ctx->geo.nx * ctx->geo.ny * ctx->geo.nz <= kGraphCells;
-}
-
-__global__ void k_graph_continue(const SolverScalars *sc, cudaGraphConditionalHandle h) {
-    cudaGraphSetConditional(h, sc->done ? 0u : 1u);
-}
-
-// drop every recorded loop and step (the settings they were recorded with changed)
-void graphs_clear(falm_ctx *ctx) {
-    if (ctx->graphs) {
-        for (auto &e : *ctx->graphs) {
-            cudaGraphExecDestroy(e.exec);
-            cudaGraphDestroy(e.graph);
-        }
-        ctx->graphs->clear();
-    }
-    if (ctx->step_graphs) {
-        for (auto &e : *ctx->step_graphs) {
-            cudaGraphExecDestroy(e.exec);
-            cudaGraphDestroy(e.graph);
-        }
-        ctx->step_graphs->clear();
-    }
-}
-
-// ---- recording on the device: the solver control the host loop does otherwise
-// the scalars of a solve's start (solver_init on the device)
-__global__ void k_solver_init(SolverScalars *sc, double gsize, double tol, int maxit) {
-    SolverScalars z;
-    memset(&z, 0, sizeof(z));
-    z.gsize = gsize;
-    z.tol = tol;
-    z.maxit = maxit;
-    *sc = z;
-}
-// a pass has ended: its iterations into the totals
-__global__ void k_pass_end(SolverScalars *sc) {
-    sc->it_total += sc->it;
-    sc->passes += 1;
-}
-// a new pass: iteration count zero, the pass's limit
-__global__ void k_pass_reset(SolverScalars *sc, int maxit) {
-    sc->it = 0;
-    sc->maxit = maxit;
-}
-// after the FP64 check of a mixed pass: another pass while the true residual
-// misses the tolerance and passes remain (a breakdown's status is cleared: the
-// pass restarts from the true residual); non-finite data ends the solve (done)
-__global__ void k_outer_cond(SolverScalars *sc, cudaGraphConditionalHandle h, int max_passes) {
-    const bool more = !sc->done && sc->passes < max_passes;
-    if (more) sc->status = FALM_OK;
-    cudaGraphSetConditional(h, more ? 1u : 0u);
-}
-
-// the recording stream's current leaf nodes after fn's launches on it, which go
-// into `graph` after `deps` (deps becomes the new leaves)
-int capture_into(falm_ctx *ctx, cudaGraph_t graph, std::vector<cudaGraphNode_t> &deps, const std::function<int()> &fn) {
-    const cudaStream_t cs = ctx->cap_stream;
-    if (cudaStreamBeginCaptureToGraph(cs, graph, deps.empty() ? nullptr : deps.data(), nullptr, deps.size(),
-                                      cudaStreamCaptureModeRelaxed) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(ctx, FALM_ERR_CUDA, "graph: begin capture");
-    }
-    int rc = fn();
-    cudaStreamCaptureStatus stt;
-    const cudaGraphNode_t *d = nullptr;
-    size_t nd = 0;
-    std::vector<cudaGraphNode_t> leaves;
-    if (cudaStreamGetCaptureInfo(cs, &stt, nullptr, nullptr, &d, &nd) == cudaSuccess && d) leaves.assign(d, d + nd);
-    cudaGraph_t got = nullptr;
-    const cudaError_t e = cudaStreamEndCapture(cs, &got);
-    cudaGetLastError();
-    if (!rc && (e != cudaSuccess || got != graph)) rc = fail(ctx, FALM_ERR_CUDA, "graph: end capture");
-    if (!rc && !leaves.empty()) deps = leaves;
-    return rc;
-}
-
-// a conditional while node after deps (deps becomes the node); its body graph in *body
-int add_while(falm_ctx *ctx, cudaGraph_t graph, std::vector<cudaGraphNode_t> &deps, cudaGraphConditionalHandle h, cudaGraph_t *body) {
-    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};   // every other byte zero
-    cp.conditional.handle = h;
-    cp.conditional.type = cudaGraphCondTypeWhile;
-    cp.conditional.size = 1;
-    cudaGraphNode_t node;
-    if (cudaGraphAddNode(&node, graph, deps.empty() ? nullptr : deps.data(), deps.size(), &cp) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(ctx, FALM_ERR_CUDA, "graph: while node");
-    }
-    deps.assign(1, node);
-    *body = cp.conditional.phGraph_out[0];
-    return FALM_OK;
-}
-
-// a solve recorded into a graph after deps (see solve_t); counts the kernels
-// recorded outside and inside the iteration loops
-struct SolveRec {
-    cudaGraph_t graph;
-    std::vector<cudaGraphNode_t> deps;
-    long long fixed = 0, per_iter = 0;
-};
-
-// the graph of a pass (built on first use: emit(itp) launches iteration itp's
-// kernels on `ist`, which points at the capture stream meanwhile); prefix and
-// per_iter: kernel launches of iterations 0-1 and of one later iteration
-int solve_graph(falm_ctx *ctx, const void *x, const void *b, const void *r, int esize, int pp_ready,
-                const std::function<int(int)> &emit, cudaStream_t &ist, cudaGraphExec_t *out, int *prefix, int *per_iter) {
-    for (auto &e : *ctx->graphs)
-        if (e.x == x && e.b == b && e.r == r && e.w0 == ctx->w_rr && e.A == ctx->A_explicit && e.esize == esize && e.pp_ready == pp_ready) {
-            *out = e.exec; *prefix = e.prefix; *per_iter = e.per_iter;
-            return FALM_OK;
-        }
-    if (!ctx->cap_stream) CK(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
-    cudaGraph_t gr = nullptr;
-    CK(cudaGraphCreate(&gr, 0));
-    cudaGraphConditionalHandle h;
-    cudaGraphExec_t ex = nullptr;
-    const cudaStream_t saved = ist;
-    ist = ctx->cap_stream;
-    // capture iterations first..last and the condition kernel into `into`
-    auto capture = [&](cudaGraph_t into, int first, int last, int *count) -> int {
-        if (cudaStreamBeginCaptureToGraph(ist, into, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
-            return fail(ctx, FALM_ERR_CUDA, "solve graph: capture");
-        const long long l0 = ctx->launches;
-        int crc = FALM_OK;
-        for (int itp = first; itp <= last && !crc; itp++) crc = emit(itp);
-        if (!crc) {
-            k_graph_continue<<<1, 1, 0, ist>>>(ctx->scal, h);
-            if (cudaGetLastError() != cudaSuccess) crc = fail(ctx, FALM_ERR_CUDA, "solve graph: condition kernel");
-        }
-        *count = (int)(ctx->launches - l0);
-        ctx->launches = l0;
-        cudaGraph_t got = nullptr;
-        const cudaError_t e = cudaStreamEndCapture(ist, &got);
-        if (!crc && (e != cudaSuccess || got != into)) crc = fail(ctx, FALM_ERR_CUDA, "solve graph: end of capture");
-        cudaGetLastError();
-        return crc;
-    };
-    int rc = FALM_OK, np = 0, nb = 0;
-    if (cudaGraphConditionalHandleCreate(&h, gr, 1, cudaGraphCondAssignDefault) != cudaSuccess) rc = fail(ctx, FALM_ERR_CUDA, "solve graph: handle");
-    if (!rc) rc = capture(gr, 0, 1, &np);
-    if (!rc) {
-        // the loop follows the prefix's last node(s)
-        size_t nn = 0, ne = 0;
-        cudaGraphGetNodes(gr, nullptr, &nn);
-        std::vector<cudaGraphNode_t> nodes(nn);
-        if (nn) cudaGraphGetNodes(gr, nodes.data(), &nn);
-        cudaGraphGetEdges(gr, nullptr, nullptr, &ne);
-        std::vector<cudaGraphNode_t> from(ne), to(ne);
-        if (ne) cudaGraphGetEdges(gr, from.data(), to.data(), &ne);
-        std::vector<cudaGraphNode_t> leaves;
-        for (auto nd : nodes)
-            if (std::find(from.begin(), from.end(), nd) == from.end()) leaves.push_back(nd);
-        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};   // every other byte zero
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = h;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        cudaGraphNode_t cn;
-        if (cudaGraphAddNode(&cn, gr, leaves.data(), leaves.size(), &cp) != cudaSuccess) rc = fail(ctx, FALM_ERR_CUDA, "solve graph: loop node");
-        else rc = capture(cp.conditional.phGraph_out[0], 2, 2, &nb);
-    }
-    if (!rc && cudaGraphInstantiate(&ex, gr, 0) != cudaSuccess) rc = fail(ctx, FALM_ERR_CUDA, "solve graph: instantiate");
-    ist = saved;
-    cudaGetLastError();
-    if (rc) {
-        if (ex) cudaGraphExecDestroy(ex);
-        cudaGraphDestroy(gr);
-        return rc;
-    }
-    ctx->graphs->push_back(falm_ctx::SolveGraph{x, b, r, ctx->w_rr, ctx->A_explicit, esize, pp_ready, np, nb, gr, ex});
-    *out = ex; *prefix = np; *per_iter = nb;
-    return FALM_OK;
-}
-
-template <typename T>
-int solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it_out, double *err_out, int *outer_out,
-            bool first_res_done = false, SolveRec *rec = nullptr) {
-    NvtxRange range("falm_solve");
-    int rc = ensure_work(ctx);
-    if (rc) return rc;
-    if (!ctx->op_ready && !ctx->A_explicit) return fail(ctx, FALM_ERR_STATE, "solve: no operator (call falm_eq_poisson_operator or falm_eq_set_matrix)");
-    if (ctx->ls_type == FALM_LS_JACOBI || ctx->ls_type == FALM_LS_SOR) {
-        if (first_res_done || rec) return fail(ctx, FALM_ERR_STATE, "solve: a BiCGStab start was prepared for a plain solver");
-        return plain_solve_t<T>(ctx, x, b, r, st, it_out, err_out, outer_out);
-    }
-    if (ctx->ls_type != FALM_LS_PBICGSTAB) return fail(ctx, FALM_ERR_ARG, "solve: unknown linear solver type");
-    const Geom &g = ctx->geo;
-    const Region3 R = interior(g);
-    const int grid = row_grid(ctx, R);
-    const int grid_p = row_grid_wave(ctx, R, k_bicg_p<T>), grid_s = row_grid_wave(ctx, R, k_bicg_s<T>);
-    const int grid_xr = row_grid_wave(ctx, R, k_bicg_xr<T>);
-    const Op7<T> op = op7<T>(ctx);
-    T *rr = (T *)ctx->w_rr, *p = (T *)ctx->w_p, *q = (T *)ctx->w_q, *s = (T *)ctx->w_s, *pp = (T *)ctx->w_pp;
-    T *ss = (T *)ctx->w_ss, *t = (T *)ctx->w_t, *xp = (T *)ctx->w_xp;
-    // first_res_done: the caller initialised the scalars (solver_init) and a
-    // kernel of its own already computed the first pass's residual into rr with
-    // the first preconditioner sweep into pp (the step's face-velocity kernel)
-    if (!first_res_done && !rec && (rc = solver_init(ctx, st))) return rc;
-    const T pcw = (T)ctx->pc_relax;
-    const int pct = ctx->pc_type, m = ctx->pc_maxit;
-    SolverScalars *sc = ctx->scal;
-    int total_it = 0, outer = 0;
-    const bool mixed = ctx->precision == FALM_MIXED;
-    // Mixed precision: a pass runs at most kMixedPassIts FP32 iterations before
-    // the FP64 true residual replaces the recursive one (a check, then a new
-    // pass from it), and as many passes as maxit needs: over longer FP32
-    // recursions BiCGStab diverged on the nearly singular operator of a long
-    // channel (unit-norm right-hand sides at 512x128x128).
-    const int pass_its = mixed ? std::min(ctx->maxit, kMixedPassIts) : ctx->maxit;
-    const int max_outer = mixed ? std::max(ctx->max_outer, (ctx->maxit + kMixedPassIts - 1) / kMixedPassIts) : 1;
-    // the stream of the iteration kernels: st, or the capture stream while a
-    // device-side loop (CUDA graph) is recorded
-    cudaStream_t ist = st;
-    const bool first_xp = pc_first_in_xp<T>(ctx);
-    auto first_target = [&](T *z) -> T * { return first_xp ? xp : z; };
-    // launch the remaining sweeps of one preconditioner application z ~ A^-1 v
-    // (the first, pointwise sweep wrote first_target(z)); the temporally blocked
-    // sweeps run out of place, alternating between xp and z
-    auto precondition_rest = [&](T *z, const T *v) -> int {
-        if (pct == FALM_LS_SOR) {
-            int hs = 1;
-            T *src = first_target(z);
-            while (hs < 2 * m) {                       // up to 3 half sweeps per pass over HBM
-                const int H = std::min(3, 2 * m - hs);
-                T *dst = src == z ? xp : z;
-                const int lr = sor_rb_launch<T>(ctx, ist, H, src, v, dst, pcw, hs & 1, sc);
-                if (lr < 0) return -lr;
-                if (lr == 0) break;
-                src = dst;
-                hs += H;
-            }
-            // a pass declined after all (pc_first_in_xp checks the same conditions)
-            if (src != z) CK(cudaMemcpyAsync(z, src, (size_t)g.n * sizeof(T), cudaMemcpyDeviceToDevice, ist));
-            for (; hs < 2 * m; hs++) {                // red, then (black, red) x (m-1)
-                const int color = hs & 1;
-                S7_OR(FALM_K_SOR, ist, T, 0, z, (SorBody<T>{op, z, v, pcw, color, sc}),
-                      (k_sor<T><<<grid, kRowThreads, 0, ist>>>(g, R, op, z, v, pcw, color, sc)));
-            }
-        } else if (pct == FALM_LS_JACOBI) {
-            // sweeps 2..m ping-pong between xp and z; the first sweep wrote to
-            // the buffer that makes the last one land in z
-            T *bufs[2] = {z, xp};
-            for (int it = 2; it <= m; it++) {
-                T *dst = bufs[(m - it) & 1], *src = bufs[(m - it + 1) & 1];
-                LAUNCH(FALM_K_SOR, ist, k_jacobi<T><<<grid, kRowThreads, 0, ist>>>(g, R, op, dst, src, v, sc));
-            }
-        }
-        return FALM_OK;
-    };
-    // a pass's residual also gives the first iteration's first preconditioner
-    // sweep (pp_ready: the stream kernel stored it, so k_bicg_p is skipped)
-    bool pp_ready = first_res_done;
-    auto res_pass = [&](int check) -> int {
-        int s7;
-        if (check) {
-            s7 = s7_launch<T, 1>(ctx, FALM_K_RES, ist, x, ResBody<T, true>{op, b, nullptr, nullptr, sc, 1});
-        } else {
-            ResBody<T> body{op, b, nullptr, rr, sc, 0};
-            body.pp = first_target(pp); body.pc_type = pct; body.pc_omega = pcw;
-            s7 = s7_launch<T, 2>(ctx, FALM_K_RES, ist, x, body);
-        }
-        if (s7 < 0) return -s7;
-        if (s7 == 0) LAUNCH(FALM_K_RES, ist, (k_res<T><<<grid, kRowThreads, 0, ist>>>(g, R, op, x, b, r, rr, ctx->red, sc, check)));
-        pp_ready = !check && s7 == 1;
-        return FALM_OK;
-    };
-    // a new pass: iteration count zero, the pass's iteration limit
-    static_assert(offsetof(SolverScalars, maxit) == offsetof(SolverScalars, it) + sizeof(int), "it, maxit adjacent");
-    auto zero_it = [&]() -> int {
-        const int itmax[2] = {0, pass_its};   // SolverScalars::it, ::maxit
-        CK(cudaMemcpyAsync(&sc->it, itmax, sizeof(itmax), cudaMemcpyHostToDevice, st));
-        return FALM_OK;
-    };
-    // the kernels of iteration itp of the pass (2 stands for every later
-    // one): r equals rr until the first k_bicg_xr, and the first
-    // iteration's p equals r, so it reads rr in their place
-    auto emit_iter = [&](int itp) -> int {
-        const T *rin = itp == 0 ? rr : r;
-        T *pout = itp == 0 ? nullptr : p;
-        const T *pin = itp == 1 ? rr : p, *pv = itp == 0 ? rr : p;
-        int erc;
-        if (!(itp == 0 && pp_ready))
-            LAUNCH(FALM_K_BICG_P, ist, k_bicg_p<T><<<grid_p, kRowThreads, 0, ist>>>(g, R, op, pout, pin, q, rin, first_target(pp), pct, pcw, sc));
-        if ((erc = precondition_rest(pp, pv))) return erc;
-        S7_OR(FALM_K_MV_DOT1, ist, T, 1, pp, (MvDot1Body<T>{op, q, rr, sc}),
-              (k_mv_dot1<T><<<grid, kRowThreads, 0, ist>>>(g, R, op, pp, q, rr, ctx->red, sc)));
-        LAUNCH(FALM_K_BICG_S, ist, k_bicg_s<T><<<grid_s, kRowThreads, 0, ist>>>(g, R, op, s, q, rin, first_target(ss), pct, pcw, sc));
-        if ((erc = precondition_rest(ss, s))) return erc;
-        S7_OR(FALM_K_MV_DOT2, ist, T, 2, ss, (MvDot2Body<T>{op, t, s, sc}),
-              (k_mv_dot2<T><<<grid, kRowThreads, 0, ist>>>(g, R, op, ss, t, s, ctx->red, sc)));
-        LAUNCH(FALM_K_BICG_XR, ist, k_bicg_xr<T><<<grid_xr, kRowThreads, 0, ist>>>(g, R, x, pp, ss, r, s, t, rr, ctx->red, sc));
-        return FALM_OK;
-    };
-    if (rec) {
-        // The whole solve recorded into rec->graph after rec->deps, with no
-        // host decision: pass 0 (solver start and first residual unless the
-        // caller recorded them), and in mixed precision a while node of FP64
-        // checks and further passes; a pass is iterations 0 and 1 and a while
-        // node of later iterations, its condition the done flag.
-        ist = ctx->cap_stream;
-        const long long l_start = ctx->launches;
-        long long fixed = 0, per_iter = 0;
-        auto cap = [&](cudaGraph_t gr, std::vector<cudaGraphNode_t> &deps, long long *cnt, const std::function<int()> &fn) -> int {
-            const long long l0 = ctx->launches;
-            const int crc = capture_into(ctx, gr, deps, fn);
-            *cnt += ctx->launches - l0;
-            ctx->launches = l0;
-            return crc;
-        };
-        auto cond = [&](cudaGraphConditionalHandle h) -> int {
-            k_graph_continue<<<1, 1, 0, ist>>>(sc, h);
-            return cudaGetLastError() == cudaSuccess ? FALM_OK : fail(ctx, FALM_ERR_CUDA, "graph: condition kernel");
-        };
-        auto rec_pass = [&](cudaGraph_t gr, std::vector<cudaGraphNode_t> &deps) -> int {
-            cudaGraphConditionalHandle h;
-            if (cudaGraphConditionalHandleCreate(&h, gr, 1, cudaGraphCondAssignDefault) != cudaSuccess)
-                return fail(ctx, FALM_ERR_CUDA, "graph: handle");
-            int e = cap(gr, deps, &fixed, [&]() -> int {
-                int q2 = emit_iter(0);
-                if (!q2) q2 = emit_iter(1);
-                if (!q2) q2 = cond(h);
-                return q2;
-            });
-            cudaGraph_t body = nullptr;
-            if (!e) e = add_while(ctx, gr, deps, h, &body);
-            std::vector<cudaGraphNode_t> bd;
-            long long pi = 0;
-            if (!e) e = cap(body, bd, &pi, [&]() -> int {
-                int q2 = emit_iter(2);
-                if (!q2) q2 = cond(h);
-                return q2;
-            });
-            per_iter = pi;
-            if (!e) e = cap(gr, deps, &fixed, [&]() -> int {
-                LAUNCH(FALM_K_OTHER, ist, k_pass_end<<<1, 1, 0, ist>>>(sc));
-                return FALM_OK;
-            });
-            return e;
-        };
-        int e = FALM_OK;
-        if (!first_res_done)
-            e = cap(rec->graph, rec->deps, &fixed, [&]() -> int {
-                LAUNCH(FALM_K_OTHER, ist, k_solver_init<<<1, 1, 0, ist>>>(sc, (double)g.nx * g.ny * g.nzg, ctx->tol, pass_its));
-                return res_pass(0);
-            });
-        if (!e) e = rec_pass(rec->graph, rec->deps);
-        if (!e && mixed && max_outer > 1) {
-            cudaGraphConditionalHandle ho;
-            if (cudaGraphConditionalHandleCreate(&ho, rec->graph, 0, cudaGraphCondAssignDefault) != cudaSuccess)
-                e = fail(ctx, FALM_ERR_CUDA, "graph: handle");
-            auto check = [&]() -> int {
-                int q2 = res_pass(1);
-                if (!q2) LAUNCH(FALM_K_OTHER, ist, k_outer_cond<<<1, 1, 0, ist>>>(sc, ho, max_outer));
-                return q2;
-            };
-            if (!e) e = cap(rec->graph, rec->deps, &fixed, check);
-            cudaGraph_t ob = nullptr;
-            if (!e) e = add_while(ctx, rec->graph, rec->deps, ho, &ob);
-            std::vector<cudaGraphNode_t> od;
-            if (!e) e = cap(ob, od, &fixed, [&]() -> int {
-                LAUNCH(FALM_K_OTHER, ist, k_pass_reset<<<1, 1, 0, ist>>>(sc, pass_its));
-                return res_pass(0);
-            });
-            if (!e) e = rec_pass(ob, od);
-            if (!e) e = cap(ob, od, &fixed, check);
-        }
-        ist = st;
-        ctx->launches = l_start;
-        rec->fixed += fixed;
-        rec->per_iter = per_iter;
-        return e;
-    }
-    if (mixed && pass_its != ctx->maxit)
-        CK(cudaMemcpyAsync(&sc->maxit, &pass_its, sizeof(int), cudaMemcpyHostToDevice, st));
-    // In mixed precision each pass but the last is followed by a check of the
-    // true residual in FP64 (stop when it meets the tolerance; the check stores
-    // nothing). The check is queued behind the pass's iterations and runs only
-    // once the pass has stopped, so one host synchronisation serves both; where
-    // the stream kernel is not available it runs at the start of the next pass.
-    // A pass stores its residual in rr only: r equals rr until the pass's first
-    // k_bicg_xr, which writes r, and the iteration reads rr before.
-    // a device-side loop (CUDA graph) runs a pass's iterations without host
-    // checks in between; the FP64 check of a mixed-precision pass then follows
-    // it as a kernel of its own
-    const bool graph = use_graph(ctx);
-    bool explicit_check = graph, pass_queued = first_res_done;
-    int passes = 0;   // passes run (a pass whose success an explicit check finds ends the loop at the next outer step)
-    bool restart_check = false;   // the previous pass broke down: check the true residual before restarting
-    for (outer = 0; outer < max_outer; outer++) {
-        if (outer > 0 && (explicit_check || restart_check)) {
-            restart_check = false;
-            if ((rc = res_pass(1))) return rc;
-            CK(cudaMemcpyAsync(ctx->scal_host, sc, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-            if (ctx->scal_host->done) break;
-        }
-        if (!pass_queued) {
-            if ((rc = res_pass(0))) return rc;
-            if (outer > 0 && (rc = zero_it())) return rc;
-        }
-        pass_queued = false;
-        const bool want_check = mixed && outer + 1 < max_outer && !explicit_check;
-        bool checked = false;
-        if (graph) {
-            // the whole pass on the device: one graph launch, one host read
-            cudaGraphExec_t ge = nullptr;
-            int prefix = 0, per_iter = 0;
-            if ((rc = solve_graph(ctx, x, b, r, (int)sizeof(T), pp_ready ? 1 : 0, emit_iter, ist, &ge, &prefix, &per_iter))) return rc;
-            CK(cudaGraphLaunch(ge, st));
-            CK(cudaMemcpyAsync(ctx->scal_host, sc, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-            ctx->launches += prefix + (long long)per_iter * std::max(0, ctx->scal_host->it - 2);
-        }
-        // otherwise iterations are queued in batches of 1, 2, 4, 8, 8, ... between
-        // host checks of the convergence flag; every kernel of an iteration
-        // queued after convergence returns at once
-        int batch = 1, queued = 0;
-        for (int itp = 0; !graph; itp++) {
-            if ((rc = emit_iter(itp))) return rc;
-            if (++queued < batch) continue;
-            if (want_check && !explicit_check) {
-                ResBody<T, true> cb{op, b, nullptr, nullptr, sc, 1};
-                cb.queued_check = 1;
-                const int s7 = s7_launch<T, 1>(ctx, FALM_K_RES, st, x, cb);
-                if (s7 < 0) return -s7;
-                if (s7 == 0) explicit_check = true;
-            }
-            CK(cudaMemcpyAsync(ctx->scal_host, sc, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-            if (want_check && !explicit_check && ctx->scal_host->checked) { checked = true; break; }
-            if (ctx->scal_host->done) break;
-            queued = 0;
-            batch = std::min(2 * batch, 8);
-        }
-        total_it += ctx->scal_host->it;
-        passes++;
-        if (ctx->scal_host->status == FALM_ERR_NAN) {
-            // In mixed precision a non-finite alpha or omega of the FP32
-            // recursion (a breakdown: the kernels after it skipped, so x is the
-            // last iterate) restarts a pass from the FP64 true residual while
-            // passes remain; non-finite data ends the solve.
-            if (!mixed || outer + 1 >= max_outer) break;
-            static const int ok = FALM_OK;
-            CK(cudaMemcpyAsync(&sc->status, &ok, sizeof(int), cudaMemcpyHostToDevice, st));
-            restart_check = true;
-            continue;
-        }
-        if (checked) {
-            if (ctx->scal_host->done) break;   // the true residual meets the tolerance
-            if ((rc = res_pass(0))) return rc;
-            if ((rc = zero_it())) return rc;
-            pass_queued = true;
-        }
-    }
-    if (mixed && outer >= max_outer) {
-        // report the true residual of the final iterate
-        LAUNCH(FALM_K_RES, st, k_res<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, r, nullptr, ctx->red, nullptr, 0));
-    } else if (std::min(outer, max_outer - 1) == 0 && ctx->scal_host->it == 0) {
-        // no iteration followed the first residual, which went to rr only
-        LAUNCH(FALM_K_RES, st, k_res<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, r, nullptr, ctx->red, nullptr, 0));
-    }
-    if (it_out) *it_out = total_it;
-    if (err_out) *err_out = ctx->scal_host->err;
-    if (outer_out) *outer_out = std::max(1, passes);
-    return ctx->scal_host->status == FALM_ERR_NAN ? fail(ctx, FALM_ERR_NAN, "solve: non-finite scalar") : FALM_OK;
-}
-
-template <typename T>
-int dot_t(falm_ctx *ctx, const T *a, const T *b, int ncol, double *out, cudaStream_t st) {
-    const Region3 R = interior(ctx->geo);
-    LAUNCH(FALM_K_OTHER, st, k_dot<T><<<row_grid(ctx, R), kRowThreads, 0, st>>>(ctx->geo, R, a, b, ncol, ctx->red, &ctx->scal->red[0]));
-    CK(cudaMemcpyAsync(ctx->scal_host, ctx->scal, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    *out = ctx->scal_host->red[0];
-    return FALM_OK;
-}
-
-AlmFuse alm_fuse(const falm_ctx *ctx) {
-    AlmFuse af;
-    memset(&af, 0, sizeof(af));
-    if (!ctx->alm_on || ctx->alm.apcount > kMaxFusedAp) return af;
-    af.apcount = ctx->alm.apcount;
-    af.xyz = ctx->alm.ap_xyz;
-    af.force = ctx->alm.ap_force;
-    af.scal = ctx->alm.scal;
-    af.eps = ctx->alm.euler_eps;
-    double sq = std::sqrt(M_PI) * af.eps;
-    af.eta = 1. / (sq * sq * sq);
-    af.rcut2 = ctx->alm.rcut2;
-    af.bs = ctx->alm.bs;
-    af.fbox = ctx->alm.fbox;
-    return af;
-}
-
-template <typename T> struct PUConf;
-template <> struct PUConf<double> { static constexpr int NS = 4; };
-template <> struct PUConf<float> { static constexpr int NS = 6; };
-
-template <typename T>
-int pseudo_u_t(falm_ctx *ctx, const T *un, const T *u, const T *uu, T *ua, const T *nut, const T *ff, double dt, bool fuse, cudaStream_t st) {
-    const Region3 R = interior(ctx->geo);
-    AlmFuse af;
-    memset(&af, 0, sizeof(af));
-    if (!ff && fuse) af = alm_fuse(ctx);
-    const Geom &g = ctx->geo;
-    constexpr int NS = PUConf<T>::NS;
-    using L = PUTile<T, NS>;
-    CUtensorMap mu, muu, mnut;
-    if (!ctx->no_tma && make_map(ctx, &mu, u, 3, L::BX, L::BY) && make_map(ctx, &muu, uu, 3, L::BX, L::BY) &&
-        make_map(ctx, &mnut, nut, 1, L::BX, L::BY)) {
-        // FP32 with a 4th-order scheme and an even interior width: the x-pair kernel
-        if constexpr (sizeof(T) == 4) {
-            if (!ctx->pu_v1 && (g.nx & 1) == 0 &&
-                (ctx->adv == FALM_ADV_UPWIND3 || ctx->adv == FALM_ADV_UTOPIA || ctx->adv == FALM_ADV_KK)) {
-                // a ring of 4 planes (49 KB) and at most 128 registers: 4 CTAs per SM
-                constexpr int NS2 = 4;
-                using L = PUTile<T, NS2>;
-                auto k2 = k_pseudo_u_tma2<NS2, FALM_ADV_UPWIND3>;
-                if (ctx->adv == FALM_ADV_UTOPIA) k2 = k_pseudo_u_tma2<NS2, FALM_ADV_UTOPIA>;
-                if (ctx->adv == FALM_ADV_KK) k2 = k_pseudo_u_tma2<NS2, FALM_ADV_KK>;
-                const int bx = (g.nx + L::TX - 1) / L::TX, by = (g.ny + L::TY - 1) / L::TY;
-                const int kc = chunk_len(ctx, (long long)bx * by, g.nz, resident_per_sm(k2, 128, L::SMEM), 64, 4);
-                cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
-                dim3 grid(bx, by, (g.nz + kc - 1) / kc);
-                LAUNCH(FALM_K_PSEUDO_U, st, k2<<<grid, 128, L::SMEM, st>>>(g, kc, mview<T>(ctx), mu, muu, mnut, un, un == u ? 1 : 0, ua, ff, af,
-                                                                         (T)(1.0 / ctx->Re), (T)dt, ctx->kerr));
-                return FALM_OK;
-            }
-        }
-        auto kern = k_pseudo_u_tma<T, NS, FALM_ADV_KK>;
-        switch (ctx->adv) {
-            case FALM_ADV_UPWIND1: kern = k_pseudo_u_tma<T, NS, FALM_ADV_UPWIND1>; break;
-            case FALM_ADV_UPWIND3: kern = k_pseudo_u_tma<T, NS, FALM_ADV_UPWIND3>; break;
-            case FALM_ADV_QUICK: kern = k_pseudo_u_tma<T, NS, FALM_ADV_QUICK>; break;
-            case FALM_ADV_UTOPIA: kern = k_pseudo_u_tma<T, NS, FALM_ADV_UTOPIA>; break;
-            default: break;
-        }
-        const int bx = (g.nx + L::TX - 1) / L::TX, by = (g.ny + L::TY - 1) / L::TY;
-        const int kc = chunk_len(ctx, (long long)bx * by, g.nz, resident_per_sm(kern, 256, L::SMEM), 64, 4);
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
-        dim3 grid(bx, by, (g.nz + kc - 1) / kc);
-        LAUNCH(FALM_K_PSEUDO_U, st, kern<<<grid, 256, L::SMEM, st>>>(g, kc, mview<T>(ctx), mu, muu, mnut, un, un == u ? 1 : 0, ua, ff, af,
-                                                                    (T)(1.0 / ctx->Re), (T)dt, ctx->kerr));
-        return FALM_OK;
-    }
-    LAUNCH(FALM_K_PSEUDO_U, st, k_pseudo_u<T><<<row_grid(ctx, R), kRowThreads, 0, st>>>(ctx->geo, R, mview<T>(ctx), un, u, uu, ua, nut, ff, af,
-                                                            (T)(1.0 / ctx->Re), (T)dt, ctx->adv));
-    return FALM_OK;
-}
-
-template <typename T>
-int alm_run_t(falm_ctx *ctx, const T *u, T *ff, double t, cudaStream_t st, const double *t_dev = nullptr) {
-    // stage the coordinate tables in shared memory when they fit in 96 KB
-    const int csm = (ctx->geo.sx + ctx->geo.sy + ctx->geo.sz) * (int)sizeof(double);
-    const int stage = csm <= 96 * 1024 ? 1 : 0;
-    if (stage && csm > 32 * 1024) cudaFuncSetAttribute(k_alm_force<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
-    LAUNCH(FALM_K_ALM, st, k_alm_force<T><<<1, 256, stage ? csm : 0, st>>>(ctx->geo, ctx->alm, ctx->m64.x[0], ctx->m64.x[1], ctx->m64.x[2], u, t, stage,
-                                                                            t_dev));
-    if (ff) {
-        const Region3 R = interior(ctx->geo);
-        LAUNCH(FALM_K_ALM, st, k_alm_project<T><<<row_grid(ctx, R), kRowThreads, 0, st>>>(ctx->geo, R, mview<T>(ctx), ctx->alm, ff));
-    } else if (ctx->alm.bs.total > 0) {
-        // force boxes for the fused projection of the plane-streaming pseudo-velocity kernel
-        const long long blocks = std::min<long long>((ctx->alm.bs.total + 255) / 256, (long long)ctx->sm_count * 8);
-        LAUNCH(FALM_K_ALM, st, k_alm_box<T><<<(int)blocks, 256, 0, st>>>(ctx->alm, ctx->m64.x[0], ctx->m64.x[1], ctx->m64.x[2]));
-    }
-    return FALM_OK;
-}
-
-template <typename T>
-int ubc_t(falm_ctx *ctx, T *u, UPrev<T> up, double dt, double t, cudaStream_t st, const double *t_dev = nullptr) {
-    Inflow inf{ctx->inflow_box, ctx->inflow_nb, ctx->inflow_dx, ctx->inlet_plane_valid ? ctx->inlet_plane : nullptr};
-    ctx->inlet_plane_valid = 0;
-    dim3 grid(face_blocks(ctx), 3);
-    LAUNCH(FALM_K_UBC, st, k_ubc<T><<<grid, 256, 0, st>>>(ctx->geo, ctx->bc_kind, u, up, ctx->m64.x[0], dt, t, ctx->u_inlet, inf, t_dev));
-    return FALM_OK;
-}
-
-// the RMCP forcing into ff over the turbines' boxes; torque and thrust sums
-// into ctx->rmcp_sums (device)
-template <typename T>
-int rmcp_run_t(falm_ctx *ctx, const T *u, T *ff, int *flag, double t, cudaStream_t st, const double *t_dev = nullptr) {
-    const RmcpDev &a = *ctx->rmcp;
-    const long long blocks = std::max(1LL, std::min<long long>((a.bs.total + 255) / 256, (long long)ctx->sm_count * 8));
-    // 2 x kMaxTurbines values per block: a quarter of the workspace's blocks
-    const RedWork rw{ctx->red.partials, ctx->red.counter, ctx->red.maxBlocks / 4};
-    LAUNCH(FALM_K_ALM, st, k_rmcp<T><<<(int)blocks, 256, 0, st>>>(ctx->geo, a, ctx->m64.x[0], ctx->m64.x[1], ctx->m64.x[2], u, ff, flag, t, rw,
-                                                                 ctx->rmcp_sums, t_dev));
-    return FALM_OK;
-}
-
-// A wait on an mbarrier that nothing ever completes, through the same bounded
-// wait the plane-stream kernels use: it gives up after `cycles` clock64 cycles
-// and records FALM_ERR_TIMEOUT in the device error word.  No copy is issued,
-// so nothing is left in flight when the block returns.
-__global__ void k_wait_probe(int *err, long long cycles) {
-    __shared__ __align__(8) uint64_t bar;
-    if (threadIdx.x == 0) {
-        mbar_init(&bar, 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) mbar_wait_cycles(&bar, 0, err, cycles);
-    __syncthreads();
-}
-
-// The phases of the step before and after the Poisson solve, shared by the
-// host-driven step and the recorded one: t_dev is the recorded step's time in
-// device memory (NULL: the host passes t), phase the NVTX phases (or NULL).
-template <typename T>
-int step_pre_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_t st, const double *t_dev, bool *fused_res_out,
-               NvtxPhases *phase) {
-    int rc;
-    const Geom &g = ctx->geo;
-    T *u = (T *)f->u, *uu = (T *)f->uu, *p = (T *)f->p, *nut = (T *)f->nut, *ff = (T *)f->ff;
-    T *ua = (T *)ctx->w_ua, *rhs = (T *)ctx->w_rhs;
-    const bool chan = ctx->bc_kind == FALM_BC_CHANNEL;
-    bool fused_res = false;
-    // 1. ALM (src/alm/alm.h:66-77) at the previous velocity, or the RMCP model
-    if (phase) phase->next("forcing");
-    if (ctx->alm_on) {
-        if ((rc = alm_run_t<T>(ctx, u, ff, t, st, t_dev))) return rc;
-    } else if (ctx->rmcp_on) {
-        ff = (T *)ctx->w_ff;
-        if ((rc = rmcp_run_t<T>(ctx, u, ff, nullptr, t, st, t_dev))) return rc;
-    }
-    // 2. pseudo-velocity into ua (ALM force projected in-kernel when ff == NULL)
-    if (phase) phase->next("pseudo_velocity");
-    if ((rc = pseudo_u_t<T>(ctx, u, u, uu, ua, nut, ff, dt, ctx->alm_on != 0, st))) return rc;
-    // 3. face velocity + [uubc] + RHS in one pass
-    if (phase) phase->next("face_velocity_rhs");
-    {
-        const Region3 R = facemap(g);
-        T scale = (T)(1.0 / (dt * ctx->maxdiag));
-        // the guide layer of ua takes the previous velocity (the reference's aliased u)
-        LAUNCH(FALM_K_OTHER, st, k_copy_shell<T><<<ctx->sm_count * 8, 256, 0, st>>>(g, u, ua));
-        // the plane stream also computes the solve's first residual (rr) and
-        // first preconditioner sweep (pp) from the pressure p, the initial guess
-        fused_res = false;
-        if (!ctx->A_explicit && ctx->ls_type == FALM_LS_PBICGSTAB && (ctx->pc_type == FALM_LS_SOR || ctx->pc_type == FALM_LS_JACOBI)) {
-            if ((rc = ensure_work(ctx))) return rc;
-            if (t_dev) {   // recording: the solver start as a kernel (the mixed pass limit included)
-                const int pass_its = ctx->precision == FALM_MIXED ? std::min(ctx->maxit, kMixedPassIts) : ctx->maxit;
-                LAUNCH(FALM_K_OTHER, st, k_solver_init<<<1, 1, 0, st>>>(ctx->scal, (double)g.nx * g.ny * g.nzg, ctx->tol, pass_its));
-            } else if ((rc = solver_init(ctx, st))) {
-                return rc;
-            }
-            T *ppt = pc_first_in_xp<T>(ctx) ? (T *)ctx->w_xp : (T *)ctx->w_pp;
-            const void *const fp[2] = {ua, p};
-            const int nc[2] = {3, 1};
-            int s3;
-            if (chan)
-                s3 = p3_launch<T, 2, 2>(ctx, FALM_K_UTOUU_RHS, st, R, 1, fp, nc,
-                                        UtoUUResBody<T, false>{UtoUUBody<T, true, false>{g, mview<T>(ctx), uu, rhs, scale}, mview<T>(ctx),
-                                                               op7<T>(ctx), (T *)ctx->w_rr, ppt, ctx->pc_type, (T)ctx->pc_relax, ctx->scal});
-            else
-                s3 = p3_launch<T, 2, 2>(ctx, FALM_K_UTOUU_RHS, st, R, 1, fp, nc,
-                                        UtoUUResBody<T, true>{UtoUUBody<T, true, true>{g, mview<T>(ctx), uu, rhs, scale}, mview<T>(ctx),
-                                                              op7<T>(ctx), (T *)ctx->w_rr, ppt, ctx->pc_type, (T)ctx->pc_relax, ctx->scal});
-            if (s3 < 0) return -s3;
-            fused_res = s3 == 1;
-        }
-        if (!fused_res) {
-            if (chan)
-                P3_OR(FALM_K_UTOUU_RHS, st, T, 1, 0, R, 1, FB_ARR(ua), FB_ARR(3), (UtoUUBody<T, true, false>{g, mview<T>(ctx), uu, rhs, scale}),
-                      (k_utouu<T, true, false><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), ua, u, uu, rhs, scale)));
-            else
-                P3_OR(FALM_K_UTOUU_RHS, st, T, 1, 0, R, 1, FB_ARR(ua), FB_ARR(3), (UtoUUBody<T, true, true>{g, mview<T>(ctx), uu, rhs, scale}),
-                      (k_utouu<T, true, true><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), ua, u, uu, rhs, scale)));
-        }
-    }
-    *fused_res_out = fused_res;
-    return FALM_OK;
-}
-
-template <typename T>
-int step_post_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_t st, const double *t_dev, NvtxPhases *phase) {
-    int rc;
-    const Geom &g = ctx->geo;
-    T *u = (T *)f->u, *uu = (T *)f->uu, *p = (T *)f->p, *nut = (T *)f->nut;
-    T *ua = (T *)ctx->w_ua;
-    const bool chan = ctx->bc_kind == FALM_BC_CHANNEL;
-    // 5. pbc
-    if (phase) phase->next("projection_bcs");
-    LAUNCH(FALM_K_PBC, st, k_pbc<T><<<dim3(face_blocks(ctx), 3), 256, 0, st>>>(g, ctx->bc_kind, p));
-    // 6. keep the previous velocity at the outlet planes, then project
-    if (chan) { LAUNCH(FALM_K_OTHER, st, k_save_outlet<T><<<std::min(ctx->sm_count * 4, (3 * g.sy * g.sz + 255) / 256), 256, 0, st>>>(g, u, (T *)ctx->w_outlet)); }
-    {
-        const Region3 R = facemap(g);
-        P3_OR(FALM_K_PROJECT, st, T, 1, 0, R, 1, FB_ARR(p), FB_ARR(1), (ProjectBody<T>{g, mview<T>(ctx), u, ua, uu, uu, (T)dt}),
-              (k_project<T><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), u, ua, uu, uu, p, (T)dt)));
-    }
-    // 7. ubc
-    if ((rc = ubc_t<T>(ctx, u, UPrev<T>{(const T *)ctx->w_outlet, 1}, dt, t, st, t_dev))) return rc;
-    // 8. SGS + divergence norm
-    if (phase) phase->next("sgs_divergence");
-    {
-        const Region3 R = interior(g);
-        P3_OR(FALM_K_SGS_DIV, st, T, 2, 1, R, 2, FB_ARR(u, uu), FB_ARR(3, 3),
-              (SgsDivBody<T>{g, mview<T>(ctx), ctx->m64, nut, (T)ctx->Cs, ctx->sgs, (T *)nullptr, &ctx->scal->red[3]}),
-              (k_sgs_div<T, true><<<row_grid(ctx, R), kRowThreads, 0, st>>>(g, R, mview<T>(ctx), ctx->m64, u, nut, (T)ctx->Cs, ctx->sgs, uu,
-                                                                            nullptr, ctx->red, &ctx->scal->red[3])));
-    }
-    return FALM_OK;
-}
-
-// the step's results into the pinned host copies
-int step_stats_copy(falm_ctx *ctx, cudaStream_t st) {
-    CK(cudaMemcpyAsync(ctx->scal_host, ctx->scal, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
-    if (ctx->alm_on) CK(cudaMemcpyAsync(ctx->alm_scal_host, ctx->alm.scal, sizeof(AlmScalars), cudaMemcpyDeviceToHost, st));
-    if (ctx->rmcp_on) CK(cudaMemcpyAsync(ctx->rmcp_sums_host, ctx->rmcp_sums, 2 * kMaxTurbines * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(&ctx->scal_host->kerr, ctx->kerr, sizeof(int), cudaMemcpyDeviceToHost, st));
-    return FALM_OK;
-}
-
-// after the step's synchronisation: the device error word, then the statistics
-int step_finish(falm_ctx *ctx, cudaStream_t st, falm_step_stats *out, int it, double err, int outer, int solve_status) {
-    const Geom &g = ctx->geo;
-    if (ctx->scal_host->kerr) {
-        cudaMemsetAsync(ctx->kerr, 0, sizeof(int), st);
-        std::string m = "step: device error word " + std::to_string(ctx->scal_host->kerr) +
-                        (ctx->scal_host->kerr >= 300 ? " (a staged stencil neighbourhood failed its self-check)"
-                         : ctx->scal_host->kerr >= 200 ? " (a TMA load request failed its self-check)" : " (a bounded wait gave up)");
-        *ctx->last_error = m;
-        return ctx->scal_host->kerr >= 200 ? FALM_ERR_ARG : FALM_ERR_TIMEOUT;
-    }
-    if (out) {
-        memset(out, 0, sizeof(*out));
-        out->it = it;
-        out->err = err;
-        out->outer = outer;
-        out->status = solve_status;
-        out->divnorm = std::sqrt(ctx->scal_host->red[3]) / ((double)g.nx * g.ny * g.nz);
-        if (ctx->alm_on)
-            for (int q = 0; q < ctx->alm.n_turbine && q < kMaxTurbines; q++) {
-                out->torque[q] = ctx->alm_scal_host->torque[q];
-                out->thrust[q] = ctx->alm_scal_host->thrust[q];
-            }
-        if (ctx->rmcp_on)
-            for (int q = 0; q < ctx->rmcp->n_turbine && q < kMaxTurbines; q++) {
-                out->torque[q] = ctx->rmcp_sums_host[q];
-                out->thrust[q] = ctx->rmcp_sums_host[kMaxTurbines + q];
-            }
-    }
-    return FALM_OK;
-}
-
-// Whole steps as CUDA graphs (grids where launch and synchronisation latency
-// dominate, see use_graph): the phases before the solve, the solve with its
-// loops on the device (solve_t's recording), the phases after it and the
-// copies of the results, recorded once per set of fields and dt; the time goes
-// in through device memory, written by the graph's first node from a pinned
-// host value; a streamed inlet plane (falm_bc_set_inlet_plane, copied into
-// the context's fixed plane buffer before the step) makes a recording of its
-// own.  Not for z slabs, the plain solvers or an explicit matrix.
-template <typename T>
-bool step_graph_ok(const falm_ctx *ctx) {
-    return use_graph(ctx) && !ctx->slab_on && ctx->wait_probe_cycles == 0 && ctx->op_ready &&
-           !ctx->A_explicit && ctx->ls_type == FALM_LS_PBICGSTAB && (ctx->pc_type == FALM_LS_SOR || ctx->pc_type == FALM_LS_JACOBI);
-}
-
-template <typename T>
-int step_graph_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_t st, falm_step_stats *out) {
-    falm_ctx::StepGraph *sg = nullptr;
-    const int inlet = ctx->inlet_plane_valid ? 1 : 0;
-    for (auto &e : *ctx->step_graphs)
-        if (e.u == f->u && e.uu == f->uu && e.p == f->p && e.nut == f->nut && e.ff == f->ff && e.dt == dt && e.inlet == inlet) sg = &e;
-    if (!sg) {
-        if (!ctx->cap_stream) CK(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
-        if (!ctx->t_dev) {
-            CK(cudaMalloc(&ctx->t_dev, sizeof(double)));
-            CK(cudaHostAlloc(&ctx->t_host, sizeof(double), cudaHostAllocDefault));
-        }
-        const cudaStream_t cs = ctx->cap_stream;
-        cudaGraph_t gr = nullptr;
-        CK(cudaGraphCreate(&gr, 0));
-        SolveRec rec;
-        rec.graph = gr;
-        bool fused = false;
-        const long long l0 = ctx->launches;
-        int rc = capture_into(ctx, gr, rec.deps, [&]() -> int {
-            CK(cudaMemcpyAsync(ctx->t_dev, ctx->t_host, sizeof(double), cudaMemcpyHostToDevice, cs));
-            return step_pre_t<T>(ctx, f, dt, t, cs, ctx->t_dev, &fused, nullptr);
-        });
-        const long long n_pre = ctx->launches - l0;
-        ctx->launches = l0;
-        int it = 0, outer = 0;
-        double err = 0;
-        if (!rc) rc = solve_t<T>(ctx, (T *)f->p, (const T *)ctx->w_rhs, (T *)ctx->w_r, st, &it, &err, &outer, fused, &rec);
-        if (!rc) rc = capture_into(ctx, gr, rec.deps, [&]() -> int {
-            int q = step_post_t<T>(ctx, f, dt, t, cs, ctx->t_dev, nullptr);
-            if (!q) q = step_stats_copy(ctx, cs);
-            return q;
-        });
-        const long long n_post = ctx->launches - l0;
-        ctx->launches = l0;
-        cudaGraphExec_t ex = nullptr;
-        if (!rc && cudaGraphInstantiate(&ex, gr, 0) != cudaSuccess) rc = fail(ctx, FALM_ERR_CUDA, "step graph: instantiate");
-        cudaGetLastError();
-        if (rc) {
-            cudaGraphDestroy(gr);
-            return rc;
-        }
-        ctx->step_graphs->push_back(falm_ctx::StepGraph{f->u, f->uu, f->p, f->nut, f->ff, dt, inlet, n_pre + rec.fixed + n_post, rec.per_iter,
-                                                        gr, ex});
-        sg = &ctx->step_graphs->back();
-    }
-    *ctx->t_host = t;
-    ctx->inlet_plane_valid = 0;   // the streamed plane serves one step
-    CK(cudaGraphLaunch(sg->exec, st));
-    CK(cudaStreamSynchronize(st));
-    const SolverScalars &sh = *ctx->scal_host;
-    ctx->launches += sg->fixed + sg->per_iter * std::max(0, sh.it_total);
-    if (sh.status == FALM_ERR_NAN) return fail(ctx, FALM_ERR_NAN, "solve: non-finite scalar");
-    return step_finish(ctx, st, out, sh.it_total, sh.err, std::max(1, sh.passes), sh.status);
-}
-
-template <typename T>
-int step_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStream_t st, falm_step_stats *out) {
-    NvtxRange whole("falm_step");
-    NvtxPhases phase;
-    int rc = ensure_work(ctx);
-    if (rc) return rc;
-    if (ctx->wait_probe_cycles > 0) {   // armed by falm_debug_arm_wait_probe: one step only
-        const long long cycles = ctx->wait_probe_cycles;
-        ctx->wait_probe_cycles = 0;
-        LAUNCH(FALM_K_OTHER, st, k_wait_probe<<<1, 32, 0, st>>>(ctx->kerr, cycles));
-    }
-    if (!ctx->op_ready) {
-        if ((rc = build_poisson(ctx, ctx->bc_kind))) return rc;
-    }
-    if (step_graph_ok<T>(ctx)) return step_graph_t<T>(ctx, f, dt, t, st, out);
-    bool fused_res = false;
-    if ((rc = step_pre_t<T>(ctx, f, dt, t, st, nullptr, &fused_res, &phase))) return rc;
-    // 4. Poisson
-    phase.next("poisson");
-    int it = 0, outer = 1;
-    double err = 0;
-    rc = solve_t<T>(ctx, (T *)f->p, (const T *)ctx->w_rhs, (T *)ctx->w_r, st, &it, &err, &outer, fused_res);
-    const int solve_status = ctx->scal_host->status;
-    if (rc) return rc;
-    if ((rc = step_post_t<T>(ctx, f, dt, t, st, nullptr, &phase))) return rc;
-    if ((rc = step_stats_copy(ctx, st))) return rc;
-    CK(cudaStreamSynchronize(st));
-    return step_finish(ctx, st, out, it, err, outer, solve_status);
-}
+#include "step.cuh"
 
 #include "slab.cuh"
 
