@@ -84,7 +84,7 @@ int falm_create(const falm_grid *grid, int precision, falm_ctx **out) {
     ctx->step_graphs = new std::vector<falm_ctx::StepGraph>();
     {
         const char *gm = getenv("FALM_B200_GRAPH");
-        ctx->graph_mode = (gm && gm[0] == '0') ? 0 : ((gm && gm[0] == '1') ? 1 : -1);
+        ctx->graph_mode = (gm && gm[0] == '0') ? 0 : 1;
     }
     ctx->precision = precision;
     ctx->esize = precision == FALM_FP64 ? sizeof(double) : sizeof(float);

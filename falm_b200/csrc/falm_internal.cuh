@@ -207,6 +207,6 @@ struct falm_ctx {
     std::vector<StepGraph> *step_graphs;
     double *t_dev;                          // the recorded step's time (device), from t_host
     double *t_host;                         // pinned
-    int graph_mode;                         // -1 small grids, 0 never, 1 always (FALM_B200_GRAPH)
+    int graph_mode;                         // 1 record steps and solver loops as CUDA graphs, 0 never (FALM_B200_GRAPH=0)
     cudaStream_t cap_stream;                // stream the graphs are captured on
 };

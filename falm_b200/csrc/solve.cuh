@@ -76,16 +76,15 @@ int plain_solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *i
 // flag (convergence, maxit, breakdown or a non-finite scalar), so the loop ends
 // on the device within maxit iterations.  Graphs are kept per solve signature
 // (vectors, element type, whether the first preconditioner sweep is ready) and
-// dropped when the solver settings or the operator change.  Used where launch
-// and host-synchronisation latency dominate: grids of at most kGraphCells
-// interior cells (FALM_B200_GRAPH=1 / 0 forces it on / off), never while
-// profiling or checking launches one by one.
-constexpr long long kGraphCells = 1ll << 22;
+// dropped when the solver settings or the operator change.  Used by default
+// (FALM_B200_GRAPH=0 turns it off), never while profiling or checking launches
+// one by one: the unconditional iteration 1 and the condition kernels cost
+// less than the host round trips they replace, even at 1-2 iterations per
+// step on the 512x256x256 grid.
 constexpr int kMixedPassIts = 50;   // FP32 BiCGStab iterations between FP64 true-residual checks
 
 bool use_graph(const falm_ctx *ctx) {
-    if (ctx->profiling || ctx->check_sync || ctx->graph_mode == 0) return false;
-    return ctx->graph_mode == 1 || (long long)ctx->geo.nx * ctx->geo.ny * ctx->geo.nz <= kGraphCells;
+    return !(ctx->profiling || ctx->check_sync || ctx->graph_mode == 0);
 }
 
 __global__ void k_graph_continue(const SolverScalars *sc, cudaGraphConditionalHandle h) {

@@ -275,8 +275,7 @@ int step_finish(falm_ctx *ctx, cudaStream_t st, falm_step_stats *out, int it, do
     return FALM_OK;
 }
 
-// Whole steps as CUDA graphs (grids where launch and synchronisation latency
-// dominate, see use_graph): the phases before the solve, the solve with its
+// Whole steps as CUDA graphs (see use_graph): the phases before the solve, the solve with its
 // loops on the device (solve_t's recording), the phases after it and the
 // copies of the results, recorded once per set of fields and dt; the time goes
 // in through device memory, written by the graph's first node from a pinned

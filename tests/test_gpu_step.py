@@ -209,7 +209,7 @@ def test_step_launch_count_and_statuses(lib_built):
 @pytest.mark.parametrize("name", ["channel", "cavity"])
 def test_device_loop_equals_host_loop(lib_built, monkeypatch, precision, name):
     """The BiCGStab iterations of a pass as one CUDA graph with a conditional
-    while node (FALM_B200_GRAPH=1; the default on grids of up to 2^22 cells)
+    while node (the default; FALM_B200_GRAPH=1)
     run the same kernels in the same order as the host loop that queues them
     in batches between reads of the convergence flag (FALM_B200_GRAPH=0): the
     same iteration counts and bitwise the same fields, in convergence mode
