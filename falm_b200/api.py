@@ -194,7 +194,8 @@ class Context:
         return xyz.reshape(apcount, 3), f.reshape(apcount, 3), tq, th
 
     def set_inlet_plane(self, plane_pinned):
-        """plane: pinned host float64 tensor/array 3 x nz x ny (interior), used by the next ubc"""
+        """plane: pinned host float64 tensor/array 3 x nz x ny (interior), used by the next
+        velocity BC (the next step), which copies it: keep it alive and unchanged until then"""
         ptr = ctypes.cast(ctypes.c_void_p(plane_pinned.data_ptr()), L.c_double_p)
         self._check(self.lib.falm_bc_set_inlet_plane(self.h, ptr, self.stream()), "set_inlet_plane")
 

@@ -1043,10 +1043,12 @@ int falm_step(falm_ctx *ctx, const falm_fields *f, double dt, double t, void *st
 extern "C" {
 
 int falm_bc_set_inlet_plane(falm_ctx *ctx, const double *plane, void *stream) {
+    (void)stream;   // the copy goes on the stream of the call that uses the plane
     if (!ctx || !plane) return FALM_ERR_ARG;
     const size_t n = 3ull * ctx->geo.ny * ctx->geo.nz;
     if (!ctx->inlet_plane) CK(cudaMalloc(&ctx->inlet_plane, n * sizeof(double)));
-    CK(cudaMemcpyAsync(ctx->inlet_plane, plane, n * sizeof(double), cudaMemcpyHostToDevice, S(stream)));
+    ctx->inlet_host = plane;
+    ctx->inlet_pending = 1;
     ctx->inlet_plane_valid = 1;
     return FALM_OK;
 }

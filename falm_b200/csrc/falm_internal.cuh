@@ -167,7 +167,9 @@ struct falm_ctx {
     long long prof_n[FALM_K_COUNT];
     // streamed inlet plane
     double *inlet_plane;                    // device 3 x nz x ny
-    int inlet_plane_valid;
+    int inlet_plane_valid;                  // the next velocity BC takes the streamed plane
+    const double *inlet_host;               // its host array, copied by that BC (or by the recorded step's copy node)
+    int inlet_pending;                      // inlet_host not yet copied
     int sm_count;
     int *kerr;                              // device error word of bounded waits (FALM_ERR_TIMEOUT)
     int no_tma;                             // force the row kernels (tests, fallback)
@@ -200,6 +202,7 @@ struct falm_ctx {
         const void *u, *uu, *p, *nut, *ff;
         double dt;
         int inlet;                      // recorded with a streamed inlet plane
+        cudaGraphNode_t inlet_node;     // its host-to-device copy (a root node; the source set per launch)
         long long fixed, per_iter;      // kernels outside the loops, kernels per iteration
         cudaGraph_t graph;
         cudaGraphExec_t exec;

@@ -99,6 +99,11 @@ int alm_run_t(falm_ctx *ctx, const T *u, T *ff, double t, cudaStream_t st, const
 
 template <typename T>
 int ubc_t(falm_ctx *ctx, T *u, UPrev<T> up, double dt, double t, cudaStream_t st, const double *t_dev = nullptr) {
+    // a streamed inlet plane: its copy, unless a recorded step's copy node makes it
+    if (ctx->inlet_plane_valid && ctx->inlet_pending && !t_dev) {
+        CK(cudaMemcpyAsync(ctx->inlet_plane, ctx->inlet_host, 3ull * ctx->geo.ny * ctx->geo.nz * sizeof(double), cudaMemcpyHostToDevice, st));
+        ctx->inlet_pending = 0;
+    }
     Inflow inf{ctx->inflow_box, ctx->inflow_nb, ctx->inflow_dx, ctx->inlet_plane_valid ? ctx->inlet_plane : nullptr};
     ctx->inlet_plane_valid = 0;
     dim3 grid(face_blocks(ctx), 3);
@@ -316,6 +321,18 @@ int step_graph_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaS
         int it = 0, outer = 0;
         double err = 0;
         if (!rc) rc = solve_t<T>(ctx, (T *)f->p, (const T *)ctx->w_rhs, (T *)ctx->w_r, st, &it, &err, &outer, fused, &rec);
+        // a streamed inlet plane: its copy as a root node that runs beside the
+        // phases before the velocity BC (its source is set at every launch)
+        cudaGraphNode_t inlet_node = nullptr;
+        if (!rc && inlet) {
+            if (cudaGraphAddMemcpyNode1D(&inlet_node, gr, nullptr, 0, ctx->inlet_plane, ctx->inlet_host,
+                                         3ull * ctx->geo.ny * ctx->geo.nz * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+                cudaGetLastError();
+                rc = fail(ctx, FALM_ERR_CUDA, "step graph: inlet copy node");
+            } else {
+                rec.deps.push_back(inlet_node);
+            }
+        }
         if (!rc) rc = capture_into(ctx, gr, rec.deps, [&]() -> int {
             int q = step_post_t<T>(ctx, f, dt, t, cs, ctx->t_dev, nullptr);
             if (!q) q = step_stats_copy(ctx, cs);
@@ -330,12 +347,16 @@ int step_graph_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaS
             cudaGraphDestroy(gr);
             return rc;
         }
-        ctx->step_graphs->push_back(falm_ctx::StepGraph{f->u, f->uu, f->p, f->nut, f->ff, dt, inlet, n_pre + rec.fixed + n_post, rec.per_iter,
-                                                        gr, ex});
+        ctx->step_graphs->push_back(falm_ctx::StepGraph{f->u, f->uu, f->p, f->nut, f->ff, dt, inlet, inlet_node, n_pre + rec.fixed + n_post,
+                                                        rec.per_iter, gr, ex});
         sg = &ctx->step_graphs->back();
     }
     *ctx->t_host = t;
+    if (inlet)
+        CK(cudaGraphExecMemcpyNodeSetParams1D(sg->exec, sg->inlet_node, ctx->inlet_plane, ctx->inlet_host,
+                                              3ull * ctx->geo.ny * ctx->geo.nz * sizeof(double), cudaMemcpyHostToDevice));
     ctx->inlet_plane_valid = 0;   // the streamed plane serves one step
+    ctx->inlet_pending = 0;
     CK(cudaGraphLaunch(sg->exec, st));
     CK(cudaStreamSynchronize(st));
     const SolverScalars &sh = *ctx->scal_host;

@@ -207,10 +207,13 @@ int falm_alm_get_aps(falm_ctx *ctx, double *xyz, double *force, double *torque, 
    SGS -> divergence norm, with the race-free pseudo-velocity convention.  t = it*dt. */
 int falm_step(falm_ctx *ctx, const falm_fields *f, double dt, double t, void *stream, falm_step_stats *st);
 
-/* Streamed inflow: the inlet velocity (u,v,w) of the NEXT ubc call as a HOST FP64 array
-   3 x (sz-2gc) x (sy-2gc) (component, then k, then j fastest), copied asynchronously on
-   `stream` (pass pinned memory).  Takes precedence over the inflow box for that one call.
-   No reference counterpart (the reference has uniform inflow only). */
+/* Streamed inflow: the inlet velocity (u,v,w) of the NEXT velocity BC (falm_step or
+   falm_bc_ubc) as a HOST FP64 array 3 x (sz-2gc) x (sy-2gc) (component, then k, then j
+   fastest).  That call copies it to the device (a step recorded as a CUDA graph does so
+   beside the phases before the BC), so the array must stay valid and unchanged until the
+   call returns; pass pinned memory.  `stream` is not used.  Takes precedence over the
+   inflow box for that one call.  No reference counterpart (the reference has uniform inflow
+   only). */
 int falm_bc_set_inlet_plane(falm_ctx *ctx, const double *plane, void *stream);
 
 /* ---------------- FalmIO (src/FalmIO.h) and time averaging (src/falm.h:433-478) ----------- */
