@@ -82,6 +82,7 @@ int plain_solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *i
 // less than the host round trips they replace, even at 1-2 iterations per
 // step on the 512x256x256 grid.
 constexpr int kMixedPassIts = 50;   // FP32 BiCGStab iterations between FP64 true-residual checks
+constexpr size_t kMaxRecordings = 16;   // recorded solves (and steps) kept per context
 
 bool use_graph(const falm_ctx *ctx) {
     return !(ctx->profiling || ctx->check_sync || ctx->graph_mode == 0);
@@ -252,6 +253,11 @@ int solve_graph(falm_ctx *ctx, const void *x, const void *b, const void *r, int 
         if (ex) cudaGraphExecDestroy(ex);
         cudaGraphDestroy(gr);
         return rc;
+    }
+    if (ctx->graphs->size() >= kMaxRecordings) {   // a caller cycling through many vectors: drop the oldest
+        cudaGraphExecDestroy(ctx->graphs->front().exec);
+        cudaGraphDestroy(ctx->graphs->front().graph);
+        ctx->graphs->erase(ctx->graphs->begin());
     }
     ctx->graphs->push_back(falm_ctx::SolveGraph{x, b, r, ctx->w_rr, ctx->A_explicit, esize, pp_ready, np, nb, gr, ex});
     *out = ex; *prefix = np; *per_iter = nb;

@@ -347,6 +347,11 @@ int step_graph_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaS
             cudaGraphDestroy(gr);
             return rc;
         }
+        if (ctx->step_graphs->size() >= kMaxRecordings) {   // many sets of fields: drop the oldest recording
+            cudaGraphExecDestroy(ctx->step_graphs->front().exec);
+            cudaGraphDestroy(ctx->step_graphs->front().graph);
+            ctx->step_graphs->erase(ctx->step_graphs->begin());
+        }
         ctx->step_graphs->push_back(falm_ctx::StepGraph{f->u, f->uu, f->p, f->nut, f->ff, dt, inlet, inlet_node, n_pre + rec.fixed + n_post,
                                                         rec.per_iter, gr, ex});
         sg = &ctx->step_graphs->back();
