@@ -206,14 +206,15 @@ def test_step_launch_count_and_statuses(lib_built):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-@pytest.mark.parametrize("name", ["channel", "cavity"])
+@pytest.mark.parametrize("name", ["channel", "cavity", "wide"])
 def test_device_loop_equals_host_loop(lib_built, monkeypatch, precision, name):
-    """The BiCGStab iterations of a pass as one CUDA graph with a conditional
-    while node (the default; FALM_B200_GRAPH=1)
-    run the same kernels in the same order as the host loop that queues them
-    in batches between reads of the convergence flag (FALM_B200_GRAPH=0): the
+    """The step recorded as one CUDA graph, its solver loops conditional while
+    nodes (the default; FALM_B200_GRAPH=1), runs the same kernels in the same
+    order as the host-driven step, whose loop queues iterations in batches
+    between reads of the convergence flag (FALM_B200_GRAPH=0): the
     same iteration counts and bitwise the same fields, in convergence mode
-    (where the loop's exit matters) and in fixed-iteration mode."""
+    (where the loop's exit matters) and in fixed-iteration mode; "wide" (72
+    cells across) runs every TMA plane stream, recorded with its tensor maps."""
     case = small_cases()[name]
     for maxit, tol in ((None, None), (6, 0.0)):
         outs = []
