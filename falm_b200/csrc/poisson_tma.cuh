@@ -343,6 +343,11 @@ struct ResBody {
     }
     __device__ void finish(const double (&tot)[NV]) const {
         if (!sc) return;
+        if (sc->defer) {   // slab mode: the totals, summed over the slabs before derive_res
+            sc->red[0] = tot[0];
+            sc->red[1] = tot[NV - 1];
+            return;
+        }
         double err = sqrt(tot[0]) / sc->gsize;
         sc->err = err;
         // a check that passes ends the solve; one that fails is followed by a

@@ -355,7 +355,10 @@ int slab_solve_t(falm_ctx *ctx, T *x, const T *b, T *r, cudaStream_t st, int *it
     for (outer = 0; outer < max_outer; outer++) {
         // a pass starts from the residual (after the first pass: a check of the true residual)
         if ((rc = slab_halo<T>(ctx, x, 1, 1, st))) return rc;
-        LAUNCH(FALM_K_RES, st, (k_res<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, r, rr, ctx->red, sc, outer > 0)));
+        {
+            const ResBody<T> body{op, b, r, rr, sc, outer > 0 ? 1 : 0};   // r, rr and the totals (deferred)
+            S7_OR(FALM_K_RES, st, T, 2, x, body, (k_res<T><<<grid, kRowThreads, 0, st>>>(g, R, op, x, b, r, rr, ctx->red, sc, outer > 0)));
+        }
         if ((rc = slab_derive(ctx, 2, outer > 0 ? 1 : 0, st))) return rc;
         CK(cudaMemcpyAsync(&sc->it, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(ctx->scal_host, sc, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st));
