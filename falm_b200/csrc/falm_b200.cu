@@ -168,6 +168,9 @@ int falm_destroy(falm_ctx *ctx) {
     delete ctx->graphs;
     delete ctx->step_graphs;
     if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
+    if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
+    if (ctx->side_fork) cudaEventDestroy(ctx->side_fork);
+    if (ctx->side_join) cudaEventDestroy(ctx->side_join);
     cudaFree(ctx->t_dev);
     if (ctx->t_host) cudaFreeHost(ctx->t_host);
     cudaFree(ctx->metric_mem);

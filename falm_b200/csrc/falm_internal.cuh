@@ -212,4 +212,6 @@ struct falm_ctx {
     double *t_host;                         // pinned
     int graph_mode;                         // 1 record steps and solver loops as CUDA graphs, 0 never (FALM_B200_GRAPH=0)
     cudaStream_t cap_stream;                // stream the graphs are captured on
+    cudaStream_t side_stream;               // a recorded step's side branch (guide-shell copy, outlet save)
+    cudaEvent_t side_fork, side_join;       // its fork from and join to the capture stream
 };

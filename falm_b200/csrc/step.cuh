@@ -151,6 +151,20 @@ int step_pre_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStr
     T *ua = (T *)ctx->w_ua, *rhs = (T *)ctx->w_rhs;
     const bool chan = ctx->bc_kind == FALM_BC_CHANNEL;
     bool fused_res = false;
+    // recording: the guide-shell copy (u -> ua) and, in a channel, the saved
+    // outlet velocity (u -> w_outlet, read by the velocity BC after the
+    // projection) depend only on the step's input velocity, so they run on a
+    // side branch beside the forcing and the pseudo-velocity, which write
+    // neither; the branch joins before the face-velocity pass reads ua
+    const bool side = t_dev && ctx->side_stream;
+    if (side) {
+        const cudaStream_t ss = ctx->side_stream;
+        CK(cudaEventRecord(ctx->side_fork, st));
+        CK(cudaStreamWaitEvent(ss, ctx->side_fork, 0));
+        LAUNCH(FALM_K_OTHER, ss, k_copy_shell<T><<<ctx->sm_count * 8, 256, 0, ss>>>(g, u, ua));
+        if (chan) { LAUNCH(FALM_K_OTHER, ss, k_save_outlet<T><<<std::min(ctx->sm_count * 4, (3 * g.sy * g.sz + 255) / 256), 256, 0, ss>>>(g, u, (T *)ctx->w_outlet)); }
+        CK(cudaEventRecord(ctx->side_join, ss));
+    }
     // 1. ALM (src/alm/alm.h:66-77) at the previous velocity, or the RMCP model
     if (phase) phase->next("forcing");
     if (ctx->alm_on) {
@@ -168,7 +182,8 @@ int step_pre_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaStr
         const Region3 R = facemap(g);
         T scale = (T)(1.0 / (dt * ctx->maxdiag));
         // the guide layer of ua takes the previous velocity (the reference's aliased u)
-        LAUNCH(FALM_K_OTHER, st, k_copy_shell<T><<<ctx->sm_count * 8, 256, 0, st>>>(g, u, ua));
+        if (side) CK(cudaStreamWaitEvent(st, ctx->side_join, 0));
+        else LAUNCH(FALM_K_OTHER, st, k_copy_shell<T><<<ctx->sm_count * 8, 256, 0, st>>>(g, u, ua));
         // the plane stream also computes the solve's first residual (rr) and
         // first preconditioner sweep (pp) from the pressure p, the initial guess
         fused_res = false;
@@ -218,8 +233,9 @@ int step_post_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaSt
     // 5. pbc
     if (phase) phase->next("projection_bcs");
     LAUNCH(FALM_K_PBC, st, k_pbc<T><<<dim3(face_blocks(ctx), 3), 256, 0, st>>>(g, ctx->bc_kind, p));
-    // 6. keep the previous velocity at the outlet planes, then project
-    if (chan) { LAUNCH(FALM_K_OTHER, st, k_save_outlet<T><<<std::min(ctx->sm_count * 4, (3 * g.sy * g.sz + 255) / 256), 256, 0, st>>>(g, u, (T *)ctx->w_outlet)); }
+    // 6. keep the previous velocity at the outlet planes (a recorded step did it
+    // on its side branch), then project
+    if (chan && !(t_dev && ctx->side_stream)) { LAUNCH(FALM_K_OTHER, st, k_save_outlet<T><<<std::min(ctx->sm_count * 4, (3 * g.sy * g.sz + 255) / 256), 256, 0, st>>>(g, u, (T *)ctx->w_outlet)); }
     {
         const Region3 R = facemap(g);
         P3_OR(FALM_K_PROJECT, st, T, 1, 0, R, 1, FB_ARR(p), FB_ARR(1), (ProjectBody<T>{g, mview<T>(ctx), u, ua, uu, uu, (T)dt}),
@@ -301,6 +317,11 @@ int step_graph_t(falm_ctx *ctx, const falm_fields *f, double dt, double t, cudaS
         if (e.u == f->u && e.uu == f->uu && e.p == f->p && e.nut == f->nut && e.ff == f->ff && e.dt == dt && e.inlet == inlet) sg = &e;
     if (!sg) {
         if (!ctx->cap_stream) CK(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
+        if (!ctx->side_stream) {
+            CK(cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking));
+            CK(cudaEventCreateWithFlags(&ctx->side_fork, cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&ctx->side_join, cudaEventDisableTiming));
+        }
         if (!ctx->t_dev) {
             CK(cudaMalloc(&ctx->t_dev, sizeof(double)));
             CK(cudaHostAlloc(&ctx->t_host, sizeof(double), cudaHostAllocDefault));
