@@ -370,6 +370,12 @@ bool pc_first_in_xp(const falm_ctx *ctx) {
 // ring depth of the multi-field plane stream: keep >= 2 planes in flight and
 // at least two CTAs per SM
 template <typename T, int NF> struct P3Conf { static constexpr int NS = NF > 1 ? 4 : 6; };
+// a body's own slot count (Body::kSlots, FP32 only): a deeper ring for a body
+// whose register use already limits the CTAs per SM, so shared memory is free
+template <typename T, int NF, class Body, class = void> struct P3NS { static constexpr int v = P3Conf<T, NF>::NS; };
+template <typename T, int NF, class Body> struct P3NS<T, NF, Body, std::void_t<decltype(Body::kSlots)>> {
+    static constexpr int v = sizeof(T) == 4 ? Body::kSlots : P3Conf<T, NF>::NS;
+};
 
 // multi-field radius-1 plane stream over region R (see plane3_tma.cuh);
 // 1 launched, 0 not eligible (row-kernel fallback), <0 launch error
@@ -378,7 +384,7 @@ int p3_launch(falm_ctx *ctx, int cls, cudaStream_t st, const Region3 &R, int org
               const int (&ncomp)[NF], const Body &body) {
     if (ctx->no_tma) return 0;
     using L = P3Layout<T, NF>;
-    constexpr int NS = P3Conf<T, NF>::NS;
+    constexpr int NS = P3NS<T, NF, Body>::v;
     MapSet<NF> maps;
     int slot = 0;
     for (int f = 0; f < NF; f++) {

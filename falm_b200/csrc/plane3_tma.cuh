@@ -173,6 +173,11 @@ __global__ void __launch_bounds__(256, (p3_minb<T, Body>())) k_plane3_tma(Geom g
         // z metric factors of planes k-1, k, k+1 (rolled)
         T hz0 = ldg(mv.m.h[2] + max(P0, 0)), kz0 = ldg(mv.m.k[2] + max(P0, 0));
         T hz1 = ldg(mv.m.h[2] + P0 + 1), kz1 = ldg(mv.m.k[2] + P0 + 1);
+        // pointwise operands, loaded one plane ahead of their use
+        typename Body::PW pwv[RY], pwn[RY];
+#pragma unroll
+        for (int r = 0; r < RY; r++)
+            if (act[r]) pwv[r] = body.pw_load(i, jr[r], P0 + 1, ccr[r]);
         // the march, unrolled over the slots: plane q = q0 + u is in slot u
         int ph = 0;   // (q0 / NS) & 1
         for (int q0 = 0; q0 < nplanes - 1; q0 += NS, ph ^= 1) {
@@ -182,10 +187,10 @@ __global__ void __launch_bounds__(256, (p3_minb<T, Body>())) k_plane3_tma(Geom g
                 if (q < 1) continue;
                 if (q >= nplanes - 1) break;
                 const int k = P0 + q;
-                typename Body::PW pwv[RY];
+                const bool ahead = q + 1 < nplanes - 1;
 #pragma unroll
                 for (int r = 0; r < RY; r++)
-                    if (act[r]) pwv[r] = body.pw_load(i, jr[r], k, ccr[r]);
+                    if (act[r] && ahead) pwn[r] = body.pw_load(i, jr[r], k + 1, ccr[r] + sxy);
                 const int kn = min(k + 1, g.sz - 1);
                 const T hz2 = ldg(mv.m.h[2] + kn), kz2 = ldg(mv.m.k[2] + kn);
                 fail = !wait_s((u + 1) % NS, (u + 1 < NS) ? ph : ph ^ 1);
@@ -209,6 +214,7 @@ __global__ void __launch_bounds__(256, (p3_minb<T, Body>())) k_plane3_tma(Geom g
                         body.cell(i, jr[r], k, ccr[r], v, cm[r], pwv[r], cst[r], zst, acc);
                     }
                     ccr[r] += sxy;
+                    pwv[r] = pwn[r];
                 }
                 hz0 = hz1; hz1 = hz2; kz0 = kz1; kz1 = kz2;
             }
@@ -292,6 +298,7 @@ struct ProjectBody {
     const T *uua;
     T dt;
     static constexpr int NC0 = 1, NC1 = 0;   // field: the pressure
+    static constexpr int kMinBlocks = 3;     // FP32: room for the pointwise operands loaded a plane ahead
     // face velocity (f) and cell velocity (a, interior cells only) before the correction
     struct PW { T f0, f1, f2, a0, a1, a2; };
     using CS = NoPW;
@@ -346,6 +353,7 @@ struct UtoUUResBody {
     SolverScalars *sc;
     static constexpr int NC0 = 3, NC1 = 1;
     static constexpr int kMinBlocks = 2;   // FP32: at most 128 registers (fewer spills than 3 CTAs per SM)
+    static constexpr int kSlots = 6;       // FP32: 2 CTAs per SM leave room for 6 planes (3 in flight)
     using PW = NoPW;
     using CS = typename Op7<T>::Col;
     using ZS = typename Op7<T>::ZPl;
