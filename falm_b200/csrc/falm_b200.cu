@@ -148,7 +148,7 @@ int falm_create(const falm_grid *grid, int precision, falm_ctx **out) {
         const char *e = getenv("FALM_B200_NO_TMA");
         ctx->no_tma = (e && e[0] == '1') ? 1 : 0;
         const char *v = getenv("FALM_B200_SOR_V1");
-        ctx->sor_v1 = (v && v[0] == '1') ? 1 : 0;
+        ctx->sor_v1 = (v && v[0] == '1') ? 1 : ((v && v[0] == '2') ? 2 : 0);
         const char *pv = getenv("FALM_B200_PU_V1");
         ctx->pu_v1 = (pv && pv[0] == '1') ? 1 : 0;
         const char *c = getenv("FALM_B200_CHECK");

@@ -173,7 +173,7 @@ struct falm_ctx {
     int sm_count;
     int *kerr;                              // device error word of bounded waits (FALM_ERR_TIMEOUT)
     int no_tma;                             // force the row kernels (tests, fallback)
-    int sor_v1;                             // FP32 blocked SOR on the 32 x 8 tile kernel (tests)
+    int sor_v1;                             // blocked SOR kernel: 0 by size, 1 the 32 x 8 tile, 2 the 28 x 16 skewed one (tests)
     int pu_v1;                              // FP32 pseudo-velocity on the one-cell-per-thread kernel (tests)
     int check_sync;                         // synchronise after every launch (fault location)
     long long wait_probe_cycles;            // >0: the next falm_step first runs a wait that nothing completes (tests)

@@ -289,7 +289,7 @@ int sor_rb_launch_h(falm_ctx *ctx, cudaStream_t st, const T *xin, const T *b, T 
     return rc ? -rc : 1;
 }
 
-// three FP32 half sweeps on the 28 x 16 tile; 1 launched, 0 not eligible, <0 launch error
+// three half sweeps on the 28 x 16 tile (skewed wavefront); 1 launched, 0 not eligible, <0 launch error
 template <typename T>
 int sor_rb2_launch(falm_ctx *ctx, cudaStream_t st, const T *xin, const T *b, T *xout, T omega, int c1, const SolverScalars *sc) {
     using L = RB2Tile<T>;
@@ -310,16 +310,29 @@ int sor_rb2_launch(falm_ctx *ctx, cudaStream_t st, const T *xin, const T *b, T *
     return rc ? -rc : 1;
 }
 
+// whether three half sweeps run on the 28 x 16 skewed kernel rather than the
+// 32 x 8 one: always in FP32; in FP64 (2 CTAs per SM instead of 3) once every
+// CTA slot marches at least 128 planes, where its single barrier per plane
+// outweighs its longer pipeline fill (512x256x256: 0.725 -> 0.631 ms per pass;
+// 256x128x128, 35 planes per slot: 0.076 -> 0.083 ms)
+template <typename T>
+bool sor_skewed(const falm_ctx *ctx) {
+    if (ctx->sor_v1) return ctx->sor_v1 == 2;
+    if (sizeof(T) == 4) return true;
+    using L = RB2Tile<T>;
+    const Geom &g = ctx->geo;
+    const long long tiles = (long long)((g.nx + L::TX - 1) / L::TX) * ((g.ny + L::TY - 1) / L::TY);
+    return tiles * g.nz >= 128LL * ctx->sm_count * L::MINB;
+}
+
 template <typename T>
 int sor_rb_launch(falm_ctx *ctx, cudaStream_t st, int H, const T *xin, const T *b, T *xout, T omega, int c1, const SolverScalars *sc) {
     // the blocked kernels take the colour parity of local plane indices: a grid
     // whose planes are offset by koff flips the first colour instead
     c1 ^= ctx->geo.koff & 1;
-    if constexpr (sizeof(T) == 4) {
-        if (H == 3 && !ctx->sor_v1) {
-            const int r = sor_rb2_launch<T>(ctx, st, xin, b, xout, omega, c1, sc);
-            if (r != 0) return r;
-        }
+    if (H == 3 && sor_skewed<T>(ctx)) {
+        const int r = sor_rb2_launch<T>(ctx, st, xin, b, xout, omega, c1, sc);
+        if (r != 0) return r;
     }
     if (H == 1) return sor_rb_launch_h<T, 1>(ctx, st, xin, b, xout, omega, c1, sc);
     if (H == 2) return sor_rb_launch_h<T, 2>(ctx, st, xin, b, xout, omega, c1, sc);
@@ -338,10 +351,8 @@ template <typename T>
 bool sor_pass_ok(const falm_ctx *ctx, int H) {
     if (ctx->no_tma || ctx->A_explicit) return false;
     const size_t e = sizeof(T);
-    if constexpr (sizeof(T) == 4) {
-        using L2 = RB2Tile<T>;
-        if (H == 3 && !ctx->sor_v1 && map_ok(ctx, e, L2::BX, L2::BY) && map_ok(ctx, e, L2::BXB, L2::BYB)) return true;
-    }
+    using L2 = RB2Tile<T>;
+    if (H == 3 && sor_skewed<T>(ctx) && map_ok(ctx, e, L2::BX, L2::BY) && map_ok(ctx, e, L2::BXB, L2::BYB)) return true;
     if (H == 1) return map_ok(ctx, e, RBTile<T, 1>::BX, RBTile<T, 1>::BY);
     if (H == 2) return map_ok(ctx, e, RBTile<T, 2>::BX, RBTile<T, 2>::BY);
     return map_ok(ctx, e, RBTile<T, 3>::BX, RBTile<T, 3>::BY);

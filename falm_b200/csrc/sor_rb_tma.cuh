@@ -18,6 +18,7 @@
 // the pair's x/y operator coefficients kept in registers.
 #pragma once
 #include <type_traits>
+#include "pair.cuh"
 #include "poisson.cuh"
 #include "tma.cuh"
 
@@ -200,7 +201,8 @@ drain:
 
 namespace fb {
 
-// Three half sweeps per pass on a 28 x 16 tile (FP32 path), skewed wavefront.
+// Three half sweeps per pass on a 28 x 16 tile, skewed wavefront (FP32 with
+// packed pair arithmetic; FP64 with the two lanes as scalar operations).
 //
 // Half sweep h of plane p runs at iteration q = p + 2h - 1 (planes q-1, q-3 and
 // q-5 at iteration q).  Half sweep h reads the other colour of planes p-1, p,
@@ -219,9 +221,9 @@ namespace fb {
 //    Same-colour cells of adjacent rows sit on opposite bank parities (the box
 //    pitch is even), so every shared access of a half sweep is one wavefront.
 //  * the two rows of a thread have the same parity, hence the same colour
-//    offset e: both updates run as one pair through the packed FP32 pipe
-//    (fma/add/mul.f32x2), each lane rounding exactly as the scalar
-//    sor_point() does.
+//    offset e: both updates run as one pair (in FP32 through the packed pipe,
+//    fma/add/mul.f32x2), each lane rounding exactly as the scalar sor_point()
+//    does.
 //  * the right-hand side is staged as its own (32 x 20) box covering just the
 //    cells a half sweep updates; the chunk's z coefficients are staged once.
 //  * the march is unrolled over the NS slots, so slot addresses are constants.
@@ -240,41 +242,47 @@ struct RB2Tile {
     static constexpr int PX = 16, PY = TY + 2 * R, HALF = PY / 2;        // pairs per row, rows, rows per set
     static constexpr int NT = PX * HALF;                                  // threads
     static constexpr int SMEM = NS * SLOT + ZMAX * 4 * (int)sizeof(T) + 128 + 128;
+    static constexpr int MINB = sizeof(T) == 4 ? 4 : 2;                   // resident CTAs per SM (shared memory)
     static_assert(PY % 4 == 0, "the two rows of a thread have the same parity");
     static_assert(R <= 2 && TX + R <= 2 * PX - 2, "the pair columns (x from i0 - 2) cover the widest ring");
 };
 
-// a . b + c etc. on both lanes, each lane rounded as the scalar operation
-__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+// the per-plane z coefficients of the chunk, staged once: ab, at, -up, -um
+template <typename T> struct alignas(4 * sizeof(T)) ZCoef { T ab, at, nup, num; };
+
+// sor_div on both lanes
+__device__ __forceinline__ float2 sor_div2(float2 d, float2 ac) { return mul2(d, mk2(rcp_approx(ac.x), rcp_approx(ac.y))); }
+__device__ __forceinline__ double2 sor_div2(double2 d, double2 ac) { return mk2(sor_div(d.x, ac.x), sor_div(d.y, ac.y)); }
 
 // the two same-colour updates of a thread (lane s: row set s), lane by lane
 // the operations of sor_point()
-__device__ __forceinline__ float2 sor_point2(float2 ac, float2 ae, float2 aw, float2 an, float2 as, float2 at, float2 ab, float2 xc,
-                                             float2 xe, float2 xw, float2 xn, float2 xs, float2 xt, float2 xb, float2 bc, float2 omega) {
-    float2 r7 = __fmul2_rn(ac, xc);
-    r7 = __ffma2_rn(ae, xe, r7);
-    r7 = __ffma2_rn(aw, xw, r7);
-    r7 = __ffma2_rn(an, xn, r7);
-    r7 = __ffma2_rn(as, xs, r7);
-    r7 = __ffma2_rn(at, xt, r7);
-    r7 = __ffma2_rn(ab, xb, r7);
-    const float2 d = __ffma2_rn(r7, f2(-1.f, -1.f), bc);                 // bc - r7, one rounding
-    const float2 c = __fmul2_rn(d, f2(rcp_approx(ac.x), rcp_approx(ac.y)));
-    return __ffma2_rn(omega, c, xc);
+template <typename V2>
+__device__ __forceinline__ V2 sor_point2(V2 ac, V2 ae, V2 aw, V2 an, V2 as, V2 at, V2 ab, V2 xc, V2 xe, V2 xw, V2 xn, V2 xs, V2 xt, V2 xb,
+                                         V2 bc, V2 omega) {
+    using S = decltype(ac.x);
+    V2 r7 = mul2(ac, xc);
+    r7 = fma2(ae, xe, r7);
+    r7 = fma2(aw, xw, r7);
+    r7 = fma2(an, xn, r7);
+    r7 = fma2(as, xs, r7);
+    r7 = fma2(at, xt, r7);
+    r7 = fma2(ab, xb, r7);
+    const V2 d = fma2(r7, mk2(S(-1), S(-1)), bc);                        // bc - r7, one rounding
+    return fma2(omega, sor_div2(d, ac), xc);
 }
 
 template <typename T>
-__global__ void __launch_bounds__(RB2Tile<T>::NT, 4) k_sor_rb2_tma(Geom g, int kc, const __grid_constant__ CUtensorMap mx,
+__global__ void __launch_bounds__(RB2Tile<T>::NT, RB2Tile<T>::MINB) k_sor_rb2_tma(Geom g, int kc, const __grid_constant__ CUtensorMap mx,
                                                                  const __grid_constant__ CUtensorMap mb, PoissonTables<T> tb,
                                                                  T *__restrict__ xout, T omega, int c1, const SolverScalars *sc,
                                                                  int *err) {
-    static_assert(std::is_same<T, float>::value, "packed FP32 arithmetic");
+    using V2 = P2<T>;
     using L = RB2Tile<T>;
     constexpr int H = L::H;
     constexpr int NS = L::NS;
     extern __shared__ unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
-    float4 *ztab = (float4 *)(smem + NS * L::SLOT);                      // per staged plane: ab, at, -up, -um
+    ZCoef<T> *ztab = (ZCoef<T> *)(smem + NS * L::SLOT);                  // per staged plane: ab, at, -up, -um
     uint64_t *bar = (uint64_t *)(smem + NS * L::SLOT + L::ZMAX * 4 * sizeof(T));
     if (sc && sc->done) return;
     const int i0 = g.gc + blockIdx.x * L::TX, j0 = g.gc + blockIdx.y * L::TY;
@@ -316,23 +324,23 @@ __global__ void __launch_bounds__(RB2Tile<T>::NT, 4) k_sor_rb2_tma(Geom g, int k
     }
     // coefficients as lane pairs: x ones (cell e, both lanes alike), y ones per
     // row set, dxy per (set, e); same association as Op7::get
-    float2 aw2[2], ae2[2], an2, as2, dxy2[2];
+    V2 aw2[2], ae2[2], an2, as2, dxy2[2];
     {
         const int xc0 = min(max(x0, 0), g.sx - 1), xc1 = min(max(x0 + 1, 0), g.sx - 1);
-        const float aw0 = ldg(tb.cm[0] + xc0), ae0 = ldg(tb.cp[0] + xc0), aw1 = ldg(tb.cm[0] + xc1), ae1 = ldg(tb.cp[0] + xc1);
-        aw2[0] = f2(aw0, aw0); aw2[1] = f2(aw1, aw1); ae2[0] = f2(ae0, ae0); ae2[1] = f2(ae1, ae1);
-        const float d0 = ldg(tb.dx0 + xc0), d1 = ldg(tb.dx0 + xc1);
-        float as_[2], an_[2], dd[2][2];
+        const T aw0 = ldg(tb.cm[0] + xc0), ae0 = ldg(tb.cp[0] + xc0), aw1 = ldg(tb.cm[0] + xc1), ae1 = ldg(tb.cp[0] + xc1);
+        aw2[0] = mk2(aw0, aw0); aw2[1] = mk2(aw1, aw1); ae2[0] = mk2(ae0, ae0); ae2[1] = mk2(ae1, ae1);
+        const T d0 = ldg(tb.dx0 + xc0), d1 = ldg(tb.dx0 + xc1);
+        T as_[2], an_[2], dd[2][2];
 #pragma unroll
         for (int s = 0; s < 2; s++) {
             const int yc = min(max(yr[s], 0), g.sy - 1);
             as_[s] = ldg(tb.cm[1] + yc); an_[s] = ldg(tb.cp[1] + yc);
-            const float up1 = ldg(tb.up[1] + yc), um1 = ldg(tb.um[1] + yc);
+            const T up1 = ldg(tb.up[1] + yc), um1 = ldg(tb.um[1] + yc);
             dd[s][0] = (d0 - up1) - um1;
             dd[s][1] = (d1 - up1) - um1;
         }
-        as2 = f2(as_[0], as_[1]); an2 = f2(an_[0], an_[1]);
-        dxy2[0] = f2(dd[0][0], dd[1][0]); dxy2[1] = f2(dd[0][1], dd[1][1]);
+        as2 = mk2(as_[0], as_[1]); an2 = mk2(an_[0], an_[1]);
+        dxy2[0] = mk2(dd[0][0], dd[1][0]); dxy2[1] = mk2(dd[0][1], dd[1][1]);
     }
     // element offsets of cell x0 of each row set in the x box and the
     // right-hand side box, clamped into the boxes (exact for live cells; a
@@ -371,7 +379,7 @@ __global__ void __launch_bounds__(RB2Tile<T>::NT, 4) k_sor_rb2_tma(Geom g, int k
     // the chunk's z coefficients
     for (int q = threadIdx.x; q < nplanes; q += blockDim.x) {
         const int kz = min(max(P0 + q, 0), g.sz - 1);
-        ztab[q] = make_float4(ldg(tb.cm[2] + kz), ldg(tb.cp[2] + kz), -ldg(tb.up[2] + kz), -ldg(tb.um[2] + kz));
+        ztab[q] = ZCoef<T>{ldg(tb.cm[2] + kz), ldg(tb.cp[2] + kz), -ldg(tb.up[2] + kz), -ldg(tb.um[2] + kz)};
     }
     __syncthreads();
     int issued = min(NS, nplanes), waited = 0;
@@ -392,7 +400,7 @@ __global__ void __launch_bounds__(RB2Tile<T>::NT, 4) k_sor_rb2_tma(Geom g, int k
         wgo[n] = wy * g.sx + wx;
         wpair[n] = wx + 1 < ihi;
     }
-    const float2 sc2 = f2(tb.scale, tb.scale), om2 = f2(omega, omega);
+    const V2 sc2 = mk2(tb.scale, tb.scale), om2 = mk2(omega, omega);
     const int nit = nplanes + H;   // the last tile plane, nplanes - H - 1, is written out at iteration nplanes + H - 1
     for (int q0 = 0, ph = 0; q0 < nit; q0 += NS, ph ^= 1) {
 #pragma unroll
@@ -411,12 +419,12 @@ __global__ void __launch_bounds__(RB2Tile<T>::NT, 4) k_sor_rb2_tma(Geom g, int k
             {
                 const int kp = P0 + q - 2 * H;
                 if (kp >= k0 && kp < k1) {
-                    const float *Xf = (const float *)sl(2 * H);
-                    float *plane = xout + (long long)kp * sxy;
+                    const T *Xf = (const T *)sl(2 * H);
+                    T *plane = xout + (long long)kp * sxy;
 #pragma unroll
                     for (int n = 0; n < NW; n++) {
                         if (wso[n] >= 0) {
-                            if (wpair[n]) *reinterpret_cast<float2 *>(plane + wgo[n]) = *reinterpret_cast<const float2 *>(Xf + wso[n]);
+                            if (wpair[n]) *reinterpret_cast<V2 *>(plane + wgo[n]) = *reinterpret_cast<const V2 *>(Xf + wso[n]);
                             else plane[wgo[n]] = Xf[wso[n]];
                         }
                     }
@@ -439,16 +447,16 @@ __global__ void __launch_bounds__(RB2Tile<T>::NT, 4) k_sor_rb2_tma(Geom g, int k
                     const int e = (color ^ par0 ^ kp) & 1;   // the pairs' cell of this colour (both row sets)
                     const unsigned l0 = (live >> (3 * e + h - 1)) & 1u, l1 = (live >> (3 * (2 + e) + h - 1)) & 1u;
                     if (l0 | l1) {
-                        float *X0 = (float *)sl(2 * h - 1);
-                        const float *Xm = (const float *)sl(2 * h), *Xp = (const float *)sl(2 * h - 2);
-                        const float *B0 = (const float *)(sl(2 * h - 1) + L::PBX);
-                        const float4 z = ztab[p];
+                        T *X0 = (T *)sl(2 * h - 1);
+                        const T *Xm = (const T *)sl(2 * h), *Xp = (const T *)sl(2 * h - 2);
+                        const T *B0 = (const T *)(sl(2 * h - 1) + L::PBX);
+                        const ZCoef<T> z = ztab[p];
                         const int o0 = ox[0] + e, o1 = ox[1] + e;
-                        const float2 ac = __fmul2_rn(__fadd2_rn(__fadd2_rn(e ? dxy2[1] : dxy2[0], f2(z.z, z.z)), f2(z.w, z.w)), sc2);
-                        const float2 r = sor_point2(ac, e ? ae2[1] : ae2[0], e ? aw2[1] : aw2[0], an2, as2, f2(z.y, z.y), f2(z.x, z.x), f2(X0[o0], X0[o1]),
-                                                    f2(X0[o0 + 1], X0[o1 + 1]), f2(X0[o0 - 1], X0[o1 - 1]),
-                                                    f2(X0[o0 + L::BX], X0[o1 + L::BX]), f2(X0[o0 - L::BX], X0[o1 - L::BX]),
-                                                    f2(Xp[o0], Xp[o1]), f2(Xm[o0], Xm[o1]), f2(B0[ob[0] + e], B0[ob[1] + e]), om2);
+                        const V2 ac = mul2(add2(add2(e ? dxy2[1] : dxy2[0], mk2(z.nup, z.nup)), mk2(z.num, z.num)), sc2);
+                        const V2 r = sor_point2(ac, e ? ae2[1] : ae2[0], e ? aw2[1] : aw2[0], an2, as2, mk2(z.at, z.at), mk2(z.ab, z.ab), mk2(X0[o0], X0[o1]),
+                                                mk2(X0[o0 + 1], X0[o1 + 1]), mk2(X0[o0 - 1], X0[o1 - 1]),
+                                                mk2(X0[o0 + L::BX], X0[o1 + L::BX]), mk2(X0[o0 - L::BX], X0[o1 - L::BX]),
+                                                mk2(Xp[o0], Xp[o1]), mk2(Xm[o0], Xm[o1]), mk2(B0[ob[0] + e], B0[ob[1] + e]), om2);
                         if (l0) X0[o0] = r.x;
                         if (l1) X0[o1] = r.y;
                     }

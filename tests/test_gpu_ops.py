@@ -210,12 +210,14 @@ def test_pbicgstab_fixed_iterations(oracle, lib_built, pc):
     assert rel_l2(interior(host(xd), g), interior(xo, g)) < 1e-11
 
 
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
 @pytest.mark.parametrize("shape", [(40, 20, 72), (64, 36, 40), (120, 52, 33)])
-def test_blocked_sor_tiles_agree(lib_built, monkeypatch, shape):
-    """The two FP32 temporally blocked red-black SOR kernels (28 x 16 and 32 x 8
-    tiles) perform the same updates with the same expressions: the mixed
-    precision solve in fixed-iteration mode gives bit-identical iterates
-    (partial tiles in x and y, several z chunks)."""
+def test_blocked_sor_tiles_agree(lib_built, monkeypatch, shape, precision):
+    """The two temporally blocked red-black SOR kernels (28 x 16 tile with the
+    skewed wavefront, 32 x 8 tile with one barrier per half sweep) perform the
+    same updates with the same expressions: the solve in fixed-iteration mode
+    gives bit-identical iterates in both precisions (partial tiles in x and y,
+    several z chunks)."""
     case = cases.small_channel(*shape, intensity=0.0)
     case.pc, case.tol, case.maxit = "SOR", 0.0, 5
     g = case.grid
@@ -224,9 +226,9 @@ def test_blocked_sor_tiles_agree(lib_built, monkeypatch, shape):
     interior(b, g)[...] = rng.standard_normal(interior(b, g).shape)
     x0 = 0.1 * rng.standard_normal(g.n)
     outs = []
-    for v1 in ("1", "0"):
+    for v1 in ("1", "2"):   # the 32 x 8 kernel, then the skewed one
         monkeypatch.setenv("FALM_B200_SOR_V1", v1)
-        ctx = make_ctx(case, "mixed")
+        ctx = make_ctx(case, precision)
         xd, bd, rd = dev(ctx, x0), dev(ctx, b), ctx.field(1)
         ctx.solve(xd, bd, rd)
         outs.append(host(xd))
