@@ -178,15 +178,31 @@ __global__ void k_alm_turbine_sums(AlmDev a) {
     }
 }
 
+// the cutoff test (double)v < r2 of a value v of type T as v < cut_bound<T>(r2):
+// in FP32 the bound is the smallest float not below r2 (rounded up), so both
+// tests agree for every float v
+template <typename T>
+__device__ __forceinline__ T cut_bound(double r2) {
+    if constexpr (sizeof(T) == 4) return __double2float_ru(r2);
+    else return r2;
+}
+
+// the APs' positions and forces, converted to T once per block
+template <typename T>
+__device__ __forceinline__ void stage_aps(const AlmDev &a, T *s_ap) {
+    for (int q = threadIdx.x; q < a.apcount; q += blockDim.x) {
+        for (int d = 0; d < 3; d++) { s_ap[6 * q + d] = (T)a.ap_xyz[3 * q + d]; s_ap[6 * q + 3 + d] = (T)a.ap_force[3 * q + d]; }
+    }
+}
+
 // DistributeAPForce (src/alm/almDevCall.cu:255-294) as a stored field, truncated at rcut
 template <typename T>
 __global__ void __launch_bounds__(kRowThreads) k_alm_project(Geom g, Region3 R, MetricView<T> mv, AlmDev a, T *__restrict__ ff) {
-    __shared__ double s_ap[6 * kMaxFusedAp];
+    __shared__ T s_ap[6 * kMaxFusedAp];
     const int na = a.apcount;
-    for (int q = threadIdx.x; q < na; q += blockDim.x) {
-        for (int d = 0; d < 3; d++) { s_ap[6 * q + d] = a.ap_xyz[3 * q + d]; s_ap[6 * q + 3 + d] = a.ap_force[3 * q + d]; }
-    }
+    stage_aps<T>(a, s_ap);
     __syncthreads();
+    const T rcut2 = cut_bound<T>(a.rcut2);
     const double eps = a.euler_eps, sq = sqrt(3.14159265358979323846) * eps, eta = 1. / (sq * sq * sq);
     const long long N = g.n;
     FB_FOR_ROWS(R, j, k) FB_FOR_I(R, i) {
@@ -195,13 +211,13 @@ __global__ void __launch_bounds__(kRowThreads) k_alm_project(Geom g, Region3 R, 
         T fx = 0, fy = 0, fz = 0;
         const T te = (T)eta, e2 = (T)eps * (T)eps;
         for (int q = 0; q < na; q++) {
-            T dx = cx - (T)s_ap[6 * q], dy = cy - (T)s_ap[6 * q + 1], dz = cz - (T)s_ap[6 * q + 2];
+            T dx = cx - s_ap[6 * q], dy = cy - s_ap[6 * q + 1], dz = cz - s_ap[6 * q + 2];
             T rr2 = dx * dx + dy * dy + dz * dz;
-            if ((double)rr2 < a.rcut2) {
+            if (rr2 < rcut2) {
                 T ex = exp(-rr2 / e2);
-                fx += (T)s_ap[6 * q + 3] * te * ex;
-                fy += (T)s_ap[6 * q + 4] * te * ex;
-                fz += (T)s_ap[6 * q + 5] * te * ex;
+                fx += s_ap[6 * q + 3] * te * ex;
+                fy += s_ap[6 * q + 4] * te * ex;
+                fz += s_ap[6 * q + 5] * te * ex;
             }
         }
         ff[c] = fx; ff[c + N] = fy; ff[c + 2 * N] = fz;
@@ -212,12 +228,11 @@ __global__ void __launch_bounds__(kRowThreads) k_alm_project(Geom g, Region3 R, 
 // farther than the cutoff from the AP bounding box get zero without the AP loop.
 template <typename T>
 __global__ void __launch_bounds__(256) k_alm_box(AlmDev a, const double *xc, const double *yc, const double *zc) {
-    __shared__ double s_ap[6 * kMaxFusedAp];
+    __shared__ T s_ap[6 * kMaxFusedAp];
     const int na = a.apcount;
-    for (int q = threadIdx.x; q < na; q += blockDim.x) {
-        for (int d = 0; d < 3; d++) { s_ap[6 * q + d] = a.ap_xyz[3 * q + d]; s_ap[6 * q + 3 + d] = a.ap_force[3 * q + d]; }
-    }
+    stage_aps<T>(a, s_ap);
     __syncthreads();
+    const T rcut2 = cut_bound<T>(a.rcut2);
     const double eps = a.euler_eps, sq = sqrt(3.14159265358979323846) * eps, eta = 1. / (sq * sq * sq);
     const double *bb = a.scal->bbox;
     const double b0 = bb[0], b1 = bb[1], b2 = bb[2], b3 = bb[3], b4 = bb[4], b5 = bb[5];
@@ -242,13 +257,13 @@ __global__ void __launch_bounds__(256) k_alm_box(AlmDev a, const double *xc, con
             const T cx = (T)cxd, cy = (T)cyd, cz = (T)czd;
             const T te = (T)eta, e2 = (T)eps * (T)eps;
             for (int p = 0; p < na; p++) {
-                T dx = cx - (T)s_ap[6 * p], dy = cy - (T)s_ap[6 * p + 1], dz = cz - (T)s_ap[6 * p + 2];
+                T dx = cx - s_ap[6 * p], dy = cy - s_ap[6 * p + 1], dz = cz - s_ap[6 * p + 2];
                 T rr2 = dx * dx + dy * dy + dz * dz;
-                if ((double)rr2 < a.rcut2) {
+                if (rr2 < rcut2) {
                     T ex = exp(-rr2 / e2);
-                    fx += (T)s_ap[6 * p + 3] * te * ex;
-                    fy += (T)s_ap[6 * p + 4] * te * ex;
-                    fz += (T)s_ap[6 * p + 5] * te * ex;
+                    fx += s_ap[6 * p + 3] * te * ex;
+                    fy += s_ap[6 * p + 4] * te * ex;
+                    fz += s_ap[6 * p + 5] * te * ex;
                 }
             }
         }
