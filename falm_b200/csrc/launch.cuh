@@ -394,7 +394,7 @@ template <typename T, int NF, int NV, class Body>
 int p3_launch(falm_ctx *ctx, int cls, cudaStream_t st, const Region3 &R, int org, const void *const (&ptr)[NF],
               const int (&ncomp)[NF], const Body &body) {
     if (ctx->no_tma) return 0;
-    using L = P3Layout<T, NF>;
+    using L = P3Layout<T, NF, P3Rows<T, Body>::v>;
     constexpr int NS = P3NS<T, NF, Body>::v;
     MapSet<NF> maps;
     int slot = 0;

@@ -24,22 +24,22 @@ struct alignas(64) MapSet {
     int ncomp[NF];
 };
 
-template <typename T, int NF>
+template <typename T, int NF, int RY_ = 2>
 struct P3Layout {
-    static constexpr int RY = 2;   // rows per thread: thread (tx, ty) computes rows ty, ty + 8
+    static constexpr int RY = RY_;   // rows per thread: thread (tx, ty) computes rows ty (, ty + 8)
     static constexpr int TX = 32, TY = 8 * RY, BX = 36, BY = TY + 2, PE = BX * BY;
     static constexpr int FB = (PE * (int)sizeof(T) + 127) / 128 * 128;   // one component plane
 };
 
 // view of the resident planes for the body
-template <typename T, int NF>
+template <typename T, int NF, int RY_ = 2>
 struct P3View {
     const T *pl[3];   // slot base of planes k-1, k, k+1
     int foff[NF];     // byte offset of field f inside a slot
     int o;            // own element offset inside a component plane
     __device__ __forceinline__ T at(int f, int d, int dz, int dx = 0, int dy = 0) const {
         const T *base = (const T *)((const unsigned char *)pl[dz + 1] + foff[f]);
-        return base[d * P3Layout<T, NF>::PE + o + dy * P3Layout<T, NF>::BX + dx];
+        return base[d * P3Layout<T, NF, RY_>::PE + o + dy * P3Layout<T, NF, RY_>::BX + dx];
     }
 };
 
@@ -67,6 +67,13 @@ template <typename T, class Body> struct P3MinB<T, Body, std::void_t<decltype(Bo
 };
 template <typename T, class Body> constexpr int p3_minb() { return P3MinB<T, Body>::v; }
 
+// rows per thread: 2, or in FP64 the body's own kRows64 (one row halves the
+// ring of a six-component stream, which otherwise admits one CTA per SM)
+template <typename T, class Body, class = void> struct P3Rows { static constexpr int v = 2; };
+template <typename T, class Body> struct P3Rows<T, Body, std::void_t<decltype(Body::kRows64)>> {
+    static constexpr int v = sizeof(T) == 8 ? Body::kRows64 : 2;
+};
+
 // Body: bool skip() const; MetricView<T> mv; type PW (the cell's pointwise
 //       operands) and PW pw_load(i, j, k, cc) const; types CS, ZS (state of a
 //       column and of a plane) with CS col_state(i, j) const, ZS plane_state(k)
@@ -78,7 +85,7 @@ template <typename T, class Body> constexpr int p3_minb() { return P3MinB<T, Bod
 template <typename T, int NF, int NS, int NV, class Body>
 __global__ void __launch_bounds__(256, (p3_minb<T, Body>())) k_plane3_tma(Geom g, Region3 R, int org, int kc, const __grid_constant__ MapSet<NF> maps,
                                                   Body body, RedWork rw, int *err) {
-    using L = P3Layout<T, NF>;
+    using L = P3Layout<T, NF, P3Rows<T, Body>::v>;
     extern __shared__ unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
     // slot layout from the body's component counts (compile-time offsets)
@@ -93,7 +100,7 @@ __global__ void __launch_bounds__(256, (p3_minb<T, Body>())) k_plane3_tma(Geom g
     const int k0 = R.k0 + blockIdx.z * kc, k1 = min(k0 + kc, R.k1);
     const int i = i0 + tx;
     const int P0 = k0 - 1, nplanes = (k1 + 1) - P0;
-    P3View<T, NF> v;
+    P3View<T, NF, L::RY> v;
     v.foff[0] = 0;
     if (NF > 1) v.foff[NF - 1] = FOFF1;
     const int xb = box_origin(i0 - org, L::BX, g.sx, 16 / (int)sizeof(T)), yb = box_origin(j0 - 1, L::BY, g.sy, 1);
@@ -426,6 +433,7 @@ struct SgsDivBody {
     T *div_out;
     double *divsum;
     static constexpr int NC0 = 3, NC1 = 3;   // fields: the cell velocity, the face velocity
+    static constexpr int kRows64 = 1;        // FP64: a 63 KB ring (2 CTAs per SM) instead of 126 KB
     using PW = NoPW;
     // filter width (cube root of the volume, as cbrt(hx) cbrt(hy) cbrt(hz)) and
     // the FP64 inverse widths, split into column and plane factors
@@ -437,7 +445,8 @@ struct SgsDivBody {
         return CS{cbrt(ldg(mv.m.h[0] + i)) * cbrt(ldg(mv.m.h[1] + j)), ldg(m64.k[0] + i) * ldg(m64.k[1] + j)};
     }
     __device__ ZS plane_state(int k) const { return ZS{cbrt(ldg(mv.m.h[2] + k)), ldg(m64.k[2] + k)}; }
-    __device__ void cell(int i, int j, int k, long long cc, const P3View<T, 2> &v, const ColMet<T> &cm, const PW &, const CS &cs,
+    template <int RYV>
+    __device__ void cell(int i, int j, int k, long long cc, const P3View<T, 2, RYV> &v, const ColMet<T> &cm, const PW &, const CS &cs,
                          const ZS &zs, double (&acc)[1]) const {
         if (sgs != FALM_SGS_EMPTY) {
             const T kxx = cm.kx[1], kxy = cm.ky[1], kxz = cm.kz[1];
